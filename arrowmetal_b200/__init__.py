@@ -1,0 +1,485 @@
+"""ArrowMetal's sort path on NVIDIA B200: Apache Arrow arrays in HBM, sorted by sm_100a kernels.
+
+A ctypes binding over ``libArrowMetalC.so`` with the names, arguments and errors of ArrowMetal's own
+Python binding for the sort path (python/arrowmetal/__init__.py: ``MetalArray.from_arrow`` / ``to_arrow``
+:265-300, ``take`` :444-450, ``argsort`` / ``sort`` / ``top_k`` :460-480 and the option form :3940-3970,
+``lexsort_indices`` :1325-1359, ``ArrowMetalError`` / ``_check`` :212-222). Results come back as pyarrow
+arrays, so they drop straight into pyarrow, Polars or pandas::
+
+    import pyarrow as pa, arrowmetal_b200 as am
+    col = am.MetalArray.from_arrow(pa.array([3, None, 1]))
+    col.argsort().to_arrow()                 # -> [2, 0, 1] (uint32)
+
+There is no CPU fallback: a missing library or a missing GPU raises.
+"""
+import contextlib
+import ctypes
+import json
+import os
+
+import pyarrow as pa
+
+__version__ = "0.6.1"
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libArrowMetalC.so")
+
+NULL_PLACEMENT = ("at_end", "at_start")
+FLOAT_ORDERS = ("ieee", "total", "nan_largest")
+
+
+def _find_library():
+    """`$ARROWMETAL_LIB` (a full path, which must exist), else the in-tree build."""
+    env = os.environ.get("ARROWMETAL_LIB")
+    if env:
+        if not os.path.exists(env):
+            raise OSError("arrowmetal_b200: $ARROWMETAL_LIB is set to " + env + ", which does not exist")
+        return env
+    if not os.path.exists(LIB_PATH):
+        raise OSError("arrowmetal_b200: " + LIB_PATH + " is missing; build it with "
+                      "`make -C arrowmetal_b200/csrc` (or __graft_entry__.build())")
+    return LIB_PATH
+
+
+_lib = ctypes.CDLL(_find_library())
+_P = ctypes.c_void_p
+_PP = ctypes.POINTER(_P)
+_I = ctypes.c_int
+_I64 = ctypes.c_int64
+_IP = ctypes.POINTER(ctypes.c_int)
+
+
+class _ArrowSchema(ctypes.Structure):
+    _fields_ = [("format", ctypes.c_char_p), ("name", ctypes.c_char_p), ("metadata", ctypes.c_char_p),
+                ("flags", _I64), ("n_children", _I64), ("children", _P), ("dictionary", _P),
+                ("release", _P), ("private_data", _P)]
+
+
+class _ArrowArray(ctypes.Structure):
+    _fields_ = [("length", _I64), ("null_count", _I64), ("offset", _I64), ("n_buffers", _I64),
+                ("n_children", _I64), ("buffers", _P), ("children", _P), ("dictionary", _P),
+                ("release", _P), ("private_data", _P)]
+
+
+class _ArrowDeviceArray(ctypes.Structure):
+    _fields_ = [("array", _ArrowArray), ("device_id", _I64), ("device_type", ctypes.c_int32),
+                ("sync_event", _P), ("reserved", _I64 * 3)]
+
+
+class SortStats(ctypes.Structure):
+    _fields_ = [("rows", _I64), ("value_rows", _I64), ("passes_run", ctypes.c_int32),
+                ("passes_skipped", ctypes.c_int32), ("kernel_us", ctypes.c_double)]
+
+
+def _sig(name, res, args):
+    f = getattr(_lib, name)
+    f.restype = res
+    f.argtypes = args
+
+
+for _name, _res, _args in [
+    ("am_version", ctypes.c_char_p, []), ("am_device_name", ctypes.c_char_p, []),
+    ("am_last_error", ctypes.c_char_p, []),
+    ("am_import", _I, [_P, _P, _PP]), ("am_import_device", _I, [_P, _P, _PP]),
+    ("am_import_chunks", _I, [_P, _P, _I64, _PP]), ("am_import_chunks_supported", _I, [_P]),
+    ("am_set_import_threads", _I, [_I]), ("am_get_import_threads", _I, []),
+    ("am_export", _I, [_P, _P, _P]), ("am_export_device", _I, [_P, _P, _P]),
+    ("am_release", None, [_P]), ("am_length", _I64, [_P]), ("am_null_count", _I64, [_P]),
+    ("am_format", ctypes.c_char_p, [_P]), ("am_compute_format", ctypes.c_char_p, [_P]),
+    ("am_take", _I, [_P, _P, _PP]), ("am_slice", _I, [_P, _I64, _I64, _PP]),
+    ("am_take_columns", _I, [_PP, _I64, _P, _PP]),
+    ("am_argsort", _I, [_P, _I, _PP]), ("am_sort", _I, [_P, _I, _PP]), ("am_top_k", _I, [_P, _I64, _I, _PP]),
+    ("am_argsort_ex", _I, [_P, _I, _I, _PP]), ("am_sort_ex", _I, [_P, _I, _I, _PP]),
+    ("am_argsort_ex2", _I, [_P, _I, _I, _I, _PP]), ("am_sort_ex2", _I, [_P, _I, _I, _I, _PP]),
+    ("am_argsort_ex3", _I, [_P, _I, _I, _I, _I, _PP]),
+    ("am_top_k_ex", _I, [_P, _I64, _I, _I, _I, _PP]),
+    ("am_lexsort", _I, [_PP, _IP, _I64, _PP]), ("am_lexsort_ex", _I, [_PP, _IP, _I64, _I, _PP]),
+    ("am_lexsort_ex2", _I, [_PP, _IP, _IP, _IP, _I64, _PP]),
+    ("am_argsort_batch", _I, [_PP, _IP, _IP, _IP, _I64, _PP]),
+    ("am_batch_begin", _I, []), ("am_batch_end", _I, []),
+    ("am_plan_source_create", _I, [ctypes.c_char_p, _PP, ctypes.POINTER(ctypes.c_char_p), _I64, _PP]),
+    ("am_plan_source_release", None, [_P]),
+    ("am_plan_run", _I, [ctypes.c_char_p, _PP, _I64, _I, _PP]),
+    ("am_plan_explain", ctypes.c_char_p, [ctypes.c_char_p, _PP, _I64, _I]),
+    ("am_plan_column_count", _I64, [_P]), ("am_plan_row_count", _I64, [_P]),
+    ("am_plan_column_name", ctypes.c_char_p, [_P, _I64]), ("am_plan_column", _I, [_P, _I64, _PP]),
+    ("am_plan_result_release", None, [_P]),
+    ("am_router_set_mode", _I, [_I]), ("am_router_get_mode", _I, []),
+    ("am_cuda_set_stream", _I, [_P]), ("am_cuda_get_stream", _P, []), ("am_cuda_synchronize", _I, []),
+    ("am_cuda_device", _I, []), ("am_last_sort_stats", _I, [ctypes.POINTER(SortStats)]),
+    ("am_cuda_profile", _I, [_I]), ("am_cuda_profile_count", _I64, []),
+    ("am_cuda_profile_entry", _I, [_I64, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(_I64),
+                                   ctypes.POINTER(ctypes.c_double)]),
+    ("am_cuda_profile_reset", _I, []),
+    ("am_debug_set_max_row_index", _I, [_I64]), ("am_debug_fail_alloc_after", _I, [_I64]),
+    ("am_debug_skip_first_tile", _I, [_I]),
+]:
+    _sig(_name, _res, _args)
+
+
+def version():
+    return _lib.am_version().decode()
+
+
+def device_name():
+    return _lib.am_device_name().decode()
+
+
+class ArrowMetalError(RuntimeError):
+    pass
+
+
+def _check(rc):
+    if rc != 0:
+        raise ArrowMetalError((_lib.am_last_error() or b"unknown error").decode())
+
+
+def _call(fn, *args):
+    out = _P()
+    _check(fn(*args, ctypes.byref(out)))
+    return MetalArray(out)
+
+
+def _index_of(names, value, what):
+    try:
+        return names.index(value)
+    except ValueError:
+        raise ArrowMetalError(f"unknown {what} {value!r}; expected one of {', '.join(names)}") from None
+
+
+def _index_array(indices):
+    """`take` indices as a pyarrow array of a type the gather reads (int32, int64, uint32)."""
+    if isinstance(indices, pa.ChunkedArray):
+        indices = indices.combine_chunks()
+    if not isinstance(indices, pa.Array):
+        if hasattr(indices, "dtype"):
+            indices = pa.array(indices)
+        else:
+            indices = pa.array(list(indices), type=pa.int64())
+    t = indices.type
+    if pa.types.is_int32(t) or pa.types.is_int64(t) or pa.types.is_uint32(t):
+        return indices
+    if pa.types.is_int8(t) or pa.types.is_int16(t):
+        return indices.cast(pa.int32())
+    if pa.types.is_uint8(t) or pa.types.is_uint16(t):
+        return indices.cast(pa.uint32())
+    return indices.cast(pa.int64())
+
+
+class MetalArray:
+    """An HBM-resident Arrow array. Immutable; every operation returns a new array."""
+
+    def __init__(self, handle):
+        self._h = handle
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _lib.am_release(h)
+            self._h = None
+
+    # ---- interop
+    @classmethod
+    def from_arrow(cls, obj):
+        """Import anything pyarrow can turn into an array (a ChunkedArray of several chunks goes
+        through the chunked import). The buffers are copied into HBM."""
+        if isinstance(obj, pa.ChunkedArray):
+            if obj.num_chunks > 1:
+                return _import_chunks(obj)
+            obj = obj.chunk(0) if obj.num_chunks == 1 else pa.array([], type=obj.type)
+        if not isinstance(obj, pa.Array):
+            obj = pa.array(obj)
+        schema, array = _ArrowSchema(), _ArrowArray()
+        obj._export_to_c(ctypes.addressof(array), ctypes.addressof(schema))
+        try:
+            return _call(_lib.am_import, ctypes.addressof(schema), ctypes.addressof(array))
+        finally:
+            if array.release:
+                ctypes.CFUNCTYPE(None, _P)(array.release)(ctypes.addressof(array))
+            if schema.release:
+                ctypes.CFUNCTYPE(None, _P)(schema.release)(ctypes.addressof(schema))
+
+    @classmethod
+    def from_device(cls, data_ptr, length, fmt, validity_ptr=0, null_count=0, offset=0, keep=None):
+        """Wrap arrays already in this GPU's memory (ARROW_DEVICE_CUDA) without a copy. `keep` is held
+        until the array is released."""
+        arr = _ArrowDeviceArray()
+        bufs = (_P * 2)(validity_ptr or None, data_ptr)
+        holder = _DeviceHolder(bufs, keep, fmt)
+        arr.array.length = length
+        arr.array.null_count = null_count
+        arr.array.offset = offset
+        arr.array.n_buffers = 2
+        arr.array.buffers = ctypes.cast(bufs, _P)
+        arr.array.release = ctypes.cast(holder.release_cb, _P)
+        arr.device_type = 2
+        arr.device_id = _lib.am_cuda_device()
+        schema = _ArrowSchema()
+        schema.format = fmt.encode()
+        out = _call(_lib.am_import_device, ctypes.addressof(schema), ctypes.addressof(arr))
+        out._device_holder = holder
+        return out
+
+    def to_arrow(self):
+        """Export as a pyarrow.Array (copied into pinned host memory owned by the array)."""
+        schema, array = _ArrowSchema(), _ArrowArray()
+        _check(_lib.am_export(self._h, ctypes.addressof(schema), ctypes.addressof(array)))
+        return pa.Array._import_from_c(ctypes.addressof(array), ctypes.addressof(schema))
+
+    def __len__(self):
+        return int(_lib.am_length(self._h))
+
+    @property
+    def null_count(self):
+        return int(_lib.am_null_count(self._h))
+
+    @property
+    def format(self):
+        return _lib.am_format(self._h).decode()
+
+    # ---- selection
+    def take(self, indices):
+        """Arrow `take`: int32, int64 and uint32 indices; a null index gives a null row."""
+        if not isinstance(indices, MetalArray):
+            indices = MetalArray.from_arrow(_index_array(indices))
+        return _call(_lib.am_take, self._h, indices._h)
+
+    def slice(self, offset, length):
+        return _call(_lib.am_slice, self._h, offset, length)
+
+    # ---- sorting (stable radix sort on the GPU)
+    def argsort(self, descending=False, null_placement="at_end", float_order="ieee"):
+        """UInt32 indices that sort the array (Arrow `array_sort_indices`; pyarrow returns uint64 with
+        the same values). `null_placement` is independent of the direction, as in Arrow.
+        `float_order`: "ieee" (pyarrow's order: -0.0 ties +0.0, NaN next to the nulls), "total"
+        (IEEE 754 totalOrder, arrow-rs), "nan_largest" (Polars)."""
+        return _call(_lib.am_argsort_ex2, self._h, 1 if descending else 0,
+                     _index_of(NULL_PLACEMENT, null_placement, "null_placement"),
+                     _index_of(FLOAT_ORDERS, float_order, "float_order"))
+
+    def argsort64(self, descending=False, null_placement="at_end", float_order="ieee"):
+        """`argsort` with uint64 indices, the type pyarrow's sort_indices returns."""
+        out = _P()
+        _check(_lib.am_argsort_ex3(self._h, 1 if descending else 0,
+                                   _index_of(NULL_PLACEMENT, null_placement, "null_placement"),
+                                   _index_of(FLOAT_ORDERS, float_order, "float_order"), 8, ctypes.byref(out)))
+        return MetalArray(out)
+
+    def sort(self, descending=False, null_placement="at_end", float_order="ieee"):
+        """Sorted copy of the array, with the ordering rules of `argsort`."""
+        return _call(_lib.am_sort_ex2, self._h, 1 if descending else 0,
+                     _index_of(NULL_PLACEMENT, null_placement, "null_placement"),
+                     _index_of(FLOAT_ORDERS, float_order, "float_order"))
+
+    def top_k(self, k, largest=True, null_placement="at_end", float_order="ieee"):
+        """UInt32 indices of the k largest (or smallest) values: the first k of `argsort`."""
+        return _call(_lib.am_top_k_ex, self._h, int(k), 1 if largest else 0,
+                     _index_of(NULL_PLACEMENT, null_placement, "null_placement"),
+                     _index_of(FLOAT_ORDERS, float_order, "float_order"))
+
+
+class _DeviceHolder:
+    """Keeps a device import's Python owner alive until the library releases the array."""
+    _live = set()
+
+    def __init__(self, bufs, keep, fmt):
+        self.bufs, self.keep, self.fmt = bufs, keep, fmt
+        _DeviceHolder._live.add(self)
+
+        def _release(p):
+            ctypes.cast(p, ctypes.POINTER(_ArrowArray)).contents.release = None
+            _DeviceHolder._live.discard(self)
+        self.release_cb = ctypes.CFUNCTYPE(None, _P)(_release)
+
+
+def _import_chunks(chunked):
+    chunks = chunked.chunks
+    n = len(chunks)
+    arrays = (_ArrowArray * n)()
+    schema = _ArrowSchema()
+    chunks[0]._export_to_c(ctypes.addressof(arrays[0]), ctypes.addressof(schema))
+    for i in range(1, n):
+        chunks[i]._export_to_c(ctypes.addressof(arrays[i]))
+    out = _P()
+    try:
+        rc = _lib.am_import_chunks(ctypes.addressof(schema), ctypes.addressof(arrays), n, ctypes.byref(out))
+        if rc == 3:
+            for a in arrays:
+                if a.release:
+                    ctypes.CFUNCTYPE(None, _P)(a.release)(ctypes.addressof(a))
+            return MetalArray.from_arrow(chunked.combine_chunks())
+        _check(rc)
+        return MetalArray(out)
+    finally:
+        for a in arrays:
+            if a.release:
+                ctypes.CFUNCTYPE(None, _P)(a.release)(ctypes.addressof(a))
+        if schema.release:
+            ctypes.CFUNCTYPE(None, _P)(schema.release)(ctypes.addressof(schema))
+
+
+def _per_key(value, n, what):
+    if isinstance(value, str):
+        return [value] * n
+    value = list(value)
+    if len(value) != n:
+        raise ArrowMetalError(f"{what} has {len(value)} entries for {n} columns")
+    return value
+
+
+def lexsort_indices(columns, descending=None, null_placement="at_end", float_order="ieee"):
+    """Multi-column sort: uint32 indices ordering the rows by each column in turn, the first column the
+    most significant. `descending` is one flag per column (None: all ascending); `null_placement` and
+    `float_order` are one value or one per key."""
+    cols = [c if isinstance(c, MetalArray) else MetalArray.from_arrow(c) for c in columns]
+    if not cols:
+        raise ArrowMetalError("lexsort needs at least one column")
+    flags = descending if descending is not None else [False] * len(cols)
+    if len(flags) != len(cols):
+        raise ArrowMetalError(f"descending has {len(flags)} entries for {len(cols)} columns")
+    n = len(cols)
+    handles = (_P * n)(*[c._h for c in cols])
+    desc = (ctypes.c_int * n)(*[1 if d else 0 for d in flags])
+    np_ = (ctypes.c_int * n)(*[_index_of(NULL_PLACEMENT, p, "null_placement")
+                               for p in _per_key(null_placement, n, "null_placement")])
+    fo = (ctypes.c_int * n)(*[_index_of(FLOAT_ORDERS, f, "float_order")
+                              for f in _per_key(float_order, n, "float_order")])
+    out = _P()
+    _check(_lib.am_lexsort_ex2(handles, desc, np_, fo, n, ctypes.byref(out)))
+    return MetalArray(out)
+
+
+def take_columns(columns, indices):
+    """`take` of several columns through one index array, with one index read on the GPU."""
+    cols = [c if isinstance(c, MetalArray) else MetalArray.from_arrow(c) for c in columns]
+    if not isinstance(indices, MetalArray):
+        indices = MetalArray.from_arrow(_index_array(indices))
+    n = len(cols)
+    handles = (_P * n)(*[c._h for c in cols])
+    outs = (_P * n)()
+    _check(_lib.am_take_columns(handles, n, indices._h, outs))
+    return [MetalArray(outs[i]) for i in range(n)]
+
+
+def argsort_batch(arrays, descending=None, null_placement=None, float_order=None):
+    """Segmented sort: uint32 indices of each array, all sorted in one call."""
+    cols = [c if isinstance(c, MetalArray) else MetalArray.from_arrow(c) for c in arrays]
+    n = len(cols)
+    handles = (_P * n)(*[c._h for c in cols])
+    d = (ctypes.c_int * n)(*[1 if x else 0 for x in (descending or [False] * n)])
+    p = (ctypes.c_int * n)(*[_index_of(NULL_PLACEMENT, x, "null_placement") for x in (null_placement or ["at_end"] * n)])
+    f = (ctypes.c_int * n)(*[_index_of(FLOAT_ORDERS, x, "float_order") for x in (float_order or ["ieee"] * n)])
+    outs = (_P * max(n, 1))()
+    _check(_lib.am_argsort_batch(handles, d, p, f, n, outs))
+    return [MetalArray(outs[i]) for i in range(n)]
+
+
+# ---- batching, router, plan ----------------------------------------------------------------------
+
+@contextlib.contextmanager
+def batch():
+    """Calls inside the block do not wait for the GPU; deferred errors raise at its end."""
+    _check(_lib.am_batch_begin())
+    try:
+        yield
+    finally:
+        _check(_lib.am_batch_end())
+
+
+_ROUTER = ("auto", "gpu", "cpu")
+
+
+def set_router(mode):
+    """Router mode ("auto", "gpu", "cpu"). The sort is never routed to the CPU."""
+    _check(_lib.am_router_set_mode(_index_of(_ROUTER, mode, "router mode")))
+
+
+def get_router():
+    return _ROUTER[_lib.am_router_get_mode()]
+
+
+class PlanSource:
+    """A named table the plan engine scans (am_plan_source_create)."""
+
+    def __init__(self, name, columns):
+        cols = {k: (v if isinstance(v, MetalArray) else MetalArray.from_arrow(v)) for k, v in columns.items()}
+        n = len(cols)
+        handles = (_P * n)(*[c._h for c in cols.values()])
+        names = (ctypes.c_char_p * n)(*[k.encode() for k in cols])
+        self._h = _P()
+        _check(_lib.am_plan_source_create(name.encode(), handles, names, n, ctypes.byref(self._h)))
+        self.name = name
+        self._cols = cols
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _lib.am_plan_source_release(h)
+            self._h = None
+
+
+def run_plan(plan, sources):
+    """Runs a plan (a dict or its JSON) over PlanSource tables; returns {name: MetalArray}."""
+    text = plan if isinstance(plan, str) else json.dumps(plan)
+    n = len(sources)
+    hs = (_P * max(n, 1))(*[s._h for s in sources])
+    r = _P()
+    _check(_lib.am_plan_run(text.encode(), hs, n, 1, ctypes.byref(r)))
+    try:
+        out = {}
+        for i in range(_lib.am_plan_column_count(r)):
+            h = _P()
+            _check(_lib.am_plan_column(r, i, ctypes.byref(h)))
+            out[_lib.am_plan_column_name(r, i).decode()] = MetalArray(h)
+        return out
+    finally:
+        _lib.am_plan_result_release(r)
+
+
+def explain_plan(plan, sources):
+    text = plan if isinstance(plan, str) else json.dumps(plan)
+    n = len(sources)
+    hs = (_P * max(n, 1))(*[s._h for s in sources])
+    s = _lib.am_plan_explain(text.encode(), hs, n, 1)
+    if s is None:
+        _check(1)
+    return s.decode()
+
+
+# ---- CUDA additions ------------------------------------------------------------------------------
+
+def set_stream(stream_ptr):
+    """Enqueue this thread's calls on an existing cudaStream_t (an int address; 0 = the library's)."""
+    _check(_lib.am_cuda_set_stream(stream_ptr or None))
+
+
+def synchronize():
+    _check(_lib.am_cuda_synchronize())
+
+
+def last_sort_stats():
+    s = SortStats()
+    _check(_lib.am_last_sort_stats(ctypes.byref(s)))
+    return {"rows": s.rows, "value_rows": s.value_rows, "passes_run": s.passes_run,
+            "passes_skipped": s.passes_skipped}
+
+
+def profile(on=True):
+    _check(_lib.am_cuda_profile(1 if on else 0))
+
+
+def profile_reset():
+    _check(_lib.am_cuda_profile_reset())
+
+
+def profile_entries():
+    """{kernel name: (launches, total ms)} of the launches timed since the last reset."""
+    out = {}
+    n = _lib.am_cuda_profile_count()
+    if n < 0:
+        _check(1)
+    for i in range(n):
+        name, launches, ms = ctypes.c_char_p(), _I64(), ctypes.c_double()
+        _check(_lib.am_cuda_profile_entry(i, ctypes.byref(name), ctypes.byref(launches), ctypes.byref(ms)))
+        out[name.value.decode()] = (launches.value, ms.value)
+    return out

@@ -1,0 +1,221 @@
+// Internal declarations of libArrowMetalC for B200: the device runtime (one CUDA device, a stream per
+// calling thread, stream-ordered allocation from the device memory pool, a pinned host pool), the
+// HBM-resident array handle behind `am_array*`, and the entry points of the sort and take engines.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <atomic>
+#include <functional>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/arrowmetal.h"
+
+namespace am {
+
+// ---------------------------------------------------------------------------------------------
+// Errors. Internal code throws; every extern "C" entry point catches and turns the exception into
+// the reference's return-code convention (Sources/ArrowMetalC/ArrowMetalC.swift:9-34).
+
+struct Error : std::runtime_error {
+  int code;
+  explicit Error(const std::string& m, int c = 1) : std::runtime_error(m), code(c) {}
+};
+
+// The reference's ArrowMetalError descriptions (Sources/ArrowMetal/MetalContext.swift:19-27).
+inline Error invalid(const std::string& m) { return Error("Invalid ArrowArray: " + m); }
+inline Error unsupported(const std::string& m) { return Error("Unsupported Arrow type: " + m); }
+inline Error length_mismatch(int64_t a, int64_t b) {
+  return Error("Array length mismatch: " + std::to_string(a) + " vs " + std::to_string(b));
+}
+
+void cuda_check(cudaError_t e, const char* what);
+#define AM_CUDA(x) ::am::cuda_check((x), #x)
+
+void set_last_error(const std::string& m);
+
+// ---------------------------------------------------------------------------------------------
+// Device runtime.
+
+struct Device {
+  int ordinal = 0;
+  int sm_count = 0;
+  std::string name;
+  cudaMemPool_t pool = nullptr;
+};
+Device& device();                       // initialises on first use; throws when no CUDA device
+cudaStream_t stream();                  // the calling thread's stream (override or its own)
+void set_stream_override(cudaStream_t s);
+cudaStream_t stream_override();
+
+// Stream-ordered device allocation from the device's memory pool (kept reserved between calls).
+void* dmalloc(size_t bytes, cudaStream_t s);
+void dfree(void* p, cudaStream_t s);
+void debug_fail_alloc_after(int64_t n);
+void debug_skip_first_tile(bool on);
+bool debug_skip_first_tile();
+
+// A device allocation, or a borrowed device range with a custom release.
+struct DevBuffer {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  cudaStream_t stream = nullptr;          // the stream its last writer / reader used
+  std::function<void()> on_release;       // borrowed memory: runs the producer's release
+  bool owned = false;
+  DevBuffer() = default;
+  DevBuffer(const DevBuffer&) = delete;
+  DevBuffer& operator=(const DevBuffer&) = delete;
+  ~DevBuffer();
+  static std::shared_ptr<DevBuffer> alloc(size_t bytes, cudaStream_t s);
+};
+using BufPtr = std::shared_ptr<DevBuffer>;
+
+// Pinned host memory from a caching pool (export buffers and staging).
+void* pinned_alloc(size_t bytes);
+void pinned_free(void* p);
+
+// Host threads used by the staged host copies (am_set_import_threads).
+int import_threads();
+void set_import_threads(int n);
+// Host <-> device copies of user memory: pinned sources copy directly; pageable ones go through a
+// ring of pinned staging slots filled by `import_threads()` host threads. copy_h2d returns true when
+// the copy may still read `src` after it returns (a pinned source): the caller keeps it alive.
+bool copy_h2d(void* dst, const void* src, size_t bytes, cudaStream_t s);
+void copy_d2h(void* dst, const void* src, size_t bytes, cudaStream_t s);
+
+// Per-thread state.
+struct ThreadState {
+  std::string last_error;
+  int batch_depth = 0;
+  cudaStream_t override_stream = nullptr;
+  cudaStream_t own_stream = nullptr;
+  am_sort_stats last_stats{};
+  cudaStream_t stats_stream = nullptr;                   // the last sort's counters are copied here
+  std::vector<std::function<void()>> deferred_checks;   // run at the batch's end
+  std::string scratch_text;                              // am_plan_explain result
+};
+ThreadState& tls();
+
+// Per-stream persistent scratch: the radix sort's look-back status words (zeroed once when grown,
+// then told apart by a per-stream epoch), and a device error word kernels OR into.
+struct StreamScratch {
+  uint64_t* status = nullptr;
+  size_t status_words = 0;
+  uint32_t epoch = 0;
+  uint32_t* err = nullptr;
+};
+StreamScratch& stream_scratch(cudaStream_t s, size_t status_words);
+// Reads and clears the stream's device error word (synchronises the stream); throws on an error.
+void check_device_errors(cudaStream_t s);
+void sync_stream(cudaStream_t s);
+
+// Kernel timing (am_cuda_profile).
+bool profiling();
+void set_profiling(bool on);
+struct KernelTimer {
+  const char* name;
+  cudaStream_t s;
+  cudaEvent_t a = nullptr, b = nullptr;
+  KernelTimer(const char* n, cudaStream_t st);
+  ~KernelTimer();
+};
+void profile_collect();
+struct ProfileEntry { std::string name; int64_t launches; double total_ms; };
+std::vector<ProfileEntry> profile_entries();
+void profile_reset();
+
+// ---------------------------------------------------------------------------------------------
+// Arrow types the sort path carries.
+
+enum PhysType : int32_t {
+  PT_BOOL = 0, PT_I8, PT_U8, PT_I16, PT_U16, PT_I32, PT_U32, PT_I64, PT_U64, PT_F16, PT_F32, PT_F64,
+};
+inline int pt_bytes(int pt) {
+  switch (pt) {
+    case PT_BOOL: return 0;   // bit-packed
+    case PT_I8: case PT_U8: return 1;
+    case PT_I16: case PT_U16: case PT_F16: return 2;
+    case PT_I32: case PT_U32: case PT_F32: return 4;
+    default: return 8;
+  }
+}
+inline bool pt_float(int pt) { return pt == PT_F16 || pt == PT_F32 || pt == PT_F64; }
+inline int pt_key_bytes(int pt) { return pt_bytes(pt) == 8 ? 8 : 4; }
+// Parses an Arrow C Data Interface format string; throws unsupported for the types this build does
+// not carry (strings, nested, dictionary, decimal, intervals).
+int parse_format(const char* fmt);
+
+// ---------------------------------------------------------------------------------------------
+// The array handle.
+
+}  // namespace am
+
+struct am_array {
+  std::atomic<int64_t> refs{1};
+  int32_t pt = 0;
+  std::string format;
+  int64_t length = 0;
+  int64_t null_count = 0;             // -1: being counted on the device (null_count_dev)
+  am::BufPtr values;                  // element 0 sits at values->ptr + value_offset * width
+  int64_t value_offset = 0;           // elements (bits for bool)
+  am::BufPtr validity;                // may be null: no nulls
+  int64_t validity_offset = 0;        // bits
+  am::BufPtr null_count_dev;          // unsigned long long, when null_count == -1
+  cudaStream_t last_stream = nullptr;
+  // >= 0 when this is an index array this library produced: no nulls and every index < perm_of.
+  int64_t perm_of = -1;
+
+  const void* data() const {
+    if (!values) return nullptr;
+    int w = am::pt_bytes(pt);
+    if (w == 0) return values->ptr;
+    return static_cast<const char*>(values->ptr) + value_offset * w;
+  }
+  const uint8_t* valid_bits() const {
+    return validity ? static_cast<const uint8_t*>(validity->ptr) : nullptr;
+  }
+};
+
+namespace am {
+
+am_array* new_array(int pt, const std::string& format, int64_t length);
+void retain(am_array* a);
+void release(am_array* a);
+// Orders the calling stream after the last work that touched `a` (when it ran on another stream).
+void use_on(am_array* a, cudaStream_t s);
+int64_t resolve_null_count(am_array* a);     // waits for a pending device count
+std::string format_of(int pt);
+
+// ---------------------------------------------------------------------------------------------
+// Engines.
+
+// Key options of one sort key (the reference's descending / NullPlacement / FloatOrder,
+// Sources/ArrowMetal/ComputeOptions.swift:15-60).
+struct SortKey {
+  am_array* col = nullptr;
+  bool descending = false;
+  bool nulls_first = false;
+  int float_order = 0;                 // 0 ieee, 1 total, 2 nan_largest
+};
+// Stable multi-key argsort; keys[0] is the most significant. Writes n row numbers of `index_width`
+// bytes (4 or 8) into `out` (device memory) on stream `s`.
+void radix_argsort(const std::vector<SortKey>& keys, int64_t n, void* out, int index_width,
+                   cudaStream_t s, am_sort_stats* stats);
+
+// Gathers `count` columns through one index array. outs[i] must be new arrays of indices' length.
+// `check_range` asks the kernel to flag an index outside [0, src length) in the stream's error word.
+void take_columns(am_array* const* cols, int count, am_array* indices, am_array** outs,
+                  bool check_range, cudaStream_t s);
+
+void fill_last_sort_stats(am_sort_stats* out);   // waits for the calling thread's last sort
+
+int64_t max_row_index();
+void set_max_row_index(int64_t v);
+void check_index_rows(int64_t rows, const char* op);
+
+}  // namespace am

@@ -1,0 +1,91 @@
+// Shared layouts of the radix sort's kernels (radix_sort.cu) and the segmented form (segmented.cu).
+#pragma once
+
+#include <stdint.h>
+
+namespace am {
+namespace rs {
+
+constexpr int RADIX = 256;                 // 8-bit digits: 4 passes for a 32-bit key, 8 for a 64-bit one
+constexpr int NAN_BIN = 256;               // routing bins of the most significant key's first pass
+constexpr int NULL_BIN = 257;
+constexpr int NBINS = 258;
+constexpr uint32_t INVALID_DIGIT = 0xFFFFu;
+constexpr int MAX_KEYS = 16;
+constexpr int MAX_SLOTS = MAX_KEYS * 9;
+
+constexpr int FO_IEEE = 0, FO_TOTAL = 1, FO_NANLARGEST = 2;
+
+// Pass flags.
+constexpr uint32_t PF_ENCODE = 1;          // first pass of a key: read the column (through the ids)
+constexpr uint32_t PF_ROUTE = 2;           // most significant key: null / NaN rows go straight out
+constexpr uint32_t PF_CATPASS = 4;         // a lower key's null category, looked up by row id
+constexpr uint32_t PF_WIDE_OUT = 8;        // the output index array is uint64
+
+// Look-back status word: epoch (30 bits) | flag (2 bits) | count (32 bits).
+constexpr uint32_t ST_AGG = 1, ST_INCL = 2;
+constexpr uint64_t LOOKBACK_TIMEOUT_NS = 1000000000ull;   // 1 s, then the pass reports an error
+
+// Device error word bits.
+constexpr uint32_t ERR_LOOKBACK_TIMEOUT = 1;
+constexpr uint32_t ERR_TAKE_RANGE = 2;
+
+// One key column as the kernels read it.
+struct ColView {
+  const void* values;        // row 0 (bool: the bitmap, row 0 at bit bool_off)
+  const uint8_t* valid;      // NULL: no nulls
+  int64_t valid_off;         // bit of row 0 in `valid`
+  int64_t bool_off;
+  int32_t pt;                // am::PhysType
+  uint8_t desc;
+  uint8_t nulls_first;
+  uint8_t float_order;
+  uint8_t nan_cat;           // ieee float: NaN rows form their own block
+};
+
+struct KeyStats {
+  uint32_t hist[8][256];     // per digit position, counts of the value keys
+  uint32_t n_value, n_null, n_nan, pad;
+  unsigned long long vmax, vmin_inv;
+};
+
+struct KeyPlan {
+  unsigned long long fold_nan, fold_null;   // keys given to a lower key's NaN / null rows
+  uint32_t fold_mode;                       // 1: no room in the key range, a category pass follows
+  uint32_t pad;
+};
+
+struct PassDesc {
+  uint32_t active, flags, count, shift;
+  int32_t src_keys, src_ids, dst_keys, dst_ids;   // -1: none / identity / the output array
+  uint32_t value_base, key;
+  uint32_t bin_base[NBINS];
+};
+
+struct SortSummary {
+  uint32_t value_rows, null_rows, nan_rows, passes_run, passes_total, pad[3];
+};
+
+struct PlanArgs {
+  uint64_t n;
+  int32_t nkeys, nslots, slot_key0_first, index_wide;
+  uint8_t key_bytes[MAX_KEYS];
+  uint8_t nulls_first[MAX_KEYS];
+  int8_t slot_key[MAX_SLOTS];
+  int8_t slot_digit[MAX_SLOTS];             // -1: category pass
+};
+
+struct PassArgs {
+  const PassDesc* desc;
+  const KeyPlan* kplan;
+  void* keys[2];
+  uint32_t* ids[2];
+  void* final_out;
+  uint64_t* status;
+  uint32_t* tile_counter;
+  uint32_t* err;
+  uint32_t epoch;
+};
+
+}  // namespace rs
+}  // namespace am

@@ -1,0 +1,327 @@
+"""Benchmark of the full-sort path: ORDER BY of a 50,000,000-row table on one B200 (per GPU).
+
+Workload (one step): a table of 3 columns -- key int64 uniform in [0, 2^40) with a 10% Bernoulli null
+bitmap, payload float64 ~ N(0, 1), payload int32 uniform -- sorted by key ascending, nulls last, stable,
+then all 3 columns taken through the permutation. It runs through the library's C ABI the way the
+DataFusion rule calls it: am_plan_run of select_all(sort(scan)). Inputs are seeded synthetic data of the
+benchmark's shape (numpy default_rng).
+
+  value    rows/s with the table already in HBM, timed with CUDA events on the library's stream, max
+           over ranks; inputs (400 MB key column) are larger than L2, so no flush is needed.
+  e2e      the same through the C ABI with host buffers: am_import of the 3 columns (host to device),
+           the plan, am_export of the 3 result columns (device to host), wall clock per step.
+  roofline the dominant kernel's algorithmic bytes / its CUDA-event time over the timed region, against
+           the measured HBM copy peak.
+  cpu_baseline  the CPU oracle (the reference algorithm restated in C) on the host's cores.
+
+python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+Multi-GPU (torchrun, one rank per GPU) runs independent replicas of the workload: the sort shards by
+table / request, with no collective on the data path ("scaling": "weak").
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_ROWS = 50_000_000
+SEED = 20260906 + 2
+METRIC = "rows/s + % HBM peak, 50M int64 argsort+take; batched vs plain; p99 latency"
+WORKLOAD = ("ORDER BY int64 key NULLS LAST + take of 3 columns (key int64 uniform [0,2^40) with 10% nulls, "
+            "float64 N(0,1), int32 uniform), 50,000,000 rows per GPU")
+
+
+def make_table(n, seed=SEED):
+    rng = np.random.default_rng(seed)
+    key = rng.integers(0, 2**40, n, dtype=np.int64)
+    valid = rng.random(n) >= 0.10
+    p1 = rng.standard_normal(n)
+    p2 = rng.integers(-2**31, 2**31 - 1, n, dtype=np.int32, endpoint=True)
+    return key, valid, p1, p2
+
+
+def arrow_columns(key, valid, p1, p2):
+    import pyarrow as pa
+    return {"c0": pa.array(key, mask=~valid), "c1": pa.array(p1), "c2": pa.array(p2)}
+
+
+PLAN = json.dumps({"op": "select", "exprs": [[f"c{i}", f'(col "c{i}")'] for i in range(3)],
+                   "input": {"op": "sort", "by": [["c0", False, {"nulls": "last"}]],
+                             "input": {"op": "scan", "source": "t"}}})
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.15)
+            self.proc.terminate()
+            self.proc.wait()
+            self.f.close()
+
+    def summary(self):
+        if not self.proc or not self.path:
+            return None
+        rows = []
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return float(json.load(open(p))["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def algorithmic_bytes(n, m, passes):
+    """Bytes each kernel must move once (the model the roofline uses; DESIGN.md states it):
+    histogram reads the key column and its bitmap; the first digit pass reads them again and writes the
+    m value rows' (key, id) plus the null rows' ids; a middle pass reads and writes m (key, id); the last
+    pass reads m (key, id) and writes m ids; the take reads the n ids, gathers and writes the 3 columns
+    (8 + 8 + 4 bytes a row) and the key's validity bit."""
+    src = 8 * n + n / 8
+    hist = src
+    if passes == 1:
+        pass_bytes = src + 4 * n
+    else:
+        pass_bytes = (src + 12 * m + 4 * (n - m)) + (passes - 2) * 24 * m + (12 * m + 4 * m)
+    take = 4 * n + 2 * (8 + 8 + 4) * n + 2 * n / 8
+    return {"radix_histogram": hist, "radix_onesweep_pass": pass_bytes, "take_gather": take}
+
+
+def cpu_oracle_rate(key, valid, p1, p2, threads):
+    """The CPU oracle on the whole workload once: argsort (C restatement, `threads` threads) and the
+    take of the 3 columns (C restatement, one thread per column)."""
+    import pyarrow as pa
+    from oracle import oracle
+    cols = arrow_columns(key, valid, p1, p2)
+    t0 = time.perf_counter()
+    idx = oracle.argsort(cols["c0"], threads=threads)
+    ia = pa.array(idx)
+    ths = [threading.Thread(target=oracle.take, args=(cols[c], ia)) for c in cols]
+    for t in ths:
+        t.start()
+    for t in ths:
+        t.join()
+    dt = time.perf_counter() - t0
+    return len(key) / dt, dt
+
+
+def run_reference_arm(args, rank):
+    """--impl reference: the reference's sort path on the host's cores. The reference is Swift + Metal
+    and runs on no machine here, so the C restatement of its algorithm in oracle/ stands in for it."""
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    # Size each step so that warm-up + timed steps take about two minutes.
+    probe = make_table(1_000_000, SEED)
+    rate, _ = cpu_oracle_rate(*probe, threads)
+    budget = 120.0 / max(1, args.steps + args.warmup)
+    n = int(min(N_ROWS, max(100_000, rate * budget)))
+    key, valid, p1, p2 = make_table(n, SEED)
+    for _ in range(args.warmup):
+        cpu_oracle_rate(key, valid, p1, p2, threads)
+    times = [cpu_oracle_rate(key, valid, p1, p2, threads)[1] for _ in range(args.steps)]
+    ms = 1e3 * sum(times) / len(times)
+    value = n / (ms / 1e3)
+    sample = f"the first {n:,} rows of the workload per step (same generator), argsort + take of 3 columns"
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "rows_per_step": n},
+        "cpu_baseline": {"value": value, "unit": "rows/s", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--rows", type=int, default=N_ROWS)
+    ap.add_argument("--impl", default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference_arm(args, rank)
+
+    os.environ["ARROWMETAL_DEVICE"] = str(local)
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    import pyarrow as pa
+    import arrowmetal_b200 as am
+
+    n = args.rows
+    key, valid, p1, p2 = make_table(n, SEED + rank)
+    m_rows = int(valid.sum())
+    cols = arrow_columns(key, valid, p1, p2)
+    stream = torch.cuda.Stream()
+    am.set_stream(stream.cuda_stream)
+
+    # ---- device-resident inputs (imported through the C ABI once)
+    dcols = {k: am.MetalArray.from_arrow(v) for k, v in cols.items()}
+    src = am.PlanSource("t", dcols)
+
+    def step():
+        out = am.run_plan(PLAN, [src])
+        del out
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    am.synchronize()
+    # passes run per sort, for the byte model
+    idx = dcols["c0"].argsort()
+    st = am.last_sort_stats()
+    del idx
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    peak, peak_kind = measured_peak()
+    am.profile(True)
+    am.profile_reset()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        barrier()
+        am.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        ev1.synchronize()
+        am.synchronize()
+        barrier()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    prof = am.profile_entries()
+    am.profile(False)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * n / (ms / 1e3)
+
+    # ---- roofline of the dominant kernel
+    model = algorithmic_bytes(n, m_rows, st["passes_run"])
+    per_kernel = {}
+    for name, (launches, total_ms) in prof.items():
+        if name in model:
+            b = model[name] * args.steps
+            per_kernel[name] = {"launches": launches, "total_ms": total_ms, "bytes": b,
+                                "gbs": b / (total_ms / 1e3) / 1e9}
+    dom = max(per_kernel, key=lambda k: per_kernel[k]["total_ms"])
+    d = per_kernel[dom]
+    gpu_launches = sum(l for l, _ in prof.values())
+
+    # ---- end to end through the C ABI with host buffers
+    h2d = sum(c.nbytes for c in (key, p1, p2)) + (n + 7) // 8
+    e2e_times = []
+    d2h = 0
+    for i in range(args.e2e_steps + 1):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        hc = {k: am.MetalArray.from_arrow(v) for k, v in cols.items()}
+        s2 = am.PlanSource("t", hc)
+        out = am.run_plan(PLAN, [s2])
+        res = {k: v.to_arrow() for k, v in out.items()}
+        dt = time.perf_counter() - t0
+        if i > 0:
+            e2e_times.append(dt)
+        d2h = sum(sum(b.size for b in r.buffers() if b is not None) for r in res.values())
+        del hc, s2, out, res
+    e2e_ms = 1e3 * statistics.median(e2e_times)
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "rows": n, "value_rows": m_rows, "radix_passes_run": st["passes_run"],
+                   "radix_passes_skipped": st["passes_skipped"], "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (400 MB key column), no flush"},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": d["gbs"], "peak": peak, "unit": "GB/s",
+                     "frac": d["gbs"] / peak, "peak_source": peak_kind, "traffic": None,
+                     "per_kernel": per_kernel},
+        "e2e": {"value": world * n / (e2e_ms / 1e3), "unit": "rows/s", "ms_per_step": e2e_ms,
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": int(gpu_launches),
+        "clocks": clocks.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        rate, dt = cpu_oracle_rate(key, valid, p1, p2, threads)
+        line["cpu_baseline"] = {"value": rate, "unit": "rows/s", "cores": threads, "kind": "port",
+                                "sample": f"the whole {n:,}-row workload once ({dt:.2f} s): C oracle argsort on "
+                                          f"{threads} threads + take of the 3 columns"}
+    if rank == 0:
+        print(json.dumps(line))
+    del src, dcols
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

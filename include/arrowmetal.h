@@ -1,0 +1,189 @@
+/* ArrowMetal C ABI, sort path, for NVIDIA B200 (sm_100a).
+ *
+ * Drop-in for the full-sort surface of ArrowMetal's include/arrowmetal.h (version 0.6.1): the same
+ * names, argument meanings, return codes and Arrow C Data Interface arrays, so the callers of that
+ * header (the Python ctypes binding, the DataFusion rule, the Polars engine and plugin) link against
+ * libArrowMetalC.so unchanged. Each declaration cites the reference declaration it replaces as
+ * include/arrowmetal.h:<line> (paths relative to the ArrowMetal source tree).
+ *
+ * Conventions (reference include/arrowmetal.h:1-3, Sources/ArrowMetalC/ArrowMetalC.swift:9-34):
+ *   return 0  success
+ *   return 1  the operation failed; am_last_error() holds the message (thread-local)
+ *   return 2  invalid argument (a NULL handle or pointer)
+ *   return 3  am_import_chunks: the type is not taken by the chunked import
+ * Handles are reference counted. Every `out` handle is new (+1) and the caller releases it with
+ * am_release; input handles are borrowed. Index arrays are uint32 ("I") holding row numbers up to
+ * 2^32 - 1; a call whose row numbers would pass that returns 1 with
+ * "<op>: row N does not fit the UInt32 index type (row numbers go up to M)".
+ *
+ * Arrays live in B200 HBM. Calls enqueue work on the calling thread's CUDA stream and return without
+ * waiting for the GPU; a call that must see a result (am_export, am_null_count of a fresh gather,
+ * am_take with indices this library did not produce, am_batch_end) waits for it. */
+#ifndef ARROWMETAL_H
+#define ARROWMETAL_H
+
+#include <stdint.h>
+#include "arrow_abi.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct am_array am_array;                 /* opaque, HBM-resident Arrow array */
+typedef struct am_plan_source_t am_plan_source;   /* include/arrowmetal.h:1419 */
+typedef struct am_plan_result_t am_plan_result;   /* include/arrowmetal.h:1420 */
+
+/* ---- library ---------------------------------------------------------------------------------- */
+const char* am_version(void);                     /* include/arrowmetal.h:15 */
+const char* am_device_name(void);                 /* include/arrowmetal.h:16 */
+const char* am_last_error(void);                  /* include/arrowmetal.h:17 */
+
+/* ---- lifecycle and interop -------------------------------------------------------------------- */
+/* Moves `array` (its release is NULL on success) and copies its buffers into HBM.
+ * include/arrowmetal.h:20 */
+int  am_import(const struct ArrowSchema* schema, struct ArrowArray* array, am_array** out);
+/* ARROW_DEVICE_CUDA arrays on this library's device are wrapped without a copy (the producer's
+ * release runs when the last handle goes); ARROW_DEVICE_CPU / CUDA_HOST arrays are copied.
+ * include/arrowmetal.h:21 */
+int  am_import_device(const struct ArrowSchema* schema, struct ArrowDeviceArray* array, am_array** out);
+/* n chunks of one type imported as one array; every chunk is moved on success.
+ * include/arrowmetal.h:34-35 */
+int  am_import_chunks(const struct ArrowSchema* schema, struct ArrowArray* arrays, int64_t n, am_array** out);
+int  am_import_chunks_supported(const struct ArrowSchema* schema);
+/* Host threads of the chunked import and of the staged host copies (0 = the built-in policy).
+ * include/arrowmetal.h:46-47 */
+int  am_set_import_threads(int n);
+int  am_get_import_threads(void);
+/* Copies the array into pinned host memory owned by the exported structs' release callbacks.
+ * include/arrowmetal.h:48 */
+int  am_export(am_array* a, struct ArrowSchema* schema, struct ArrowArray* array);
+/* Zero-copy export of the HBM buffers with device_type ARROW_DEVICE_CUDA (the reference exports
+ * ARROW_DEVICE_METAL). include/arrowmetal.h:49 */
+int  am_export_device(am_array* a, struct ArrowSchema* schema, struct ArrowDeviceArray* array);
+void am_release(am_array* a);                     /* include/arrowmetal.h:50 */
+int64_t     am_length(am_array* a);               /* include/arrowmetal.h:51 */
+int64_t     am_null_count(am_array* a);           /* include/arrowmetal.h:52 */
+const char* am_format(am_array* a);               /* include/arrowmetal.h:53 */
+const char* am_compute_format(am_array* a);       /* include/arrowmetal.h:58 */
+
+/* ---- selection -------------------------------------------------------------------------------- */
+/* Arrow `take`: indices int32, int64 or uint32; a null index gives a null row; an index out of range
+ * returns 1 ("take: index out of range (array length N)"). include/arrowmetal.h:93 */
+int  am_take(am_array* a, am_array* indices, am_array** out);
+int  am_slice(am_array* a, int64_t offset, int64_t length, am_array** out);   /* include/arrowmetal.h:94 */
+
+/* ---- sorting ---------------------------------------------------------------------------------- */
+/* Stable; nulls last; float -0.0 ties +0.0 and NaN sits next to the nulls in both directions.
+ * include/arrowmetal.h:96-110 */
+int  am_argsort(am_array* a, int descending, am_array** out);                 /* :108 */
+int  am_sort(am_array* a, int descending, am_array** out);                    /* :109 */
+int  am_top_k(am_array* a, int64_t k, int largest, am_array** out);           /* :110 */
+
+/* Option-carrying forms. null_placement: 0 at_end, 1 at_start. float_order: 0 ieee (Arrow C++),
+ * 1 total (IEEE 754 totalOrder, arrow-rs), 2 nan_largest (Polars). include/arrowmetal.h:1302-1352 */
+int  am_argsort_ex(am_array* a, int descending, int null_placement, am_array** out);          /* :1331 */
+int  am_sort_ex(am_array* a, int descending, int null_placement, am_array** out);             /* :1332 */
+int  am_lexsort_ex(am_array** columns, const int* descending, int64_t count,
+                   int null_placement, am_array** out);                                      /* :1333 */
+int  am_argsort_ex2(am_array* a, int descending, int null_placement, int float_order,
+                    am_array** out);                                                         /* :1348 */
+int  am_sort_ex2(am_array* a, int descending, int null_placement, int float_order,
+                 am_array** out);                                                            /* :1349 */
+int  am_top_k_ex(am_array* a, int64_t k, int largest, int null_placement, int float_order,
+                 am_array** out);                                                            /* :1350 */
+int  am_lexsort_ex2(am_array** columns, const int* descending, const int* null_placement,
+                    const int* float_order, int64_t count, am_array** out);                  /* :1352 */
+/* Multi-column sort, first column most significant. include/arrowmetal.h:458 */
+int  am_lexsort(am_array** columns, const int* descending, int64_t count, am_array** out);
+
+/* ---- batching --------------------------------------------------------------------------------- */
+/* Between begin and end the calls of this thread do not wait for the GPU; deferred errors (a take
+ * out of range) surface from am_batch_end. include/arrowmetal.h:184-185 */
+int  am_batch_begin(void);
+int  am_batch_end(void);
+
+/* ---- plan engine (the subset the DataFusion rule and the Polars engine emit for a sort) -------- */
+/* Grammar taken: scan {source, columns?}; select / with_columns of [name, "(col \"x\")"] pairs;
+ * sort {by: [KEY...], nulls?, float_order?}; limit {count, offset?}. include/arrowmetal.h:1369-1433 */
+int  am_plan_source_create(const char* name, am_array** columns, const char** names,
+                           int64_t n_columns, am_plan_source** out);                         /* :1422 */
+void am_plan_source_release(am_plan_source* s);                                              /* :1424 */
+int  am_plan_run(const char* plan_json, am_plan_source** sources, int64_t n_sources, int optimize,
+                 am_plan_result** out);                                                      /* :1425 */
+const char* am_plan_explain(const char* plan_json, am_plan_source** sources, int64_t n_sources,
+                            int optimize);                                                   /* :1427 */
+int64_t     am_plan_column_count(am_plan_result* r);                                         /* :1428 */
+int64_t     am_plan_row_count(am_plan_result* r);                                            /* :1429 */
+const char* am_plan_column_name(am_plan_result* r, int64_t i);                               /* :1430 */
+int         am_plan_column(am_plan_result* r, int64_t i, am_array** out);                    /* :1431 */
+void        am_plan_result_release(am_plan_result* r);                                       /* :1432 */
+
+/* ---- router ------------------------------------------------------------------------------------ */
+/* Modes 0 auto, 1 gpu, 2 cpu are recorded (2 returned for an unknown mode); the sort is never routed
+ * to the CPU (include/arrowmetal.h:1785-1797), so the mode changes nothing on this path. The
+ * binding's test set-up calls it. include/arrowmetal.h:1799-1800 */
+int  am_router_set_mode(int mode);
+int  am_router_get_mode(void);
+
+/* ================================================================================================
+ * Additions with no counterpart in the reference header. They stand beside the drop-in surface and
+ * change nothing in it.
+ * ============================================================================================== */
+
+/* The CUDA stream the calling thread's calls enqueue on (a cudaStream_t). NULL restores the
+ * library's own non-blocking stream for this thread. Lets a host that already owns a stream (a
+ * PyTorch program, a server worker) order the sort with its own work. */
+int   am_cuda_set_stream(void* stream);
+void* am_cuda_get_stream(void);
+/* Waits for every call this thread has enqueued, then reports any deferred device error. */
+int   am_cuda_synchronize(void);
+/* CUDA device ordinal the library runs on (the ARROWMETAL_DEVICE variable, else the current one). */
+int   am_cuda_device(void);
+
+/* am_argsort_ex2 with the index width chosen: 4 gives uint32 ("I", as am_argsort_ex2), 8 gives
+ * uint64 ("L", the type pyarrow's sort_indices returns). */
+int  am_argsort_ex3(am_array* a, int descending, int null_placement, int float_order,
+                    int index_width, am_array** out);
+
+/* Multi-column take with one index read: outs[i] = take(columns[i], indices). Same rules as
+ * am_take; one gather kernel serves every column. */
+int  am_take_columns(am_array** columns, int64_t count, am_array* indices, am_array** outs);
+
+/* Segmented (batched) argsort: `count` independent arrays sorted in one pipeline, each with its own
+ * options (descending / null_placement / float_order hold `count` entries or are NULL). outs[i]
+ * receives uint32 indices into arrays[i], identical to am_argsort_ex2 on that array alone. */
+int  am_argsort_batch(am_array** arrays, const int* descending, const int* null_placement,
+                      const int* float_order, int64_t count, am_array** outs);
+
+/* Per-call counters of the calling thread's last sort: rows, radix passes run and skipped, and the
+ * device time of the sort's kernels in microseconds (0 unless am_cuda_profile(1) is on). */
+typedef struct am_sort_stats {
+  int64_t rows;
+  int64_t value_rows;
+  int32_t passes_run;
+  int32_t passes_skipped;
+  double  kernel_us;
+} am_sort_stats;
+int  am_last_sort_stats(am_sort_stats* out);
+/* Kernel timing with CUDA events around every launch of this library (1 on, 0 off), and the
+ * accumulated per-kernel totals: name, launches, total milliseconds. */
+int  am_cuda_profile(int on);
+int64_t am_cuda_profile_count(void);
+int  am_cuda_profile_entry(int64_t i, const char** name, int64_t* launches, double* total_ms);
+int  am_cuda_profile_reset(void);
+
+/* Test hooks: the largest row number an index array may hold (2^32 - 1 by default; tests lower it to
+ * reach the refusal at small sizes), and a host allocation failure after `n` more device
+ * allocations (-1 disables it). */
+int  am_debug_set_max_row_index(int64_t max_row);
+int  am_debug_fail_alloc_after(int64_t n);
+/* Test hook for the bounded look-back: with `on` set, the calling process's next sorts never process
+ * their first tile, so the tiles after it wait on a status nothing writes; each such wait gives up
+ * after one second and the call returns 1 ("look-back wait timed out"). No GPU fault is involved. */
+int  am_debug_skip_first_tile(int on);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ARROWMETAL_H */

@@ -1,0 +1,238 @@
+"""CPU oracle of the full-sort path -- TEST INFRASTRUCTURE ONLY.
+
+Only the tests, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg import this module; the
+product (``arrowmetal_b200`` and ``libArrowMetalC.so``) never does.
+
+Two independent restatements of ArrowMetal 0.6.1's sort semantics:
+
+* ``argsort`` / ``lexsort`` / ``take`` call ``liboracle.so`` (``sort_oracle.c``), a C restatement of the
+  reference's Metal algorithm: key maps (Sources/ArrowMetal/Kernels/SortSource.swift:131-190), stable
+  three-way partition (SortSource.swift:226-330), 8-bit LSD passes with constant-digit skipping
+  (Sort.swift:404-494), lexsort by take + argsort + compose (Kernels/MultiSort.swift:56-64), take with
+  null indices and range errors (Kernels/Take.swift:41-79).
+* ``np_argsort`` / ``np_lexsort`` restate the same orders from their definitions with numpy's stable
+  sort (the reference's CPU reference of SortOptionsTests.swift:15-62 and the ``total_order_indices``
+  oracle of python/tests/test_sort_options.py:58-76).
+
+Both are pinned by the reference's known-answer vectors (tests/test_oracle.py) and by pyarrow's own
+``sort_indices`` / ``take`` (the reference's oracle for the ieee order) through the fixtures in
+tests/golden/.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+import pyarrow as pa
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "liboracle.so")
+
+PT = {"bool": 0, "int8": 1, "uint8": 2, "int16": 3, "uint16": 4, "int32": 5, "uint32": 6,
+      "int64": 7, "uint64": 8, "halffloat": 9, "float": 10, "double": 11}
+FLOAT_ORDERS = {"ieee": 0, "total": 1, "nan_largest": 2}
+
+_lib = None
+
+
+def build():
+    """Compiles liboracle.so with gcc (the oracle's own Makefile)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        P, I64, I = ctypes.c_void_p, ctypes.c_int64, ctypes.c_int
+        L.oracle_argsort.argtypes = [P, P, I64, I64, I64, I, I, I, I, P, I]
+        L.oracle_take.argtypes = [P, P, I64, I64, I64, I, P, I, P, I64, I64, P, P]
+        L.oracle_lexsort.argtypes = [I, P, P, P, P, P, P, P, P, I64, P, I]
+        _lib = L
+    return _lib
+
+
+def _physical(arr):
+    """(pt code, values address, validity address or 0, offset, byte width, keep-alive) of a pyarrow
+    primitive array, read straight from its buffers (temporal types by their integer storage)."""
+    t = arr.type
+    if pa.types.is_timestamp(t) or pa.types.is_date64(t) or pa.types.is_time64(t) or pa.types.is_duration(t):
+        storage = "int64"
+    elif pa.types.is_date32(t) or pa.types.is_time32(t):
+        storage = "int32"
+    elif pa.types.is_boolean(t):
+        storage = "bool"
+    else:
+        storage = str(t)   # 'int8' ... 'uint64', 'halffloat', 'float', 'double'
+    if storage not in PT:
+        raise TypeError(f"oracle: type {t} is not on the sort path")
+    bufs = arr.buffers()
+    vb = bufs[0] if arr.null_count > 0 else None
+    width = {0: 0, 1: 1, 2: 1, 3: 2, 4: 2, 5: 4, 6: 4, 7: 8, 8: 8, 9: 2, 10: 4, 11: 8}[PT[storage]]
+    return PT[storage], bufs[1].address, (vb.address if vb is not None else 0), arr.offset, width, bufs
+
+
+def _as_array(a):
+    if isinstance(a, pa.ChunkedArray):
+        a = a.combine_chunks()
+    return a
+
+
+def argsort(arr, descending=False, null_placement="at_end", float_order="ieee", threads=1):
+    """uint32 indices of Arrow's stable array_sort_indices, by the C restatement."""
+    arr = _as_array(arr)
+    n = len(arr)
+    out = np.empty(max(n, 1), dtype=np.uint32)
+    pt, va, vb, off, width, keep = _physical(arr)
+    # Values are addressed from element 0 of the buffer: fold the array offset into the address.
+    vaddr = va + off * width if width else va
+    boff = off if width == 0 else 0
+    lib().oracle_argsort(vaddr, vb or None, off, boff, n, pt, int(bool(descending)),
+                         1 if null_placement == "at_start" else 0, FLOAT_ORDERS[float_order],
+                         out.ctypes.data, int(threads))
+    del keep
+    return out[:n]
+
+
+def lexsort(arrays, descending=None, null_placement="at_end", float_order="ieee", threads=1):
+    """uint32 indices of Arrow's multi-key sort_indices, by the C restatement (first key most
+    significant); options are one value or one per key."""
+    arrays = [_as_array(a) for a in arrays]
+    K = len(arrays)
+    n = len(arrays[0])
+    desc = list(descending) if descending is not None else [False] * K
+    place = [null_placement] * K if isinstance(null_placement, str) else list(null_placement)
+    order = [float_order] * K if isinstance(float_order, str) else list(float_order)
+    parts = [_physical(a) for a in arrays]
+    P = ctypes.c_void_p * K
+    I64 = ctypes.c_int64 * K
+    Ia = ctypes.c_int * K
+    vals = P(*[p[1] + (a.offset * p[4] if p[4] else 0) for p, a in zip(parts, arrays)])
+    valid = P(*[p[2] or None for p in parts])
+    voff = I64(*[a.offset for a in arrays])
+    boff = I64(*[(a.offset if p[4] == 0 else 0) for p, a in zip(parts, arrays)])
+    pts = Ia(*[p[0] for p in parts])
+    out = np.empty(max(n, 1), dtype=np.uint32)
+    lib().oracle_lexsort(K, vals, valid, voff, boff, pts, Ia(*[int(bool(d)) for d in desc]),
+                         Ia(*[1 if p == "at_start" else 0 for p in place]),
+                         Ia(*[FLOAT_ORDERS[f] for f in order]), n, out.ctypes.data, 1 if threads is None else int(threads))
+    return out[:n]
+
+
+def take(arr, indices):
+    """(values as a numpy array of the storage type / packed bits for bool, validity bool array) of
+    Arrow's take, by the C restatement; raises IndexError for an index out of range."""
+    arr = _as_array(arr)
+    indices = _as_array(indices)
+    pt, va, vb, off, width, keep = _physical(arr)
+    it = indices.type
+    kind = 0 if it == pa.uint32() else 1 if it == pa.int32() else 2
+    if it not in (pa.uint32(), pa.int32(), pa.int64()):
+        raise TypeError("take indices must be int32, int64 or uint32")
+    ib = indices.buffers()
+    iwidth = 4 if kind < 2 else 8
+    n = len(indices)
+    if width:
+        out = np.zeros(max(n, 1), dtype={1: np.uint8, 2: np.uint16, 4: np.uint32, 8: np.uint64}[width])
+    else:
+        out = np.zeros(max((n + 7) // 8, 1), dtype=np.uint8)
+    outv = np.zeros(max(n, 1), dtype=np.uint8)
+    ivb = ib[0].address if indices.null_count > 0 else None
+    vaddr = va + off * width if width else va
+    bad = lib().oracle_take(vaddr, vb or None, off, off if width == 0 else 0, len(arr), width,
+                            ib[1].address + indices.offset * iwidth, kind, ivb, indices.offset, n,
+                            out.ctypes.data, outv.ctypes.data)
+    del keep
+    if bad:
+        raise IndexError("take: index out of range")
+    return (out[:n] if width else out), outv[:n].astype(bool)
+
+
+# ---- numpy restatement (independent of the C one) --------------------------------------------------
+
+def _keys_and_categories(arr, descending, float_order):
+    """Order-preserving keys (uint64) and categories (0 value, 1 NaN block, 2 null) of every row."""
+    arr = _as_array(arr)
+    n = len(arr)
+    valid = np.ones(n, bool) if arr.null_count == 0 else np.asarray(arr.is_valid().to_numpy(zero_copy_only=False))
+    t = arr.type
+    cat = np.where(valid, 0, 2).astype(np.int8)
+    if pa.types.is_floating(t):
+        if t == pa.float16():
+            raw = np.asarray(arr.cast(pa.float32()).fill_null(0).to_numpy(zero_copy_only=False), dtype=np.float32)
+            t32 = True
+        else:
+            raw = np.asarray(arr.fill_null(0).to_numpy(zero_copy_only=False))
+            t32 = t == pa.float32()
+        bits = raw.view(np.uint32).astype(np.uint64) if t32 else raw.view(np.uint64).copy()
+        width = 32 if t32 else 64
+        S = np.uint64(1 << (width - 1))
+        full = np.uint64((1 << width) - 1)
+        expmask = np.uint64(0x7F800000 if t32 else 0x7FF0000000000000)
+        mag = bits & ~S & full
+        nan = mag > expmask
+        if float_order != "total":
+            bits = np.where(mag == 0, np.uint64(0), bits)
+            bits = np.where(nan, np.uint64(0x7F800001 if t32 else 0x7FF0000000000001), bits)
+            if float_order == "ieee":
+                cat = np.where(valid & nan, 1, cat).astype(np.int8)
+        key = np.where(bits & S, ~bits & full, bits | S)
+        if descending:
+            key = ~key & full
+        return key.astype(np.uint64), cat
+    if pa.types.is_boolean(t):
+        v = np.asarray(arr.fill_null(False).to_numpy(zero_copy_only=False)).astype(np.int64)
+        key = (v.astype(np.int64) + (1 << 31)).astype(np.uint64)
+        full = np.uint64(0xFFFFFFFF)
+    else:
+        storage = arr
+        if pa.types.is_temporal(t):
+            storage = arr.view(pa.int64() if t.bit_width == 64 else pa.int32())
+        v = np.asarray(storage.fill_null(0).to_numpy(zero_copy_only=False))
+        if v.dtype == np.uint64:
+            key, full = v.astype(np.uint64), np.uint64(0xFFFFFFFFFFFFFFFF)
+        elif v.dtype == np.int64:
+            key, full = v.view(np.uint64) ^ np.uint64(1 << 63), np.uint64(0xFFFFFFFFFFFFFFFF)
+        elif v.dtype == np.uint32:
+            key, full = v.astype(np.uint64), np.uint64(0xFFFFFFFF)
+        else:  # narrow integers widen to int32
+            key = (v.astype(np.int64) + (1 << 31)).astype(np.uint64)
+            full = np.uint64(0xFFFFFFFF)
+    if descending:
+        key = ~key & full
+    return key, cat
+
+
+def np_argsort(arr, descending=False, null_placement="at_end", float_order="ieee"):
+    key, cat = _keys_and_categories(arr, descending, float_order)
+    order = np.argsort(key, kind="stable")
+    vals = order[cat[order] == 0]
+    nans = np.nonzero(cat == 1)[0]
+    nulls = np.nonzero(cat == 2)[0]
+    parts = [nulls, nans, vals] if null_placement == "at_start" else [vals, nans, nulls]
+    return np.concatenate(parts).astype(np.uint32)
+
+
+def np_lexsort(arrays, descending=None, null_placement="at_end", float_order="ieee"):
+    """Multi-key order from the definition: per key a (category, key) pair, compared lexicographically
+    over the keys, ties broken by row number."""
+    K = len(arrays)
+    desc = list(descending) if descending is not None else [False] * K
+    place = [null_placement] * K if isinstance(null_placement, str) else list(null_placement)
+    order = [float_order] * K if isinstance(float_order, str) else list(float_order)
+    cols = []
+    for a, d, p, f in zip(arrays, desc, place, order):
+        key, cat = _keys_and_categories(a, d, f)
+        rank = np.where(cat == 0, 2, np.where(cat == 1, 1, 0)) if p == "at_start" else cat
+        key = np.where(cat == 0, key, np.uint64(0))
+        cols.append((rank.astype(np.int64), key))
+    # np.lexsort sorts by the last key first; give it (least significant ... most significant).
+    seq = []
+    for rank, key in reversed(cols):
+        seq.extend([key, rank])
+    n = len(arrays[0])
+    if n == 0:
+        return np.empty(0, np.uint32)
+    return np.lexsort(seq).astype(np.uint32)

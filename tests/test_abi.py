@@ -1,0 +1,139 @@
+"""The C-ABI library without a GPU: it loads, exports every symbol include/*.h declares, and keeps the
+reference's return-code and error conventions for calls that fail before touching the device."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from conftest import ROOT
+
+LIB = os.path.join(ROOT, "arrowmetal_b200", "lib", "libArrowMetalC.so")
+
+
+def declared_symbols():
+    names = set()
+    for h in os.listdir(os.path.join(ROOT, "include")):
+        if not h.endswith(".h"):
+            continue
+        text = open(os.path.join(ROOT, "include", h)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names |= set(re.findall(r"\b(am_[a-z0-9_]+)\s*\(", text))
+    return names
+
+
+@pytest.fixture(scope="module")
+def lib():
+    assert os.path.exists(LIB), "build the library first (make -C arrowmetal_b200/csrc)"
+    return ctypes.CDLL(LIB)
+
+
+def test_exports_every_declared_symbol(lib):
+    names = declared_symbols()
+    assert len(names) >= 50
+    missing = [n for n in sorted(names) if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_exports_nothing_else():
+    out = os.popen(f"nm -D --defined-only {LIB}").read().split("\n")
+    exported = {l.split()[-1] for l in out if l.strip()}
+    extra = {e for e in exported if not e.startswith("am_")}
+    assert not extra, sorted(extra)[:20]
+    assert exported <= declared_symbols() | extra
+
+
+def test_reference_binding_sort_symbols_present(lib):
+    # The sort-path symbols ArrowMetal's Python binding binds at import
+    # (python/arrowmetal/__init__.py:80-118, :1219-1226, :3793-3794, :5684-5685).
+    for n in ["am_version", "am_device_name", "am_last_error", "am_format", "am_compute_format", "am_length",
+              "am_null_count", "am_release", "am_import", "am_import_chunks", "am_import_chunks_supported",
+              "am_set_import_threads", "am_get_import_threads", "am_export", "am_take", "am_slice", "am_argsort",
+              "am_sort", "am_top_k", "am_lexsort", "am_lexsort_ex", "am_lexsort_ex2", "am_argsort_ex",
+              "am_argsort_ex2", "am_sort_ex", "am_sort_ex2", "am_top_k_ex", "am_batch_begin", "am_batch_end",
+              "am_plan_source_create", "am_plan_run", "am_plan_column", "am_plan_result_release",
+              "am_router_set_mode", "am_router_get_mode"]:
+        assert hasattr(lib, n), n
+
+
+def test_version_and_router(lib):
+    lib.am_version.restype = ctypes.c_char_p
+    assert lib.am_version() == b"0.6.1"
+    assert lib.am_router_set_mode(1) == 0
+    assert lib.am_router_get_mode() == 1
+    assert lib.am_router_set_mode(7) == 2          # unknown mode (include/arrowmetal.h:1799)
+    assert lib.am_router_set_mode(0) == 0
+
+
+def test_null_handles_are_invalid_arguments(lib):
+    P = ctypes.c_void_p
+    out = P()
+    lib.am_length.restype = ctypes.c_int64
+    lib.am_length.argtypes = [P]
+    assert lib.am_length(None) == -1
+    lib.am_argsort.argtypes = [P, ctypes.c_int, ctypes.POINTER(P)]
+    assert lib.am_argsort(None, 0, ctypes.byref(out)) == 2
+    lib.am_take.argtypes = [P, P, ctypes.POINTER(P)]
+    assert lib.am_take(None, None, ctypes.byref(out)) == 2
+    lib.am_import.argtypes = [P, P, ctypes.POINTER(P)]
+    assert lib.am_import(None, None, ctypes.byref(out)) == 2
+    lib.am_lexsort.argtypes = [P, P, ctypes.c_int64, ctypes.POINTER(P)]
+    assert lib.am_lexsort(None, None, 0, ctypes.byref(out)) == 2
+    lib.am_plan_run.argtypes = [ctypes.c_char_p, P, ctypes.c_int64, ctypes.c_int, ctypes.POINTER(P)]
+    assert lib.am_plan_run(None, None, 0, 0, ctypes.byref(out)) == 2
+    lib.am_release.argtypes = [P]
+    lib.am_release(None)   # a no-op, as in the reference
+
+
+def test_plan_errors_without_a_device(lib):
+    lib.am_plan_explain.restype = ctypes.c_char_p
+    lib.am_plan_explain.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int]
+    lib.am_last_error.restype = ctypes.c_char_p
+    assert lib.am_plan_explain(b'{"op": "scan", ', None, 0, 0) is None
+    assert b"JSON" in lib.am_last_error()
+    assert lib.am_plan_explain(b'{"op": "join", "input": {"op": "scan", "source": "t"}}', None, 0, 0) is None
+    assert b"not supported" in lib.am_last_error()
+    assert lib.am_plan_explain(b'{"op": "scan", "source": "t"}', None, 0, 0) is None
+    assert b"unknown source" in lib.am_last_error()
+
+
+def test_import_chunks_refuses_unsupported_types(lib):
+    import pyarrow as pa
+    from arrowmetal_b200 import _ArrowSchema
+    s = _ArrowSchema()
+    pa.array(["a"]).type._export_to_c(ctypes.addressof(s))
+    lib.am_import_chunks_supported.argtypes = [ctypes.c_void_p]
+    assert lib.am_import_chunks_supported(ctypes.addressof(s)) == 0
+    out = ctypes.c_void_p()
+    lib.am_import_chunks.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_void_p)]
+    assert lib.am_import_chunks(ctypes.addressof(s), None, 0, ctypes.byref(out)) == 3
+    ctypes.CFUNCTYPE(None, ctypes.c_void_p)(s.release)(ctypes.addressof(s))
+
+
+def test_binding_validates_options_before_the_device():
+    import arrowmetal_b200 as am
+    with pytest.raises(am.ArrowMetalError, match="null_placement"):
+        am._index_of(am.NULL_PLACEMENT, "middle", "null_placement")
+    with pytest.raises(am.ArrowMetalError, match="float_order"):
+        am._index_of(am.FLOAT_ORDERS, "lexicographic", "float_order")
+    with pytest.raises(am.ArrowMetalError, match="lexsort needs"):
+        am.lexsort_indices([])
+
+
+def test_no_device_fails_loudly():
+    import arrowmetal_b200 as am
+    if os.environ.get("CUDA_VISIBLE_DEVICES", None) == "" or not _has_gpu():
+        name = am.device_name()
+        assert name.startswith("unavailable")
+        with pytest.raises(am.ArrowMetalError, match="CUDA"):
+            am.MetalArray.from_arrow([1, 2, 3])
+    else:
+        pytest.skip("a GPU is present")
+
+
+def _has_gpu():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False

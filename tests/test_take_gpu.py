@@ -1,0 +1,103 @@
+"""Take on the GPU: the golden fixtures (pyarrow's take), every index type, null indices, boolean and
+narrow columns, slices, the multi-column form, and the out-of-range error."""
+import numpy as np
+import pyarrow as pa
+import pyarrow.compute as pc
+import pytest
+
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+
+def test_golden_take(am):
+    g = golden()
+    n = 0
+    for c in g.cases:
+        if c["kind"] != "take":
+            continue
+        src = am.MetalArray.from_arrow(g.array(c["array"], c["type"]))
+        idx = am.MetalArray.from_arrow(g.array(c["index"], c["index_type"]))
+        got = src.take(idx).to_arrow()
+        valid = np.asarray(got.is_valid().to_numpy(zero_copy_only=False))
+        assert np.array_equal(valid, g[c["index"] + "_expect_valid"]), c
+        vals = got.fill_null(0).to_numpy(zero_copy_only=False)
+        want = g[c["index"] + "_expect_values"]
+        assert np.array_equal(vals.view(want.dtype)[valid], want[valid]), c
+        assert got.null_count == int((~valid).sum())
+        n += 1
+    assert n > 30
+
+
+@pytest.mark.parametrize("t", [pa.int8(), pa.uint16(), pa.int32(), pa.float32(), pa.int64(), pa.float64(),
+                               pa.bool_(), pa.timestamp("us"), pa.date32()])
+def test_take_types_match_pyarrow(am, t):
+    rng = np.random.default_rng(1)
+    n = 100_003
+    if t == pa.bool_():
+        src = pa.array(rng.random(n) < 0.5, mask=rng.random(n) < 0.1)
+    elif pa.types.is_floating(t):
+        src = pa.array(rng.normal(size=n), mask=rng.random(n) < 0.1).cast(t)
+    elif pa.types.is_temporal(t):
+        src = pa.array(rng.integers(0, 10**6, n), mask=rng.random(n) < 0.1).cast(t)
+    else:
+        info = np.iinfo(t.to_pandas_dtype())
+        src = pa.array(rng.integers(info.min, info.max, n, dtype=t.to_pandas_dtype()), mask=rng.random(n) < 0.1)
+    m = am.MetalArray.from_arrow(src)
+    for it in (pa.uint32(), pa.int32(), pa.int64()):
+        for k in (0, 1, 127, 128, 129, 100_003):
+            idx = pa.array(rng.integers(0, n, k), mask=rng.random(k) < 0.05).cast(it)
+            got = m.take(idx).to_arrow()
+            want = pc.take(src, idx)
+            assert got.type == src.type
+            assert got.equals(want), (t, it, k)
+
+
+def test_take_through_argsort_is_sorted_copy(am):
+    rng = np.random.default_rng(2)
+    src = pa.array(rng.integers(-10**9, 10**9, 500_000), mask=rng.random(500_000) < 0.1)
+    m = am.MetalArray.from_arrow(src)
+    got = m.take(m.argsort()).to_arrow()
+    assert got.equals(pc.take(src, pc.array_sort_indices(src)))
+
+
+def test_take_columns_one_index_read(am):
+    rng = np.random.default_rng(3)
+    n = 300_001
+    cols = [pa.array(rng.integers(0, 2**40, n), mask=rng.random(n) < 0.1), pa.array(rng.normal(size=n)),
+            pa.array(rng.integers(-2**31, 2**31 - 1, n, dtype=np.int32)), pa.array(rng.random(n) < 0.5)]
+    idx = pa.array(rng.permutation(n).astype(np.uint32))
+    outs = am.take_columns([am.MetalArray.from_arrow(c) for c in cols], idx)
+    for c, o in zip(cols, outs):
+        assert o.to_arrow().equals(pc.take(c, idx))
+
+
+def test_take_from_slices(am):
+    rng = np.random.default_rng(4)
+    src = pa.array(rng.integers(0, 100, 10_000), mask=rng.random(10_000) < 0.3)
+    m = am.MetalArray.from_arrow(src).slice(13, 5000)
+    idx = pa.array(rng.integers(0, 5000, 777), type=pa.int64())
+    assert m.take(idx).to_arrow().equals(pc.take(src.slice(13, 5000), idx))
+    bsrc = pa.array(rng.random(10_000) < 0.5)
+    bm = am.MetalArray.from_arrow(bsrc).slice(3, 9000)
+    assert bm.take(idx).to_arrow().equals(pc.take(bsrc.slice(3, 9000), idx))
+
+
+def test_take_out_of_range_raises(am):
+    # IndexTypeTests.swift:109 and Take.swift:70-72: the error surfaces from the call.
+    m = am.MetalArray.from_arrow(pa.array([1, 2, 3]))
+    with pytest.raises(am.ArrowMetalError, match="out of range"):
+        m.take(pa.array([0, 3], type=pa.int64()))
+    with pytest.raises(am.ArrowMetalError, match="out of range"):
+        m.take(pa.array([-1], type=pa.int32()))
+    # The library stays usable afterwards.
+    assert m.take(pa.array([2, 0], type=pa.uint32())).to_arrow().to_pylist() == [3, 1]
+
+
+def test_take_error_deferred_to_batch_end(am):
+    # BatchTests.swift:61: inside a batch the range error surfaces at the batch's end.
+    m = am.MetalArray.from_arrow(pa.array([1, 2, 3]))
+    with pytest.raises(am.ArrowMetalError, match="out of range"):
+        with am.batch():
+            m.take(pa.array([5], type=pa.int64()))
+    assert m.take(pa.array([1], type=pa.int64())).to_arrow().to_pylist() == [2]
