@@ -19,8 +19,6 @@
 // instead of being written by an iota kernel. A lexsort carries the row ids through every pass, so
 // the reference's "take the next key column, argsort, compose" becomes one gather of the next key
 // inside its first pass.
-#include <cuda_fp16.h>
-
 #include <algorithm>
 #include <cstring>
 
@@ -88,6 +86,20 @@ __device__ __forceinline__ uint64_t key_f64_bits(uint64_t b, const ColView& c, i
   return c.desc ? ~k : k;
 }
 
+// Binary16 to binary32 bits, exactly and bit for bit: sign kept, exponent rebiased, subnormals
+// normalised, a NaN's payload shifted into the wider mantissa. (A hardware conversion returns one
+// canonical NaN, which would lose the sign totalOrder sorts -NaN by.)
+__device__ __forceinline__ uint32_t f16_to_f32_bits(uint32_t h) {
+  const uint32_t sign = (h & 0x8000u) << 16, exp = (h >> 10) & 0x1Fu, man = h & 0x3FFu;
+  if (exp == 0x1Fu) return sign | 0x7F800000u | (man << 13);
+  if (exp == 0u) {
+    if (man == 0u) return sign;
+    const uint32_t shift = uint32_t(__clz(int(man))) - 21u;   // brings the leading 1 to bit 10
+    return sign | ((113u - shift) << 23) | (((man << shift) & 0x3FFu) << 13);
+  }
+  return sign | ((exp + 112u) << 23) | (man << 13);
+}
+
 // Key of row `row` of column `c`; `cat` is 0 for a value, 1 for a NaN block row, 2 for a null.
 template <typename KeyT> __device__ __forceinline__ KeyT encode_key(const ColView& c, uint64_t row, int& cat);
 
@@ -106,10 +118,8 @@ template <> __device__ __forceinline__ uint32_t encode_key<uint32_t>(const ColVi
       uint32_t k = static_cast<const uint32_t*>(c.values)[row];
       return c.desc ? ~k : k;
     }
-    case PT_F16: {
-      const float f = __half2float(__ushort_as_half(static_cast<const unsigned short*>(c.values)[row]));
-      return key_f32_bits(__float_as_uint(f), c, cat);
-    }
+    case PT_F16:
+      return key_f32_bits(f16_to_f32_bits(static_cast<const unsigned short*>(c.values)[row]), c, cat);
     default:  // PT_F32
       return key_f32_bits(static_cast<const uint32_t*>(c.values)[row], c, cat);
   }
@@ -464,10 +474,8 @@ struct PassShared {
   uint32_t scan_total;
   uint32_t tile;
   uint16_t dig[TILE];
-  union {
-    KeyT keys[TILE];
-    uint32_t ids[TILE];
-  } stage;
+  KeyT keys[TILE];
+  uint32_t ids[TILE];
 };
 
 template <typename KeyT, int THREADS, int ITEMS>
@@ -582,42 +590,54 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
     }
     __syncthreads();
 
-    // ---- stage keys and digits at their tile-local sorted slot
+    // ---- stage keys, ids and digits at their tile-local sorted slot (frees the registers)
 #pragma unroll
     for (int i = 0; i < ITEMS; i++) {
       const uint32_t d = dg[i] & 0xFFFFu;
       if (d != INVALID_DIGIT) {
         const uint32_t pos = sm.local[d] + sm.whist[warp][d] + (dg[i] >> 16);
-        sm.stage.keys[pos] = key[i];
+        sm.keys[pos] = key[i];
+        sm.ids[pos] = id[i];
         sm.dig[pos] = uint16_t(d);
       }
     }
 
-    // ---- decoupled look-back, one thread per digit, bounded in time
+    // ---- decoupled look-back, one thread per digit, LOOKBACK_WINDOW predecessors per round trip:
+    // the window's loads are independent, so the inclusive-prefix frontier moves a whole window of
+    // tiles per L2 round trip instead of one. Every wait is bounded in time.
     for (int b = threadIdx.x; b < NBINS; b += THREADS) {
       uint32_t excl = 0;
       if (tile > 0) {
         int64_t j = int64_t(tile) - 1;
-        for (;;) {
-          const uint64_t* p = pa.status + uint64_t(j) * NBINS + b;
-          uint64_t s = ld_relaxed_u64(p);
-          if (uint32_t(s >> 34) != epoch || ((s >> 32) & 3u) == 0u) {
-            const uint64_t t0 = globaltimer_ns();
-            uint32_t polls = 0;
-            for (;;) {
-              s = ld_relaxed_u64(p);
-              if (uint32_t(s >> 34) == epoch && ((s >> 32) & 3u) != 0u) break;
-              if (++polls > 4) __nanosleep(64);
-              if ((polls & 63u) == 0u && globaltimer_ns() - t0 > LOOKBACK_TIMEOUT_NS) {
-                atomicOr(pa.err, ERR_LOOKBACK_TIMEOUT);
-                s = pack_status(epoch, ST_INCL, 0);
-                break;
+        bool done = false;
+        while (!done) {
+          uint64_t st[LOOKBACK_WINDOW];
+#pragma unroll
+          for (int i = 0; i < LOOKBACK_WINDOW; i++)
+            st[i] = (j - i >= 0) ? ld_relaxed_u64(pa.status + uint64_t(j - i) * NBINS + b) : pack_status(epoch, ST_INCL, 0);
+#pragma unroll
+          for (int i = 0; i < LOOKBACK_WINDOW; i++) {
+            uint64_t s = st[i];
+            if (uint32_t(s >> 34) != epoch || ((s >> 32) & 3u) == 0u) {
+              const uint64_t* p = pa.status + uint64_t(j - i) * NBINS + b;
+              const uint64_t t0 = globaltimer_ns();
+              uint32_t polls = 0;
+              for (;;) {
+                s = ld_relaxed_u64(p);
+                if (uint32_t(s >> 34) == epoch && ((s >> 32) & 3u) != 0u) break;
+                if (++polls > 8) __nanosleep(32);
+                if ((polls & 63u) == 0u && globaltimer_ns() - t0 > LOOKBACK_TIMEOUT_NS) {
+                  atomicOr(pa.err, ERR_LOOKBACK_TIMEOUT);
+                  s = pack_status(epoch, ST_INCL, 0);
+                  break;
+                }
               }
             }
+            excl += uint32_t(s);
+            if (((s >> 32) & 3u) == ST_INCL) { done = true; break; }
           }
-          excl += uint32_t(s);
-          if (((s >> 32) & 3u) == ST_INCL || j == 0) break;
-          j--;
+          j -= LOOKBACK_WINDOW;
+          if (j < 0) done = true;
         }
         st_relaxed_u64(pa.status + uint64_t(tile) * NBINS + b, pack_status(epoch, ST_INCL, excl + sm.cnt[b]));
       }
@@ -626,24 +646,16 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
     __syncthreads();
 
     const uint32_t tile_n = uint32_t((count - tile_base) < uint64_t(TILE) ? (count - tile_base) : uint64_t(TILE));
-    // ---- keys out
+    // ---- keys out, then ids out; consecutive threads write consecutive addresses of a digit run
     if (keys_out) {
       for (uint32_t j = threadIdx.x; j < tile_n; j += THREADS) {
         const uint32_t d = sm.dig[j];
-        if (d < RADIX) keys_out[sm.gdelta[d] + j] = sm.stage.keys[j];
+        if (d < RADIX) keys_out[sm.gdelta[d] + j] = sm.keys[j];
       }
     }
-    __syncthreads();
-    // ---- ids out (staged the same way, over the keys' shared memory)
-#pragma unroll
-    for (int i = 0; i < ITEMS; i++) {
-      const uint32_t d = dg[i] & 0xFFFFu;
-      if (d != INVALID_DIGIT) sm.stage.ids[sm.local[d] + sm.whist[warp][d] + (dg[i] >> 16)] = id[i];
-    }
-    __syncthreads();
     for (uint32_t j = threadIdx.x; j < tile_n; j += THREADS) {
       const uint32_t d = sm.dig[j];
-      const uint32_t v = sm.stage.ids[j];
+      const uint32_t v = sm.ids[j];
       uint32_t dst = sm.gdelta[d] + j;
       if (d >= RADIX || !ids_out) {
         if (d < RADIX) dst += sm.desc.value_base;

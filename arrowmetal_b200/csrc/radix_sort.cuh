@@ -25,6 +25,7 @@ constexpr uint32_t PF_WIDE_OUT = 8;        // the output index array is uint64
 // Look-back status word: epoch (30 bits) | flag (2 bits) | count (32 bits).
 constexpr uint32_t ST_AGG = 1, ST_INCL = 2;
 constexpr uint64_t LOOKBACK_TIMEOUT_NS = 1000000000ull;   // 1 s, then the pass reports an error
+constexpr int LOOKBACK_WINDOW = 16;                       // predecessor tiles read per round trip
 
 // Device error word bits.
 constexpr uint32_t ERR_LOOKBACK_TIMEOUT = 1;

@@ -276,7 +276,7 @@ def main():
     h2d = sum(c.nbytes for c in (key, p1, p2)) + (n + 7) // 8
     e2e_times = []
     d2h = 0
-    for i in range(args.e2e_steps + 1):
+    for i in range(args.e2e_steps + 1 if args.e2e_steps > 0 else 0):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         hc = {k: am.MetalArray.from_arrow(v) for k, v in cols.items()}
@@ -288,7 +288,7 @@ def main():
             e2e_times.append(dt)
         d2h = sum(sum(b.size for b in r.buffers() if b is not None) for r in res.values())
         del hc, s2, out, res
-    e2e_ms = 1e3 * statistics.median(e2e_times)
+    e2e_ms = 1e3 * statistics.median(e2e_times) if e2e_times else float("nan")
     if dist:
         t = torch.tensor([e2e_ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)

@@ -39,7 +39,8 @@ def test_take_types_match_pyarrow(am, t):
     elif pa.types.is_floating(t):
         src = pa.array(rng.normal(size=n), mask=rng.random(n) < 0.1).cast(t)
     elif pa.types.is_temporal(t):
-        src = pa.array(rng.integers(0, 10**6, n), mask=rng.random(n) < 0.1).cast(t)
+        storage = pa.int32() if t.bit_width == 32 else pa.int64()
+        src = pa.array(rng.integers(0, 10**6, n), mask=rng.random(n) < 0.1).cast(storage).view(t)
     else:
         info = np.iinfo(t.to_pandas_dtype())
         src = pa.array(rng.integers(info.min, info.max, n, dtype=t.to_pandas_dtype()), mask=rng.random(n) < 0.1)
