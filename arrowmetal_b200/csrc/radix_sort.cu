@@ -25,6 +25,7 @@
 #include "am_internal.h"
 #include "radix_sort.cuh"
 
+
 namespace am {
 namespace rs {
 
@@ -47,6 +48,37 @@ __device__ __forceinline__ void st_relaxed_u64(uint64_t* p, uint64_t v) {
 __device__ __forceinline__ uint64_t pack_status(uint32_t epoch, uint32_t flag, uint32_t count) {
   return (uint64_t(epoch) << 34) | (uint64_t(flag) << 32) | uint64_t(count);
 }
+__device__ __forceinline__ uint32_t ld_relaxed_u32(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed_u32(uint32_t* p, uint32_t v) {
+  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Look-back status words. 32-bit: flag (2 bits) | count (30 bits), zeroed before every pass; used when a
+// pass has fewer than 2^30 rows, and twice as many predecessors fit a look-back window. 64-bit: the pass
+// epoch (30 bits) | flag | count (32 bits), never cleared: a word of an older pass has another epoch.
+template <typename S> struct Status;
+template <> struct Status<uint32_t> {
+  static constexpr int WINDOW = 32;
+  static __device__ __forceinline__ uint32_t make(uint32_t, uint32_t flag, uint32_t count) { return (flag << 30) | count; }
+  static __device__ __forceinline__ bool ready(uint32_t s, uint32_t) { return (s >> 30) != 0u; }
+  static __device__ __forceinline__ uint32_t flag(uint32_t s) { return s >> 30; }
+  static __device__ __forceinline__ uint32_t count(uint32_t s) { return s & 0x3FFFFFFFu; }
+  static __device__ __forceinline__ uint32_t load(const uint32_t* p) { return ld_relaxed_u32(p); }
+  static __device__ __forceinline__ void store(uint32_t* p, uint32_t v) { st_relaxed_u32(p, v); }
+};
+template <> struct Status<uint64_t> {
+  static constexpr int WINDOW = 16;
+  static __device__ __forceinline__ uint64_t make(uint32_t e, uint32_t flag, uint32_t count) { return pack_status(e, flag, count); }
+  static __device__ __forceinline__ bool ready(uint64_t s, uint32_t e) { return uint32_t(s >> 34) == e && ((s >> 32) & 3u) != 0u; }
+  static __device__ __forceinline__ uint32_t flag(uint64_t s) { return uint32_t(s >> 32) & 3u; }
+  static __device__ __forceinline__ uint32_t count(uint64_t s) { return uint32_t(s); }
+  static __device__ __forceinline__ uint64_t load(const uint64_t* p) { return ld_relaxed_u64(p); }
+  static __device__ __forceinline__ void store(uint64_t* p, uint64_t v) { st_relaxed_u64(p, v); }
+};
 
 __device__ __forceinline__ bool bit_at(const uint8_t* p, int64_t i) {
   return (p[i >> 3] >> (i & 7)) & 1;
@@ -100,40 +132,86 @@ __device__ __forceinline__ uint32_t f16_to_f32_bits(uint32_t h) {
   return sign | ((exp + 112u) << 23) | (man << 13);
 }
 
-// Key of row `row` of column `c`; `cat` is 0 for a value, 1 for a NaN block row, 2 for a null.
-template <typename KeyT> __device__ __forceinline__ KeyT encode_key(const ColView& c, uint64_t row, int& cat);
-
-template <> __device__ __forceinline__ uint32_t encode_key<uint32_t>(const ColView& c, uint64_t row, int& cat) {
-  cat = 0;
-  if (c.valid && !bit_at(c.valid, c.valid_off + int64_t(row))) { cat = 2; return 0u; }
-  int32_t v;
+// Raw bits of row `row`, widened to the key width: narrow integers sign- or zero-extended to 32 bits
+// (the reference widens them to int32, Sort.swift:220-221), float16 as its 16 bits, boolean as its bit.
+template <typename KeyT> __device__ __forceinline__ KeyT load_raw(const ColView& c, uint64_t row);
+template <> __device__ __forceinline__ uint32_t load_raw<uint32_t>(const ColView& c, uint64_t row) {
   switch (c.pt) {
-    case PT_BOOL: v = bit_at(static_cast<const uint8_t*>(c.values), c.bool_off + int64_t(row)) ? 1 : 0; break;
-    case PT_I8: v = static_cast<const int8_t*>(c.values)[row]; break;
-    case PT_U8: v = static_cast<const uint8_t*>(c.values)[row]; break;
-    case PT_I16: v = static_cast<const int16_t*>(c.values)[row]; break;
-    case PT_U16: v = static_cast<const uint16_t*>(c.values)[row]; break;
-    case PT_I32: v = static_cast<const int32_t*>(c.values)[row]; break;
-    case PT_U32: {
-      uint32_t k = static_cast<const uint32_t*>(c.values)[row];
-      return c.desc ? ~k : k;
-    }
-    case PT_F16:
-      return key_f32_bits(f16_to_f32_bits(static_cast<const unsigned short*>(c.values)[row]), c, cat);
-    default:  // PT_F32
-      return key_f32_bits(static_cast<const uint32_t*>(c.values)[row], c, cat);
+    case PT_BOOL: return bit_at(static_cast<const uint8_t*>(c.values), c.bool_off + int64_t(row)) ? 1u : 0u;
+    case PT_I8: return uint32_t(int32_t(static_cast<const int8_t*>(c.values)[row]));
+    case PT_U8: return static_cast<const uint8_t*>(c.values)[row];
+    case PT_I16: return uint32_t(int32_t(static_cast<const int16_t*>(c.values)[row]));
+    case PT_U16: case PT_F16: return static_cast<const uint16_t*>(c.values)[row];
+    default: return static_cast<const uint32_t*>(c.values)[row];
   }
-  const uint32_t k = uint32_t(v) ^ 0x80000000u;
+}
+template <> __device__ __forceinline__ uint64_t load_raw<uint64_t>(const ColView& c, uint64_t row) {
+  return static_cast<const uint64_t*>(c.values)[row];
+}
+
+// Loads the raw bits of ITEMS rows with the type dispatch outside the loop, so the loads are issued
+// back to back. ok bit i: row i exists.
+template <typename KeyT, int ITEMS>
+__device__ __forceinline__ void load_raw_rows(const ColView& c, const uint32_t (&row)[ITEMS], uint32_t ok, KeyT (&raw)[ITEMS]) {
+  if constexpr (sizeof(KeyT) == 8) {
+    const uint64_t* v = static_cast<const uint64_t*>(c.values);
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++) raw[i] = ((ok >> i) & 1u) ? v[row[i]] : 0ull;
+  } else {
+    switch (c.pt) {
+      case PT_I32: case PT_U32: case PT_F32: {
+        const uint32_t* v = static_cast<const uint32_t*>(c.values);
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++) raw[i] = ((ok >> i) & 1u) ? v[row[i]] : 0u;
+        break;
+      }
+      default:
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++) raw[i] = ((ok >> i) & 1u) ? load_raw<uint32_t>(c, row[i]) : 0u;
+    }
+  }
+}
+
+// Key of raw bits `raw` (valid or null); `cat` is 0 for a value, 1 for a NaN block row, 2 for a null.
+template <typename KeyT> __device__ __forceinline__ KeyT key_from_raw(const ColView& c, KeyT raw, bool valid, int& cat);
+
+template <> __device__ __forceinline__ uint32_t key_from_raw<uint32_t>(const ColView& c, uint32_t raw, bool valid, int& cat) {
+  cat = 0;
+  if (!valid) { cat = 2; return 0u; }
+  uint32_t k;
+  switch (c.pt) {
+    case PT_U32: k = raw; break;
+    case PT_F16: return key_f32_bits(f16_to_f32_bits(raw), c, cat);
+    case PT_F32: return key_f32_bits(raw, c, cat);
+    default: k = raw ^ 0x80000000u;   // int32 and the narrow types widened to it
+  }
   return c.desc ? ~k : k;
 }
 
-template <> __device__ __forceinline__ uint64_t encode_key<uint64_t>(const ColView& c, uint64_t row, int& cat) {
+template <> __device__ __forceinline__ uint64_t key_from_raw<uint64_t>(const ColView& c, uint64_t raw, bool valid, int& cat) {
   cat = 0;
-  if (c.valid && !bit_at(c.valid, c.valid_off + int64_t(row))) { cat = 2; return 0ull; }
-  const uint64_t b = static_cast<const uint64_t*>(c.values)[row];
-  if (c.pt == PT_F64) return key_f64_bits(b, c, cat);
-  const uint64_t k = (c.pt == PT_I64) ? (b ^ 0x8000000000000000ull) : b;
+  if (!valid) { cat = 2; return 0ull; }
+  if (c.pt == PT_F64) return key_f64_bits(raw, c, cat);
+  const uint64_t k = (c.pt == PT_I64) ? (raw ^ 0x8000000000000000ull) : raw;
   return c.desc ? ~k : k;
+}
+
+// Keys of ITEMS rows: all loads first (values and validity bytes), then the arithmetic.
+template <typename KeyT, int ITEMS>
+__device__ __forceinline__ void encode_rows(const ColView& c, const uint32_t (&row)[ITEMS], uint32_t ok, KeyT (&key)[ITEMS],
+                                            int (&cat)[ITEMS]) {
+  KeyT raw[ITEMS];
+  uint32_t vb[ITEMS];
+  load_raw_rows<KeyT, ITEMS>(c, row, ok, raw);
+  if (c.valid) {
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++) vb[i] = ((ok >> i) & 1u) ? c.valid[(c.valid_off + int64_t(row[i])) >> 3] : 0u;
+  }
+#pragma unroll
+  for (int i = 0; i < ITEMS; i++) {
+    const bool valid = !c.valid || ((vb[i] >> ((c.valid_off + int64_t(row[i])) & 7)) & 1u);
+    key[i] = key_from_raw<KeyT>(c, raw[i], valid, cat[i]);
+  }
 }
 
 template <typename T> __device__ __forceinline__ T warp_or(T v);
@@ -185,29 +263,34 @@ __global__ void __launch_bounds__(THREADS) key_histogram_kernel(const __grid_con
 
   for (uint64_t base = uint64_t(blockIdx.x) * CHUNK; base < n; base += uint64_t(gridDim.x) * CHUNK) {
     KeyT k[ITEMS];
+    int cat[ITEMS];
+    uint32_t row[ITEMS];
+    uint32_t ok = 0;
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++) {
+      const uint64_t g = base + uint64_t(warp) * (ITEMS * 32) + uint64_t(i) * 32 + lane;
+      row[i] = uint32_t(g);
+      if (g < n) ok |= 1u << i;
+    }
+    encode_rows<KeyT, ITEMS>(col, row, ok, k, cat);
     uint32_t valid_mask = 0;
     KeyT o = 0, a = KeyT(~KeyT(0));
     uint32_t nv = 0;
 #pragma unroll
     for (int i = 0; i < ITEMS; i++) {
-      const uint64_t g = base + uint64_t(warp) * (ITEMS * 32) + uint64_t(i) * 32 + lane;
-      k[i] = 0;
-      if (g < n) {
-        int cat;
-        const KeyT kk = encode_key<KeyT>(col, g, cat);
-        if (cat == 0) {
-          k[i] = kk;
-          valid_mask |= 1u << i;
-          o |= kk;
-          a &= kk;
-          nv++;
-          vmax = kk > vmax ? kk : vmax;
-          vmin_inv = KeyT(~kk) > vmin_inv ? KeyT(~kk) : vmin_inv;
-        } else if (cat == 1) {
-          n_nan++;
-        } else {
-          n_null++;
-        }
+      if (!((ok >> i) & 1u)) continue;
+      if (cat[i] == 0) {
+        const KeyT kk = k[i];
+        valid_mask |= 1u << i;
+        o |= kk;
+        a &= kk;
+        nv++;
+        vmax = kk > vmax ? kk : vmax;
+        vmin_inv = KeyT(~kk) > vmin_inv ? KeyT(~kk) : vmin_inv;
+      } else if (cat[i] == 1) {
+        n_nan++;
+      } else {
+        n_null++;
       }
     }
     n_val += nv;
@@ -256,17 +339,21 @@ __global__ void __launch_bounds__(THREADS) key_histogram_kernel(const __grid_con
 // Kernel 2: the plan. One block decides, from the histograms alone, which digit passes run, where
 // each pass reads and writes, and every pass's per-digit global base; the passes read it from HBM.
 
+// Exclusive scan of 256 values held in shared memory; the first 256 threads of the block take part in
+// the arithmetic and every thread in the barriers.
 __device__ void block_exclusive_scan_256(const uint32_t* in, uint32_t* out, uint32_t* total, uint32_t* s_warp) {
-  // 256 threads, one value each.
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  uint32_t v = in[t];
-  uint32_t x = v;
+  uint32_t v = 0, x = 0;
+  if (t < 256) {
+    v = in[t];
+    x = v;
 #pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += y;
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[warp] = x;
   }
-  if (lane == 31) s_warp[warp] = x;
   __syncthreads();
   if (warp == 0) {
     uint32_t w = lane < 8 ? s_warp[lane] : 0u;
@@ -280,7 +367,7 @@ __device__ void block_exclusive_scan_256(const uint32_t* in, uint32_t* out, uint
     if (lane == 7) *total = z;
   }
   __syncthreads();
-  out[t] = x - v + s_warp[8 + warp];
+  if (t < 256) out[t] = x - v + s_warp[8 + warp];
   __syncthreads();
 }
 
@@ -402,6 +489,8 @@ __global__ void __launch_bounds__(256) plan_kernel(PlanArgs a, KeyStats* __restr
         p.dst_ids = (ids_src == 0) ? 1 : 0;
       }
       p.value_base = (k == 0 && a.nulls_first[0]) ? (st[0].n_null + st[0].n_nan) : 0u;
+      p.buf_rows = n;         // the ping-pong buffers and the output hold n rows
+      p.out_rows = n;
       ids_src = p.dst_ids;
       keys_src = is_last_of_key ? -1 : p.dst_keys;
     }
@@ -454,12 +543,12 @@ __global__ void __launch_bounds__(256) plan_kernel(PlanArgs a, KeyStats* __restr
 // Tiles of THREADS x ITEMS rows are claimed with an atomic ticket, so a tile only ever waits on tiles
 // that have already started. Rows are held warp-striped (row = tile + warp*ITEMS*32 + i*32 + lane),
 // which makes every load a coalesced warp access and makes "item i before item i+1, lower lane first"
-// the input order; each warp ranks its rows with one __match_any_sync per item against its own
-// per-digit counters in shared memory (the reference's ballot ranking, SortSource.swift:334-386, in
-// one instruction). The tile's per-digit counts go out as look-back aggregates right away, the rows
-// are staged in shared memory at their tile-local sorted slot, the look-back (bounded in time) turns
-// the counts into global offsets, and the rows leave shared memory in order, so consecutive threads
-// write consecutive addresses within every digit run.
+// the input order. The tile's digit counts go out as look-back aggregates before any ranking; each
+// warp then ranks its rows (one ballot per digit bit, the reference's ballot multisplit of
+// SortSource.swift:334-386) and stages them in shared memory at their tile-local sorted slot; the
+// decoupled look-back (a window of predecessors per L2 round trip, bounded in time) turns the counts
+// into global offsets; and the rows leave shared memory in order, so consecutive threads write
+// consecutive addresses within every digit run.
 
 template <typename KeyT, int THREADS, int ITEMS>
 struct PassShared {
@@ -472,22 +561,24 @@ struct PassShared {
   uint32_t gdelta[NBINS];
   uint32_t scan_warp[16];
   uint32_t scan_total;
-  uint32_t tile;
+  uint32_t ticket;
   uint16_t dig[TILE];
   KeyT keys[TILE];
   uint32_t ids[TILE];
 };
 
-template <typename KeyT, int THREADS, int ITEMS>
+template <typename KeyT, typename StatusT, int THREADS, int ITEMS>
 __global__ void __launch_bounds__(THREADS, 2)
 onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant__ ColView col) {
-  static_assert(THREADS == 256, "the digit scan assumes one thread per value digit");
+  static_assert(THREADS >= NBINS && THREADS % 32 == 0, "one thread per digit bin");
   static_assert(THREADS * ITEMS <= 65536, "tile-local ranks are 16-bit");
+  using ST = Status<StatusT>;
   using SM = PassShared<KeyT, THREADS, ITEMS>;
   constexpr int TILE = SM::TILE;
   constexpr int WARPS = SM::WARPS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   SM& sm = *reinterpret_cast<SM*>(smem_raw);
+  StatusT* __restrict__ status = static_cast<StatusT*>(pa.status);
 
   {
     const uint32_t* src = reinterpret_cast<const uint32_t*>(pa.desc);
@@ -512,63 +603,62 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
   const uint32_t lt_mask = (1u << lane) - 1u;
 
   for (;;) {
-    if (threadIdx.x == 0) sm.tile = atomicAdd(pa.tile_counter, 1u);
+    if (threadIdx.x == 0) sm.ticket = atomicAdd(pa.tile_counter, 1u);
     for (int b = lane; b < NBINS; b += 32) sm.whist[warp][b] = 0;
     __syncthreads();
-    const uint32_t tile = sm.tile;
+    const uint32_t tile = sm.ticket;
     if (tile >= ntiles) break;
     const uint64_t tile_base = uint64_t(tile) * TILE;
 
-    // ---- load and digit
+    // ---- load and digit: row ids first, then every item's key load back to back
     KeyT key[ITEMS];
     uint32_t id[ITEMS];
     uint32_t dg[ITEMS];
+    const uint64_t wbase = tile_base + uint64_t(warp) * (ITEMS * 32) + lane;
+    uint32_t ok = 0;
 #pragma unroll
-    for (int i = 0; i < ITEMS; i++) {
-      const uint64_t g = tile_base + uint64_t(warp) * (ITEMS * 32) + uint64_t(i) * 32 + lane;
-      key[i] = 0;
-      id[i] = 0;
-      dg[i] = INVALID_DIGIT;
-      if (g < count) {
-        id[i] = ids_in ? ids_in[g] : uint32_t(g);
-        if (flags & PF_CATPASS) {
-          const bool is_null = col.valid && !bit_at(col.valid, col.valid_off + int64_t(id[i]));
-          dg[i] = (is_null != bool(col.nulls_first)) ? 1u : 0u;
-        } else if (flags & PF_ENCODE) {
-          int cat;
-          KeyT k = encode_key<KeyT>(col, id[i], cat);
-          if (cat && (flags & PF_ROUTE)) {
-            dg[i] = (cat == 1) ? uint32_t(NAN_BIN) : uint32_t(NULL_BIN);
-          } else {
-            if (cat) k = kplan.fold_mode ? KeyT(0) : KeyT(cat == 1 ? kplan.fold_nan : kplan.fold_null);
-            key[i] = k;
-            dg[i] = uint32_t(k >> shift) & 255u;
-          }
+    for (int i = 0; i < ITEMS; i++)
+      if (wbase + uint64_t(i) * 32 < count) ok |= 1u << i;
+    if (ids_in) {
+#pragma unroll
+      for (int i = 0; i < ITEMS; i++) id[i] = ((ok >> i) & 1u) ? ids_in[wbase + uint64_t(i) * 32] : 0u;
+    } else {
+#pragma unroll
+      for (int i = 0; i < ITEMS; i++) id[i] = uint32_t(wbase + uint64_t(i) * 32);
+    }
+    if (flags & PF_CATPASS) {
+#pragma unroll
+      for (int i = 0; i < ITEMS; i++) {
+        key[i] = 0;
+        const bool is_null = ((ok >> i) & 1u) && col.valid && !bit_at(col.valid, col.valid_off + int64_t(id[i]));
+        dg[i] = ((ok >> i) & 1u) ? ((is_null != bool(col.nulls_first)) ? 1u : 0u) : INVALID_DIGIT;
+      }
+    } else if (flags & PF_ENCODE) {
+      int cat[ITEMS];
+      encode_rows<KeyT, ITEMS>(col, id, ok, key, cat);
+#pragma unroll
+      for (int i = 0; i < ITEMS; i++) {
+        if (cat[i] && (flags & PF_ROUTE)) {
+          dg[i] = (cat[i] == 1) ? uint32_t(NAN_BIN) : uint32_t(NULL_BIN);
         } else {
-          key[i] = keys_in[g];
+          if (cat[i]) key[i] = kplan.fold_mode ? KeyT(0) : KeyT(cat[i] == 1 ? kplan.fold_nan : kplan.fold_null);
           dg[i] = uint32_t(key[i] >> shift) & 255u;
         }
+        if (!((ok >> i) & 1u)) dg[i] = INVALID_DIGIT;
       }
-    }
-
-    // ---- warp ranking: rank among this warp's rows of the same digit, in input order
+    } else {
 #pragma unroll
-    for (int i = 0; i < ITEMS; i++) {
-      const uint32_t d = dg[i];
-      const uint32_t peers = __match_any_sync(0xffffffffu, d);
-      const int leader = __ffs(peers) - 1;
-      uint32_t base = 0;
-      if (lane == leader && d != INVALID_DIGIT) {
-        base = sm.whist[warp][d];
-        sm.whist[warp][d] = base + __popc(peers);
-      }
-      base = __shfl_sync(0xffffffffu, base, leader);
-      __syncwarp();
-      dg[i] = d | ((base + __popc(peers & lt_mask)) << 16);
+      for (int i = 0; i < ITEMS; i++) key[i] = ((ok >> i) & 1u) ? keys_in[wbase + uint64_t(i) * 32] : KeyT(0);
+#pragma unroll
+      for (int i = 0; i < ITEMS; i++) dg[i] = ((ok >> i) & 1u) ? (uint32_t(key[i] >> shift) & 255u) : INVALID_DIGIT;
     }
-    __syncthreads();
 
-    // ---- per digit: warps' exclusive offsets and the tile's count; publish the aggregate
+    // ---- early counts: the tile's per-digit counts go out as look-back aggregates before any
+    // ranking, so the tiles after this one can resolve their prefixes as early as possible.
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++)
+      if (dg[i] != INVALID_DIGIT) atomicAdd(&sm.whist[warp][dg[i]], 1u);
+    __syncthreads();
     for (int b = threadIdx.x; b < NBINS; b += THREADS) {
       uint32_t run = 0;
 #pragma unroll
@@ -578,31 +668,56 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
         run += c;
       }
       sm.cnt[b] = run;
-      st_relaxed_u64(pa.status + uint64_t(tile) * NBINS + b, pack_status(epoch, tile == 0 ? ST_INCL : ST_AGG, run));
+      ST::store(status + uint64_t(tile) * NBINS + b, ST::make(epoch, tile == 0 ? ST_INCL : ST_AGG, run));
     }
-    __syncthreads();
     // Tile-local digit starts: value digits in order, then the NaN and null routing bins.
     block_exclusive_scan_256(sm.cnt, sm.local, &sm.scan_total, sm.scan_warp);
     if (threadIdx.x == 0) {
-      const uint32_t tot = sm.local[255] + sm.cnt[255];
-      sm.local[NAN_BIN] = tot;
-      sm.local[NULL_BIN] = tot + sm.cnt[NAN_BIN];
+      const uint32_t t = sm.local[255] + sm.cnt[255];
+      sm.local[NAN_BIN] = t;
+      sm.local[NULL_BIN] = t + sm.cnt[NAN_BIN];
     }
     __syncthreads();
 
-    // ---- stage keys, ids and digits at their tile-local sorted slot (frees the registers)
+    // ---- warp ranking and staging: each row goes to its tile-local sorted slot. The rows of a lane's
+    // item that share its digit come from one ballot per digit bit; the ballots of different items are
+    // independent, and only the warp's running digit counters advance item by item.
+    {
+      const int nbits = (flags & PF_ROUTE) ? 9 : 8;
+      uint32_t peers_of[ITEMS];
 #pragma unroll
-    for (int i = 0; i < ITEMS; i++) {
-      const uint32_t d = dg[i] & 0xFFFFu;
-      if (d != INVALID_DIGIT) {
-        const uint32_t pos = sm.local[d] + sm.whist[warp][d] + (dg[i] >> 16);
-        sm.keys[pos] = key[i];
-        sm.ids[pos] = id[i];
-        sm.dig[pos] = uint16_t(d);
+      for (int i = 0; i < ITEMS; i++) {
+        const uint32_t d = dg[i];
+        uint32_t peers = __ballot_sync(0xffffffffu, d != INVALID_DIGIT);
+#pragma unroll
+        for (int k = 0; k < 9; k++) {
+          if (k < nbits) {
+            const uint32_t bit = (d >> k) & 1u;
+            const uint32_t bl = __ballot_sync(0xffffffffu, bit);
+            peers &= bit ? bl : ~bl;
+          }
+        }
+        peers_of[i] = peers;
+      }
+#pragma unroll
+      for (int i = 0; i < ITEMS; i++) {
+        const uint32_t d = dg[i];
+        const uint32_t peers = peers_of[i];
+        uint32_t base = 0;
+        if (d != INVALID_DIGIT) base = sm.whist[warp][d];
+        __syncwarp();
+        if (d != INVALID_DIGIT) {
+          if (lane == __ffs(peers) - 1) sm.whist[warp][d] = base + __popc(peers);
+          const uint32_t pos = sm.local[d] + base + __popc(peers & lt_mask);
+          sm.keys[pos] = key[i];
+          sm.ids[pos] = id[i];
+          sm.dig[pos] = uint16_t(d);
+        }
+        __syncwarp();
       }
     }
 
-    // ---- decoupled look-back, one thread per digit, LOOKBACK_WINDOW predecessors per round trip:
+    // ---- decoupled look-back, one thread per digit, a window of predecessors per round trip:
     // the window's loads are independent, so the inclusive-prefix frontier moves a whole window of
     // tiles per L2 round trip instead of one. Every wait is bounded in time.
     for (int b = threadIdx.x; b < NBINS; b += THREADS) {
@@ -611,46 +726,53 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
         int64_t j = int64_t(tile) - 1;
         bool done = false;
         while (!done) {
-          uint64_t st[LOOKBACK_WINDOW];
+          constexpr int W = ST::WINDOW;
+          StatusT st[W];
 #pragma unroll
-          for (int i = 0; i < LOOKBACK_WINDOW; i++)
-            st[i] = (j - i >= 0) ? ld_relaxed_u64(pa.status + uint64_t(j - i) * NBINS + b) : pack_status(epoch, ST_INCL, 0);
+          for (int i = 0; i < W; i++)
+            st[i] = (j - i >= 0) ? ST::load(status + uint64_t(j - i) * NBINS + b) : ST::make(epoch, ST_INCL, 0);
 #pragma unroll
-          for (int i = 0; i < LOOKBACK_WINDOW; i++) {
-            uint64_t s = st[i];
-            if (uint32_t(s >> 34) != epoch || ((s >> 32) & 3u) == 0u) {
-              const uint64_t* p = pa.status + uint64_t(j - i) * NBINS + b;
+          for (int i = 0; i < W; i++) {
+            StatusT s = st[i];
+            if (!ST::ready(s, epoch)) {
+              const StatusT* p = status + uint64_t(j - i) * NBINS + b;
               const uint64_t t0 = globaltimer_ns();
               uint32_t polls = 0;
               for (;;) {
-                s = ld_relaxed_u64(p);
-                if (uint32_t(s >> 34) == epoch && ((s >> 32) & 3u) != 0u) break;
+                s = ST::load(p);
+                if (ST::ready(s, epoch)) break;
                 if (++polls > 8) __nanosleep(32);
                 if ((polls & 63u) == 0u && globaltimer_ns() - t0 > LOOKBACK_TIMEOUT_NS) {
                   atomicOr(pa.err, ERR_LOOKBACK_TIMEOUT);
-                  s = pack_status(epoch, ST_INCL, 0);
+                  s = ST::make(epoch, ST_INCL, 0);
                   break;
                 }
               }
             }
-            excl += uint32_t(s);
-            if (((s >> 32) & 3u) == ST_INCL) { done = true; break; }
+            excl += ST::count(s);
+            if (ST::flag(s) == ST_INCL) { done = true; break; }
           }
-          j -= LOOKBACK_WINDOW;
+          j -= W;
           if (j < 0) done = true;
         }
-        st_relaxed_u64(pa.status + uint64_t(tile) * NBINS + b, pack_status(epoch, ST_INCL, excl + sm.cnt[b]));
+        ST::store(status + uint64_t(tile) * NBINS + b, ST::make(epoch, ST_INCL, excl + sm.cnt[b]));
       }
       sm.gdelta[b] = sm.desc.bin_base[b] + excl - sm.local[b];
     }
     __syncthreads();
 
     const uint32_t tile_n = uint32_t((count - tile_base) < uint64_t(TILE) ? (count - tile_base) : uint64_t(TILE));
-    // ---- keys out, then ids out; consecutive threads write consecutive addresses of a digit run
+    // ---- keys out, then ids out; consecutive threads write consecutive addresses of a digit run.
+    // Every destination is checked against its array: an offset error is reported, never written.
+    const uint32_t buf_rows = sm.desc.buf_rows, out_rows = sm.desc.out_rows;
     if (keys_out) {
       for (uint32_t j = threadIdx.x; j < tile_n; j += THREADS) {
         const uint32_t d = sm.dig[j];
-        if (d < RADIX) keys_out[sm.gdelta[d] + j] = sm.keys[j];
+        const uint32_t dst = sm.gdelta[d] + j;
+        if (d < RADIX) {
+          if (dst < buf_rows) keys_out[dst] = sm.keys[j];
+          else atomicOr(pa.err, ERR_BOUNDS);
+        }
       }
     }
     for (uint32_t j = threadIdx.x; j < tile_n; j += THREADS) {
@@ -659,10 +781,12 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
       uint32_t dst = sm.gdelta[d] + j;
       if (d >= RADIX || !ids_out) {
         if (d < RADIX) dst += sm.desc.value_base;
+        if (dst >= out_rows) { atomicOr(pa.err, ERR_BOUNDS); continue; }
         if (flags & PF_WIDE_OUT) static_cast<uint64_t*>(pa.final_out)[dst] = v;
         else static_cast<uint32_t*>(pa.final_out)[dst] = v;
       } else {
-        ids_out[dst] = v;
+        if (dst < buf_rows) ids_out[dst] = v;
+        else atomicOr(pa.err, ERR_BOUNDS);
       }
     }
     __syncthreads();
@@ -674,8 +798,8 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
 
 template <typename KeyT>
 struct PassConfig;
-template <> struct PassConfig<uint32_t> { static constexpr int THREADS = 256, ITEMS = 16; };
-template <> struct PassConfig<uint64_t> { static constexpr int THREADS = 256, ITEMS = 16; };
+template <> struct PassConfig<uint32_t> { static constexpr int THREADS = 512, ITEMS = 8; };
+template <> struct PassConfig<uint64_t> { static constexpr int THREADS = 512, ITEMS = 8; };
 
 constexpr int HIST_THREADS = 256, HIST_ITEMS = 8;
 
@@ -685,13 +809,13 @@ static size_t pass_smem() {
   return sizeof(PassShared<KeyT, C::THREADS, C::ITEMS>);
 }
 
-template <typename KeyT>
+template <typename KeyT, typename StatusT>
 static int pass_blocks_per_sm() {
   using C = PassConfig<KeyT>;
   static int cached = -1;
   static std::once_flag once;
   std::call_once(once, [] {
-    auto fn = onesweep_pass_kernel<KeyT, C::THREADS, C::ITEMS>;
+    auto fn = onesweep_pass_kernel<KeyT, StatusT, C::THREADS, C::ITEMS>;
     AM_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(pass_smem<KeyT>())));
     int b = 0;
     AM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, C::THREADS, pass_smem<KeyT>()));
@@ -710,20 +834,22 @@ static void launch_histogram(const ColView& cv, KeyStats* st, uint64_t n, cudaSt
   AM_CUDA(cudaGetLastError());
 }
 
-template <typename KeyT>
+template <typename KeyT, typename StatusT>
 static void launch_pass(const PassArgs& pa, const ColView& cv, uint64_t n, cudaStream_t s) {
   using C = PassConfig<KeyT>;
   constexpr int TILE = C::THREADS * C::ITEMS;
   const uint64_t tiles = (n + TILE - 1) / TILE;
-  const int grid = int(std::min<uint64_t>(tiles, uint64_t(device().sm_count) * pass_blocks_per_sm<KeyT>()));
+  const int grid = int(std::min<uint64_t>(tiles, uint64_t(device().sm_count) * pass_blocks_per_sm<KeyT, StatusT>()));
   KernelTimer kt("radix_onesweep_pass", s);
-  onesweep_pass_kernel<KeyT, C::THREADS, C::ITEMS><<<std::max(grid, 1), C::THREADS, pass_smem<KeyT>(), s>>>(pa, cv);
+  onesweep_pass_kernel<KeyT, StatusT, C::THREADS, C::ITEMS><<<std::max(grid, 1), C::THREADS, pass_smem<KeyT>(), s>>>(pa, cv);
   AM_CUDA(cudaGetLastError());
 }
 
-static int min_tile() {
-  return std::min(PassConfig<uint32_t>::THREADS * PassConfig<uint32_t>::ITEMS,
-                  PassConfig<uint64_t>::THREADS * PassConfig<uint64_t>::ITEMS);
+// Rows per look-back entry (a tile), the smallest over the key widths.
+static uint64_t min_super() {
+  using A = PassConfig<uint32_t>;
+  using B = PassConfig<uint64_t>;
+  return std::min<uint64_t>(uint64_t(A::THREADS) * A::ITEMS, uint64_t(B::THREADS) * B::ITEMS);
 }
 
 ColView make_view(const SortKey& k) {
@@ -840,10 +966,14 @@ void radix_argsort(const std::vector<SortKey>& keys, int64_t n64, void* out, int
     AM_CUDA(cudaGetLastError());
   }
 
-  const uint64_t max_tiles = (n + min_tile() - 1) / min_tile();
+  const uint64_t max_tiles = (n + min_super() - 1) / min_super();
+  // Passes of fewer than 2^30 rows use 32-bit look-back words, zeroed before each pass.
+  const bool narrow_status = n < (uint64_t(1) << 30);
   StreamScratch& sc = stream_scratch(s, size_t(max_tiles) * NBINS);
   for (int sl = 0; sl < S; sl++) {
-    if (sc.epoch >= (1u << 30) - 1) {
+    if (narrow_status) {
+      AM_CUDA(cudaMemsetAsync(sc.status, 0, size_t(max_tiles) * NBINS * sizeof(uint32_t), s));
+    } else if (sc.epoch >= (1u << 30) - 1) {
       AM_CUDA(cudaMemsetAsync(sc.status, 0, sc.status_words * sizeof(uint64_t), s));
       sc.epoch = 0;
     }
@@ -860,8 +990,13 @@ void radix_argsort(const std::vector<SortKey>& keys, int64_t n64, void* out, int
     a.tile_counter = tick + sl;
     a.err = sc.err;
     const ColView& cv = views[pa.slot_key[sl]];
-    if (slot_bytes[sl] == 8) launch_pass<uint64_t>(a, cv, n, s);
-    else launch_pass<uint32_t>(a, cv, n, s);
+    if (slot_bytes[sl] == 8) {
+      if (narrow_status) launch_pass<uint64_t, uint32_t>(a, cv, n, s);
+      else launch_pass<uint64_t, uint64_t>(a, cv, n, s);
+    } else {
+      if (narrow_status) launch_pass<uint32_t, uint32_t>(a, cv, n, s);
+      else launch_pass<uint32_t, uint64_t>(a, cv, n, s);
+    }
   }
   if (stats) {
     // Counters arrive asynchronously; am_last_sort_stats waits for them.

@@ -25,11 +25,11 @@ constexpr uint32_t PF_WIDE_OUT = 8;        // the output index array is uint64
 // Look-back status word: epoch (30 bits) | flag (2 bits) | count (32 bits).
 constexpr uint32_t ST_AGG = 1, ST_INCL = 2;
 constexpr uint64_t LOOKBACK_TIMEOUT_NS = 1000000000ull;   // 1 s, then the pass reports an error
-constexpr int LOOKBACK_WINDOW = 16;                       // predecessor tiles read per round trip
 
 // Device error word bits.
 constexpr uint32_t ERR_LOOKBACK_TIMEOUT = 1;
 constexpr uint32_t ERR_TAKE_RANGE = 2;
+constexpr uint32_t ERR_BOUNDS = 4;                        // a kernel computed a destination outside its array
 
 // One key column as the kernels read it.
 struct ColView {
@@ -60,6 +60,8 @@ struct PassDesc {
   uint32_t active, flags, count, shift;
   int32_t src_keys, src_ids, dst_keys, dst_ids;   // -1: none / identity / the output array
   uint32_t value_base, key;
+  uint32_t buf_rows, out_rows;                    // bounds of the key / id buffers and of the output
+  uint32_t pad2[2];
   uint32_t bin_base[NBINS];
 };
 
@@ -82,7 +84,7 @@ struct PassArgs {
   void* keys[2];
   uint32_t* ids[2];
   void* final_out;
-  uint64_t* status;
+  void* status;
   uint32_t* tile_counter;
   uint32_t* err;
   uint32_t epoch;

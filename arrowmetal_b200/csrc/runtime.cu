@@ -398,6 +398,7 @@ void check_device_errors(cudaStream_t s) {
   AM_CUDA(cudaMemsetAsync(sc.err, 0, sizeof(uint32_t), s));
   if (e & rs::ERR_TAKE_RANGE) throw invalid("take: index out of range");
   if (e & rs::ERR_LOOKBACK_TIMEOUT) throw Error("radix sort: a look-back wait timed out on the device");
+  if (e & rs::ERR_BOUNDS) throw Error("radix sort: a destination fell outside its array (write skipped)");
   throw Error("device error word " + std::to_string(e));
 }
 

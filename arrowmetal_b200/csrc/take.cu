@@ -193,6 +193,9 @@ void take_columns(am_array* const* cols, int count, am_array* indices, am_array*
   }
   use_on(indices, s);
   for (int base = 0; base < count; base += kMaxTakeCols) {
+    const int m0 = std::min(kMaxTakeCols, count - base);
+    for (int c = 1; c < m0; c++)
+      if (cols[base + c]->length != cols[base]->length) throw length_mismatch(cols[base]->length, cols[base + c]->length);
     const int m = std::min(kMaxTakeCols, count - base);
     TakeArgs a{};
     a.ncols = m;

@@ -260,15 +260,23 @@ def main():
         ms = float(t.item())
     value = world * n / (ms / 1e3)
 
-    # ---- roofline of the dominant kernel
+    # ---- roofline of the dominant kernel (the take's kernels count as one stage: their model bytes
+    # are the take's, however the gather is organised)
     model = algorithmic_bytes(n, m_rows, st["passes_run"])
-    per_kernel = {}
+    stages = {}
     for name, (launches, total_ms) in prof.items():
-        if name in model:
-            b = model[name] * args.steps
-            per_kernel[name] = {"launches": launches, "total_ms": total_ms, "bytes": b,
-                                "gbs": b / (total_ms / 1e3) / 1e9}
-    dom = max(per_kernel, key=lambda k: per_kernel[k]["total_ms"])
+        stage = "take_gather" if name.startswith("take_") else name
+        e = stages.setdefault(stage, {"launches": 0, "total_ms": 0.0, "kernels": {}})
+        e["launches"] += launches
+        e["total_ms"] += total_ms
+        e["kernels"][name] = {"launches": launches, "ms_per_step": total_ms / args.steps}
+    per_kernel = {}
+    for stage, e in stages.items():
+        if stage in model:
+            b = model[stage] * args.steps
+            e.update({"bytes": b, "gbs": b / (e["total_ms"] / 1e3) / 1e9})
+        per_kernel[stage] = e
+    dom = max((k for k in per_kernel if "gbs" in per_kernel[k]), key=lambda k: per_kernel[k]["total_ms"])
     d = per_kernel[dom]
     gpu_launches = sum(l for l, _ in prof.values())
 

@@ -33,10 +33,11 @@ def test_row_limit_refusal(am):
 
 
 def test_lookback_wait_runs_out_and_reports(am):
-    # int32 keys in [0, 100): one active digit pass over 3 tiles. With tile 0 skipped, tile 1's
-    # look-back waits on a status nothing writes, gives up after its time limit and sets the error word.
+    # int32 keys in [0, 100): one active digit pass over several look-back entries. With the first one
+    # skipped, the next one's look-back waits on a status nothing writes, gives up after its time limit
+    # and sets the error word.
     rng = np.random.default_rng(1)
-    m = am.MetalArray.from_arrow(pa.array(rng.integers(0, 100, 10_000).astype(np.int32)))
+    m = am.MetalArray.from_arrow(pa.array(rng.integers(0, 100, 100_000).astype(np.int32)))
     am._lib.am_debug_skip_first_tile(1)
     try:
         with pytest.raises(am.ArrowMetalError, match="look-back"):

@@ -102,3 +102,46 @@ def test_take_error_deferred_to_batch_end(am):
         with am.batch():
             m.take(pa.array([5], type=pa.int64()))
     assert m.take(pa.array([1], type=pa.int64())).to_arrow().to_pylist() == [2]
+
+
+@pytest.mark.parametrize("idx_type", [pa.uint32(), pa.int64()])
+def test_take_large(am, idx_type):
+    # 6M output rows over 5M-row sources of every width, boolean and nullable ones included.
+    rng = np.random.default_rng(12)
+    n_src, n = 5_000_000, 6_000_000
+    cols = [pa.array(rng.integers(-2**62, 2**62, n_src), mask=rng.random(n_src) < 0.1),
+            pa.array(rng.standard_normal(n_src)),
+            pa.array(rng.integers(-2**31, 2**31 - 1, n_src, dtype=np.int32)),
+            pa.array(rng.random(n_src) < 0.5),
+            pa.array(rng.integers(0, 255, n_src, dtype=np.uint8), mask=rng.random(n_src) < 0.3)]
+    idx = pa.array(rng.integers(0, n_src, n), mask=rng.random(n) < 0.02).cast(idx_type)
+    outs = am.take_columns([am.MetalArray.from_arrow(c) for c in cols], idx)
+    for c, o in zip(cols, outs):
+        got = o.to_arrow()
+        want = pc.take(c, idx)
+        assert got.null_count == want.null_count
+        assert got.equals(want)
+
+
+def test_take_through_sort_large(am):
+    # The sorted-table gather of the ORDER BY workload shape, checked against numpy indexing.
+    rng = np.random.default_rng(13)
+    n = 8_000_000
+    key = pa.array(rng.integers(0, 2**40, n), mask=rng.random(n) < 0.1)
+    p1 = pa.array(rng.standard_normal(n))
+    k, p = am.MetalArray.from_arrow(key), am.MetalArray.from_arrow(p1)
+    idx = k.argsort()
+    ko, po = am.take_columns([k, p], idx)
+    ii = idx.to_arrow().to_numpy()
+    assert np.array_equal(po.to_arrow().to_numpy(), p1.to_numpy()[ii])
+    kv = ko.to_arrow()
+    assert kv.equals(pc.take(key, pa.array(ii)))
+
+
+def test_take_large_out_of_range(am):
+    rng = np.random.default_rng(14)
+    src = am.MetalArray.from_arrow(pa.array(rng.integers(0, 100, 5_000_000)))
+    idx = rng.integers(0, 5_000_000, 5_000_000)
+    idx[4_999_999] = 5_000_000
+    with pytest.raises(am.ArrowMetalError, match="out of range"):
+        am.take_columns([src, src], pa.array(idx))
