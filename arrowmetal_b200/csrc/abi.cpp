@@ -608,6 +608,23 @@ int am_sort_ex2(am_array* a, int descending, int null_placement, int float_order
   return guard([&] {
     std::vector<SortKey> k(1);
     k[0] = SortKey{a, descending != 0, null_placement == 1, float_order};
+    // A key map that is a bijection: the sorted column is rebuilt from the sorted keys, no gather
+    // (the reference's sortedByInvertingKeys, Sources/ArrowMetal/Kernels/Sort.swift:509-619).
+    if (a->length > 0 && float_order_ok(float_order) >= 0 && key_invertible(k[0])) {
+      check_index_rows(a->length, "sort");
+      cudaStream_t s = stream();
+      use_on(a, s);
+      SortCarry carry;
+      carry.key_dst = new_array(a->pt, a->format, a->length);
+      try {
+        radix_sort(k, a->length, nullptr, 4, &carry, s, &tls().last_stats);
+      } catch (...) {
+        am::release(carry.key_dst);
+        throw;
+      }
+      *out = carry.key_dst;
+      return 0;
+    }
     am_array* idx = argsort_keys(k, 4, "sort");
     am_array* r = nullptr;
     try {

@@ -16,6 +16,12 @@
 
 #include "../../include/arrowmetal.h"
 
+#ifdef __CUDACC__
+#define AM_HD __host__ __device__
+#else
+#define AM_HD
+#endif
+
 namespace am {
 
 // ---------------------------------------------------------------------------------------------
@@ -135,7 +141,7 @@ void profile_reset();
 enum PhysType : int32_t {
   PT_BOOL = 0, PT_I8, PT_U8, PT_I16, PT_U16, PT_I32, PT_U32, PT_I64, PT_U64, PT_F16, PT_F32, PT_F64,
 };
-inline int pt_bytes(int pt) {
+AM_HD inline int pt_bytes(int pt) {
   switch (pt) {
     case PT_BOOL: return 0;   // bit-packed
     case PT_I8: case PT_U8: return 1;
@@ -144,8 +150,8 @@ inline int pt_bytes(int pt) {
     default: return 8;
   }
 }
-inline bool pt_float(int pt) { return pt == PT_F16 || pt == PT_F32 || pt == PT_F64; }
-inline int pt_key_bytes(int pt) { return pt_bytes(pt) == 8 ? 8 : 4; }
+AM_HD inline bool pt_float(int pt) { return pt == PT_F16 || pt == PT_F32 || pt == PT_F64; }
+AM_HD inline int pt_key_bytes(int pt) { return pt_bytes(pt) == 8 ? 8 : 4; }
 // Parses an Arrow C Data Interface format string; throws unsupported for the types this build does
 // not carry (strings, nested, dictionary, decimal, intervals).
 int parse_format(const char* fmt);
@@ -206,6 +212,21 @@ struct SortKey {
 // bytes (4 or 8) into `out` (device memory) on stream `s`.
 void radix_argsort(const std::vector<SortKey>& keys, int64_t n, void* out, int index_width,
                    cudaStream_t s, am_sort_stats* stats);
+
+// Columns a sort carries with its rows (a key-value sort), so that they come out sorted without a
+// gather: src[i] (length n) is sorted into dst[i] (a new array of the same type, filled here).
+// key_dst, for a single integer (or totalOrder float) key, receives the sorted key column, rebuilt
+// from the sorted keys. `out` may be NULL when no index array is wanted.
+struct SortCarry {
+  std::vector<am_array*> src;
+  std::vector<am_array*> dst;
+  am_array* key_dst = nullptr;
+};
+constexpr int kMaxCarried = 6;
+// True when the key column can be rebuilt from its sorted keys (the key map is a bijection).
+bool key_invertible(const SortKey& k);
+void radix_sort(const std::vector<SortKey>& keys, int64_t n, void* out, int index_width, SortCarry* carry,
+                cudaStream_t s, am_sort_stats* stats);
 
 // Gathers `count` columns through one index array. outs[i] must be new arrays of indices' length.
 // `check_range` asks the kernel to flag an index outside [0, src length) in the stream's error word.

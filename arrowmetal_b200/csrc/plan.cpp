@@ -4,9 +4,10 @@
 // optionally with_columns below it and limit above it).
 //
 // Grammar and key options follow the reference's PlanJSON (Sources/ArrowMetal/Engine/PlanJSON.swift:
-// 80-140) and include/arrowmetal.h:1369-1404. Frames are evaluated lazily: a sort yields a row
-// permutation instead of gathered columns, a limit slices that permutation, a select picks columns,
-// and only the columns the plan returns are gathered, in one fused take launch.
+// 80-140) and include/arrowmetal.h:1369-1404. A one-key sort of a plain frame carries every column
+// through its radix passes (a key-value sort), so the sorted table leaves the last pass with no
+// gather; other sorts yield a row permutation, a limit slices it, a select picks columns, and only
+// the columns the plan returns are gathered, in one fused take launch.
 #include <sstream>
 
 #include "am_internal.h"
@@ -248,6 +249,41 @@ Frame eval(const json::Value& node, am_plan_source** sources, int64_t nsrc, std:
       const int i = f.find(k.col);
       if (i < 0) throw invalid("plan: unknown sort column \"" + k.col + "\"");
       which.push_back(i);
+    }
+    // One key over an unpermuted frame: every column rides through the sort with its row (a key-value
+    // sort), so the sorted table comes out of the last pass with no gather. An integer key column is
+    // rebuilt from the sorted keys instead of being carried.
+    if (keys.size() == 1 && !f.perm && f.rows > 0) {
+      SortKey key{f.cols[size_t(which[0])], keys[0].desc, keys[0].nulls_first, keys[0].float_order};
+      if (key.float_order < 0 || key.float_order > 2) throw invalid("unknown float_order " + std::to_string(key.float_order));
+      const bool rebuild_key = key_invertible(key);
+      SortCarry carry;
+      std::vector<am_array*> outs(f.cols.size(), nullptr);
+      for (size_t c = 0; c < f.cols.size(); c++) {
+        am_array* col = f.cols[c];
+        outs[c] = new_array(col->pt, col->format, f.rows);
+        if (rebuild_key && int(c) == which[0]) {
+          carry.key_dst = outs[c];
+        } else {
+          carry.src.push_back(col);
+          carry.dst.push_back(outs[c]);
+        }
+      }
+      if (int(carry.src.size()) <= kMaxCarried) {
+        check_index_rows(f.rows, "sort");
+        try {
+          radix_sort({key}, f.rows, nullptr, 4, &carry, stream(), &tls().last_stats);
+        } catch (...) {
+          for (am_array* o : outs) am::release(o);
+          throw;
+        }
+        for (size_t c = 0; c < f.cols.size(); c++) {
+          am::release(f.cols[c]);
+          f.cols[c] = outs[c];
+        }
+        return f;
+      }
+      for (am_array* o : outs) am::release(o);
     }
     std::vector<am_array*> kc = materialize(f, which);
     std::vector<am_array*> handles = kc;

@@ -471,6 +471,7 @@ __global__ void __launch_bounds__(256) plan_kernel(PlanArgs a, KeyStats* __restr
       else if (keys_src < 0) flags |= PF_ENCODE;
       if (k == 0 && (flags & PF_ENCODE)) flags |= PF_ROUTE;
       if (a.index_wide) flags |= PF_WIDE_OUT;
+      if (is_last) flags |= PF_LAST;
       p.flags = flags;
       p.key = uint32_t(k);
       p.shift = d < 0 ? 0u : uint32_t(8 * d);
@@ -563,9 +564,49 @@ struct PassShared {
   uint32_t scan_total;
   uint32_t ticket;
   uint16_t dig[TILE];
-  KeyT keys[TILE];
+  uint16_t slot_of_item[TILE];   // tile-local sorted slot of each item (payload staging)
+  union {
+    KeyT keys[TILE];
+    uint64_t pay64[TILE];        // payload staging, after the keys have left
+  };
   uint32_t ids[TILE];
+  uint8_t payv[TILE];
 };
+
+// Inverse of the integer and totalOrder key maps (SortSource.swift:131-190 read backwards): the value
+// bits of a key, at the key's width.
+template <typename KeyT>
+__device__ __forceinline__ uint64_t unkey_bits(KeyT k, int pt, int desc) {
+  if (desc) k = KeyT(~k);
+  if constexpr (sizeof(KeyT) == 8) {
+    const uint64_t S = 0x8000000000000000ull;
+    if (pt == PT_I64) return k ^ S;
+    if (pt == PT_F64) return (k & S) ? (k ^ S) : ~k;
+    return k;
+  } else {
+    const uint32_t S = 0x80000000u;
+    if (pt == PT_U32) return k;
+    if (pt == PT_F32) return (k & S) ? (k ^ S) : uint32_t(~k);
+    return uint32_t(k ^ S);          // int32 and the narrow types widened to it (truncated on store)
+  }
+}
+
+__device__ __forceinline__ void store_width(void* base, uint64_t i, int width, uint64_t v) {
+  switch (width) {
+    case 8: static_cast<uint64_t*>(base)[i] = v; break;
+    case 4: static_cast<uint32_t*>(base)[i] = uint32_t(v); break;
+    case 2: static_cast<uint16_t*>(base)[i] = uint16_t(v); break;
+    default: static_cast<uint8_t*>(base)[i] = uint8_t(v); break;
+  }
+}
+__device__ __forceinline__ uint64_t load_width(const void* base, uint64_t i, int width) {
+  switch (width) {
+    case 8: return static_cast<const uint64_t*>(base)[i];
+    case 4: return static_cast<const uint32_t*>(base)[i];
+    case 2: return static_cast<const uint16_t*>(base)[i];
+    default: return static_cast<const uint8_t*>(base)[i];
+  }
+}
 
 template <typename KeyT, typename StatusT, int THREADS, int ITEMS>
 __global__ void __launch_bounds__(THREADS, 2)
@@ -619,7 +660,7 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
 #pragma unroll
     for (int i = 0; i < ITEMS; i++)
       if (wbase + uint64_t(i) * 32 < count) ok |= 1u << i;
-    if (ids_in) {
+    if (ids_in && pa.carry_ids) {
 #pragma unroll
       for (int i = 0; i < ITEMS; i++) id[i] = ((ok >> i) & 1u) ? ids_in[wbase + uint64_t(i) * 32] : 0u;
     } else {
@@ -710,8 +751,9 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
           if (lane == __ffs(peers) - 1) sm.whist[warp][d] = base + __popc(peers);
           const uint32_t pos = sm.local[d] + base + __popc(peers & lt_mask);
           sm.keys[pos] = key[i];
-          sm.ids[pos] = id[i];
+          if (pa.carry_ids) sm.ids[pos] = id[i];
           sm.dig[pos] = uint16_t(d);
+          if (pa.npay) sm.slot_of_item[warp * (ITEMS * 32) + i * 32 + lane] = uint16_t(pos);
         }
         __syncwarp();
       }
@@ -765,6 +807,7 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
     // ---- keys out, then ids out; consecutive threads write consecutive addresses of a digit run.
     // Every destination is checked against its array: an offset error is reported, never written.
     const uint32_t buf_rows = sm.desc.buf_rows, out_rows = sm.desc.out_rows;
+    const bool last = (flags & PF_LAST) != 0;
     if (keys_out) {
       for (uint32_t j = threadIdx.x; j < tile_n; j += THREADS) {
         const uint32_t d = sm.dig[j];
@@ -775,22 +818,118 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
         }
       }
     }
-    for (uint32_t j = threadIdx.x; j < tile_n; j += THREADS) {
-      const uint32_t d = sm.dig[j];
-      const uint32_t v = sm.ids[j];
-      uint32_t dst = sm.gdelta[d] + j;
-      if (d >= RADIX || !ids_out) {
+    // The sorted key column: value rows from their keys in the last pass, null rows (first pass of the
+    // most significant key) as zero.
+    if (pa.key_out_mode == KEY_OUT_UNKEY && (last || (flags & PF_ROUTE))) {
+      const int kw = pt_bytes(pa.key_out_pt);
+      for (uint32_t j = threadIdx.x; j < tile_n; j += THREADS) {
+        const uint32_t d = sm.dig[j];
+        if (d < RADIX && !last) continue;
+        uint32_t dst = sm.gdelta[d] + j;
         if (d < RADIX) dst += sm.desc.value_base;
         if (dst >= out_rows) { atomicOr(pa.err, ERR_BOUNDS); continue; }
-        if (flags & PF_WIDE_OUT) static_cast<uint64_t*>(pa.final_out)[dst] = v;
-        else static_cast<uint32_t*>(pa.final_out)[dst] = v;
-      } else {
-        if (dst < buf_rows) ids_out[dst] = v;
-        else atomicOr(pa.err, ERR_BOUNDS);
+        const uint64_t v = d < RADIX ? unkey_bits<KeyT>(sm.keys[j], pa.key_out_pt, pa.key_desc) : 0ull;
+        store_width(pa.key_out, dst, kw, v);
+      }
+    }
+    if (pa.carry_ids) {
+      for (uint32_t j = threadIdx.x; j < tile_n; j += THREADS) {
+        const uint32_t d = sm.dig[j];
+        const uint32_t v = sm.ids[j];
+        uint32_t dst = sm.gdelta[d] + j;
+        if (d >= RADIX || !ids_out) {
+          if (!pa.final_out) continue;
+          if (d < RADIX) dst += sm.desc.value_base;
+          if (dst >= out_rows) { atomicOr(pa.err, ERR_BOUNDS); continue; }
+          if (flags & PF_WIDE_OUT) static_cast<uint64_t*>(pa.final_out)[dst] = v;
+          else static_cast<uint32_t*>(pa.final_out)[dst] = v;
+        } else {
+          if (dst < buf_rows) ids_out[dst] = v;
+          else atomicOr(pa.err, ERR_BOUNDS);
+        }
+      }
+    }
+    // ---- payload columns: each is read at the rows' input positions, staged at their sorted slots,
+    // and written out in order like the ids (on the ids' ping-pong schedule).
+    for (int c = 0; c < pa.npay; c++) {
+      const PayCol& pc = pa.pay[c];
+      __syncthreads();   // the staging area is free
+      const void* vin = si < 0 ? pc.src : pc.buf[si];
+      const uint8_t* vvin = si < 0 ? nullptr : pc.vbuf[si];
+#pragma unroll
+      for (int i = 0; i < ITEMS; i++) {
+        if (!((ok >> i) & 1u)) continue;
+        const uint64_t g = wbase + uint64_t(i) * 32;
+        uint64_t v;
+        if (si < 0 && pc.is_bool) v = bit_at(static_cast<const uint8_t*>(pc.src), pc.src_bool_off + int64_t(g)) ? 1u : 0u;
+        else v = load_width(vin, g, pc.width);
+        const uint32_t slot = sm.slot_of_item[warp * (ITEMS * 32) + i * 32 + lane];
+        sm.pay64[slot] = v;
+        if (pc.src_valid) sm.payv[slot] = si < 0 ? (bit_at(pc.src_valid, pc.src_voff + int64_t(g)) ? 1 : 0) : vvin[g];
+      }
+      __syncthreads();
+      void* vout = di < 0 ? pc.out : pc.buf[di];
+      uint8_t* vvout = di < 0 ? pc.vout : pc.vbuf[di];
+      for (uint32_t j = threadIdx.x; j < tile_n; j += THREADS) {
+        const uint32_t d = sm.dig[j];
+        uint32_t dst = sm.gdelta[d] + j;
+        void* to = vout;
+        uint8_t* vto = vvout;
+        if (d >= RADIX) {           // a routed null / NaN row: straight to its final place
+          to = pc.out;
+          vto = pc.vout;
+        } else if (di < 0) {
+          dst += sm.desc.value_base;
+        }
+        if (dst >= out_rows) { atomicOr(pa.err, ERR_BOUNDS); continue; }
+        store_width(to, dst, pc.width, sm.pay64[j]);
+        if (pc.src_valid) vto[dst] = sm.payv[j];
       }
     }
     __syncthreads();
   }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Kernel 4: after the passes, bytes become Arrow bitmaps (32 rows per warp ballot).
+
+// bits[w] = the 32 bytes bytes[32w .. 32w + 31] as bits; zero bytes counted into *zeros (optional).
+__global__ void __launch_bounds__(256) pack_bytes_kernel(const uint8_t* __restrict__ bytes, uint32_t* __restrict__ bits,
+                                                         uint64_t n, unsigned long long* zeros) {
+  const int lane = threadIdx.x & 31;
+  unsigned long long z = 0;
+  const uint64_t words = (n + 31) / 32;
+  for (uint64_t w = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) / 32; w < words;
+       w += uint64_t(gridDim.x) * blockDim.x / 32) {
+    const uint64_t r = w * 32 + lane;
+    const bool live = r < n;
+    const uint32_t b = __ballot_sync(0xffffffffu, live && bytes[r] != 0);
+    const uint32_t l = __ballot_sync(0xffffffffu, live);
+    if (lane == 0) {
+      bits[w] = b;
+      z += __popc(l & ~b);
+    }
+  }
+  if (zeros && lane == 0 && z) atomicAdd(zeros, z);
+}
+
+// The sorted key column's validity: the null block of the most significant key is
+// [0, nulls) with nulls first, [n - nulls, n) with nulls last; its null count is that block's size.
+__global__ void __launch_bounds__(256) key_validity_kernel(const SortSummary* __restrict__ sum, int nulls_first,
+                                                           uint32_t* __restrict__ bits, uint64_t n,
+                                                           unsigned long long* null_count) {
+  const uint64_t nn = sum->null_rows;
+  const uint64_t lo = nulls_first ? 0 : n - nn, hi = nulls_first ? nn : n;   // null rows [lo, hi)
+  const uint64_t words = (n + 31) / 32;
+  for (uint64_t w = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; w < words; w += uint64_t(gridDim.x) * blockDim.x) {
+    uint32_t v = 0;
+    for (int b = 0; b < 32; b++) {
+      const uint64_t r = w * 32 + b;
+      if (r < n && !(r >= lo && r < hi)) v |= 1u << b;
+    }
+    bits[w] = v;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) *null_count = nn;
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -887,13 +1026,35 @@ void fill_last_sort_stats(am_sort_stats* out) {
   out->passes_skipped = int32_t(h->passes_total - h->passes_run);
 }
 
-void radix_argsort(const std::vector<SortKey>& keys, int64_t n64, void* out, int index_width, cudaStream_t s,
+bool key_invertible(const SortKey& k) {
+  switch (k.col->pt) {
+    case PT_I8: case PT_U8: case PT_I16: case PT_U16: case PT_I32: case PT_U32: case PT_I64: case PT_U64:
+      return true;
+    case PT_F32: case PT_F64:
+      return k.float_order == rs::FO_TOTAL;
+    default:
+      return false;
+  }
+}
+
+void radix_argsort(const std::vector<SortKey>& keys, int64_t n, void* out, int index_width, cudaStream_t s,
                    am_sort_stats* stats) {
+  radix_sort(keys, n, out, index_width, nullptr, s, stats);
+}
+
+void radix_sort(const std::vector<SortKey>& keys, int64_t n64, void* out, int index_width, SortCarry* carry,
+                cudaStream_t s, am_sort_stats* stats) {
   using namespace rs;
   const int K = int(keys.size());
   if (K < 1 || K > MAX_KEYS) throw invalid("sort takes 1 to " + std::to_string(MAX_KEYS) + " key columns");
   if (n64 <= 0) return;
   const uint64_t n = uint64_t(n64);
+  const int npay = carry ? int(carry->src.size()) : 0;
+  if (npay > MAX_PAY) throw invalid("a sort carries at most " + std::to_string(MAX_PAY) + " columns");
+  if (carry && carry->key_dst && (K != 1 || !key_invertible(keys[0])))
+    throw invalid("the sorted key column is rebuilt only for one integer or totalOrder float key");
+  // Row ids move through the passes when an index is wanted or a lower key's column is gathered.
+  const bool carry_ids = out != nullptr || K > 1;
 
   // Slots: least significant key first; its digits low to high, then (lower keys) a category slot.
   PlanArgs pa{};
@@ -934,8 +1095,16 @@ void radix_argsort(const std::vector<SortKey>& keys, int64_t n64, void* out, int
   const size_t off_sum = (off_tick + sizeof(uint32_t) * S + 15) & ~size_t(15);
   const size_t header = (off_sum + sizeof(SortSummary) + 255) & ~size_t(255);
   const size_t kbuf = ((n * max_kb) + 255) & ~size_t(255);
-  const size_t ibuf = ((n * 4) + 255) & ~size_t(255);
-  char* base = static_cast<char*>(dmalloc(header + 2 * kbuf + 2 * ibuf, s));
+  const size_t ibuf = carry_ids ? ((n * 4) + 255) & ~size_t(255) : 0;
+  size_t pbytes = 0;
+  for (int c = 0; c < npay; c++) {
+    const am_array* src = carry->src[c];
+    const size_t w = size_t(std::max(pt_bytes(src->pt), 1));
+    pbytes += 2 * ((n * w + 255) & ~size_t(255));                       // ping-pong values
+    if (src->null_count != 0) pbytes += 3 * ((n + 255) & ~size_t(255));  // ping-pong + final validity bytes
+    if (src->pt == PT_BOOL) pbytes += (n + 255) & ~size_t(255);          // final value bytes
+  }
+  char* base = static_cast<char*>(dmalloc(header + 2 * kbuf + 2 * ibuf + pbytes, s));
   AM_CUDA(cudaMemsetAsync(base, 0, header, s));
   KeyStats* st = reinterpret_cast<KeyStats*>(base + off_stats);
   KeyPlan* kp = reinterpret_cast<KeyPlan*>(base + off_kplan);
@@ -944,8 +1113,64 @@ void radix_argsort(const std::vector<SortKey>& keys, int64_t n64, void* out, int
   SortSummary* sum = reinterpret_cast<SortSummary*>(base + off_sum);
   void* kbufA = base + header;
   void* kbufB = base + header + kbuf;
-  uint32_t* ibufA = reinterpret_cast<uint32_t*>(base + header + 2 * kbuf);
-  uint32_t* ibufB = reinterpret_cast<uint32_t*>(base + header + 2 * kbuf + ibuf);
+  uint32_t* ibufA = carry_ids ? reinterpret_cast<uint32_t*>(base + header + 2 * kbuf) : nullptr;
+  uint32_t* ibufB = carry_ids ? reinterpret_cast<uint32_t*>(base + header + 2 * kbuf + ibuf) : nullptr;
+  PayCol pays[MAX_PAY] = {};
+  std::vector<std::pair<uint8_t*, am_array*>> pack_values, pack_valid;   // bytes -> bitmaps afterwards
+  {
+    char* p = base + header + 2 * kbuf + 2 * ibuf;
+    auto take = [&](size_t bytes) { char* q = p; p += (bytes + 255) & ~size_t(255); return q; };
+    for (int c = 0; c < npay; c++) {
+      am_array* src = carry->src[c];
+      am_array* dst = carry->dst[c];
+      if (src->length != n64) throw length_mismatch(n64, src->length);
+      use_on(src, s);
+      PayCol& pc = pays[c];
+      pc.src = src->data();
+      pc.src_valid = src->null_count != 0 ? src->valid_bits() : nullptr;
+      pc.src_voff = src->validity_offset;
+      pc.src_bool_off = src->pt == PT_BOOL ? src->value_offset : 0;
+      pc.is_bool = src->pt == PT_BOOL ? 1 : 0;
+      pc.width = std::max(pt_bytes(src->pt), 1);
+      pc.buf[0] = take(n * pc.width);
+      pc.buf[1] = take(n * pc.width);
+      const size_t words = size_t((n + 127) / 128) * 4;
+      dst->values = DevBuffer::alloc(pc.is_bool ? words * 4 : n * pc.width + 16, s);
+      if (pc.is_bool) {
+        uint8_t* bytes = reinterpret_cast<uint8_t*>(take(n));
+        pc.out = bytes;
+        pack_values.push_back({bytes, dst});
+      } else {
+        pc.out = dst->values->ptr;
+      }
+      if (pc.src_valid) {
+        pc.vbuf[0] = reinterpret_cast<uint8_t*>(take(n));
+        pc.vbuf[1] = reinterpret_cast<uint8_t*>(take(n));
+        pc.vout = reinterpret_cast<uint8_t*>(take(n));
+        dst->validity = DevBuffer::alloc(words * 4, s);
+        dst->null_count_dev = DevBuffer::alloc(sizeof(unsigned long long), s);
+        AM_CUDA(cudaMemsetAsync(dst->null_count_dev->ptr, 0, sizeof(unsigned long long), s));
+        dst->null_count = -1;
+        pack_valid.push_back({pc.vout, dst});
+      } else {
+        dst->null_count = 0;
+      }
+      dst->last_stream = s;
+    }
+  }
+  am_array* key_dst = carry ? carry->key_dst : nullptr;
+  if (key_dst) {
+    const size_t words = size_t((n + 127) / 128) * 4;
+    key_dst->values = DevBuffer::alloc(n * pt_bytes(keys[0].col->pt) + 16, s);
+    key_dst->last_stream = s;
+    if (keys[0].col->null_count != 0) {
+      key_dst->validity = DevBuffer::alloc(words * 4, s);
+      key_dst->null_count_dev = DevBuffer::alloc(sizeof(unsigned long long), s);
+      key_dst->null_count = -1;
+    } else {
+      key_dst->null_count = 0;
+    }
+  }
   if (debug_skip_first_tile()) {
     // Test hook: every pass's ticket starts at 1, so tile 0 is never processed and the look-back of
     // tile 1 runs into its time limit.
@@ -989,6 +1214,16 @@ void radix_argsort(const std::vector<SortKey>& keys, int64_t n64, void* out, int
     a.epoch = ++sc.epoch;
     a.tile_counter = tick + sl;
     a.err = sc.err;
+    a.carry_ids = carry_ids ? 1 : 0;
+    a.npay = npay;
+    for (int c = 0; c < npay; c++) a.pay[c] = pays[c];
+    if (key_dst) {
+      a.key_out_mode = KEY_OUT_UNKEY;
+      a.key_out_pt = keys[0].col->pt;
+      a.key_desc = keys[0].descending ? 1 : 0;
+      a.key_float_order = keys[0].float_order;
+      a.key_out = key_dst->values->ptr;
+    }
     const ColView& cv = views[pa.slot_key[sl]];
     if (slot_bytes[sl] == 8) {
       if (narrow_status) launch_pass<uint64_t, uint32_t>(a, cv, n, s);
@@ -997,6 +1232,26 @@ void radix_argsort(const std::vector<SortKey>& keys, int64_t n64, void* out, int
       if (narrow_status) launch_pass<uint32_t, uint32_t>(a, cv, n, s);
       else launch_pass<uint32_t, uint64_t>(a, cv, n, s);
     }
+  }
+  // Bytes to bitmaps: boolean values and validity of the carried columns, the key column's validity.
+  const int fin_grid = int(std::min<uint64_t>((n + 8191) / 8192, uint64_t(device().sm_count) * 4));
+  for (auto& pv : pack_values) {
+    KernelTimer kt("sort_finish", s);
+    pack_bytes_kernel<<<std::max(fin_grid, 1), 256, 0, s>>>(pv.first, static_cast<uint32_t*>(pv.second->values->ptr), n, nullptr);
+    AM_CUDA(cudaGetLastError());
+  }
+  for (auto& pv : pack_valid) {
+    KernelTimer kt("sort_finish", s);
+    pack_bytes_kernel<<<std::max(fin_grid, 1), 256, 0, s>>>(pv.first, static_cast<uint32_t*>(pv.second->validity->ptr), n,
+                                                      static_cast<unsigned long long*>(pv.second->null_count_dev->ptr));
+    AM_CUDA(cudaGetLastError());
+  }
+  if (key_dst && key_dst->validity) {
+    KernelTimer kt("sort_finish", s);
+    key_validity_kernel<<<std::max(fin_grid, 1), 256, 0, s>>>(sum, keys[0].nulls_first ? 1 : 0,
+                                                            static_cast<uint32_t*>(key_dst->validity->ptr), n,
+                                                            static_cast<unsigned long long*>(key_dst->null_count_dev->ptr));
+    AM_CUDA(cudaGetLastError());
   }
   if (stats) {
     // Counters arrive asynchronously; am_last_sort_stats waits for them.

@@ -70,3 +70,85 @@ def test_plan_errors(am):
         am.run_plan({"op": "sort", "by": [["y", False]], "input": {"op": "scan", "source": "t"}}, [src])
     with pytest.raises(am.ArrowMetalError, match="float_order"):
         am.run_plan({"op": "sort", "by": [["x", False, {"float_order": "x"}]], "input": {"op": "scan", "source": "t"}}, [src])
+
+
+@pytest.mark.parametrize("key_kind", ["int64", "uint32", "int8", "float64_ieee", "float64_total", "float32_nan_largest", "bool"])
+@pytest.mark.parametrize("desc,nulls", [(False, "last"), (True, "first")])
+def test_single_key_sort_carries_columns(am, key_kind, desc, nulls):
+    # One key: every column rides through the radix passes (integer keys rebuilt from their keys).
+    rng = np.random.default_rng(len(key_kind) * 7 + desc)
+    n = 300_001
+    fo = "ieee"
+    if key_kind == "int64":
+        key = pa.array(rng.integers(-2**62, 2**62, n), mask=rng.random(n) < 0.1)
+    elif key_kind == "uint32":
+        key = pa.array(rng.integers(0, 2**32, n, dtype=np.uint32), mask=rng.random(n) < 0.1)
+    elif key_kind == "int8":
+        key = pa.array(rng.integers(-128, 127, n, dtype=np.int8), mask=rng.random(n) < 0.1)
+    elif key_kind == "bool":
+        key = pa.array(rng.random(n) < 0.5, mask=rng.random(n) < 0.1)
+    else:
+        v = rng.normal(0, 100, n).astype(np.float64)
+        v[rng.random(n) < 0.03] = np.nan
+        v[rng.random(n) < 0.03] = -0.0
+        key = pa.array(v, mask=rng.random(n) < 0.1)
+        if key_kind.startswith("float32"):
+            key = key.cast(pa.float32())
+        fo = key_kind.split("_", 1)[1]
+    cols = {"k": key, "f": pa.array(rng.standard_normal(n)), "i": pa.array(rng.integers(0, 9, n, dtype=np.int16)),
+            "b": pa.array(rng.random(n) < 0.5, mask=rng.random(n) < 0.2),
+            "u": pa.array(rng.integers(0, 200, n, dtype=np.uint8), mask=rng.random(n) < 0.3)}
+    src = am.PlanSource("t", cols)
+    plan = {"op": "sort", "input": {"op": "scan", "source": "t"},
+            "by": [["k", desc, {"nulls": nulls, "float_order": fo}]]}
+    out = am.run_plan(plan, [src])
+    from oracle import oracle
+    idx = oracle.argsort(key, desc, "at_start" if nulls == "first" else "at_end", fo)
+    for name, col in cols.items():
+        got = out[name].to_arrow()
+        want = col.take(pa.array(idx))
+        assert got.null_count == want.null_count, name
+        assert same_bits(got, want), name
+
+
+def same_bits(a, b):
+    """Equal validity and equal value bits at every valid row (NaN payloads and -0.0 included;
+    Array.equals treats NaN as unequal to itself)."""
+    if len(a) != len(b) or a.type != b.type:
+        return False
+    va = np.asarray(a.is_valid().to_numpy(zero_copy_only=False))
+    vb = np.asarray(b.is_valid().to_numpy(zero_copy_only=False))
+    if not np.array_equal(va, vb):
+        return False
+    if pa.types.is_boolean(a.type):
+        return np.array_equal(np.asarray(a.fill_null(False))[va], np.asarray(b.fill_null(False))[vb])
+    width = a.type.bit_width // 8
+    view = {1: np.uint8, 2: np.uint16, 4: np.uint32, 8: np.uint64}[width]
+    xa = np.frombuffer(a.buffers()[1], dtype=view)[a.offset:a.offset + len(a)]
+    xb = np.frombuffer(b.buffers()[1], dtype=view)[b.offset:b.offset + len(b)]
+    return np.array_equal(xa[va], xb[vb])
+
+
+@pytest.mark.parametrize("t", [pa.int64(), pa.uint64(), pa.int32(), pa.int16(), pa.uint8()])
+def test_sorted_copy_rebuilt_from_keys(am, t):
+    rng = np.random.default_rng(3)
+    n = 500_003
+    info = np.iinfo(t.to_pandas_dtype())
+    col = pa.array(rng.integers(info.min, info.max, n, dtype=t.to_pandas_dtype(), endpoint=True), mask=rng.random(n) < 0.05)
+    m = am.MetalArray.from_arrow(col)
+    for desc in (False, True):
+        for place in ("at_end", "at_start"):
+            got = m.sort(desc, place).to_arrow()
+            want = pc.take(col, pc.array_sort_indices(col, order="descending" if desc else "ascending", null_placement=place))
+            assert got.equals(want), (desc, place)
+
+
+def test_sorted_copy_total_order_floats(am):
+    rng = np.random.default_rng(4)
+    bits = rng.integers(0, 2**64, 200_000, dtype=np.uint64)
+    col = pa.Array.from_buffers(pa.float64(), len(bits), [None, pa.py_buffer(bits.tobytes())])
+    m = am.MetalArray.from_arrow(col)
+    got = m.sort(float_order="total").to_arrow()
+    key = np.where(bits >> np.uint64(63), ~bits, bits | np.uint64(1 << 63))
+    want = bits[np.argsort(key, kind="stable")]
+    assert np.array_equal(got.to_numpy(zero_copy_only=False).view(np.uint64), want)
