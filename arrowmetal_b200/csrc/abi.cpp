@@ -595,6 +595,16 @@ int am_argsort_ex3(am_array* a, int descending, int null_placement, int float_or
     return 0;
   });
 }
+int am_argsort_device_noalloc(const char* format, const void* values, const void* validity, int64_t offset,
+                              int64_t length, int descending, int null_placement, int float_order,
+                              uint32_t* indices, void* stream) {
+  return guard([&] {
+    const int pt = parse_format(format);
+    argsort_noalloc(pt, values, static_cast<const uint8_t*>(validity), offset, length, descending != 0,
+                    null_placement == 1, float_order, indices, static_cast<cudaStream_t>(stream));
+    return 0;
+  });
+}
 int am_argsort_ex2(am_array* a, int descending, int null_placement, int float_order, am_array** out) {
   return am_argsort_ex3(a, descending, null_placement, float_order, 4, out);
 }

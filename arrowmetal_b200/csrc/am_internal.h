@@ -227,6 +227,11 @@ constexpr int kMaxCarried = 6;
 bool key_invertible(const SortKey& k);
 void radix_sort(const std::vector<SortKey>& keys, int64_t n, void* out, int index_width, SortCarry* carry,
                 cudaStream_t s, am_sort_stats* stats);
+// Single-key argsort of a device column into a caller's uint32 array with no allocation: all
+// scratch sits in a fixed device block of the library (radix_sort.cu). Waits for its work.
+uint64_t noalloc_max_rows();
+void argsort_noalloc(int pt, const void* values, const uint8_t* validity, int64_t offset, int64_t length,
+                     bool descending, bool nulls_first, int float_order, uint32_t* indices, cudaStream_t s);
 
 // Gathers `count` columns through one index array. outs[i] must be new arrays of indices' length.
 // `check_range` asks the kernel to flag an index outside [0, src length) in the stream's error word.

@@ -1262,4 +1262,215 @@ void radix_sort(const std::vector<SortKey>& keys, int64_t n64, void* out, int in
   dfree(base, s);
 }
 
+
+// ------------------------------------------------------------------------------------------------
+// Argsort that allocates nothing.
+//
+// Some callers cannot allocate device memory when they need a sort. A process whose device memory
+// is owned by its own pool allocator (a framework's caching allocator, an RMM pool reserved at start)
+// has no room outside that pool and must not have a library take memory behind it. A serving loop
+// that must not stall cannot call cudaFree, which waits for the whole device. For them
+// am_argsort_device_noalloc sorts one key column with all of its scratch in one fixed block of device
+// memory that belongs to this library's image: every GPU the library is loaded on holds the block,
+// about 6.1 MiB, until the process exits. The caller passes the input column and the output index
+// array as device pointers. One call sorts at most NOALLOC_MAX_ROWS rows.
+
+namespace rs {
+
+constexpr uint64_t NOALLOC_MAX_ROWS = uint64_t(1) << 18;   // 262,144 rows per call
+constexpr uint64_t NOALLOC_TILE_ROWS = uint64_t(PassConfig<uint64_t>::THREADS) * PassConfig<uint64_t>::ITEMS;
+static_assert(NOALLOC_TILE_ROWS == uint64_t(PassConfig<uint32_t>::THREADS) * PassConfig<uint32_t>::ITEMS,
+              "both key widths use the same tile");
+constexpr int NOALLOC_MAX_PASSES = 8;                       // one key of at most 8 bytes
+
+// What one call keeps besides the ping-pong buffers. All of it must be zero when a call starts (the
+// histogram adds into `stats`, the passes take tiles from `tickets`, kernels OR into `err`), and so
+// must the look-back status words before every pass.
+struct NoAllocHeader {
+  KeyStats stats;
+  KeyPlan kplan;
+  PassDesc desc[NOALLOC_MAX_PASSES];
+  uint32_t tickets[NOALLOC_MAX_PASSES];
+  SortSummary summary;
+  uint32_t err;
+};
+
+constexpr size_t round256(size_t b) { return (b + 255) & ~size_t(255); }
+constexpr size_t NOALLOC_HEADER = round256(sizeof(NoAllocHeader));
+constexpr size_t NOALLOC_KEYS = round256(NOALLOC_MAX_ROWS * 8);
+constexpr size_t NOALLOC_IDS = round256(NOALLOC_MAX_ROWS * 4);
+constexpr size_t NOALLOC_TILES = (NOALLOC_MAX_ROWS + NOALLOC_TILE_ROWS - 1) / NOALLOC_TILE_ROWS;
+constexpr size_t NOALLOC_STATUS = round256(NOALLOC_TILES * NBINS * sizeof(uint32_t));
+constexpr size_t NOALLOC_BYTES = NOALLOC_HEADER + 2 * NOALLOC_KEYS + 2 * NOALLOC_IDS + NOALLOC_STATUS;
+
+// The block. In host code this name is only a stand-in for the device variable, never an address a
+// kernel may be given: the host looks the address up per device (cudaGetSymbolAddress) and passes that.
+static __device__ __align__(256) unsigned char noalloc_scratch[NOALLOC_BYTES];
+
+namespace {
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+
+struct NoAllocDevice {
+  bool ready = false;
+  unsigned char* scratch = nullptr;   // device address of noalloc_scratch on this device
+  int hist_grid_cap = 0;
+  int pass_grid_cap[2] = {0, 0};      // 4-byte and 8-byte keys
+};
+
+// Calls share the block, so they take turns: the lock is held until the call's work has finished on
+// its stream.
+std::mutex g_noalloc_mu;
+NoAllocDevice g_noalloc[NOALLOC_MAX_DEVICES];
+
+template <typename KeyT>
+int noalloc_pass_cap(int sm_count) {
+  using C = PassConfig<KeyT>;
+  auto fn = onesweep_pass_kernel<KeyT, uint32_t, C::THREADS, C::ITEMS>;
+  AM_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(pass_smem<KeyT>())));
+  int b = 0;
+  AM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, C::THREADS, pass_smem<KeyT>()));
+  return sm_count * std::max(1, b);
+}
+
+// Set-up of the calling thread's current device, once: the block's device address, the kernels'
+// shared-memory limit and grid caps. It runs inside the first call on each device.
+NoAllocDevice& noalloc_device() {
+  int dev = 0;
+  AM_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES)
+    throw unsupported("argsort without allocation runs on devices 0 to " + std::to_string(NOALLOC_MAX_DEVICES - 1));
+  NoAllocDevice& d = g_noalloc[dev];
+  if (d.ready) return d;
+  unsigned char* ptr = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress((void**)&ptr, noalloc_scratch);
+  if (e != cudaSuccess || ptr == nullptr) {
+    (void)cudaGetLastError();
+    throw Error(std::string("argsort without allocation: no device address for its scratch block on device ") +
+                std::to_string(dev) + ": " + (e != cudaSuccess ? cudaGetErrorString(e) : "null address"));
+  }
+  int sm = 0;
+  AM_CUDA(cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, dev));
+  d.scratch = ptr;
+  d.hist_grid_cap = std::max(1, sm) * 8;
+  d.pass_grid_cap[0] = noalloc_pass_cap<uint32_t>(std::max(1, sm));
+  d.pass_grid_cap[1] = noalloc_pass_cap<uint64_t>(std::max(1, sm));
+  d.ready = true;
+  return d;
+}
+
+template <typename KeyT>
+void noalloc_launch_pass(const PassArgs& a, const ColView& cv, uint64_t n, int cap, cudaStream_t s) {
+  using C = PassConfig<KeyT>;
+  const uint64_t tiles = (n + NOALLOC_TILE_ROWS - 1) / NOALLOC_TILE_ROWS;
+  const int grid = int(std::min<uint64_t>(tiles, uint64_t(cap)));
+  onesweep_pass_kernel<KeyT, uint32_t, C::THREADS, C::ITEMS><<<std::max(grid, 1), C::THREADS, pass_smem<KeyT>(), s>>>(a, cv);
+  AM_CUDA(cudaGetLastError());
+}
+
+template <typename KeyT>
+void noalloc_launch_histogram(const ColView& cv, KeyStats* st, uint64_t n, int cap, cudaStream_t s) {
+  constexpr int CHUNK = HIST_THREADS * HIST_ITEMS;
+  const uint64_t chunks = (n + CHUNK - 1) / CHUNK;
+  const int grid = int(std::min<uint64_t>(chunks, uint64_t(cap)));
+  key_histogram_kernel<KeyT, HIST_THREADS, HIST_ITEMS><<<std::max(grid, 1), HIST_THREADS, 0, s>>>(cv, st, n);
+  AM_CUDA(cudaGetLastError());
+}
+
+}  // namespace
+}  // namespace rs
+
+uint64_t noalloc_max_rows() { return rs::NOALLOC_MAX_ROWS; }
+
+void argsort_noalloc(int pt, const void* values, const uint8_t* validity, int64_t offset, int64_t length,
+                     bool descending, bool nulls_first, int float_order, uint32_t* indices, cudaStream_t s) {
+  using namespace rs;
+  if (length < 0) throw invalid("negative length " + std::to_string(length));
+  if (offset < 0) throw invalid("negative offset " + std::to_string(offset));
+  if (uint64_t(length) > NOALLOC_MAX_ROWS)
+    throw invalid("argsort without allocation takes at most " + std::to_string(NOALLOC_MAX_ROWS) + " rows (" +
+                  std::to_string(length) + " given): its fixed scratch block holds no more");
+  if (float_order < 0 || float_order > 2) throw invalid("unknown float_order " + std::to_string(float_order));
+  if (length == 0) return;
+  if (!values) throw invalid("no values buffer");
+  if (!indices) throw invalid("no output index buffer");
+  const uint64_t n = uint64_t(length);
+  const int kb = pt_key_bytes(pt);
+
+  ColView cv{};
+  cv.values = pt == PT_BOOL ? values : static_cast<const void*>(static_cast<const char*>(values) + offset * pt_bytes(pt));
+  cv.valid = validity;
+  cv.valid_off = offset;
+  cv.bool_off = pt == PT_BOOL ? offset : 0;
+  cv.pt = pt;
+  cv.desc = descending ? 1 : 0;
+  cv.nulls_first = nulls_first ? 1 : 0;
+  const bool fl = pt_float(pt);
+  cv.float_order = fl ? uint8_t(float_order) : uint8_t(FO_IEEE);
+  cv.nan_cat = (fl && float_order == FO_IEEE) ? 1 : 0;
+
+  PlanArgs pa{};
+  pa.n = n;
+  pa.nkeys = 1;
+  pa.nslots = kb;
+  pa.slot_key0_first = 0;
+  pa.index_wide = 0;
+  pa.key_bytes[0] = uint8_t(kb);
+  pa.nulls_first[0] = nulls_first ? 1 : 0;
+  for (int d = 0; d < kb; d++) {
+    pa.slot_key[d] = 0;
+    pa.slot_digit[d] = int8_t(d);
+  }
+
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  NoAllocDevice& dev = noalloc_device();
+  unsigned char* base = dev.scratch;
+  NoAllocHeader* h = reinterpret_cast<NoAllocHeader*>(base);
+  unsigned char* keysA = base + NOALLOC_HEADER;
+  unsigned char* keysB = keysA + NOALLOC_KEYS;
+  uint32_t* idsA = reinterpret_cast<uint32_t*>(keysB + NOALLOC_KEYS);
+  uint32_t* idsB = reinterpret_cast<uint32_t*>(keysB + NOALLOC_KEYS + NOALLOC_IDS);
+  uint32_t* status = reinterpret_cast<uint32_t*>(keysB + NOALLOC_KEYS + 2 * NOALLOC_IDS);
+  const size_t status_bytes = ((n + NOALLOC_TILE_ROWS - 1) / NOALLOC_TILE_ROWS) * NBINS * sizeof(uint32_t);
+
+  try {
+    // The block keeps whatever the previous call left in it.
+    AM_CUDA(cudaMemsetAsync(h, 0, sizeof(NoAllocHeader), s));
+    if (kb == 8) noalloc_launch_histogram<uint64_t>(cv, &h->stats, n, dev.hist_grid_cap, s);
+    else noalloc_launch_histogram<uint32_t>(cv, &h->stats, n, dev.hist_grid_cap, s);
+    plan_kernel<<<1, 256, 0, s>>>(pa, &h->stats, &h->kplan, h->desc, &h->summary);
+    AM_CUDA(cudaGetLastError());
+    for (int sl = 0; sl < kb; sl++) {
+      AM_CUDA(cudaMemsetAsync(status, 0, status_bytes, s));
+      PassArgs a{};
+      a.desc = h->desc + sl;
+      a.kplan = &h->kplan;
+      a.keys[0] = keysA;
+      a.keys[1] = keysB;
+      a.ids[0] = idsA;
+      a.ids[1] = idsB;
+      a.final_out = indices;
+      a.status = status;
+      a.epoch = 1;
+      a.tile_counter = h->tickets + sl;
+      a.err = &h->err;
+      a.carry_ids = 1;
+      if (kb == 8) noalloc_launch_pass<uint64_t>(a, cv, n, dev.pass_grid_cap[1], s);
+      else noalloc_launch_pass<uint32_t>(a, cv, n, dev.pass_grid_cap[0], s);
+    }
+    // Wait for the sort and read its error word into a host variable.
+    uint32_t err = 0;
+    AM_CUDA(cudaMemcpyAsync(&err, &h->err, sizeof(err), cudaMemcpyDeviceToHost, s));
+    AM_CUDA(cudaStreamSynchronize(s));
+    if (err & ERR_LOOKBACK_TIMEOUT) throw Error("radix sort: a look-back wait timed out on the device");
+    if (err & ERR_BOUNDS) throw Error("radix sort: a destination fell outside its array (write skipped)");
+    if (err) throw Error("device error word " + std::to_string(err));
+  } catch (...) {
+    // Leave no work in flight on the block for the next call.
+    (void)cudaStreamSynchronize(s);
+    (void)cudaGetLastError();
+    throw;
+  }
+}
+
 }  // namespace am

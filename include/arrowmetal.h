@@ -182,6 +182,24 @@ int  am_debug_fail_alloc_after(int64_t n);
  * after one second and the call returns 1 ("look-back wait timed out"). No GPU fault is involved. */
 int  am_debug_skip_first_tile(int on);
 
+/* Argsort that allocates no device memory. No counterpart in the reference.
+ * For callers that cannot allocate on the device when they sort: a process whose device memory
+ * belongs to its own pool allocator (a framework's caching allocator, an RMM pool), or a serving loop
+ * that cannot afford cudaFree's wait for the whole device. The column and the output are the caller's
+ * device memory: `values` (Arrow values buffer; a bitmap for "b"), `validity` (bitmap, or NULL for no
+ * nulls), row i at element / bit offset + i, `format` an Arrow format string of a fixed-width type.
+ * `indices` receives `length` uint32 row numbers, the same as am_argsort_ex2 gives for that array.
+ * All scratch lives in one fixed block inside the library (about 6.1 MiB on each GPU the library is
+ * loaded on, held until exit), so one call sorts at most 262,144 rows; longer inputs return 2 with an
+ * error naming the limit. The work runs on `stream` (NULL: the default stream) on the calling thread's
+ * current device, and the call returns once it has finished there. The first call on each device
+ * looks up the block's device address and sets up the kernels; make it before any stream capture.
+ * Calls share the block: they take turns inside this process, and work that overlapped on the GPU
+ * would race on it. */
+int  am_argsort_device_noalloc(const char* format, const void* values, const void* validity,
+                               int64_t offset, int64_t length, int descending, int null_placement,
+                               int float_order, uint32_t* indices, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
