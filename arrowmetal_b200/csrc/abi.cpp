@@ -624,15 +624,14 @@ int am_sort_ex2(am_array* a, int descending, int null_placement, int float_order
       check_index_rows(a->length, "sort");
       cudaStream_t s = stream();
       use_on(a, s);
-      SortCarry carry;
-      carry.key_dst = new_array(a->pt, a->format, a->length);
+      am_array* sorted = new_array(a->pt, a->format, a->length);
       try {
-        radix_sort(k, a->length, nullptr, 4, &carry, s, &tls().last_stats);
+        radix_sort(k, a->length, nullptr, 4, sorted, s, &tls().last_stats);
       } catch (...) {
-        am::release(carry.key_dst);
+        am::release(sorted);
         throw;
       }
-      *out = carry.key_dst;
+      *out = sorted;
       return 0;
     }
     am_array* idx = argsort_keys(k, 4, "sort");

@@ -213,19 +213,12 @@ struct SortKey {
 void radix_argsort(const std::vector<SortKey>& keys, int64_t n, void* out, int index_width,
                    cudaStream_t s, am_sort_stats* stats);
 
-// Columns a sort carries with its rows (a key-value sort), so that they come out sorted without a
-// gather: src[i] (length n) is sorted into dst[i] (a new array of the same type, filled here).
-// key_dst, for a single integer (or totalOrder float) key, receives the sorted key column, rebuilt
-// from the sorted keys. `out` may be NULL when no index array is wanted.
-struct SortCarry {
-  std::vector<am_array*> src;
-  std::vector<am_array*> dst;
-  am_array* key_dst = nullptr;
-};
-constexpr int kMaxCarried = 6;
 // True when the key column can be rebuilt from its sorted keys (the key map is a bijection).
 bool key_invertible(const SortKey& k);
-void radix_sort(const std::vector<SortKey>& keys, int64_t n, void* out, int index_width, SortCarry* carry,
+// The sort engine. `out` (may be NULL) receives the index array; `key_dst` (may be NULL; one
+// key_invertible key only) receives the sorted key column, rebuilt from the sorted keys by the last
+// pass, so a sorted copy of the key needs no gather.
+void radix_sort(const std::vector<SortKey>& keys, int64_t n, void* out, int index_width, am_array* key_dst,
                 cudaStream_t s, am_sort_stats* stats);
 // Single-key argsort of a device column into a caller's uint32 array with no allocation: all
 // scratch sits in a fixed device block of the library (radix_sort.cu). Waits for its work.

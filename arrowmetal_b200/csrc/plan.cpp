@@ -250,40 +250,43 @@ Frame eval(const json::Value& node, am_plan_source** sources, int64_t nsrc, std:
       if (i < 0) throw invalid("plan: unknown sort column \"" + k.col + "\"");
       which.push_back(i);
     }
-    // One key over an unpermuted frame: every column rides through the sort with its row (a key-value
-    // sort), so the sorted table comes out of the last pass with no gather. An integer key column is
-    // rebuilt from the sorted keys instead of being carried.
+    // One integer (or totalOrder float) key over an unpermuted frame: the last pass rebuilds the sorted
+    // key column from the sorted keys while it writes the permutation, and the other columns come
+    // through one fused gather. The key column is never gathered.
     if (keys.size() == 1 && !f.perm && f.rows > 0) {
       SortKey key{f.cols[size_t(which[0])], keys[0].desc, keys[0].nulls_first, keys[0].float_order};
       if (key.float_order < 0 || key.float_order > 2) throw invalid("unknown float_order " + std::to_string(key.float_order));
-      const bool rebuild_key = key_invertible(key);
-      SortCarry carry;
-      std::vector<am_array*> outs(f.cols.size(), nullptr);
-      for (size_t c = 0; c < f.cols.size(); c++) {
-        am_array* col = f.cols[c];
-        outs[c] = new_array(col->pt, col->format, f.rows);
-        if (rebuild_key && int(c) == which[0]) {
-          carry.key_dst = outs[c];
-        } else {
-          carry.src.push_back(col);
-          carry.dst.push_back(outs[c]);
-        }
-      }
-      if (int(carry.src.size()) <= kMaxCarried) {
+      if (key_invertible(key)) {
         check_index_rows(f.rows, "sort");
+        cudaStream_t s = stream();
+        use_on(key.col, s);
+        am_array* sorted_key = new_array(key.col->pt, key.col->format, f.rows);
+        am_array* idx = new_array(PT_U32, "I", f.rows);
+        std::vector<am_array*> src, taken;
         try {
-          radix_sort({key}, f.rows, nullptr, 4, &carry, stream(), &tls().last_stats);
+          idx->values = DevBuffer::alloc(size_t(f.rows) * 4 + 16, s);
+          idx->null_count = 0;
+          idx->perm_of = f.rows;
+          idx->last_stream = s;
+          radix_sort({key}, f.rows, idx->values->ptr, 4, sorted_key, s, &tls().last_stats);
+          for (size_t c = 0; c < f.cols.size(); c++)
+            if (int(c) != which[0]) src.push_back(f.cols[c]);
+          taken.assign(src.size(), nullptr);
+          if (!src.empty() && am_take_columns(src.data(), int64_t(src.size()), idx, taken.data()) != 0)
+            throw Error(am_last_error());
         } catch (...) {
-          for (am_array* o : outs) am::release(o);
+          am::release(sorted_key);
+          am::release(idx);
           throw;
         }
+        am::release(idx);
+        size_t t = 0;
         for (size_t c = 0; c < f.cols.size(); c++) {
           am::release(f.cols[c]);
-          f.cols[c] = outs[c];
+          f.cols[c] = int(c) == which[0] ? sorted_key : taken[t++];
         }
         return f;
       }
-      for (am_array* o : outs) am::release(o);
     }
     std::vector<am_array*> kc = materialize(f, which);
     std::vector<am_array*> handles = kc;

@@ -564,13 +564,8 @@ struct PassShared {
   uint32_t scan_total;
   uint32_t ticket;
   uint16_t dig[TILE];
-  uint16_t slot_of_item[TILE];   // tile-local sorted slot of each item (payload staging)
-  union {
-    KeyT keys[TILE];
-    uint64_t pay64[TILE];        // payload staging, after the keys have left
-  };
+  KeyT keys[TILE];
   uint32_t ids[TILE];
-  uint8_t payv[TILE];
 };
 
 // Inverse of the integer and totalOrder key maps (SortSource.swift:131-190 read backwards): the value
@@ -599,15 +594,6 @@ __device__ __forceinline__ void store_width(void* base, uint64_t i, int width, u
     default: static_cast<uint8_t*>(base)[i] = uint8_t(v); break;
   }
 }
-__device__ __forceinline__ uint64_t load_width(const void* base, uint64_t i, int width) {
-  switch (width) {
-    case 8: return static_cast<const uint64_t*>(base)[i];
-    case 4: return static_cast<const uint32_t*>(base)[i];
-    case 2: return static_cast<const uint16_t*>(base)[i];
-    default: return static_cast<const uint8_t*>(base)[i];
-  }
-}
-
 template <typename KeyT, typename StatusT, int THREADS, int ITEMS>
 __global__ void __launch_bounds__(THREADS, 2)
 onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant__ ColView col) {
@@ -753,7 +739,6 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
           sm.keys[pos] = key[i];
           if (pa.carry_ids) sm.ids[pos] = id[i];
           sm.dig[pos] = uint16_t(d);
-          if (pa.npay) sm.slot_of_item[warp * (ITEMS * 32) + i * 32 + lane] = uint16_t(pos);
         }
         __syncwarp();
       }
@@ -849,69 +834,12 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
         }
       }
     }
-    // ---- payload columns: each is read at the rows' input positions, staged at their sorted slots,
-    // and written out in order like the ids (on the ids' ping-pong schedule).
-    for (int c = 0; c < pa.npay; c++) {
-      const PayCol& pc = pa.pay[c];
-      __syncthreads();   // the staging area is free
-      const void* vin = si < 0 ? pc.src : pc.buf[si];
-      const uint8_t* vvin = si < 0 ? nullptr : pc.vbuf[si];
-#pragma unroll
-      for (int i = 0; i < ITEMS; i++) {
-        if (!((ok >> i) & 1u)) continue;
-        const uint64_t g = wbase + uint64_t(i) * 32;
-        uint64_t v;
-        if (si < 0 && pc.is_bool) v = bit_at(static_cast<const uint8_t*>(pc.src), pc.src_bool_off + int64_t(g)) ? 1u : 0u;
-        else v = load_width(vin, g, pc.width);
-        const uint32_t slot = sm.slot_of_item[warp * (ITEMS * 32) + i * 32 + lane];
-        sm.pay64[slot] = v;
-        if (pc.src_valid) sm.payv[slot] = si < 0 ? (bit_at(pc.src_valid, pc.src_voff + int64_t(g)) ? 1 : 0) : vvin[g];
-      }
-      __syncthreads();
-      void* vout = di < 0 ? pc.out : pc.buf[di];
-      uint8_t* vvout = di < 0 ? pc.vout : pc.vbuf[di];
-      for (uint32_t j = threadIdx.x; j < tile_n; j += THREADS) {
-        const uint32_t d = sm.dig[j];
-        uint32_t dst = sm.gdelta[d] + j;
-        void* to = vout;
-        uint8_t* vto = vvout;
-        if (d >= RADIX) {           // a routed null / NaN row: straight to its final place
-          to = pc.out;
-          vto = pc.vout;
-        } else if (di < 0) {
-          dst += sm.desc.value_base;
-        }
-        if (dst >= out_rows) { atomicOr(pa.err, ERR_BOUNDS); continue; }
-        store_width(to, dst, pc.width, sm.pay64[j]);
-        if (pc.src_valid) vto[dst] = sm.payv[j];
-      }
-    }
     __syncthreads();
   }
 }
 
 // ------------------------------------------------------------------------------------------------
-// Kernel 4: after the passes, bytes become Arrow bitmaps (32 rows per warp ballot).
-
-// bits[w] = the 32 bytes bytes[32w .. 32w + 31] as bits; zero bytes counted into *zeros (optional).
-__global__ void __launch_bounds__(256) pack_bytes_kernel(const uint8_t* __restrict__ bytes, uint32_t* __restrict__ bits,
-                                                         uint64_t n, unsigned long long* zeros) {
-  const int lane = threadIdx.x & 31;
-  unsigned long long z = 0;
-  const uint64_t words = (n + 31) / 32;
-  for (uint64_t w = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) / 32; w < words;
-       w += uint64_t(gridDim.x) * blockDim.x / 32) {
-    const uint64_t r = w * 32 + lane;
-    const bool live = r < n;
-    const uint32_t b = __ballot_sync(0xffffffffu, live && bytes[r] != 0);
-    const uint32_t l = __ballot_sync(0xffffffffu, live);
-    if (lane == 0) {
-      bits[w] = b;
-      z += __popc(l & ~b);
-    }
-  }
-  if (zeros && lane == 0 && z) atomicAdd(zeros, z);
-}
+// Kernel 4: after the passes, the sorted key column's validity bitmap.
 
 // The sorted key column's validity: the null block of the most significant key is
 // [0, nulls) with nulls first, [n - nulls, n) with nulls last; its null count is that block's size.
@@ -1042,16 +970,14 @@ void radix_argsort(const std::vector<SortKey>& keys, int64_t n, void* out, int i
   radix_sort(keys, n, out, index_width, nullptr, s, stats);
 }
 
-void radix_sort(const std::vector<SortKey>& keys, int64_t n64, void* out, int index_width, SortCarry* carry,
+void radix_sort(const std::vector<SortKey>& keys, int64_t n64, void* out, int index_width, am_array* key_dst,
                 cudaStream_t s, am_sort_stats* stats) {
   using namespace rs;
   const int K = int(keys.size());
   if (K < 1 || K > MAX_KEYS) throw invalid("sort takes 1 to " + std::to_string(MAX_KEYS) + " key columns");
   if (n64 <= 0) return;
   const uint64_t n = uint64_t(n64);
-  const int npay = carry ? int(carry->src.size()) : 0;
-  if (npay > MAX_PAY) throw invalid("a sort carries at most " + std::to_string(MAX_PAY) + " columns");
-  if (carry && carry->key_dst && (K != 1 || !key_invertible(keys[0])))
+  if (key_dst && (K != 1 || !key_invertible(keys[0])))
     throw invalid("the sorted key column is rebuilt only for one integer or totalOrder float key");
   // Row ids move through the passes when an index is wanted or a lower key's column is gathered.
   const bool carry_ids = out != nullptr || K > 1;
@@ -1096,15 +1022,7 @@ void radix_sort(const std::vector<SortKey>& keys, int64_t n64, void* out, int in
   const size_t header = (off_sum + sizeof(SortSummary) + 255) & ~size_t(255);
   const size_t kbuf = ((n * max_kb) + 255) & ~size_t(255);
   const size_t ibuf = carry_ids ? ((n * 4) + 255) & ~size_t(255) : 0;
-  size_t pbytes = 0;
-  for (int c = 0; c < npay; c++) {
-    const am_array* src = carry->src[c];
-    const size_t w = size_t(std::max(pt_bytes(src->pt), 1));
-    pbytes += 2 * ((n * w + 255) & ~size_t(255));                       // ping-pong values
-    if (src->null_count != 0) pbytes += 3 * ((n + 255) & ~size_t(255));  // ping-pong + final validity bytes
-    if (src->pt == PT_BOOL) pbytes += (n + 255) & ~size_t(255);          // final value bytes
-  }
-  char* base = static_cast<char*>(dmalloc(header + 2 * kbuf + 2 * ibuf + pbytes, s));
+  char* base = static_cast<char*>(dmalloc(header + 2 * kbuf + 2 * ibuf, s));
   AM_CUDA(cudaMemsetAsync(base, 0, header, s));
   KeyStats* st = reinterpret_cast<KeyStats*>(base + off_stats);
   KeyPlan* kp = reinterpret_cast<KeyPlan*>(base + off_kplan);
@@ -1115,50 +1033,6 @@ void radix_sort(const std::vector<SortKey>& keys, int64_t n64, void* out, int in
   void* kbufB = base + header + kbuf;
   uint32_t* ibufA = carry_ids ? reinterpret_cast<uint32_t*>(base + header + 2 * kbuf) : nullptr;
   uint32_t* ibufB = carry_ids ? reinterpret_cast<uint32_t*>(base + header + 2 * kbuf + ibuf) : nullptr;
-  PayCol pays[MAX_PAY] = {};
-  std::vector<std::pair<uint8_t*, am_array*>> pack_values, pack_valid;   // bytes -> bitmaps afterwards
-  {
-    char* p = base + header + 2 * kbuf + 2 * ibuf;
-    auto take = [&](size_t bytes) { char* q = p; p += (bytes + 255) & ~size_t(255); return q; };
-    for (int c = 0; c < npay; c++) {
-      am_array* src = carry->src[c];
-      am_array* dst = carry->dst[c];
-      if (src->length != n64) throw length_mismatch(n64, src->length);
-      use_on(src, s);
-      PayCol& pc = pays[c];
-      pc.src = src->data();
-      pc.src_valid = src->null_count != 0 ? src->valid_bits() : nullptr;
-      pc.src_voff = src->validity_offset;
-      pc.src_bool_off = src->pt == PT_BOOL ? src->value_offset : 0;
-      pc.is_bool = src->pt == PT_BOOL ? 1 : 0;
-      pc.width = std::max(pt_bytes(src->pt), 1);
-      pc.buf[0] = take(n * pc.width);
-      pc.buf[1] = take(n * pc.width);
-      const size_t words = size_t((n + 127) / 128) * 4;
-      dst->values = DevBuffer::alloc(pc.is_bool ? words * 4 : n * pc.width + 16, s);
-      if (pc.is_bool) {
-        uint8_t* bytes = reinterpret_cast<uint8_t*>(take(n));
-        pc.out = bytes;
-        pack_values.push_back({bytes, dst});
-      } else {
-        pc.out = dst->values->ptr;
-      }
-      if (pc.src_valid) {
-        pc.vbuf[0] = reinterpret_cast<uint8_t*>(take(n));
-        pc.vbuf[1] = reinterpret_cast<uint8_t*>(take(n));
-        pc.vout = reinterpret_cast<uint8_t*>(take(n));
-        dst->validity = DevBuffer::alloc(words * 4, s);
-        dst->null_count_dev = DevBuffer::alloc(sizeof(unsigned long long), s);
-        AM_CUDA(cudaMemsetAsync(dst->null_count_dev->ptr, 0, sizeof(unsigned long long), s));
-        dst->null_count = -1;
-        pack_valid.push_back({pc.vout, dst});
-      } else {
-        dst->null_count = 0;
-      }
-      dst->last_stream = s;
-    }
-  }
-  am_array* key_dst = carry ? carry->key_dst : nullptr;
   if (key_dst) {
     const size_t words = size_t((n + 127) / 128) * 4;
     key_dst->values = DevBuffer::alloc(n * pt_bytes(keys[0].col->pt) + 16, s);
@@ -1215,8 +1089,6 @@ void radix_sort(const std::vector<SortKey>& keys, int64_t n64, void* out, int in
     a.tile_counter = tick + sl;
     a.err = sc.err;
     a.carry_ids = carry_ids ? 1 : 0;
-    a.npay = npay;
-    for (int c = 0; c < npay; c++) a.pay[c] = pays[c];
     if (key_dst) {
       a.key_out_mode = KEY_OUT_UNKEY;
       a.key_out_pt = keys[0].col->pt;
@@ -1233,19 +1105,8 @@ void radix_sort(const std::vector<SortKey>& keys, int64_t n64, void* out, int in
       else launch_pass<uint32_t, uint64_t>(a, cv, n, s);
     }
   }
-  // Bytes to bitmaps: boolean values and validity of the carried columns, the key column's validity.
+  // The sorted key column's validity: one block of nulls at one end.
   const int fin_grid = int(std::min<uint64_t>((n + 8191) / 8192, uint64_t(device().sm_count) * 4));
-  for (auto& pv : pack_values) {
-    KernelTimer kt("sort_finish", s);
-    pack_bytes_kernel<<<std::max(fin_grid, 1), 256, 0, s>>>(pv.first, static_cast<uint32_t*>(pv.second->values->ptr), n, nullptr);
-    AM_CUDA(cudaGetLastError());
-  }
-  for (auto& pv : pack_valid) {
-    KernelTimer kt("sort_finish", s);
-    pack_bytes_kernel<<<std::max(fin_grid, 1), 256, 0, s>>>(pv.first, static_cast<uint32_t*>(pv.second->validity->ptr), n,
-                                                      static_cast<unsigned long long*>(pv.second->null_count_dev->ptr));
-    AM_CUDA(cudaGetLastError());
-  }
   if (key_dst && key_dst->validity) {
     KernelTimer kt("sort_finish", s);
     key_validity_kernel<<<std::max(fin_grid, 1), 256, 0, s>>>(sum, keys[0].nulls_first ? 1 : 0,

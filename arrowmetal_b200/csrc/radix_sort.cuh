@@ -79,24 +79,6 @@ struct PlanArgs {
   int8_t slot_digit[MAX_SLOTS];             // -1: category pass
 };
 
-// A column carried through the passes beside the keys (a key-value sort): it is read from its source
-// in the first pass, moves with its row in every pass (ping-pong buffers on the ids' schedule) and is
-// written in sorted order by the last pass, so no gather is needed afterwards. Validity and boolean
-// values travel as bytes and are packed into bitmaps once the passes are done.
-constexpr int MAX_PAY = 6;
-struct PayCol {
-  const void* src;            // source row 0
-  const uint8_t* src_valid;   // NULL: no nulls
-  int64_t src_voff;
-  int64_t src_bool_off;
-  int32_t width;              // bytes moved per row: 1, 2, 4 or 8 (boolean values move as bytes)
-  int32_t is_bool;
-  void* buf[2];
-  uint8_t* vbuf[2];
-  void* out;                  // sorted values (bytes for boolean)
-  uint8_t* vout;              // sorted validity bytes, when src_valid
-};
-
 // key_out modes: the sorted key column itself, produced by inverting the key map in the last pass.
 constexpr int KEY_OUT_NONE = 0, KEY_OUT_UNKEY = 1;
 
@@ -110,15 +92,12 @@ struct PassArgs {
   uint32_t* tile_counter;
   uint32_t* err;
   uint32_t epoch;
-  int32_t carry_ids;          // 0: row ids are never stored (payload-only sorts)
-  int32_t npay;
+  int32_t carry_ids;          // 0: row ids are never stored (a sorted copy only)
   int32_t key_out_mode;
   int32_t key_out_pt;         // physical type of the key column (for the inverse map)
   int32_t key_desc;
   int32_t key_float_order;
-  int32_t pad;
   void* key_out;              // sorted key values
-  PayCol pay[MAX_PAY];
 };
 
 }  // namespace rs

@@ -2,9 +2,10 @@
 
 Workload (one step): a table of 3 columns -- key int64 uniform in [0, 2^40) with a 10% Bernoulli null
 bitmap, payload float64 ~ N(0, 1), payload int32 uniform -- sorted by key ascending, nulls last, stable,
-then all 3 columns taken through the permutation. It runs through the library's C ABI the way the
-DataFusion rule calls it: am_plan_run of select_all(sort(scan)). Inputs are seeded synthetic data of the
-benchmark's shape (numpy default_rng).
+then the table taken through the permutation (the sorted key column comes out of the sort's last pass,
+rebuilt from the sorted keys; the two payload columns through one fused gather). It runs through the
+library's C ABI the way the DataFusion rule calls it: am_plan_run of select_all(sort(scan)). Inputs are
+seeded synthetic data of the benchmark's shape (numpy default_rng).
 
   value    rows/s with the table already in HBM, timed with CUDA events on the library's stream, max
            over ranks; inputs (400 MB key column) are larger than L2, so no flush is needed.
@@ -47,6 +48,32 @@ def make_table(n, seed=SEED):
     p1 = rng.standard_normal(n)
     p2 = rng.integers(-2**31, 2**31 - 1, n, dtype=np.int32, endpoint=True)
     return key, valid, p1, p2
+
+
+def make_full_range_keys(n, seed=SEED - 1):
+    """1,000,000 int64 keys uniform over the whole int64 range, no nulls (the single-key scale case)."""
+    rng = np.random.default_rng(seed)
+    return rng.integers(np.iinfo(np.int64).min, np.iinfo(np.int64).max, n, dtype=np.int64, endpoint=True)
+
+
+def make_multikey_table(n, seed=SEED + 1):
+    """The multi-key case: key1 int32 from 200 distinct values drawn by a bounded Zipf(s=1.1) over their
+    ranks (sorted descending); key2 float64 ~ N(0, 1e6) with 0.5% each of -0.0 / +0.0 / +inf / -inf,
+    1% NaN and 5% nulls (ascending); a float64 payload ~ N(0, 1)."""
+    rng = np.random.default_rng(seed)
+    distinct = (rng.choice(2**32, 200, replace=False) - 2**31).astype(np.int32)
+    p = np.arange(1, 201, dtype=np.float64) ** -1.1
+    key1 = distinct[rng.choice(200, n, p=p / p.sum())]
+    key2 = rng.normal(0.0, 1e6, n)
+    pos = rng.permutation(n)
+    start = 0
+    for value, frac in ((-0.0, 0.005), (0.0, 0.005), (np.inf, 0.005), (-np.inf, 0.005), (np.nan, 0.01)):
+        cnt = int(n * frac)
+        key2[pos[start:start + cnt]] = value
+        start += cnt
+    valid2 = rng.random(n) >= 0.05
+    payload = rng.standard_normal(n)
+    return key1, key2, valid2, payload
 
 
 def arrow_columns(key, valid, p1, p2):
@@ -120,19 +147,33 @@ def measured_peak():
 
 
 def algorithmic_bytes(n, m, passes):
-    """Bytes each kernel must move once (the model the roofline uses; DESIGN.md states it):
-    histogram reads the key column and its bitmap; the first digit pass reads them again and writes the
-    m value rows' (key, id) plus the null rows' ids; a middle pass reads and writes m (key, id); the last
-    pass reads m (key, id) and writes m ids; the take reads the n ids, gathers and writes the 3 columns
-    (8 + 8 + 4 bytes a row) and the key's validity bit."""
+    """Bytes each kernel of one step must move once (the roofline's model, per step):
+    - histogram: reads the key column (8 B a row) and its validity bitmap;
+    - digit passes: the first reads the key column and bitmap again and writes the m value rows'
+      (key, id) and the n - m null rows' id and zeroed key straight to their final places; a middle
+      pass reads and writes m (key, id); the last reads m (key, id) and writes m ids and m rebuilt key
+      values;
+    - take: reads the n ids once and gathers and writes the two payload columns (8 + 4 B a row);
+    - sort_finish: writes the sorted key column's validity bitmap."""
     src = 8 * n + n / 8
-    hist = src
-    if passes == 1:
-        pass_bytes = src + 4 * n
+    if passes <= 1:
+        pass_bytes = src + 12 * n
     else:
-        pass_bytes = (src + 12 * m + 4 * (n - m)) + (passes - 2) * 24 * m + (12 * m + 4 * m)
-    take = 4 * n + 2 * (8 + 8 + 4) * n + 2 * n / 8
-    return {"radix_histogram": hist, "radix_onesweep_pass": pass_bytes, "take_gather": take}
+        first = src + 12 * m + 12 * (n - m)
+        pass_bytes = first + (passes - 2) * 24 * m + 24 * m
+    return {"radix_histogram": src, "radix_onesweep_pass": pass_bytes,
+            "take_gather": 4 * n + 2 * (8 + 4) * n, "sort_finish": n / 8}
+
+
+# DRAM bytes (read + write) per row of the workload, per kernel and step, from an ncu capture of this
+# benchmark at 20,000,000 rows (dram__bytes_read.sum + dram__bytes_write.sum summed over the kernel's
+# launches in one step, profiles/order_by_int64_20M_dram_traffic.md), scaled by rows.
+TRAFFIC_PER_ROW = {"radix_histogram": 8.17, "radix_onesweep_pass": 94.70, "take_gather": 173.47}
+
+
+def traffic_per_step(kernel, n):
+    b = TRAFFIC_PER_ROW.get(kernel)
+    return None if b is None else b * n
 
 
 def cpu_oracle_rate(key, valid, p1, p2, threads):
@@ -151,6 +192,21 @@ def cpu_oracle_rate(key, valid, p1, p2, threads):
         t.join()
     dt = time.perf_counter() - t0
     return len(key) / dt, dt
+
+
+def max_over_ranks(x, dist, device):
+    """The largest of every rank's `x` (a time): the whole job is as slow as its slowest replica."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(rows_per_rank, world, ms):
+    """Rows all replicas processed per second, over the slowest replica's time per step."""
+    return world * rows_per_rank / (ms / 1e3)
 
 
 def run_reference_arm(args, rank):
@@ -254,11 +310,8 @@ def main():
     ms = ev0.elapsed_time(ev1) / args.steps
     prof = am.profile_entries()
     am.profile(False)
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * n / (ms / 1e3)
+    ms = max_over_ranks(ms, dist, "cuda")
+    value = whole_job_rate(n, world, ms)
 
     # ---- roofline of the dominant kernel (the take's kernels count as one stage: their model bytes
     # are the take's, however the gather is organised)
@@ -296,11 +349,7 @@ def main():
             e2e_times.append(dt)
         d2h = sum(sum(b.size for b in r.buffers() if b is not None) for r in res.values())
         del hc, s2, out, res
-    e2e_ms = 1e3 * statistics.median(e2e_times) if e2e_times else float("nan")
-    if dist:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(1e3 * statistics.median(e2e_times) if e2e_times else float("nan"), dist, "cuda")
 
     line = {
         "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
@@ -310,9 +359,12 @@ def main():
                    "radix_passes_skipped": st["passes_skipped"], "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (400 MB key column), no flush"},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": d["gbs"], "peak": peak, "unit": "GB/s",
-                     "frac": d["gbs"] / peak, "peak_source": peak_kind, "traffic": None,
+                     "frac": d["gbs"] / peak, "peak_source": peak_kind,
+                     "traffic": traffic_per_step(dom, n), "per": "one step (all launches of the kernel in one sort)",
+                     "pipeline": {"bytes": sum(model.values()), "gbs": sum(model.values()) / (ms / 1e3) / 1e9,
+                                  "frac": sum(model.values()) / (ms / 1e3) / 1e9 / peak},
                      "per_kernel": per_kernel},
-        "e2e": {"value": world * n / (e2e_ms / 1e3), "unit": "rows/s", "ms_per_step": e2e_ms,
+        "e2e": {"value": whole_job_rate(n, world, e2e_ms), "unit": "rows/s", "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(gpu_launches),
         "clocks": clocks.summary(),

@@ -74,8 +74,9 @@ def test_plan_errors(am):
 
 @pytest.mark.parametrize("key_kind", ["int64", "uint32", "int8", "float64_ieee", "float64_total", "float32_nan_largest", "bool"])
 @pytest.mark.parametrize("desc,nulls", [(False, "last"), (True, "first")])
-def test_single_key_sort_carries_columns(am, key_kind, desc, nulls):
-    # One key: every column rides through the radix passes (integer keys rebuilt from their keys).
+def test_single_key_sort_all_columns(am, key_kind, desc, nulls):
+    # One key: integer and totalOrder keys are rebuilt from the sorted keys, the other columns gathered;
+    # other keys go through the permutation like every column.
     rng = np.random.default_rng(len(key_kind) * 7 + desc)
     n = 300_001
     fo = "ieee"
