@@ -220,6 +220,9 @@ bool key_invertible(const SortKey& k);
 // pass, so a sorted copy of the key needs no gather.
 void radix_sort(const std::vector<SortKey>& keys, int64_t n, void* out, int index_width, am_array* key_dst,
                 cudaStream_t s, am_sort_stats* stats);
+// Segmented argsort: outs[i] (a uint32 array of keys[i].col->length rows) receives the argsort of
+// keys[i], one key per array; the arrays of a key width share every launch.
+void radix_argsort_batch(const std::vector<SortKey>& keys, const std::vector<void*>& outs, cudaStream_t s);
 // Single-key argsort of a device column into a caller's uint32 array with no allocation: all
 // scratch sits in a fixed device block of the library (radix_sort.cu). Waits for its work.
 uint64_t noalloc_max_rows();

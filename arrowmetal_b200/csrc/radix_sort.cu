@@ -246,10 +246,12 @@ __device__ __forceinline__ uint64_t warp_max_u64(uint64_t v) {
 // adds its count with one atomic instead of 32, so a digit that is constant over the column (the
 // high bytes of keys drawn from [0, 2^40)) costs almost nothing.
 
+// The block's share of one column: rows [first, end) in chunks of THREADS x ITEMS rows, `stride` rows
+// apart, added into `st`.
 template <typename KeyT, int THREADS, int ITEMS>
-__global__ void __launch_bounds__(THREADS) key_histogram_kernel(const __grid_constant__ ColView col, KeyStats* __restrict__ st, uint64_t n) {
+__device__ __forceinline__ void histogram_rows(const ColView& col, KeyStats* __restrict__ st, uint64_t first,
+                                               uint64_t end, uint64_t stride) {
   constexpr int D = int(sizeof(KeyT));
-  constexpr int CHUNK = THREADS * ITEMS;
   __shared__ uint32_t sh[D * 256];
   __shared__ uint32_t s_null, s_nan, s_val;
   __shared__ unsigned long long s_max, s_min_inv;
@@ -261,7 +263,7 @@ __global__ void __launch_bounds__(THREADS) key_histogram_kernel(const __grid_con
   uint32_t n_null = 0, n_nan = 0, n_val = 0;
   KeyT vmax = 0, vmin_inv = 0;
 
-  for (uint64_t base = uint64_t(blockIdx.x) * CHUNK; base < n; base += uint64_t(gridDim.x) * CHUNK) {
+  for (uint64_t base = first; base < end; base += stride) {
     KeyT k[ITEMS];
     int cat[ITEMS];
     uint32_t row[ITEMS];
@@ -270,7 +272,7 @@ __global__ void __launch_bounds__(THREADS) key_histogram_kernel(const __grid_con
     for (int i = 0; i < ITEMS; i++) {
       const uint64_t g = base + uint64_t(warp) * (ITEMS * 32) + uint64_t(i) * 32 + lane;
       row[i] = uint32_t(g);
-      if (g < n) ok |= 1u << i;
+      if (g < end) ok |= 1u << i;
     }
     encode_rows<KeyT, ITEMS>(col, row, ok, k, cat);
     uint32_t valid_mask = 0;
@@ -335,6 +337,12 @@ __global__ void __launch_bounds__(THREADS) key_histogram_kernel(const __grid_con
   }
 }
 
+template <typename KeyT, int THREADS, int ITEMS>
+__global__ void __launch_bounds__(THREADS) key_histogram_kernel(const __grid_constant__ ColView col, KeyStats* __restrict__ st, uint64_t n) {
+  constexpr uint64_t CHUNK = uint64_t(THREADS) * ITEMS;
+  histogram_rows<KeyT, THREADS, ITEMS>(col, st, uint64_t(blockIdx.x) * CHUNK, n, uint64_t(gridDim.x) * CHUNK);
+}
+
 // ------------------------------------------------------------------------------------------------
 // Kernel 2: the plan. One block decides, from the histograms alone, which digit passes run, where
 // each pass reads and writes, and every pass's per-digit global base; the passes read it from HBM.
@@ -373,8 +381,8 @@ __device__ void block_exclusive_scan_256(const uint32_t* in, uint32_t* out, uint
 
 __device__ __forceinline__ uint64_t key_max(int bytes) { return bytes == 8 ? ~0ull : 0xFFFFFFFFull; }
 
-__global__ void __launch_bounds__(256) plan_kernel(PlanArgs a, KeyStats* __restrict__ st, KeyPlan* __restrict__ kp,
-                                                   PassDesc* __restrict__ pd, SortSummary* __restrict__ sum) {
+__device__ void plan_body(const PlanArgs& a, KeyStats* __restrict__ st, KeyPlan* __restrict__ kp,
+                          PassDesc* __restrict__ pd, SortSummary* __restrict__ sum) {
   __shared__ uint32_t s_vals[256];
   __shared__ uint32_t s_out[256];
   __shared__ uint32_t s_warp[16];
@@ -538,6 +546,58 @@ __global__ void __launch_bounds__(256) plan_kernel(PlanArgs a, KeyStats* __restr
   }
 }
 
+__global__ void __launch_bounds__(256) plan_kernel(PlanArgs a, KeyStats* __restrict__ st, KeyPlan* __restrict__ kp,
+                                                   PassDesc* __restrict__ pd, SortSummary* __restrict__ sum) {
+  plan_body(a, st, kp, pd, sum);
+}
+
+// Segmented sorts: one histogram launch and one plan launch for all arrays of a key width.
+
+// The last s in [0, count) with start[s] <= x (start ascending, start[0] = 0).
+__device__ __forceinline__ uint32_t segment_of(const uint32_t* __restrict__ start, uint32_t count, uint32_t x) {
+  uint32_t lo = 0, hi = count;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (start[mid] <= x) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Block b histograms rows [r, r + rows_per_item) of the array whose items contain b.
+template <typename KeyT, int THREADS, int ITEMS>
+__global__ void __launch_bounds__(THREADS) segmented_histogram_kernel(const SegDesc* __restrict__ segs,
+                                                                      const uint32_t* __restrict__ item_start,
+                                                                      uint32_t nsegs, uint32_t rows_per_item,
+                                                                      KeyStats* __restrict__ st) {
+  const uint32_t seg = segment_of(item_start, nsegs, blockIdx.x);
+  const ColView col = segs[seg].col;
+  const uint64_t n = segs[seg].n;
+  const uint64_t lo = uint64_t(blockIdx.x - item_start[seg]) * rows_per_item;
+  const uint64_t hi = lo + rows_per_item < n ? lo + rows_per_item : n;
+  histogram_rows<KeyT, THREADS, ITEMS>(col, st + seg, lo, hi, uint64_t(THREADS) * ITEMS);
+}
+
+// Block s plans array s: one key of `key_bytes` bytes, uint32 indices.
+__global__ void __launch_bounds__(256) segmented_plan_kernel(const SegDesc* __restrict__ segs, int key_bytes,
+                                                             KeyStats* __restrict__ st, KeyPlan* __restrict__ kp,
+                                                             PassDesc* __restrict__ pd, SortSummary* __restrict__ sum) {
+  const uint32_t seg = blockIdx.x;
+  PlanArgs a{};
+  a.n = segs[seg].n;
+  a.nkeys = 1;
+  a.nslots = key_bytes;
+  a.slot_key0_first = 0;
+  a.index_wide = 0;
+  a.key_bytes[0] = uint8_t(key_bytes);
+  a.nulls_first[0] = segs[seg].col.nulls_first;
+  for (int d = 0; d < key_bytes; d++) {
+    a.slot_key[d] = 0;
+    a.slot_digit[d] = int8_t(d);
+  }
+  plan_body(a, st + seg, kp + seg, pd + size_t(seg) * key_bytes, sum + seg);
+}
+
 // ------------------------------------------------------------------------------------------------
 // Kernel 3: one onesweep digit pass.
 //
@@ -555,6 +615,7 @@ template <typename KeyT, int THREADS, int ITEMS>
 struct PassShared {
   static constexpr int WARPS = THREADS / 32;
   static constexpr int TILE = THREADS * ITEMS;
+  SegDesc sdesc;                 // segmented passes: the tile's array
   PassDesc desc;
   uint32_t whist[WARPS][NBINS];
   uint32_t cnt[NBINS];
@@ -563,6 +624,7 @@ struct PassShared {
   uint32_t scan_warp[16];
   uint32_t scan_total;
   uint32_t ticket;
+  uint32_t seg;
   uint16_t dig[TILE];
   KeyT keys[TILE];
   uint32_t ids[TILE];
@@ -594,9 +656,9 @@ __device__ __forceinline__ void store_width(void* base, uint64_t i, int width, u
     default: static_cast<uint8_t*>(base)[i] = uint8_t(v); break;
   }
 }
-template <typename KeyT, typename StatusT, int THREADS, int ITEMS>
+template <typename KeyT, typename StatusT, int THREADS, int ITEMS, bool SEG>
 __global__ void __launch_bounds__(THREADS, 2)
-onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant__ ColView col) {
+onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant__ ColView col_arg) {
   static_assert(THREADS >= NBINS && THREADS % 32 == 0, "one thread per digit bin");
   static_assert(THREADS * ITEMS <= 65536, "tile-local ranks are 16-bit");
   using ST = Status<StatusT>;
@@ -607,34 +669,86 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
   SM& sm = *reinterpret_cast<SM*>(smem_raw);
   StatusT* __restrict__ status = static_cast<StatusT*>(pa.status);
 
-  {
-    const uint32_t* src = reinterpret_cast<const uint32_t*>(pa.desc);
-    uint32_t* dst = reinterpret_cast<uint32_t*>(&sm.desc);
-    for (int i = threadIdx.x; i < int(sizeof(PassDesc) / 4); i += THREADS) dst[i] = src[i];
+  auto copy_words = [](void* dst, const void* src, int words) {
+    for (int i = threadIdx.x; i < words; i += THREADS)
+      static_cast<uint32_t*>(dst)[i] = static_cast<const uint32_t*>(src)[i];
+  };
+  // What the pass descriptor says, for the arrays at `row_off` of the buffers.
+  uint32_t flags = 0, shift = 0, ntiles = 0;
+  uint64_t count = 0;
+  int si = -1, di = -1;
+  const KeyT* __restrict__ keys_in = nullptr;
+  const uint32_t* __restrict__ ids_in = nullptr;
+  KeyT* __restrict__ keys_out = nullptr;
+  uint32_t* __restrict__ ids_out = nullptr;
+  auto bind = [&](uint64_t row_off) {
+    flags = sm.desc.flags;
+    count = sm.desc.count;
+    shift = sm.desc.shift;
+    ntiles = uint32_t((count + TILE - 1) / TILE);
+    const int sk = sm.desc.src_keys, dk = sm.desc.dst_keys;
+    si = sm.desc.src_ids;
+    di = sm.desc.dst_ids;
+    keys_in = sk < 0 ? nullptr : static_cast<const KeyT*>(sk == 0 ? pa.keys[0] : pa.keys[1]) + row_off;
+    ids_in = si < 0 ? nullptr : (si == 0 ? pa.ids[0] : pa.ids[1]) + row_off;
+    keys_out = dk < 0 ? nullptr : static_cast<KeyT*>(dk == 0 ? pa.keys[0] : pa.keys[1]) + row_off;
+    ids_out = di < 0 ? nullptr : (di == 0 ? pa.ids[0] : pa.ids[1]) + row_off;
+  };
+  KeyPlan kplan{};
+  void* final_out = pa.final_out;
+  const ColView* colp = &col_arg;
+  if constexpr (!SEG) {
+    copy_words(&sm.desc, pa.desc, int(sizeof(PassDesc) / 4));
+    __syncthreads();
+    if (!sm.desc.active) return;
+    bind(0);
+    kplan = *pa.kplan;
   }
-  __syncthreads();
-  if (!sm.desc.active) return;
-
-  const uint32_t flags = sm.desc.flags;
-  const uint64_t count = sm.desc.count;
-  const uint32_t shift = sm.desc.shift;
-  const uint32_t ntiles = uint32_t((count + TILE - 1) / TILE);
-  const int sk = sm.desc.src_keys, si = sm.desc.src_ids, dk = sm.desc.dst_keys, di = sm.desc.dst_ids;
-  const KeyT* __restrict__ keys_in = sk < 0 ? nullptr : static_cast<const KeyT*>(sk == 0 ? pa.keys[0] : pa.keys[1]);
-  const uint32_t* __restrict__ ids_in = si < 0 ? nullptr : (si == 0 ? pa.ids[0] : pa.ids[1]);
-  KeyT* __restrict__ keys_out = dk < 0 ? nullptr : static_cast<KeyT*>(dk == 0 ? pa.keys[0] : pa.keys[1]);
-  uint32_t* __restrict__ ids_out = di < 0 ? nullptr : (di == 0 ? pa.ids[0] : pa.ids[1]);
-  const KeyPlan kplan = *pa.kplan;
   const uint32_t epoch = pa.epoch;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t lt_mask = (1u << lane) - 1u;
 
   for (;;) {
-    if (threadIdx.x == 0) sm.ticket = atomicAdd(pa.tile_counter, 1u);
+    if (threadIdx.x == 0) {
+      const uint32_t t = atomicAdd(pa.tile_counter, 1u);
+      sm.ticket = t;
+      if constexpr (SEG) {
+        // The segment of tile t: the last s with tile_start[s] <= t.
+        uint32_t lo = 0, hi = pa.nsegs;
+        if (t < pa.total_tiles) {
+          while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (pa.tile_start[mid] <= t) lo = mid;
+            else hi = mid;
+          }
+        }
+        sm.seg = lo;
+      }
+    }
     for (int b = lane; b < NBINS; b += 32) sm.whist[warp][b] = 0;
     __syncthreads();
-    const uint32_t tile = sm.ticket;
-    if (tile >= ntiles) break;
+    const uint32_t T = sm.ticket;   // the launch's tile number
+    uint32_t tile;                   // the tile within its array
+    if constexpr (SEG) {
+      if (T >= pa.total_tiles) break;
+      const uint32_t seg = sm.seg;
+      copy_words(&sm.desc, pa.desc + size_t(seg) * pa.nslots + pa.slot, int(sizeof(PassDesc) / 4));
+      copy_words(&sm.sdesc, pa.segs + seg, int(sizeof(SegDesc) / 4));
+      __syncthreads();
+      bind(sm.sdesc.row_off);
+      kplan = pa.kplan[seg];
+      colp = &sm.sdesc.col;
+      final_out = sm.sdesc.out;
+      tile = T - pa.tile_start[seg];
+      // An array whose digit is constant, or a tile past its rows (its later passes see only its value
+      // rows): nothing to do, and no tile of the array waits on it.
+      if (!sm.desc.active || tile >= ntiles) continue;
+    } else {
+      tile = T;
+      if (tile >= ntiles) break;
+    }
+    const ColView& col = *colp;
+    const uint64_t first_tile = uint64_t(T) - tile;   // status index of the array's tile 0
     const uint64_t tile_base = uint64_t(tile) * TILE;
 
     // ---- load and digit: row ids first, then every item's key load back to back
@@ -695,7 +809,7 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
         run += c;
       }
       sm.cnt[b] = run;
-      ST::store(status + uint64_t(tile) * NBINS + b, ST::make(epoch, tile == 0 ? ST_INCL : ST_AGG, run));
+      ST::store(status + uint64_t(T) * NBINS + b, ST::make(epoch, tile == 0 ? ST_INCL : ST_AGG, run));
     }
     // Tile-local digit starts: value digits in order, then the NaN and null routing bins.
     block_exclusive_scan_256(sm.cnt, sm.local, &sm.scan_total, sm.scan_warp);
@@ -757,12 +871,12 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
           StatusT st[W];
 #pragma unroll
           for (int i = 0; i < W; i++)
-            st[i] = (j - i >= 0) ? ST::load(status + uint64_t(j - i) * NBINS + b) : ST::make(epoch, ST_INCL, 0);
+            st[i] = (j - i >= 0) ? ST::load(status + (first_tile + uint64_t(j - i)) * NBINS + b) : ST::make(epoch, ST_INCL, 0);
 #pragma unroll
           for (int i = 0; i < W; i++) {
             StatusT s = st[i];
             if (!ST::ready(s, epoch)) {
-              const StatusT* p = status + uint64_t(j - i) * NBINS + b;
+              const StatusT* p = status + (first_tile + uint64_t(j - i)) * NBINS + b;
               const uint64_t t0 = globaltimer_ns();
               uint32_t polls = 0;
               for (;;) {
@@ -782,7 +896,7 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
           j -= W;
           if (j < 0) done = true;
         }
-        ST::store(status + uint64_t(tile) * NBINS + b, ST::make(epoch, ST_INCL, excl + sm.cnt[b]));
+        ST::store(status + uint64_t(T) * NBINS + b, ST::make(epoch, ST_INCL, excl + sm.cnt[b]));
       }
       sm.gdelta[b] = sm.desc.bin_base[b] + excl - sm.local[b];
     }
@@ -823,11 +937,11 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
         const uint32_t v = sm.ids[j];
         uint32_t dst = sm.gdelta[d] + j;
         if (d >= RADIX || !ids_out) {
-          if (!pa.final_out) continue;
+          if (!final_out) continue;
           if (d < RADIX) dst += sm.desc.value_base;
           if (dst >= out_rows) { atomicOr(pa.err, ERR_BOUNDS); continue; }
-          if (flags & PF_WIDE_OUT) static_cast<uint64_t*>(pa.final_out)[dst] = v;
-          else static_cast<uint32_t*>(pa.final_out)[dst] = v;
+          if (flags & PF_WIDE_OUT) static_cast<uint64_t*>(final_out)[dst] = v;
+          else static_cast<uint32_t*>(final_out)[dst] = v;
         } else {
           if (dst < buf_rows) ids_out[dst] = v;
           else atomicOr(pa.err, ERR_BOUNDS);
@@ -876,13 +990,13 @@ static size_t pass_smem() {
   return sizeof(PassShared<KeyT, C::THREADS, C::ITEMS>);
 }
 
-template <typename KeyT, typename StatusT>
+template <typename KeyT, typename StatusT, bool SEG = false>
 static int pass_blocks_per_sm() {
   using C = PassConfig<KeyT>;
   static int cached = -1;
   static std::once_flag once;
   std::call_once(once, [] {
-    auto fn = onesweep_pass_kernel<KeyT, StatusT, C::THREADS, C::ITEMS>;
+    auto fn = onesweep_pass_kernel<KeyT, StatusT, C::THREADS, C::ITEMS, SEG>;
     AM_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(pass_smem<KeyT>())));
     int b = 0;
     AM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, C::THREADS, pass_smem<KeyT>()));
@@ -908,7 +1022,7 @@ static void launch_pass(const PassArgs& pa, const ColView& cv, uint64_t n, cudaS
   const uint64_t tiles = (n + TILE - 1) / TILE;
   const int grid = int(std::min<uint64_t>(tiles, uint64_t(device().sm_count) * pass_blocks_per_sm<KeyT, StatusT>()));
   KernelTimer kt("radix_onesweep_pass", s);
-  onesweep_pass_kernel<KeyT, StatusT, C::THREADS, C::ITEMS><<<std::max(grid, 1), C::THREADS, pass_smem<KeyT>(), s>>>(pa, cv);
+  onesweep_pass_kernel<KeyT, StatusT, C::THREADS, C::ITEMS, false><<<std::max(grid, 1), C::THREADS, pass_smem<KeyT>(), s>>>(pa, cv);
   AM_CUDA(cudaGetLastError());
 }
 
@@ -1125,6 +1239,147 @@ void radix_sort(const std::vector<SortKey>& keys, int64_t n64, void* out, int in
 
 
 // ------------------------------------------------------------------------------------------------
+// Segmented (batched) argsort: the arrays of one key width share every launch.
+
+namespace rs {
+namespace {
+
+constexpr uint32_t SEG_HIST_ROWS = 32768;   // rows per histogram block
+
+template <typename KeyT>
+void sort_segment_group(const std::vector<SortKey>& keys, const std::vector<void*>& outs,
+                        const std::vector<size_t>& group, cudaStream_t s) {
+  using C = PassConfig<KeyT>;
+  constexpr uint64_t TILE = uint64_t(C::THREADS) * C::ITEMS;
+  constexpr int S = int(sizeof(KeyT));
+  const uint32_t G = uint32_t(group.size());
+
+  std::vector<SegDesc> segs(G);
+  std::vector<uint32_t> tile_start(G + 1), item_start(G + 1);
+  uint64_t rows = 0, tiles = 0, items = 0, max_n = 0;
+  for (uint32_t g = 0; g < G; g++) {
+    const SortKey& k = keys[group[g]];
+    const uint64_t n = uint64_t(k.col->length);
+    segs[g].col = make_view(k);
+    segs[g].row_off = rows;
+    segs[g].out = outs[group[g]];
+    segs[g].n = uint32_t(n);
+    tile_start[g] = uint32_t(tiles);
+    item_start[g] = uint32_t(items);
+    rows += n;
+    tiles += (n + TILE - 1) / TILE;
+    items += (n + SEG_HIST_ROWS - 1) / SEG_HIST_ROWS;
+    max_n = std::max(max_n, n);
+  }
+  tile_start[G] = uint32_t(tiles);
+  item_start[G] = uint32_t(items);
+  if (tiles >= (uint64_t(1) << 32) || items >= (uint64_t(1) << 31))
+    throw invalid("a batch of " + std::to_string(rows) + " rows is too large for one segmented sort");
+
+  // Scratch: tables (copied from the host), then statistics, plans, descriptors, summaries and
+  // tickets (zeroed), then the ping-pong key and id buffers.
+  auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
+  const size_t off_segs = 0;
+  const size_t off_tiles = up(off_segs + sizeof(SegDesc) * G);
+  const size_t off_items = up(off_tiles + sizeof(uint32_t) * (G + 1));
+  const size_t tables = up(off_items + sizeof(uint32_t) * (G + 1));
+  const size_t off_stats = tables;
+  const size_t off_kplan = up(off_stats + sizeof(KeyStats) * G);
+  const size_t off_desc = up(off_kplan + sizeof(KeyPlan) * G);
+  const size_t off_sum = up(off_desc + sizeof(PassDesc) * G * S);
+  const size_t off_tick = up(off_sum + sizeof(SortSummary) * G);
+  const size_t header = up(off_tick + sizeof(uint32_t) * S);
+  const size_t kbuf = up(rows * sizeof(KeyT)), ibuf = up(rows * 4);
+  char* base = static_cast<char*>(dmalloc(header + 2 * kbuf + 2 * ibuf, s));
+  std::vector<char> host(tables);
+  std::memcpy(host.data() + off_segs, segs.data(), sizeof(SegDesc) * G);
+  std::memcpy(host.data() + off_tiles, tile_start.data(), sizeof(uint32_t) * (G + 1));
+  std::memcpy(host.data() + off_items, item_start.data(), sizeof(uint32_t) * (G + 1));
+  copy_h2d(base, host.data(), tables, s);
+  AM_CUDA(cudaMemsetAsync(base + tables, 0, header - tables, s));
+  const SegDesc* d_segs = reinterpret_cast<const SegDesc*>(base + off_segs);
+  const uint32_t* d_tiles = reinterpret_cast<const uint32_t*>(base + off_tiles);
+  const uint32_t* d_items = reinterpret_cast<const uint32_t*>(base + off_items);
+  KeyStats* st = reinterpret_cast<KeyStats*>(base + off_stats);
+  KeyPlan* kp = reinterpret_cast<KeyPlan*>(base + off_kplan);
+  PassDesc* pd = reinterpret_cast<PassDesc*>(base + off_desc);
+  SortSummary* sum = reinterpret_cast<SortSummary*>(base + off_sum);
+  uint32_t* tick = reinterpret_cast<uint32_t*>(base + off_tick);
+  char* kbufA = base + header;
+  char* kbufB = kbufA + kbuf;
+  uint32_t* ibufA = reinterpret_cast<uint32_t*>(kbufB + kbuf);
+  uint32_t* ibufB = reinterpret_cast<uint32_t*>(kbufB + kbuf + ibuf);
+
+  {
+    KernelTimer kt("batch_histogram", s);
+    segmented_histogram_kernel<KeyT, HIST_THREADS, HIST_ITEMS><<<uint32_t(items), HIST_THREADS, 0, s>>>(
+        d_segs, d_items, G, SEG_HIST_ROWS, st);
+    AM_CUDA(cudaGetLastError());
+  }
+  {
+    KernelTimer kt("batch_plan", s);
+    segmented_plan_kernel<<<G, 256, 0, s>>>(d_segs, S, st, kp, pd, sum);
+    AM_CUDA(cudaGetLastError());
+  }
+  // Every array's counts fit 30 bits below 2^30 rows: 32-bit look-back words, zeroed per pass.
+  const bool narrow = max_n < (uint64_t(1) << 30);
+  StreamScratch& sc = stream_scratch(s, size_t(tiles) * NBINS);
+  for (int sl = 0; sl < S; sl++) {
+    if (narrow) {
+      AM_CUDA(cudaMemsetAsync(sc.status, 0, size_t(tiles) * NBINS * sizeof(uint32_t), s));
+    } else if (sc.epoch >= (1u << 30) - 1) {
+      AM_CUDA(cudaMemsetAsync(sc.status, 0, sc.status_words * sizeof(uint64_t), s));
+      sc.epoch = 0;
+    }
+    PassArgs a{};
+    a.desc = pd;
+    a.kplan = kp;
+    a.keys[0] = kbufA;
+    a.keys[1] = kbufB;
+    a.ids[0] = ibufA;
+    a.ids[1] = ibufB;
+    a.final_out = nullptr;
+    a.status = sc.status;
+    a.epoch = ++sc.epoch;
+    a.tile_counter = tick + sl;
+    a.err = sc.err;
+    a.carry_ids = 1;
+    a.segs = d_segs;
+    a.tile_start = d_tiles;
+    a.nsegs = G;
+    a.total_tiles = uint32_t(tiles);
+    a.slot = uint32_t(sl);
+    a.nslots = uint32_t(S);
+    const ColView none{};
+    KernelTimer kt("batch_pass", s);
+    if (narrow) {
+      auto fn = onesweep_pass_kernel<KeyT, uint32_t, C::THREADS, C::ITEMS, true>;
+      const int grid = int(std::min<uint64_t>(tiles, uint64_t(device().sm_count) * pass_blocks_per_sm<KeyT, uint32_t, true>()));
+      fn<<<std::max(grid, 1), C::THREADS, pass_smem<KeyT>(), s>>>(a, none);
+    } else {
+      auto fn = onesweep_pass_kernel<KeyT, uint64_t, C::THREADS, C::ITEMS, true>;
+      const int grid = int(std::min<uint64_t>(tiles, uint64_t(device().sm_count) * pass_blocks_per_sm<KeyT, uint64_t, true>()));
+      fn<<<std::max(grid, 1), C::THREADS, pass_smem<KeyT>(), s>>>(a, none);
+    }
+    AM_CUDA(cudaGetLastError());
+  }
+  dfree(base, s);
+}
+
+}  // namespace
+}  // namespace rs
+
+void radix_argsort_batch(const std::vector<SortKey>& keys, const std::vector<void*>& outs, cudaStream_t s) {
+  std::vector<size_t> g4, g8;
+  for (size_t i = 0; i < keys.size(); i++) {
+    if (keys[i].col->length <= 0) continue;
+    (pt_key_bytes(keys[i].col->pt) == 8 ? g8 : g4).push_back(i);
+  }
+  if (!g4.empty()) rs::sort_segment_group<uint32_t>(keys, outs, g4, s);
+  if (!g8.empty()) rs::sort_segment_group<uint64_t>(keys, outs, g8, s);
+}
+
+// ------------------------------------------------------------------------------------------------
 // Argsort that allocates nothing.
 //
 // Some callers cannot allocate device memory when they need a sort. A process whose device memory
@@ -1187,7 +1442,7 @@ NoAllocDevice g_noalloc[NOALLOC_MAX_DEVICES];
 template <typename KeyT>
 int noalloc_pass_cap(int sm_count) {
   using C = PassConfig<KeyT>;
-  auto fn = onesweep_pass_kernel<KeyT, uint32_t, C::THREADS, C::ITEMS>;
+  auto fn = onesweep_pass_kernel<KeyT, uint32_t, C::THREADS, C::ITEMS, false>;
   AM_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(pass_smem<KeyT>())));
   int b = 0;
   AM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, C::THREADS, pass_smem<KeyT>()));
@@ -1225,7 +1480,7 @@ void noalloc_launch_pass(const PassArgs& a, const ColView& cv, uint64_t n, int c
   using C = PassConfig<KeyT>;
   const uint64_t tiles = (n + NOALLOC_TILE_ROWS - 1) / NOALLOC_TILE_ROWS;
   const int grid = int(std::min<uint64_t>(tiles, uint64_t(cap)));
-  onesweep_pass_kernel<KeyT, uint32_t, C::THREADS, C::ITEMS><<<std::max(grid, 1), C::THREADS, pass_smem<KeyT>(), s>>>(a, cv);
+  onesweep_pass_kernel<KeyT, uint32_t, C::THREADS, C::ITEMS, false><<<std::max(grid, 1), C::THREADS, pass_smem<KeyT>(), s>>>(a, cv);
   AM_CUDA(cudaGetLastError());
 }
 

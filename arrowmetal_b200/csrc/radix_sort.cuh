@@ -79,6 +79,17 @@ struct PlanArgs {
   int8_t slot_digit[MAX_SLOTS];             // -1: category pass
 };
 
+// One array of a segmented (batched) sort. The batch's arrays of one key width share one launch per
+// digit pass; each has its own plan and pass descriptors, and its rows sit at `row_off` in the group's
+// ping-pong buffers.
+struct SegDesc {
+  ColView col;
+  uint64_t row_off;
+  void* out;                 // its uint32 index array
+  uint32_t n;
+  uint32_t pad;
+};
+
 // key_out modes: the sorted key column itself, produced by inverting the key map in the last pass.
 constexpr int KEY_OUT_NONE = 0, KEY_OUT_UNKEY = 1;
 
@@ -98,6 +109,11 @@ struct PassArgs {
   int32_t key_desc;
   int32_t key_float_order;
   void* key_out;              // sorted key values
+  // Segmented passes: `desc` and `kplan` are per-segment arrays (desc[seg * nslots + slot]); tile T of
+  // the launch belongs to the segment s with tile_start[s] <= T < tile_start[s + 1].
+  const SegDesc* segs;
+  const uint32_t* tile_start;
+  uint32_t nsegs, total_tiles, slot, nslots;
 };
 
 }  // namespace rs

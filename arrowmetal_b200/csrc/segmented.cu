@@ -4,6 +4,9 @@
 
 using namespace am;
 
+// am_argsort_batch: every array's argsort, identical to am_argsort_ex2 on that array alone, with the
+// arrays of each key width sorted together: one histogram launch, one plan launch and one launch per
+// digit pass for all of them (radix_argsort_batch), instead of a sort's ~11 launches per array.
 extern "C" int am_argsort_batch(am_array** arrays, const int* descending, const int* null_placement,
                                 const int* float_order, int64_t count, am_array** outs) {
   if (!arrays || !outs || count < 0) return 2;
@@ -11,6 +14,8 @@ extern "C" int am_argsort_batch(am_array** arrays, const int* descending, const 
   try {
     cudaStream_t s = stream();
     std::vector<am_array*> res;
+    std::vector<SortKey> keys;
+    std::vector<void*> ptrs;
     try {
       for (int64_t i = 0; i < count; i++) {
         SortKey k{arrays[i], descending ? descending[i] != 0 : false, null_placement ? null_placement[i] == 1 : false,
@@ -25,8 +30,10 @@ extern "C" int am_argsort_batch(am_array** arrays, const int* descending, const 
         o->null_count = 0;
         o->perm_of = n;
         o->last_stream = s;
-        if (n > 0) radix_argsort({k}, n, o->values->ptr, 4, s, nullptr);
+        keys.push_back(k);
+        ptrs.push_back(o->values->ptr);
       }
+      radix_argsort_batch(keys, ptrs, s);
     } catch (...) {
       for (am_array* r : res) am::release(r);
       throw;
