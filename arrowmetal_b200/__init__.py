@@ -66,6 +66,11 @@ class _ArrowDeviceArray(ctypes.Structure):
                 ("sync_event", _P), ("reserved", _I64 * 3)]
 
 
+class ServerStats(ctypes.Structure):
+    _fields_ = [(n, _I64) for n in ("requests", "solo_requests", "batches", "batched_requests", "rows",
+                                    "peak_in_flight_bytes", "in_flight_bytes", "queued")]
+
+
 class SortStats(ctypes.Structure):
     _fields_ = [("rows", _I64), ("value_rows", _I64), ("passes_run", ctypes.c_int32),
                 ("passes_skipped", ctypes.c_int32), ("kernel_us", ctypes.c_double)]
@@ -113,6 +118,12 @@ for _name, _res, _args in [
     ("am_cuda_profile_reset", _I, []),
     ("am_debug_set_max_row_index", _I, [_I64]), ("am_debug_fail_alloc_after", _I, [_I64]),
     ("am_debug_skip_first_tile", _I, [_I]),
+    ("am_server_create", _I, [_I, _I64, _I64, _PP]),
+    ("am_server_submit", _I, [_P, _P, _I64, _I64, ctypes.POINTER(ctypes.c_char_p), _IP, _IP, _IP, _I64,
+                              ctypes.POINTER(ctypes.c_char_p), _I64, ctypes.POINTER(_I64)]),
+    ("am_server_wait", _I, [_P, _I64, _PP, ctypes.POINTER(ctypes.c_double)]),
+    ("am_server_get_stats", _I, [_P, ctypes.POINTER(ServerStats)]),
+    ("am_server_release", _I, [_P]),
 ]:
     _sig(_name, _res, _args)
 
@@ -434,6 +445,78 @@ def run_plan(plan, sources):
         return out
     finally:
         _lib.am_plan_result_release(r)
+
+
+def _plan_result_columns(r):
+    try:
+        out = {}
+        for i in range(_lib.am_plan_column_count(r)):
+            h = _P()
+            _check(_lib.am_plan_column(r, i, ctypes.byref(h)))
+            out[_lib.am_plan_column_name(r, i).decode()] = MetalArray(h)
+        return out
+    finally:
+        _lib.am_plan_result_release(r)
+
+
+class Server:
+    """Sort server over tables resident in HBM (am_server_*): requests are admitted by their HBM
+    footprint under `hbm_cap_bytes`, run by `workers` threads with a CUDA stream each, and single-key
+    requests of at most `batch_rows` rows waiting together are sorted as one segmented batch.
+
+    submit(source, offset, length, keys, payload) sorts rows [offset, offset + length) of a PlanSource
+    by `keys` and takes `payload`; wait(ticket) returns ({name: MetalArray}, latency in ms)."""
+
+    def __init__(self, workers=4, hbm_cap_bytes=120 * 10**9, batch_rows=1 << 20):
+        self._h = _P()
+        _check(_lib.am_server_create(int(workers), int(hbm_cap_bytes), int(batch_rows), ctypes.byref(self._h)))
+        self._sources = {}
+
+    def submit(self, source, offset, length, keys, payload=(), descending=None, null_placement="at_end",
+               float_order="ieee"):
+        keys = [keys] if isinstance(keys, str) else list(keys)
+        n = len(keys)
+        desc = descending if descending is not None else [False] * n
+        if isinstance(desc, bool):
+            desc = [desc] * n
+        kn = (ctypes.c_char_p * n)(*[k.encode() for k in keys])
+        d = (ctypes.c_int * n)(*[1 if x else 0 for x in desc])
+        p = (ctypes.c_int * n)(*[_index_of(NULL_PLACEMENT, x, "null_placement")
+                                 for x in _per_key(null_placement, n, "null_placement")])
+        f = (ctypes.c_int * n)(*[_index_of(FLOAT_ORDERS, x, "float_order") for x in _per_key(float_order, n, "float_order")])
+        payload = list(payload)
+        pn = (ctypes.c_char_p * max(len(payload), 1))(*[c.encode() for c in payload])
+        t = _I64()
+        self._sources[id(source)] = source          # the table outlives its requests
+        _check(_lib.am_server_submit(self._h, source._h, int(offset), int(length), kn, d, p, f, n, pn,
+                                     len(payload), ctypes.byref(t)))
+        return t.value
+
+    def wait(self, ticket):
+        r = _P()
+        lat = ctypes.c_double()
+        _check(_lib.am_server_wait(self._h, int(ticket), ctypes.byref(r), ctypes.byref(lat)))
+        return _plan_result_columns(r), lat.value
+
+    def stats(self):
+        s = ServerStats()
+        _check(_lib.am_server_get_stats(self._h, ctypes.byref(s)))
+        return {name: getattr(s, name) for name, _ in ServerStats._fields_}
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _lib.am_server_release(h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        self.close()
 
 
 def explain_plan(plan, sources):

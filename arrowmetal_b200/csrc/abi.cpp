@@ -225,6 +225,7 @@ am_array* slice_of(am_array* a, int64_t offset, int64_t length) {
   o->validity = a->validity;
   o->validity_offset = a->validity_offset + offset;
   o->last_stream = a->last_stream;
+  o->shared_read = a->shared_read;
   if (a->perm_of >= 0) o->perm_of = a->perm_of;
   if (a->null_count == 0 || !a->validity) {
     o->null_count = 0;
@@ -237,7 +238,7 @@ am_array* slice_of(am_array* a, int64_t offset, int64_t length) {
     std::vector<uint8_t> h(size_t(std::max<int64_t>(nb, 1)));
     if (a->null_count < 0) resolve_null_count(a);
     if (!a->validity) { o->null_count = 0; o->validity.reset(); return o; }
-    cudaStream_t s = a->last_stream ? a->last_stream : stream();
+    cudaStream_t s = (a->last_stream && !a->shared_read) ? a->last_stream : stream();
     AM_CUDA(cudaMemcpyAsync(h.data(), static_cast<const uint8_t*>(a->validity->ptr) + o->validity_offset / 8, size_t(nb),
                             cudaMemcpyDeviceToHost, s));
     AM_CUDA(cudaStreamSynchronize(s));

@@ -175,6 +175,10 @@ struct am_array {
   cudaStream_t last_stream = nullptr;
   // >= 0 when this is an index array this library produced: no nulls and every index < perm_of.
   int64_t perm_of = -1;
+  // Settled and read by many streams at once (a served table's columns): its contents are complete,
+  // so readers neither wait for nor record a stream; its buffers outlive every reader, which holds
+  // them through its own slices.
+  bool shared_read = false;
 
   const void* data() const {
     if (!values) return nullptr;

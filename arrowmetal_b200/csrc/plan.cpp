@@ -4,35 +4,17 @@
 // optionally with_columns below it and limit above it).
 //
 // Grammar and key options follow the reference's PlanJSON (Sources/ArrowMetal/Engine/PlanJSON.swift:
-// 80-140) and include/arrowmetal.h:1369-1404. A one-key sort of a plain frame carries every column
-// through its radix passes (a key-value sort), so the sorted table leaves the last pass with no
-// gather; other sorts yield a row permutation, a limit slices it, a select picks columns, and only
-// the columns the plan returns are gathered, in one fused take launch.
+// 80-140) and include/arrowmetal.h:1369-1404. A one-key sort of a plain frame on an integer (or
+// totalOrder float) key gets its sorted key column from the sort's last pass and the other columns
+// from one fused gather; other sorts yield a row permutation, a limit slices it, a select picks
+// columns, and only the columns the plan returns are gathered, in one fused take launch.
 #include <sstream>
 
 #include "am_internal.h"
 #include "json.h"
+#include "plan_types.h"
 
 using namespace am;
-
-struct am_plan_source_t {
-  std::string name;
-  std::vector<std::string> names;
-  std::vector<am_array*> cols;
-  int64_t rows = 0;
-  ~am_plan_source_t() {
-    for (am_array* c : cols) am::release(c);
-  }
-};
-
-struct am_plan_result_t {
-  std::vector<std::string> names;
-  std::vector<am_array*> cols;
-  int64_t rows = 0;
-  ~am_plan_result_t() {
-    for (am_array* c : cols) am::release(c);
-  }
-};
 
 namespace {
 

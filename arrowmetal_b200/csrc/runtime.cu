@@ -526,7 +526,7 @@ void release(am_array* a) {
 }
 
 void use_on(am_array* a, cudaStream_t s) {
-  if (!a) return;
+  if (!a || a->shared_read) return;
   if (a->last_stream && a->last_stream != s) {
     cudaEvent_t e;
     AM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));

@@ -1,0 +1,384 @@
+// Sort server: sort requests over tables resident in HBM, admitted by their HBM footprint and batched
+// as they arrive (continuous batching).
+//
+// A request sorts rows [offset, offset + length) of a resident table by one or more key columns and
+// returns the sorted keys with the payload columns taken through the same permutation -- the ORDER BY
+// of the plan entry points (include/arrowmetal.h:1419-1433), addressed to a slice of a table. Worker
+// threads each own a CUDA stream. A free worker takes, in arrival order, the first queued request
+// whose footprint fits under the admission cap beside the work already on the GPU; a single-key request
+// of at most `batch_rows` rows takes every other such request that fits with it, and they are sorted as
+// one segmented batch (am_argsort_batch) followed by one fused gather per request. Larger and
+// multi-key requests run alone through am_plan_run. Requests that arrive while others run are picked
+// up by the next free worker, so their work overlaps on the device.
+//
+// The reference has no server: its callers make one call per query. Every result equals the same
+// request run alone through am_plan_run.
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <sstream>
+#include <thread>
+#include <unordered_map>
+
+#include "am_internal.h"
+#include "plan_types.h"
+
+using namespace am;
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct ServeRequest {
+  int64_t id = 0;
+  am_plan_source* table = nullptr;
+  int64_t offset = 0, length = 0;
+  std::vector<int> key_cols, pay_cols;          // column positions in the table
+  std::vector<int> desc, nulls_first, float_order;
+  int64_t footprint = 0;
+  bool batchable = false;
+  Clock::time_point arrival, finished;
+  bool done = false;
+  int rc = 0;
+  std::string error;
+  am_plan_result* result = nullptr;
+};
+using ReqPtr = std::shared_ptr<ServeRequest>;
+
+std::string json_str(const std::string& s) {
+  std::string o = "\"";
+  for (char c : s) {
+    if (c == '"' || c == '\\') o += '\\';
+    o += c;
+  }
+  return o + "\"";
+}
+
+// select(sort(select(limit(scan)))): the slice, only the columns the request returns, sorted.
+std::string plan_of(const ServeRequest& r) {
+  const am_plan_source_t& t = *r.table;
+  std::ostringstream sel, by;
+  std::vector<int> cols = r.key_cols;
+  cols.insert(cols.end(), r.pay_cols.begin(), r.pay_cols.end());
+  for (size_t i = 0; i < cols.size(); i++) {
+    const std::string& n = t.names[size_t(cols[i])];
+    const std::string e = "[" + json_str(n) + "," + json_str("(col \"" + n + "\")") + "]";
+    sel << (i ? "," : "") << e;
+  }
+  for (size_t k = 0; k < r.key_cols.size(); k++) {
+    static const char* orders[] = {"ieee", "total", "nan_largest"};
+    by << (k ? "," : "") << "[" << json_str(t.names[size_t(r.key_cols[k])]) << "," << (r.desc[k] ? "true" : "false")
+       << ",{\"nulls\":\"" << (r.nulls_first[k] ? "first" : "last") << "\",\"float_order\":\""
+       << orders[r.float_order[k]] << "\"}]";
+  }
+  std::ostringstream p;
+  p << "{\"op\":\"select\",\"exprs\":[" << sel.str() << "],\"input\":{\"op\":\"sort\",\"by\":[" << by.str()
+    << "],\"input\":{\"op\":\"select\",\"exprs\":[" << sel.str() << "],\"input\":{\"op\":\"limit\",\"count\":"
+    << r.length << ",\"offset\":" << r.offset << ",\"input\":{\"op\":\"scan\",\"source\":" << json_str(t.name)
+    << "}}}}}";
+  return p.str();
+}
+
+int64_t width_of(const am_array* a) { return std::max(pt_bytes(a->pt), 1); }
+
+}  // namespace
+
+struct am_server_t {
+  std::mutex mu;
+  std::mutex settle_mu;            // settling a table's columns, once, for shared reading
+  std::condition_variable work_cv, done_cv;
+  std::deque<ReqPtr> queue;
+  std::unordered_map<int64_t, ReqPtr> requests;
+  int64_t next_id = 1;
+  int64_t cap = 0, batch_rows = 0;
+  int64_t in_flight = 0;
+  bool stop = false;
+  am_server_stats stats{};
+  std::vector<std::thread> workers;
+
+  void run_worker();
+  std::vector<ReqPtr> next_unit(int64_t* footprint);
+  void execute(std::vector<ReqPtr>& unit);
+};
+
+// Under the lock: the first queued request that fits, with the batchable requests that fit beside it.
+std::vector<ReqPtr> am_server_t::next_unit(int64_t* footprint) {
+  std::vector<ReqPtr> unit;
+  int64_t fp = 0, rows = 0;
+  for (auto it = queue.begin(); it != queue.end(); ++it) {
+    const ReqPtr& r = *it;
+    if (in_flight > 0 && in_flight + r->footprint > cap) continue;
+    unit.push_back(r);
+    fp = r->footprint;
+    rows = r->length;
+    queue.erase(it);
+    break;
+  }
+  if (!unit.empty() && unit[0]->batchable) {
+    for (auto it = queue.begin(); it != queue.end();) {
+      const ReqPtr& r = *it;
+      if (r->batchable && rows + r->length <= batch_rows * 4 && in_flight + fp + r->footprint <= cap) {
+        fp += r->footprint;
+        rows += r->length;
+        unit.push_back(r);
+        it = queue.erase(it);
+      } else {
+        ++it;
+      }
+    }
+  }
+  *footprint = fp;
+  return unit;
+}
+
+void am_server_t::execute(std::vector<ReqPtr>& unit) {
+  auto fail_all = [&](int rc, const std::string& msg) {
+    for (auto& r : unit) {
+      if (r->result) {
+        am_plan_result_release(r->result);
+        r->result = nullptr;
+      }
+      r->rc = rc;
+      r->error = msg;
+    }
+  };
+  if (unit.size() == 1 && !unit[0]->batchable) {
+    ServeRequest& r = *unit[0];
+    const std::string plan = plan_of(r);
+    am_plan_source* src = r.table;
+    int rc = am_plan_run(plan.c_str(), &src, 1, 0, &r.result);
+    if (rc == 0) rc = am_cuda_synchronize();
+    if (rc != 0) fail_all(rc, am_last_error());
+    return;
+  }
+  // A segmented batch: slices of every request's key, one am_argsort_batch, one fused gather each.
+  std::vector<am_array*> keys, idx(unit.size(), nullptr), temps;
+  std::vector<int> desc, np, fo;
+  auto cleanup = [&] {
+    for (am_array* a : temps) am_release(a);
+    for (am_array* a : idx) if (a) am_release(a);
+  };
+  int rc = 0;
+  for (auto& r : unit) {
+    am_array* k = nullptr;
+    rc = am_slice(r->table->cols[size_t(r->key_cols[0])], r->offset, r->length, &k);
+    if (rc != 0) break;
+    temps.push_back(k);
+    keys.push_back(k);
+    desc.push_back(r->desc[0]);
+    np.push_back(r->nulls_first[0]);
+    fo.push_back(r->float_order[0]);
+  }
+  if (rc == 0) rc = am_argsort_batch(keys.data(), desc.data(), np.data(), fo.data(), int64_t(keys.size()), idx.data());
+  for (size_t i = 0; rc == 0 && i < unit.size(); i++) {
+    ServeRequest& r = *unit[i];
+    std::vector<am_array*> cols{keys[i]};
+    for (int c : r.pay_cols) {
+      am_array* p = nullptr;
+      rc = am_slice(r.table->cols[size_t(c)], r.offset, r.length, &p);
+      if (rc != 0) break;
+      temps.push_back(p);
+      cols.push_back(p);
+    }
+    if (rc != 0) break;
+    auto* res = new am_plan_result_t();
+    res->rows = r.length;
+    res->cols.assign(cols.size(), nullptr);
+    rc = am_take_columns(cols.data(), int64_t(cols.size()), idx[i], res->cols.data());
+    if (rc != 0) {
+      res->cols.clear();
+      delete res;
+      break;
+    }
+    res->names.push_back(r.table->names[size_t(r.key_cols[0])]);
+    for (int c : r.pay_cols) res->names.push_back(r.table->names[size_t(c)]);
+    r.result = res;
+  }
+  if (rc == 0) rc = am_cuda_synchronize();
+  if (rc != 0) fail_all(rc, am_last_error());
+  cleanup();
+}
+
+void am_server_t::run_worker() {
+  for (;;) {
+    std::vector<ReqPtr> unit;
+    int64_t fp = 0;
+    {
+      std::unique_lock<std::mutex> lk(mu);
+      work_cv.wait(lk, [&] {
+        if (stop && queue.empty()) return true;
+        for (auto& r : queue)
+          if (in_flight == 0 || in_flight + r->footprint <= cap) return true;
+        return false;
+      });
+      if (stop && queue.empty()) return;
+      unit = next_unit(&fp);
+      if (unit.empty()) continue;
+      in_flight += fp;
+      stats.peak_in_flight_bytes = std::max(stats.peak_in_flight_bytes, in_flight);
+      if (unit.size() > 1 || unit[0]->batchable) {
+        stats.batches++;
+        stats.batched_requests += int64_t(unit.size());
+      } else {
+        stats.solo_requests++;
+      }
+    }
+    execute(unit);
+    const Clock::time_point t = Clock::now();
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      in_flight -= fp;
+      for (auto& r : unit) {
+        r->finished = t;
+        r->done = true;
+        stats.requests++;
+        if (r->rc == 0) stats.rows += r->length;
+      }
+    }
+    done_cv.notify_all();
+    work_cv.notify_all();
+  }
+}
+
+extern "C" {
+
+int am_server_create(int workers, int64_t hbm_cap_bytes, int64_t batch_rows, am_server** out) {
+  if (!out || workers < 1 || workers > 64 || hbm_cap_bytes <= 0 || batch_rows < 0) return 2;
+  try {
+    (void)device();
+    auto* s = new am_server_t();
+    s->cap = hbm_cap_bytes;
+    s->batch_rows = batch_rows;
+    for (int i = 0; i < workers; i++) s->workers.emplace_back([s] { s->run_worker(); });
+    *out = s;
+    return 0;
+  } catch (const Error& e) {
+    set_last_error(e.what());
+    return e.code;
+  } catch (const std::exception& e) {
+    set_last_error(e.what());
+    return 1;
+  }
+}
+
+int am_server_submit(am_server* srv, am_plan_source* table, int64_t offset, int64_t length, const char** keys,
+                     const int* descending, const int* null_placement, const int* float_order, int64_t nkeys,
+                     const char** payload, int64_t npayload, int64_t* ticket) {
+  if (!srv || !table || !keys || nkeys < 1 || npayload < 0 || (npayload > 0 && !payload) || !ticket) return 2;
+  if (offset < 0 || length < 0 || offset + length > table->rows) {
+    set_last_error("Invalid ArrowArray: request rows [" + std::to_string(offset) + ", " +
+                   std::to_string(offset + length) + ") outside the table's " + std::to_string(table->rows));
+    return 2;
+  }
+  try {
+    auto r = std::make_shared<ServeRequest>();
+    r->table = table;
+    r->offset = offset;
+    r->length = length;
+    auto find = [&](const char* name) {
+      if (!name) throw invalid("null column name");
+      const std::string n(name);
+      if (n.find('"') != std::string::npos || n.find('\\') != std::string::npos)
+        throw invalid("column names with quotes or backslashes are not served: " + n);
+      for (size_t i = 0; i < table->names.size(); i++) if (table->names[i] == n) return int(i);
+      throw invalid("unknown column \"" + n + "\" in table \"" + table->name + "\"");
+    };
+    int64_t bytes_per_row = 12;                 // ids (two buffers) and the index array
+    for (int64_t k = 0; k < nkeys; k++) {
+      const int c = find(keys[k]);
+      r->key_cols.push_back(c);
+      r->desc.push_back(descending && descending[k] ? 1 : 0);
+      r->nulls_first.push_back(null_placement && null_placement[k] == 1 ? 1 : 0);
+      const int fo = float_order ? float_order[k] : 0;
+      if (fo < 0 || fo > 2) throw invalid("unknown float_order " + std::to_string(fo));
+      r->float_order.push_back(fo);
+      const am_array* col = table->cols[size_t(c)];
+      bytes_per_row += 2 * pt_key_bytes(col->pt) + width_of(col);
+    }
+    for (int64_t p = 0; p < npayload; p++) {
+      const int c = find(payload[p]);
+      r->pay_cols.push_back(c);
+      bytes_per_row += width_of(table->cols[size_t(c)]);
+    }
+    r->footprint = length * bytes_per_row + (int64_t(1) << 20);
+    r->batchable = nkeys == 1 && length <= srv->batch_rows;
+    // A served table is read by many streams at once: settle it once (its producer done, null
+    // counts known) and let readers skip stream tracking.
+    std::lock_guard<std::mutex> settle(srv->settle_mu);
+    for (am_array* col : table->cols) {
+      if (col->shared_read) continue;
+      if (col->last_stream) AM_CUDA(cudaStreamSynchronize(col->last_stream));
+      resolve_null_count(col);
+      col->shared_read = true;
+    }
+    {
+      std::lock_guard<std::mutex> lk(srv->mu);
+      if (srv->stop) throw Error("the server is shutting down");
+      r->id = srv->next_id++;
+      r->arrival = Clock::now();
+      srv->requests[r->id] = r;
+      srv->queue.push_back(r);
+      *ticket = r->id;
+    }
+    srv->work_cv.notify_one();
+    return 0;
+  } catch (const Error& e) {
+    set_last_error(e.what());
+    return e.code;
+  } catch (const std::exception& e) {
+    set_last_error(e.what());
+    return 1;
+  }
+}
+
+int am_server_wait(am_server* srv, int64_t ticket, am_plan_result** out, double* latency_ms) {
+  if (!srv || !out) return 2;
+  ReqPtr r;
+  {
+    std::unique_lock<std::mutex> lk(srv->mu);
+    auto it = srv->requests.find(ticket);
+    if (it == srv->requests.end()) {
+      set_last_error("unknown request " + std::to_string(ticket));
+      return 2;
+    }
+    r = it->second;
+    srv->done_cv.wait(lk, [&] { return r->done; });
+    srv->requests.erase(it);
+  }
+  if (latency_ms) latency_ms[0] = std::chrono::duration<double, std::milli>(r->finished - r->arrival).count();
+  if (r->rc != 0) {
+    set_last_error(r->error);
+    *out = nullptr;
+    return r->rc;
+  }
+  *out = r->result;
+  r->result = nullptr;
+  return 0;
+}
+
+int am_server_get_stats(am_server* srv, am_server_stats* out) {
+  if (!srv || !out) return 2;
+  std::lock_guard<std::mutex> lk(srv->mu);
+  *out = srv->stats;
+  out->in_flight_bytes = srv->in_flight;
+  out->queued = int64_t(srv->queue.size());
+  return 0;
+}
+
+int am_server_release(am_server* srv) {
+  if (!srv) return 2;
+  {
+    std::lock_guard<std::mutex> lk(srv->mu);
+    srv->stop = true;
+  }
+  srv->work_cv.notify_all();
+  for (auto& t : srv->workers) t.join();
+  for (auto& kv : srv->requests)
+    if (kv.second->result) am_plan_result_release(kv.second->result);
+  delete srv;
+  return 0;
+}
+
+}  // extern "C"

@@ -182,6 +182,38 @@ int  am_debug_fail_alloc_after(int64_t n);
  * after one second and the call returns 1 ("look-back wait timed out"). No GPU fault is involved. */
 int  am_debug_skip_first_tile(int on);
 
+/* Sort server: continuous batching of sort requests over tables resident in HBM. No counterpart in
+ * the reference, whose callers make one call per query (include/arrowmetal.h:1419-1433 is the call a
+ * request stands for). A request sorts rows [offset, offset + length) of a plan source by `nkeys`
+ * key columns (options per key as in am_lexsort_ex2) and returns an am_plan_result holding the sorted
+ * key columns followed by the `npayload` payload columns taken through the same permutation: the
+ * same result am_plan_run gives for select(sort(limit(scan))). `workers` threads, each with its own
+ * CUDA stream, take requests in arrival order as long as their estimated HBM footprint fits under
+ * `hbm_cap_bytes` beside the work in flight; single-key requests of at most `batch_rows` rows that
+ * are waiting together are sorted as one segmented batch. The table must stay alive until every
+ * request on it has been waited for. am_server_wait blocks until the request is done, hands its
+ * result to the caller and gives the latency from submission to completion. */
+typedef struct am_server_t am_server;
+typedef struct am_server_stats {
+  int64_t requests;               /* completed */
+  int64_t solo_requests;          /* run alone through the plan path */
+  int64_t batches;                /* segmented batches run */
+  int64_t batched_requests;       /* requests served inside those batches */
+  int64_t rows;                   /* rows of the completed, successful requests */
+  int64_t peak_in_flight_bytes;   /* largest admitted footprint on the GPU at once */
+  int64_t in_flight_bytes;
+  int64_t queued;
+} am_server_stats;
+int  am_server_create(int workers, int64_t hbm_cap_bytes, int64_t batch_rows, am_server** out);
+int  am_server_submit(am_server* server, am_plan_source* table, int64_t offset, int64_t length,
+                      const char** keys, const int* descending, const int* null_placement,
+                      const int* float_order, int64_t nkeys, const char** payload, int64_t npayload,
+                      int64_t* ticket);
+int  am_server_wait(am_server* server, int64_t ticket, am_plan_result** out, double* latency_ms);
+int  am_server_get_stats(am_server* server, am_server_stats* out);
+/* Finishes the queued requests, stops the workers and frees the server. */
+int  am_server_release(am_server* server);
+
 /* Argsort that allocates no device memory. No counterpart in the reference.
  * For callers that cannot allocate on the device when they sort: a process whose device memory
  * belongs to its own pool allocator (a framework's caching allocator, an RMM pool), or a serving loop

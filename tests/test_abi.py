@@ -127,8 +127,20 @@ def test_no_device_fails_loudly():
         assert name.startswith("unavailable")
         with pytest.raises(am.ArrowMetalError, match="CUDA"):
             am.MetalArray.from_arrow([1, 2, 3])
+        with pytest.raises(am.ArrowMetalError, match="CUDA"):
+            am.Server(workers=2)
     else:
         pytest.skip("a GPU is present")
+
+
+def test_server_rejects_bad_arguments(lib):
+    import ctypes
+    out = ctypes.c_void_p()
+    i64 = ctypes.c_int64
+    assert lib.am_server_create(0, i64(1 << 30), i64(0), ctypes.byref(out)) == 2
+    assert lib.am_server_create(2, i64(0), i64(0), ctypes.byref(out)) == 2
+    assert lib.am_server_wait(None, i64(1), ctypes.byref(out), None) == 2
+    assert lib.am_server_release(None) == 2
 
 
 def _has_gpu():

@@ -1,0 +1,125 @@
+"""The sort server (am_server_*): each request's result in a mix of concurrent, batched requests equals
+the same request run alone through am_plan_run; admission keeps the footprint in flight under the cap;
+bad requests fail at submission with the library's error convention."""
+import json
+
+import numpy as np
+import pyarrow as pa
+import pytest
+
+from conftest import build_array
+
+pytestmark = pytest.mark.gpu
+
+N = 600_000
+
+
+def table(am, seed=5):
+    rng = np.random.default_rng(seed)
+    k64 = build_array("int64", rng.integers(-2**40, 2**40, N, dtype=np.int64), rng.random(N) > 0.05)
+    fv = rng.standard_normal(N)
+    fv[rng.random(N) < 0.02] = np.nan
+    fv[rng.random(N) < 0.01] = -0.0
+    kf = build_array("double", fv, rng.random(N) > 0.03)
+    k32 = pa.array(rng.integers(0, 300, N).astype(np.int32))
+    p1 = pa.array(rng.standard_normal(N))
+    p2 = pa.array(rng.integers(-2**31, 2**31 - 1, N, dtype=np.int32, endpoint=True))
+    cols = {"k64": k64, "kf": kf, "k32": k32, "p1": p1, "p2": p2}
+    return am.PlanSource("t", {k: am.MetalArray.from_arrow(v) for k, v in cols.items()})
+
+
+def plan_alone(offset, length, keys, desc, nulls, orders, payload):
+    cols = list(keys) + list(payload)
+    sel = [[c, f'(col "{c}")'] for c in cols]
+    by = [[k, d, {"nulls": "first" if n == "at_start" else "last", "float_order": o}]
+          for k, d, n, o in zip(keys, desc, nulls, orders)]
+    return json.dumps({"op": "select", "exprs": sel, "input": {"op": "sort", "by": by, "input": {
+        "op": "select", "exprs": sel, "input": {"op": "limit", "count": length, "offset": offset,
+                                                "input": {"op": "scan", "source": "t"}}}}})
+
+
+def same(a, b):
+    """Equal validity and equal value bits at every valid row."""
+    if len(a) != len(b) or a.type != b.type or a.null_count != b.null_count:
+        return False
+    va = np.asarray(a.is_valid().to_numpy(zero_copy_only=False))
+    vb = np.asarray(b.is_valid().to_numpy(zero_copy_only=False))
+    if not np.array_equal(va, vb):
+        return False
+    view = {1: np.uint8, 2: np.uint16, 4: np.uint32, 8: np.uint64}[a.type.bit_width // 8]
+    xa = np.frombuffer(a.buffers()[1], dtype=view)[a.offset:a.offset + len(a)]
+    xb = np.frombuffer(b.buffers()[1], dtype=view)[b.offset:b.offset + len(b)]
+    return np.array_equal(xa[va], xb[vb])
+
+
+def random_requests(rng, count):
+    reqs = []
+    for _ in range(count):
+        length = int(min(N, round(10 ** rng.uniform(0, np.log10(N)))))
+        offset = int(rng.integers(0, N - length + 1))
+        kind = rng.integers(4)
+        if kind == 0:
+            keys, orders = ["k64"], ["ieee"]
+        elif kind == 1:
+            keys, orders = ["kf"], [["ieee", "total", "nan_largest"][rng.integers(3)]]
+        elif kind == 2:
+            keys, orders = ["k32", "k64"], ["ieee", "ieee"]
+        else:
+            keys, orders = ["k32", "kf"], ["ieee", "total"]
+        desc = [bool(rng.integers(2)) for _ in keys]
+        nulls = [["at_end", "at_start"][rng.integers(2)] for _ in keys]
+        reqs.append((offset, length, keys, desc, nulls, orders, ["p1", "p2"]))
+    return reqs
+
+
+def test_mix_equals_alone(am):
+    src = table(am)
+    rng = np.random.default_rng(9)
+    reqs = random_requests(rng, 80)
+    alone = [am.run_plan(plan_alone(*r), [src]) for r in reqs]
+    with am.Server(workers=4, hbm_cap_bytes=8 << 30, batch_rows=1 << 17) as srv:
+        tickets = [srv.submit(src, o, n, k, p, descending=d, null_placement=nl, float_order=fo)
+                   for (o, n, k, d, nl, fo, p) in reqs]
+        results = [srv.wait(t) for t in tickets]
+        stats = srv.stats()
+    assert stats["requests"] == len(reqs)
+    assert stats["batches"] > 0 and stats["solo_requests"] > 0
+    for r, want, (got, latency) in zip(reqs, alone, results):
+        assert latency >= 0
+        assert list(got) == list(want), r
+        for name in want:
+            assert same(got[name].to_arrow(), want[name].to_arrow()), (r, name)
+
+
+def test_admission_keeps_footprint_under_cap(am):
+    src = table(am, seed=6)
+    # Each 200,000-row request needs about 200,000 x 45 B + 1 MiB (~10 MB); a 25 MB cap admits two.
+    cap = 25_000_000
+    with am.Server(workers=4, hbm_cap_bytes=cap, batch_rows=0) as srv:
+        tickets = [srv.submit(src, 1000 * i, 200_000, ["k64"], ["p1", "p2"]) for i in range(12)]
+        for t in tickets:
+            srv.wait(t)
+        stats = srv.stats()
+    assert stats["requests"] == 12
+    assert 0 < stats["peak_in_flight_bytes"] <= cap
+    assert stats["in_flight_bytes"] == 0 and stats["queued"] == 0
+
+
+def test_request_larger_than_the_cap_runs_alone(am):
+    src = table(am, seed=7)
+    with am.Server(workers=2, hbm_cap_bytes=1_000_000, batch_rows=0) as srv:
+        got, _ = srv.wait(srv.submit(src, 0, N, ["k64"], ["p2"]))
+    want = am.run_plan(plan_alone(0, N, ["k64"], [False], ["at_end"], ["ieee"], ["p2"]), [src])
+    for name in want:
+        assert same(got[name].to_arrow(), want[name].to_arrow())
+
+
+def test_bad_requests_fail_at_submission(am):
+    src = table(am, seed=8)
+    with am.Server(workers=1) as srv:
+        with pytest.raises(am.ArrowMetalError, match="unknown column"):
+            srv.submit(src, 0, 10, ["nope"], ["p1"])
+        with pytest.raises(am.ArrowMetalError, match="outside the table"):
+            srv.submit(src, N - 5, 10, ["k64"], ["p1"])
+        got, _ = srv.wait(srv.submit(src, 10, 0, ["k64"], ["p1"]))
+        assert all(len(v) == 0 for v in got.values())
