@@ -14,6 +14,8 @@
 // The reference has no server: its callers make one call per query. Every result equals the same
 // request run alone through am_plan_run.
 #include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <condition_variable>
 #include <deque>
 #include <memory>
@@ -33,6 +35,7 @@ using Clock = std::chrono::steady_clock;
 
 struct ServeRequest {
   int64_t id = 0;
+  Clock::time_point enqueued;       // host work of the request done, device work in flight
   am_plan_source* table = nullptr;
   int64_t offset = 0, length = 0;
   std::vector<int> key_cols, pay_cols;          // column positions in the table
@@ -97,8 +100,11 @@ struct am_server_t {
   bool stop = false;
   am_server_stats stats{};
   std::vector<std::thread> workers;
+  Clock::time_point created = Clock::now();
+  FILE* trace = nullptr;           // ARROWMETAL_SERVER_TRACE: one line per unit of work
+  std::mutex trace_mu;
 
-  void run_worker();
+  void run_worker(int index);
   std::vector<ReqPtr> next_unit(int64_t* footprint);
   void execute(std::vector<ReqPtr>& unit);
 };
@@ -149,6 +155,7 @@ void am_server_t::execute(std::vector<ReqPtr>& unit) {
     const std::string plan = plan_of(r);
     am_plan_source* src = r.table;
     int rc = am_plan_run(plan.c_str(), &src, 1, 0, &r.result);
+    r.enqueued = Clock::now();
     if (rc == 0) rc = am_cuda_synchronize();
     if (rc != 0) fail_all(rc, am_last_error());
     return;
@@ -196,12 +203,13 @@ void am_server_t::execute(std::vector<ReqPtr>& unit) {
     for (int c : r.pay_cols) res->names.push_back(r.table->names[size_t(c)]);
     r.result = res;
   }
+  for (auto& r : unit) r->enqueued = Clock::now();
   if (rc == 0) rc = am_cuda_synchronize();
   if (rc != 0) fail_all(rc, am_last_error());
   cleanup();
 }
 
-void am_server_t::run_worker() {
+void am_server_t::run_worker(int index) {
   for (;;) {
     std::vector<ReqPtr> unit;
     int64_t fp = 0;
@@ -225,8 +233,21 @@ void am_server_t::run_worker() {
         stats.solo_requests++;
       }
     }
+    const Clock::time_point t_start = Clock::now();
     execute(unit);
     const Clock::time_point t = Clock::now();
+    if (trace) {
+      // worker, dispatch and finish (ms since the server started), requests, rows, first request's
+      // arrival; a unit of several requests is a segmented batch.
+      auto ms = [&](Clock::time_point x) { return std::chrono::duration<double, std::milli>(x - created).count(); };
+      int64_t rows = 0;
+      for (auto& r : unit) rows += r->length;
+      std::lock_guard<std::mutex> lk(trace_mu);
+      std::fprintf(trace, "worker %d start %.3f enqueued %.3f end %.3f requests %zu rows %lld first_id %lld arrival %.3f "
+                   "table %s keys %zu rc %d\n", index, ms(t_start), ms(unit[0]->enqueued), ms(t), unit.size(),
+                   (long long)rows, (long long)unit[0]->id, ms(unit[0]->arrival), unit[0]->table->name.c_str(),
+                   unit[0]->key_cols.size(), unit[0]->rc);
+    }
     {
       std::lock_guard<std::mutex> lk(mu);
       in_flight -= fp;
@@ -248,10 +269,31 @@ int am_server_create(int workers, int64_t hbm_cap_bytes, int64_t batch_rows, am_
   if (!out || workers < 1 || workers > 64 || hbm_cap_bytes <= 0 || batch_rows < 0) return 2;
   try {
     (void)device();
+    // Reserve the admission budget in the device's memory pool (allocated, freed and kept: the pool
+    // never releases memory), so that the workers' allocations are served from memory already
+    // mapped. Growing the pool while other streams keep the GPU busy stalls the allocating thread
+    // for up to hundreds of milliseconds.
+    {
+      size_t free_b = 0, total_b = 0;
+      AM_CUDA(cudaMemGetInfo(&free_b, &total_b));
+      const int64_t spare = int64_t(free_b) - (int64_t(2) << 30);
+      const int64_t reserve = std::min<int64_t>(hbm_cap_bytes, spare);
+      if (reserve > 0) {
+        cudaStream_t st = stream();
+        void* p = dmalloc(size_t(reserve), st);
+        dfree(p, st);
+        AM_CUDA(cudaStreamSynchronize(st));
+      }
+    }
     auto* s = new am_server_t();
     s->cap = hbm_cap_bytes;
     s->batch_rows = batch_rows;
-    for (int i = 0; i < workers; i++) s->workers.emplace_back([s] { s->run_worker(); });
+    if (const char* path = std::getenv("ARROWMETAL_SERVER_TRACE")) {
+      s->trace = std::fopen(path, "a");
+      if (s->trace) std::fprintf(s->trace, "server workers %d cap %lld batch_rows %lld\n", workers,
+                                 (long long)hbm_cap_bytes, (long long)batch_rows);
+    }
+    for (int i = 0; i < workers; i++) s->workers.emplace_back([s, i] { s->run_worker(i); });
     *out = s;
     return 0;
   } catch (const Error& e) {
@@ -377,6 +419,7 @@ int am_server_release(am_server* srv) {
   for (auto& t : srv->workers) t.join();
   for (auto& kv : srv->requests)
     if (kv.second->result) am_plan_result_release(kv.second->result);
+  if (srv->trace) std::fclose(srv->trace);
   delete srv;
   return 0;
 }

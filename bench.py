@@ -164,6 +164,157 @@ def run_segmented(args, am, torch, stream, local):
     print(json.dumps(line))
 
 
+SERVE_TABLE_ROWS = 50_000_000
+
+
+def make_serving_tables(am, rows=SERVE_TABLE_ROWS, seed=SEED + 3):
+    """The served stream's resident tables: an int64 key over the whole range (as the single-key case),
+    a float64 key ~ N(0, 1), and an (int32 uniform, int64 in [0, 2^40) with 10% nulls) key pair; each
+    with a float64 ~ N(0, 1) and an int32 payload column."""
+    import pyarrow as pa
+    rng = np.random.default_rng(seed)
+
+    def payload():
+        return {"p1": pa.array(rng.standard_normal(rows)),
+                "p2": pa.array(rng.integers(-2**31, 2**31 - 1, rows, dtype=np.int32, endpoint=True))}
+
+    def resident(name, cols):
+        return am.PlanSource(name, {k: am.MetalArray.from_arrow(v) for k, v in cols.items()})
+
+    t_int = resident("t_int64", {"k": pa.array(rng.integers(np.iinfo(np.int64).min, np.iinfo(np.int64).max, rows,
+                                                            dtype=np.int64, endpoint=True)), **payload()})
+    t_f64 = resident("t_float64", {"k": pa.array(rng.standard_normal(rows)), **payload()})
+    k2 = rng.integers(0, 2**40, rows, dtype=np.int64)
+    t_two = resident("t_pair", {"k1": pa.array(rng.integers(-2**31, 2**31 - 1, rows, dtype=np.int32, endpoint=True)),
+                                "k2": pa.array(k2, mask=rng.random(rows) < 0.10), **payload()})
+    return [(t_int, ["k"]), (t_f64, ["k"]), (t_two, ["k1", "k2"])]
+
+
+def serving_requests(count, rows=SERVE_TABLE_ROWS, seed=SEED + 5):
+    """Request i: (table index, offset, length); lengths log-uniform in [1e4, 5e7]."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        n = int(round(10 ** rng.uniform(4, np.log10(5e7))))
+        out.append((int(rng.integers(3)), int(rng.integers(0, rows - n + 1)), n))
+    return out
+
+
+def run_serving(args, am, torch, local):
+    """The served stream: open-loop Poisson arrivals at --rate requests/s against resident tables for
+    --serve-seconds, each request sorting a slice by its table's key(s) and taking the 2 payload columns;
+    admission cap 120 GB. Reports p50/p99 latency (submission to completion) and rows/s; then the same
+    kind of requests all at once through the server against one thread running them back to back
+    through am_plan_run (the plain per-call path)."""
+    import threading as th
+    tables = make_serving_tables(am)
+    am.synchronize()
+    rate = args.rate
+    count = int(rate * args.serve_seconds)
+    reqs = serving_requests(count)
+    gaps = np.random.default_rng(SEED + 6).exponential(1.0 / rate, count)
+    arrivals = np.cumsum(gaps)
+
+    def submit(srv, r):
+        t, off, n = r
+        src, keys = tables[t]
+        return srv.submit(src, off, n, keys, ["p1", "p2"])
+
+    lat = []
+    with ClockSampler(local) as clocks, am.Server(workers=4, hbm_cap_bytes=120 * 10**9, batch_rows=1 << 20) as srv:
+        tickets = []
+        done = th.Event()
+
+        def collect():
+            for i in range(count):
+                while i >= len(tickets):
+                    time.sleep(0.0005)
+                _, ms = srv.wait(tickets[i])
+                lat.append(ms)
+            done.set()
+
+        c = th.Thread(target=collect)
+        c.start()
+        t0 = time.perf_counter()
+        for i, r in enumerate(reqs):
+            delay = arrivals[i] - (time.perf_counter() - t0)
+            if delay > 0:
+                time.sleep(delay)
+            tickets.append(submit(srv, r))
+        c.join()
+        wall = time.perf_counter() - t0
+        open_stats = srv.stats()
+    served_rows = sum(r[2] for r in reqs)
+    by_size = {}
+    sizes = np.array([r[2] for r in reqs])
+    tabs = np.array([r[0] for r in reqs])
+    latv = np.array(lat)
+    for lo in (1e4, 1e5, 1e6, 1e7):
+        m = (sizes >= lo) & (sizes < lo * 10)
+        if m.any():
+            by_size[f"{int(lo):.0e}"] = {"count": int(m.sum()), "p50_ms": float(np.percentile(latv[m], 50)),
+                                         "p99_ms": float(np.percentile(latv[m], 99)), "max_ms": float(latv[m].max()),
+                                         "by_table_max_ms": [float(latv[m & (tabs == t)].max()) if (m & (tabs == t)).any()
+                                                             else None for t in range(3)]}
+    slow = np.argsort(latv)[-8:]
+    slowest = [{"i": int(i), "table": int(tabs[i]), "rows": int(sizes[i]), "ms": float(latv[i]),
+                "arrival_s": float(arrivals[i])} for i in slow]
+
+    # Saturation: the same distribution, all requests at once, against the plain per-call path.
+    sat = serving_requests(args.sat_requests, seed=SEED + 7)
+    sat_rows = sum(r[2] for r in sat)
+    with am.Server(workers=4, hbm_cap_bytes=120 * 10**9, batch_rows=1 << 20) as srv:
+        for r in sat[:8]:                       # warm-up
+            srv.wait(submit(srv, r))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ts = [submit(srv, r) for r in sat]
+        for t in ts:
+            srv.wait(t)
+        served_s = time.perf_counter() - t0
+        sat_stats = srv.stats()
+    for r in sat[:8]:
+        t, off, n = r
+        plain_run(am, tables[t], off, n)
+    am.synchronize()
+    t0 = time.perf_counter()
+    for t, off, n in sat:
+        plain_run(am, tables[t], off, n)
+    am.synchronize()
+    plain_s = time.perf_counter() - t0
+
+    line = {
+        "metric": METRIC, "value": sat_rows / served_s, "unit": "rows/s", "n_gpus": 1,
+        "steps": args.sat_requests, "warmup": 8, "ms_per_step": 1e3 * served_s / args.sat_requests,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64/float64/int32",
+        "data": "synthetic",
+        "config": {"workload": "served sort stream: resident 50M-row tables (int64, float64, (int32, int64) keys, "
+                               "2 payload columns), requests of log-uniform 1e4-5e7 rows sorting a slice and "
+                               "taking both payloads, HBM admission cap 120 GB, 4 worker streams, batches of "
+                               "single-key requests up to 2^20 rows",
+                   "rate_req_s": rate, "requests": count, "saturation_requests": args.sat_requests},
+        "open_loop": {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                      "mean_ms": float(np.mean(lat)), "rows_per_s": served_rows / wall, "seconds": wall,
+                      "by_size": by_size, "slowest": slowest, "server": open_stats},
+        "saturation": {"served_rows_per_s": sat_rows / served_s, "plain_rows_per_s": sat_rows / plain_s,
+                       "speedup_served_over_plain": plain_s / served_s, "rows": sat_rows, "server": sat_stats},
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line))
+
+
+def plain_run(am, table, offset, n):
+    """One request through am_plan_run on the calling thread (the plain per-call path)."""
+    src, keys = table
+    cols = list(keys) + ["p1", "p2"]
+    sel = [[c, f'(col "{c}")'] for c in cols]
+    plan = {"op": "select", "exprs": sel, "input": {"op": "sort", "by": [[k, False, {"nulls": "last"}] for k in keys],
+            "input": {"op": "select", "exprs": sel, "input": {"op": "limit", "count": n, "offset": offset,
+                                                                "input": {"op": "scan", "source": src.name}}}}}
+    out = am.run_plan(plan, [src])
+    del out
+
+
 def arrow_columns(key, valid, p1, p2):
     import pyarrow as pa
     return {"c0": pa.array(key, mask=~valid), "c1": pa.array(p1), "c2": pa.array(p2)}
@@ -333,8 +484,12 @@ def main():
     ap.add_argument("--rows", type=int, default=N_ROWS)
     ap.add_argument("--impl", default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="order_by", choices=["order_by", "segmented"],
-                    help="order_by: the 50M-row ORDER BY (the headline); segmented: 2,048 arrays in one call")
+    ap.add_argument("--workload", default="order_by", choices=["order_by", "segmented", "serving"],
+                    help="order_by: the 50M-row ORDER BY (the headline); segmented: 2,048 arrays in one call; "
+                         "serving: the served request stream")
+    ap.add_argument("--rate", type=float, default=200.0, help="serving: requests per second")
+    ap.add_argument("--serve-seconds", type=float, default=30.0, help="serving: length of the open-loop stream")
+    ap.add_argument("--sat-requests", type=int, default=400, help="serving: requests of the saturation run")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -360,6 +515,10 @@ def main():
         am.set_stream(stream.cuda_stream)
         if rank == 0:
             run_segmented(args, am, torch, stream, local)
+        return
+    if args.workload == "serving":
+        if rank == 0:
+            run_serving(args, am, torch, local)
         return
 
     n = args.rows
