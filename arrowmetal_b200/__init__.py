@@ -185,7 +185,7 @@ class MetalArray:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and _lib is not None:          # module globals are cleared at interpreter exit
             _lib.am_release(h)
             self._h = None
 
@@ -424,7 +424,7 @@ class PlanSource:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and _lib is not None:
             _lib.am_plan_source_release(h)
             self._h = None
 
@@ -505,7 +505,7 @@ class Server:
 
     def close(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and _lib is not None:
             _lib.am_server_release(h)
             self._h = None
 

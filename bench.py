@@ -303,6 +303,82 @@ def run_serving(args, am, torch, local):
     print(json.dumps(line))
 
 
+def run_single(args, am, torch, stream, local):
+    """--workload full_range: argsort of 1,000,000 int64 keys over the whole range, uint64 indices
+    (am_argsort_ex3, index width 8); --workload multikey: the 50M-row two-key sort (key1 int32 Zipf
+    descending, key2 float64 with specials and nulls ascending) and the take of its float64 payload."""
+    import pyarrow as pa
+    if args.workload == "full_range":
+        arr = pa.array(make_full_range_keys(1_000_000))
+        src = am.MetalArray.from_arrow(arr)
+        rows = len(arr)
+
+        def step():
+            out = src.argsort64()
+            del out
+        workload = "argsort of 1,000,000 int64 keys uniform over the whole int64 range, no nulls, uint64 indices"
+        h2d, d2h = arr.nbytes, 8 * rows
+        e2e_fn = lambda: am.MetalArray.from_arrow(arr).argsort64().to_arrow()
+        dtype = "int64"
+    else:
+        key1, key2, valid2, payload = make_multikey_table(N_ROWS)
+        a1, a2 = pa.array(key1), pa.array(key2, mask=~valid2, from_pandas=False)
+        ap = pa.array(payload)
+        d1, d2, dp = (am.MetalArray.from_arrow(x) for x in (a1, a2, ap))
+        rows = N_ROWS
+
+        def step():
+            idx = am.lexsort_indices([d1, d2], descending=[True, False], null_placement="at_end", float_order="ieee")
+            out = am.take_columns([d1, d2, dp], idx)
+            del idx, out
+        workload = ("ORDER BY key1 DESC (int32, 200 distinct values, Zipf 1.1), key2 ASC (float64 N(0,1e6) with "
+                    "-0.0/+0.0/+inf/-inf 0.5% each, 1% NaN, 5% nulls), nulls last, ieee order; take of the 2 keys "
+                    "and a float64 payload; 50,000,000 rows")
+        h2d = a1.nbytes + a2.nbytes + ap.nbytes
+        d2h = 4 * rows + 8 * rows + rows // 8 + 8 * rows
+
+        def e2e_fn():
+            h = [am.MetalArray.from_arrow(x) for x in (a1, a2, ap)]
+            idx = am.lexsort_indices(h[:2], descending=[True, False], null_placement="at_end", float_order="ieee")
+            return [o.to_arrow() for o in am.take_columns(h, idx)]
+        dtype = "int32/float64"
+    for _ in range(max(args.warmup, 3)):
+        step()
+    am.synchronize()
+    steps = max(3, min(args.steps, 100))
+    am.profile(True)
+    am.profile_reset()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(steps):
+            step()
+        ev1.record(stream)
+        ev1.synchronize()
+        am.synchronize()
+    ms = ev0.elapsed_time(ev1) / steps
+    prof = am.profile_entries()
+    am.profile(False)
+    e2e = []
+    for i in range(4):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = e2e_fn()
+        e2e.append(time.perf_counter() - t0)
+        del r
+    e2e_ms = 1e3 * statistics.median(e2e[1:])
+    print(json.dumps({
+        "metric": METRIC, "value": rows / (ms / 1e3), "unit": "rows/s", "n_gpus": 1, "steps": steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": dtype, "data": "synthetic", "config": {"workload": workload, "rows": rows},
+        "per_kernel_ms_per_step": {k: t / steps for k, (l, t) in prof.items()},
+        "gpu_launches": int(sum(l for l, _ in prof.values())),
+        "e2e": {"value": rows / (e2e_ms / 1e3), "unit": "rows/s", "ms_per_step": e2e_ms,
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "clocks": clocks.summary()}))
+
+
 def plain_run(am, table, offset, n):
     """One request through am_plan_run on the calling thread (the plain per-call path)."""
     src, keys = table
@@ -484,9 +560,11 @@ def main():
     ap.add_argument("--rows", type=int, default=N_ROWS)
     ap.add_argument("--impl", default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="order_by", choices=["order_by", "segmented", "serving"],
+    ap.add_argument("--workload", default="order_by",
+                    choices=["order_by", "segmented", "serving", "full_range", "multikey"],
                     help="order_by: the 50M-row ORDER BY (the headline); segmented: 2,048 arrays in one call; "
-                         "serving: the served request stream")
+                         "serving: the served request stream; full_range: 1M full-range int64 keys; multikey: "
+                         "the 50M-row two-key sort")
     ap.add_argument("--rate", type=float, default=200.0, help="serving: requests per second")
     ap.add_argument("--serve-seconds", type=float, default=30.0, help="serving: length of the open-loop stream")
     ap.add_argument("--sat-requests", type=int, default=400, help="serving: requests of the saturation run")
@@ -519,6 +597,12 @@ def main():
     if args.workload == "serving":
         if rank == 0:
             run_serving(args, am, torch, local)
+        return
+    if args.workload in ("full_range", "multikey"):
+        stream = torch.cuda.Stream()
+        am.set_stream(stream.cuda_stream)
+        if rank == 0:
+            run_single(args, am, torch, stream, local)
         return
 
     n = args.rows
