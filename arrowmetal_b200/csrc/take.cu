@@ -10,6 +10,9 @@
 // values and writes them with 128-bit stores, and the four validity bits of eight lanes are OR-ed
 // into one 32-bit bitmap word with three shuffles, so the bitmap is written packed and the null count
 // comes from its popcount.
+#include <algorithm>
+#include <type_traits>
+
 #include "am_internal.h"
 #include "radix_sort.cuh"
 #include "take.cuh"
@@ -163,6 +166,198 @@ __global__ void __launch_bounds__(256) take_kernel(const __grid_constant__ TakeA
   }
 }
 
+// ---- row records
+
+// Column c's value of row j, zero-extended (booleans as 0/1).
+__device__ __forceinline__ uint64_t record_value(const RecArgs& r, int c, uint64_t j) {
+  switch (r.width[c]) {
+    case 8: return static_cast<const uint64_t*>(r.src[c])[j];
+    case 4: return static_cast<const uint32_t*>(r.src[c])[j];
+    case 2: return static_cast<const uint16_t*>(r.src[c])[j];
+    case 1: return static_cast<const uint8_t*>(r.src[c])[j];
+    default: return bit_at(static_cast<const uint8_t*>(r.src[c]), r.src_bit_off[c] + int64_t(j)) ? 1u : 0u;
+  }
+}
+
+// Each thread packs two rows (a block's two halves of 2 x 256 consecutive rows) into W-byte records:
+// every column's two loads are issued before any is used.
+template <int W>
+__global__ void __launch_bounds__(256) pack_records_kernel(const __grid_constant__ RecArgs r) {
+  constexpr int WORDS = W / 8;
+  const uint64_t step = uint64_t(gridDim.x) * 512;
+  for (uint64_t base = uint64_t(blockIdx.x) * 512; base < r.n; base += step) {
+    const uint64_t row[2] = {base + threadIdx.x, base + 256 + threadIdx.x};
+    uint64_t w[2][WORDS];
+    uint32_t valid[2] = {0, 0};
+#pragma unroll
+    for (int h = 0; h < 2; h++)
+#pragma unroll
+      for (int k = 0; k < WORDS; k++) w[h][k] = 0;
+#pragma unroll
+    for (int c = 0; c < kMaxTakeCols; c++) {
+      if (c >= r.ncols) break;
+      const int o = r.rec_off[c];
+      uint64_t v[2];
+#pragma unroll
+      for (int h = 0; h < 2; h++) v[h] = row[h] < r.n ? record_value(r, c, row[h]) : 0;
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+#pragma unroll
+        for (int k = 0; k < WORDS; k++)
+          if ((o >> 3) == k) w[h][k] |= v[h] << (8 * (o & 7));
+        if (row[h] < r.n && (!r.src_valid[c] || bit_at(r.src_valid[c], r.src_voff[c] + int64_t(row[h]))))
+          valid[h] |= 1u << c;
+      }
+    }
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      if (row[h] >= r.n) continue;
+      if (r.valid_off >= 0) {
+#pragma unroll
+        for (int k = 0; k < WORDS; k++)
+          if ((r.valid_off >> 3) == k) w[h][k] |= uint64_t(valid[h]) << (8 * (r.valid_off & 7));
+      }
+      uint64_t* dst = static_cast<uint64_t*>(r.rec) + row[h] * WORDS;
+      if constexpr (WORDS == 1) {
+        dst[0] = w[h][0];
+      } else {
+#pragma unroll
+        for (int k = 0; k < WORDS; k += 2) reinterpret_cast<ulonglong2*>(dst)[k / 2] = make_ulonglong2(w[h][k], w[h][k + 1]);
+      }
+    }
+  }
+}
+
+template <int W>
+__device__ __forceinline__ void load_record(const uint64_t* rec, uint64_t row, uint64_t (&w)[W / 8]) {
+  const uint64_t* p = rec + row * (W / 8);
+  if constexpr (W == 8) {
+    w[0] = p[0];
+  } else {
+#pragma unroll
+    for (int k = 0; k < W / 8; k += 2) {
+      const ulonglong2 v = reinterpret_cast<const ulonglong2*>(p)[k / 2];
+      w[k] = v.x;
+      w[k + 1] = v.y;
+    }
+  }
+}
+
+// take_kernel with every column read from the packed records: per gathered row one record load. The
+// index array is one this library produced (no nulls, in range).
+// Bytes [o, o + bytes) of a record held in registers (o a multiple of bytes, so never across words).
+template <int WORDS>
+__device__ __forceinline__ uint64_t record_field(const uint64_t (&w)[WORDS], int o, int bytes) {
+  const int k = o >> 3;
+  uint64_t x = w[0];
+#pragma unroll
+  for (int q = 1; q < WORDS; q++) x = (k == q) ? w[q] : x;
+  x >>= 8 * (o & 7);
+  return bytes == 8 ? x : (x & ((uint64_t(1) << (8 * bytes)) - 1));
+}
+
+template <int KIND, int W>
+__global__ void __launch_bounds__(256) take_records_kernel(const __grid_constant__ TakeArgs a,
+                                                           const __grid_constant__ RecArgs r) {
+  constexpr int WORDS = W / 8;
+  const int lane = threadIdx.x & 31;
+  const uint64_t warps = uint64_t(gridDim.x) * (blockDim.x >> 5);
+  const uint64_t chunks = (a.n + 127) / 128;
+  const uint64_t* rec = static_cast<const uint64_t*>(r.rec);
+  unsigned long long nulls[kMaxTakeCols];
+#pragma unroll
+  for (int c = 0; c < kMaxTakeCols; c++) nulls[c] = 0;
+
+  for (uint64_t ch = uint64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); ch < chunks; ch += warps) {
+    const uint64_t row0 = ch * 128 + uint64_t(lane) * 4;
+    int64_t ix[4];
+    load4<KIND>(a.idx, row0, a.idx_vec, a.n, ix);
+    uint32_t ok = 0;
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+      if (row0 + j < a.n && ix[j] >= 0 && uint64_t(ix[j]) < a.src_len) ok |= 1u << j;
+    uint64_t w[4][WORDS];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      if ((ok >> j) & 1u) load_record<W>(rec, uint64_t(ix[j]), w[j]);
+      else {
+#pragma unroll
+        for (int k = 0; k < WORDS; k++) w[j][k] = 0;
+      }
+    }
+    const bool full = row0 + 4 <= a.n;
+    const uint32_t rows_mask = full ? 0xFu : ((1u << uint32_t(a.n > row0 ? a.n - row0 : 0)) - 1u);
+    const uint64_t word = ch * 4 + (lane >> 3);
+#define AM_FIELD(j, o, bytes) record_field<WORDS>(w[j], (o), (bytes))
+    for (int c = 0; c < a.ncols; c++) {
+      const TakeCol& col = a.col[c];
+      uint32_t vb = ok;
+      if (r.valid_off >= 0 && col.dst_valid) {
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+          if (!((AM_FIELD(j, r.valid_off, 1) >> c) & 1u)) vb &= ~(1u << j);
+      }
+      const int o = r.rec_off[c];
+      switch (col.width) {
+        case 8: {
+          uint64_t* d = static_cast<uint64_t*>(col.dst) + row0;
+          if (full) {
+            reinterpret_cast<ulonglong2*>(d)[0] = make_ulonglong2(AM_FIELD(0, o, 8), AM_FIELD(1, o, 8));
+            reinterpret_cast<ulonglong2*>(d)[1] = make_ulonglong2(AM_FIELD(2, o, 8), AM_FIELD(3, o, 8));
+          } else {
+#pragma unroll
+            for (int j = 0; j < 4; j++) if (row0 + j < a.n) d[j] = AM_FIELD(j, o, 8);
+          }
+          break;
+        }
+        case 4: {
+          uint32_t* d = static_cast<uint32_t*>(col.dst) + row0;
+          if (full) *reinterpret_cast<uint4*>(d) = make_uint4(uint32_t(AM_FIELD(0, o, 4)), uint32_t(AM_FIELD(1, o, 4)),
+                                                             uint32_t(AM_FIELD(2, o, 4)), uint32_t(AM_FIELD(3, o, 4)));
+          else _Pragma("unroll") for (int j = 0; j < 4; j++) if (row0 + j < a.n) d[j] = uint32_t(AM_FIELD(j, o, 4));
+          break;
+        }
+        case 2: {
+          uint16_t* d = static_cast<uint16_t*>(col.dst) + row0;
+          if (full) *reinterpret_cast<uint2*>(d) = make_uint2(uint32_t(AM_FIELD(0, o, 2)) | (uint32_t(AM_FIELD(1, o, 2)) << 16),
+                                                             uint32_t(AM_FIELD(2, o, 2)) | (uint32_t(AM_FIELD(3, o, 2)) << 16));
+          else _Pragma("unroll") for (int j = 0; j < 4; j++) if (row0 + j < a.n) d[j] = uint16_t(AM_FIELD(j, o, 2));
+          break;
+        }
+        case 1: {
+          uint8_t* d = static_cast<uint8_t*>(col.dst) + row0;
+          if (full) *reinterpret_cast<uint32_t*>(d) = uint32_t(AM_FIELD(0, o, 1)) | (uint32_t(AM_FIELD(1, o, 1)) << 8) |
+                                                      (uint32_t(AM_FIELD(2, o, 1)) << 16) | (uint32_t(AM_FIELD(3, o, 1)) << 24);
+          else _Pragma("unroll") for (int j = 0; j < 4; j++) if (row0 + j < a.n) d[j] = uint8_t(AM_FIELD(j, o, 1));
+          break;
+        }
+        default: {  // boolean: the record's 0/1 byte
+          uint32_t bits = 0;
+#pragma unroll
+          for (int j = 0; j < 4; j++)
+            if (((ok >> j) & 1u) && AM_FIELD(j, o, 1)) bits |= 1u << j;
+          const uint32_t wd = gather_word(bits, lane);
+          if ((lane & 7) == 0) static_cast<uint32_t*>(col.dst)[word] = wd;
+          break;
+        }
+      }
+      if (col.dst_valid) {
+        const uint32_t wd = gather_word(vb, lane);
+        if ((lane & 7) == 0) col.dst_valid[word] = wd;
+        nulls[c] += __popc(rows_mask & ~vb);
+      }
+    }
+  }
+  for (int c = 0; c < a.ncols; c++) {
+    if (!a.col[c].dst_valid) continue;
+    unsigned long long v = nulls[c];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0 && v) atomicAdd(a.col[c].dst_nulls, v);
+  }
+}
+#undef AM_FIELD
+
 }  // namespace tk
 
 void launch_take(const tk::TakeArgs& a, cudaStream_t s) {
@@ -177,6 +372,87 @@ void launch_take(const tk::TakeArgs& a, cudaStream_t s) {
     default: tk::take_kernel<tk::IDX_U64><<<grid, 256, 0, s>>>(a); break;
   }
   AM_CUDA(cudaGetLastError());
+}
+
+// Gathers through row records pay off when the sources are far larger than L2 (each random read then
+// costs a DRAM burst) and most of their rows are gathered (the records are built from every row).
+constexpr uint64_t kRecordMinSourceBytes = uint64_t(256) << 20;
+
+// Record width (8, 16 or 32) for gathering these columns through row records, or 0 for the direct
+// gather: at least two columns, indices that need no checks, rows that fit 32 bytes.
+static int record_bytes(am_array* const* cols, int m, bool checked, int64_t n) {
+  if (m < 2 || checked) return 0;
+  const int64_t src_len = cols[0]->length;
+  if (n < src_len / 2) return 0;
+  int bytes = 0;
+  bool nullable = false;
+  for (int c = 0; c < m; c++) {
+    bytes += std::max(pt_bytes(cols[c]->pt), 1);
+    if (cols[c]->null_count != 0) nullable = true;
+  }
+  if (uint64_t(src_len) * uint64_t(bytes) < kRecordMinSourceBytes) return 0;
+  bytes += nullable ? 1 : 0;
+  return bytes <= 8 ? 8 : bytes <= 16 ? 16 : bytes <= 32 ? 32 : 0;
+}
+
+static void take_through_records(const tk::TakeArgs& a, am_array* const* cols, int rec_w, cudaStream_t s) {
+  using namespace tk;
+  RecArgs r{};
+  r.ncols = a.ncols;
+  r.n = a.src_len;
+  // Widest first, so every field sits at a multiple of its width.
+  int order[kMaxTakeCols];
+  for (int c = 0; c < a.ncols; c++) order[c] = c;
+  std::stable_sort(order, order + a.ncols, [&](int x, int y) { return a.col[x].width > a.col[y].width; });
+  int off = 0;
+  bool nullable = false;
+  for (int k = 0; k < a.ncols; k++) {
+    const int c = order[k];
+    r.rec_off[c] = off;
+    off += std::max(a.col[c].width, 1);
+  }
+  for (int c = 0; c < a.ncols; c++) {
+    r.src[c] = a.col[c].src;
+    r.src_valid[c] = a.col[c].src_valid;
+    r.src_voff[c] = a.col[c].src_voff;
+    r.src_bit_off[c] = a.col[c].src_bit_off;
+    r.width[c] = a.col[c].width;
+    if (a.col[c].src_valid) nullable = true;
+    (void)cols;
+  }
+  r.valid_off = nullable ? off : -1;
+  r.rec = dmalloc(size_t(a.src_len) * size_t(rec_w), s);
+  const int pack_grid = int(std::min<uint64_t>((a.src_len + 511) / 512, uint64_t(device().sm_count) * 16));
+  const uint64_t chunks = (a.n + 127) / 128;
+  const int grid = int(std::min<uint64_t>((chunks + 7) / 8, uint64_t(device().sm_count) * 8));
+  {
+    KernelTimer kt("take_pack_records", s);
+    switch (rec_w) {
+      case 8: pack_records_kernel<8><<<std::max(pack_grid, 1), 256, 0, s>>>(r); break;
+      case 16: pack_records_kernel<16><<<std::max(pack_grid, 1), 256, 0, s>>>(r); break;
+      default: pack_records_kernel<32><<<std::max(pack_grid, 1), 256, 0, s>>>(r); break;
+    }
+    AM_CUDA(cudaGetLastError());
+  }
+  {
+    KernelTimer kt("take_gather_records", s);
+    auto go = [&](auto kind_tag) {
+      constexpr int KIND = decltype(kind_tag)::value;
+      switch (rec_w) {
+        case 8: take_records_kernel<KIND, 8><<<std::max(grid, 1), 256, 0, s>>>(a, r); break;
+        case 16: take_records_kernel<KIND, 16><<<std::max(grid, 1), 256, 0, s>>>(a, r); break;
+        default: take_records_kernel<KIND, 32><<<std::max(grid, 1), 256, 0, s>>>(a, r); break;
+      }
+    };
+    switch (a.idx_kind) {
+      case IDX_U32: go(std::integral_constant<int, IDX_U32>{}); break;
+      case IDX_I32: go(std::integral_constant<int, IDX_I32>{}); break;
+      case IDX_I64: go(std::integral_constant<int, IDX_I64>{}); break;
+      default: go(std::integral_constant<int, IDX_U64>{}); break;
+    }
+    AM_CUDA(cudaGetLastError());
+  }
+  dfree(r.rec, s);
 }
 
 void take_columns(am_array* const* cols, int count, am_array* indices, am_array** outs, bool check_range,
@@ -238,7 +514,9 @@ void take_columns(am_array* const* cols, int count, am_array* indices, am_array*
       }
       o->last_stream = s;
     }
-    launch_take(a, s);
+    const int rec_w = record_bytes(cols + base, m, check_range || a.idx_valid != nullptr, n);
+    if (rec_w) take_through_records(a, cols + base, rec_w, s);
+    else launch_take(a, s);
   }
 }
 

@@ -34,6 +34,23 @@ struct TakeArgs {
   uint32_t* err;
 };
 
+// Row records: the columns of a multi-column gather packed row by row, so that one random read of a
+// record (8, 16 or 32 bytes: one DRAM burst) fetches every column of a gathered row instead of one
+// burst per column. Column c sits at byte rec_off[c] (booleans as a 0/1 byte); bit c of the byte at
+// valid_off is the row's validity of column c.
+struct RecArgs {
+  const void* src[kMaxTakeCols];
+  const uint8_t* src_valid[kMaxTakeCols];
+  int64_t src_voff[kMaxTakeCols];
+  int64_t src_bit_off[kMaxTakeCols];
+  int32_t width[kMaxTakeCols];    // bytes per value; 0 for boolean (a byte in the record)
+  int32_t rec_off[kMaxTakeCols];
+  int32_t ncols;
+  int32_t valid_off;              // -1: no column has nulls
+  uint64_t n;                     // source rows
+  void* rec;
+};
+
 }  // namespace tk
 
 void launch_take(const tk::TakeArgs& a, cudaStream_t s);

@@ -145,3 +145,39 @@ def test_take_large_out_of_range(am):
     idx[4_999_999] = 5_000_000
     with pytest.raises(am.ArrowMetalError, match="out of range"):
         am.take_columns([src, src], pa.array(idx))
+
+
+def test_take_columns_through_row_records(am):
+    # Several large columns through a permutation this library produced: the gather packs them into
+    # 32-byte row records (7 columns of 27 bytes + a validity byte) and reads one record per row.
+    rng = np.random.default_rng(15)
+    n = 10_000_000
+    cols = [pa.array(rng.integers(-2**62, 2**62, n), mask=rng.random(n) < 0.1),
+            pa.array(rng.standard_normal(n)),
+            pa.array(rng.integers(-2**31, 2**31 - 1, n, dtype=np.int32)),
+            pa.array(rng.standard_normal(n).astype(np.float32), mask=rng.random(n) < 0.5),
+            pa.array(rng.integers(0, 2**16, n).astype(np.uint16)),
+            pa.array(rng.integers(0, 255, n, dtype=np.uint8), mask=rng.random(n) < 0.3),
+            pa.array(rng.random(n) < 0.5, mask=rng.random(n) < 0.05)]
+    handles = [am.MetalArray.from_arrow(c) for c in cols]
+    idx = am.MetalArray.from_arrow(pa.array(rng.integers(0, 2**40, n))).argsort()
+    ii = pa.array(idx.to_arrow().to_numpy())
+    for c, o in zip(cols, am.take_columns(handles, idx)):
+        got = o.to_arrow()
+        want = pc.take(c, ii)
+        assert got.null_count == want.null_count
+        assert got.equals(want)
+
+
+def test_take_two_columns_through_16_byte_records(am):
+    # The ORDER BY payload shape (float64 + int32, no nulls): 16-byte records, bit-exact values.
+    rng = np.random.default_rng(16)
+    n = 25_000_000
+    p1 = rng.standard_normal(n)
+    p2 = rng.integers(-2**31, 2**31 - 1, n, dtype=np.int32)
+    handles = [am.MetalArray.from_arrow(pa.array(p1)), am.MetalArray.from_arrow(pa.array(p2))]
+    idx = am.MetalArray.from_arrow(pa.array(rng.integers(0, 2**40, n))).argsort()
+    ii = idx.to_arrow().to_numpy()
+    o1, o2 = am.take_columns(handles, idx)
+    assert np.array_equal(o1.to_arrow().to_numpy().view(np.uint64), p1.view(np.uint64)[ii])
+    assert np.array_equal(o2.to_arrow().to_numpy(), p2[ii])
