@@ -903,11 +903,30 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
     __syncthreads();
 
     const uint32_t tile_n = uint32_t((count - tile_base) < uint64_t(TILE) ? (count - tile_base) : uint64_t(TILE));
-    // ---- keys out, then ids out; consecutive threads write consecutive addresses of a digit run.
-    // Every destination is checked against its array: an offset error is reported, never written.
+    // ---- keys and ids out; consecutive threads write consecutive addresses of a digit run. A pass that
+    // moves both writes them in one loop (one digit and base lookup per row). Every destination is
+    // checked against its array: an offset error is reported, never written.
     const uint32_t buf_rows = sm.desc.buf_rows, out_rows = sm.desc.out_rows;
     const bool last = (flags & PF_LAST) != 0;
-    if (keys_out) {
+    const bool merged = keys_out && ids_out && pa.carry_ids;
+    if (merged) {
+      for (uint32_t j = threadIdx.x; j < tile_n; j += THREADS) {
+        const uint32_t d = sm.dig[j];
+        const uint32_t dst = sm.gdelta[d] + j;
+        if (d < RADIX) {
+          if (dst < buf_rows) {
+            keys_out[dst] = sm.keys[j];
+            ids_out[dst] = sm.ids[j];
+          } else {
+            atomicOr(pa.err, ERR_BOUNDS);
+          }
+        } else if (final_out) {
+          if (dst >= out_rows) atomicOr(pa.err, ERR_BOUNDS);
+          else if (flags & PF_WIDE_OUT) static_cast<uint64_t*>(final_out)[dst] = sm.ids[j];
+          else static_cast<uint32_t*>(final_out)[dst] = sm.ids[j];
+        }
+      }
+    } else if (keys_out) {
       for (uint32_t j = threadIdx.x; j < tile_n; j += THREADS) {
         const uint32_t d = sm.dig[j];
         const uint32_t dst = sm.gdelta[d] + j;
@@ -931,7 +950,7 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
         store_width(pa.key_out, dst, kw, v);
       }
     }
-    if (pa.carry_ids) {
+    if (pa.carry_ids && !merged) {
       for (uint32_t j = threadIdx.x; j < tile_n; j += THREADS) {
         const uint32_t d = sm.dig[j];
         const uint32_t v = sm.ids[j];
