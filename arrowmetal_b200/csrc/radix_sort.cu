@@ -20,6 +20,9 @@
 // the reference's "take the next key column, argsort, compose" becomes one gather of the next key
 // inside its first pass.
 #include <algorithm>
+#include <cstdlib>
+#include <list>
+#include <memory>
 #include <cstring>
 
 #include "am_internal.h"
@@ -1265,91 +1268,106 @@ namespace {
 
 constexpr uint32_t SEG_HIST_ROWS = 32768;   // rows per histogram block
 
+// One key width's arrays of a batch: the tables the kernels read and where everything sits in the
+// group's scratch.
 template <typename KeyT>
-void sort_segment_group(const std::vector<SortKey>& keys, const std::vector<void*>& outs,
-                        const std::vector<size_t>& group, cudaStream_t s) {
-  using C = PassConfig<KeyT>;
-  constexpr uint64_t TILE = uint64_t(C::THREADS) * C::ITEMS;
-  constexpr int S = int(sizeof(KeyT));
-  const uint32_t G = uint32_t(group.size());
-
-  std::vector<SegDesc> segs(G);
-  std::vector<uint32_t> tile_start(G + 1), item_start(G + 1);
+struct GroupLayout {
+  static constexpr uint64_t TILE = uint64_t(PassConfig<KeyT>::THREADS) * PassConfig<KeyT>::ITEMS;
+  static constexpr int S = int(sizeof(KeyT));
+  uint32_t G = 0;
   uint64_t rows = 0, tiles = 0, items = 0, max_n = 0;
-  for (uint32_t g = 0; g < G; g++) {
-    const SortKey& k = keys[group[g]];
-    const uint64_t n = uint64_t(k.col->length);
-    segs[g].col = make_view(k);
-    segs[g].row_off = rows;
-    segs[g].out = outs[group[g]];
-    segs[g].n = uint32_t(n);
-    tile_start[g] = uint32_t(tiles);
-    item_start[g] = uint32_t(items);
-    rows += n;
-    tiles += (n + TILE - 1) / TILE;
-    items += (n + SEG_HIST_ROWS - 1) / SEG_HIST_ROWS;
-    max_n = std::max(max_n, n);
-  }
-  tile_start[G] = uint32_t(tiles);
-  item_start[G] = uint32_t(items);
-  if (tiles >= (uint64_t(1) << 32) || items >= (uint64_t(1) << 31))
-    throw invalid("a batch of " + std::to_string(rows) + " rows is too large for one segmented sort");
+  std::vector<uint32_t> lens;
+  std::vector<char> host;              // segment table, tile starts, item starts
+  size_t off_tiles = 0, off_items = 0, tables = 0;
+  size_t off_stats = 0, off_kplan = 0, off_desc = 0, off_sum = 0, off_tick = 0, header = 0;
+  size_t kbuf = 0, ibuf = 0;
+  size_t bytes() const { return header + 2 * kbuf + 2 * ibuf; }
+  bool narrow() const { return max_n < (uint64_t(1) << 30); }
 
-  // Scratch: tables (copied from the host), then statistics, plans, descriptors, summaries and
-  // tickets (zeroed), then the ping-pong key and id buffers.
-  auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
-  const size_t off_segs = 0;
-  const size_t off_tiles = up(off_segs + sizeof(SegDesc) * G);
-  const size_t off_items = up(off_tiles + sizeof(uint32_t) * (G + 1));
-  const size_t tables = up(off_items + sizeof(uint32_t) * (G + 1));
-  const size_t off_stats = tables;
-  const size_t off_kplan = up(off_stats + sizeof(KeyStats) * G);
-  const size_t off_desc = up(off_kplan + sizeof(KeyPlan) * G);
-  const size_t off_sum = up(off_desc + sizeof(PassDesc) * G * S);
-  const size_t off_tick = up(off_sum + sizeof(SortSummary) * G);
-  const size_t header = up(off_tick + sizeof(uint32_t) * S);
-  const size_t kbuf = up(rows * sizeof(KeyT)), ibuf = up(rows * 4);
-  char* base = static_cast<char*>(dmalloc(header + 2 * kbuf + 2 * ibuf, s));
-  std::vector<char> host(tables);
-  std::memcpy(host.data() + off_segs, segs.data(), sizeof(SegDesc) * G);
-  std::memcpy(host.data() + off_tiles, tile_start.data(), sizeof(uint32_t) * (G + 1));
-  std::memcpy(host.data() + off_items, item_start.data(), sizeof(uint32_t) * (G + 1));
-  copy_h2d(base, host.data(), tables, s);
-  AM_CUDA(cudaMemsetAsync(base + tables, 0, header - tables, s));
-  const SegDesc* d_segs = reinterpret_cast<const SegDesc*>(base + off_segs);
-  const uint32_t* d_tiles = reinterpret_cast<const uint32_t*>(base + off_tiles);
-  const uint32_t* d_items = reinterpret_cast<const uint32_t*>(base + off_items);
-  KeyStats* st = reinterpret_cast<KeyStats*>(base + off_stats);
-  KeyPlan* kp = reinterpret_cast<KeyPlan*>(base + off_kplan);
-  PassDesc* pd = reinterpret_cast<PassDesc*>(base + off_desc);
-  SortSummary* sum = reinterpret_cast<SortSummary*>(base + off_sum);
-  uint32_t* tick = reinterpret_cast<uint32_t*>(base + off_tick);
-  char* kbufA = base + header;
-  char* kbufB = kbufA + kbuf;
-  uint32_t* ibufA = reinterpret_cast<uint32_t*>(kbufB + kbuf);
-  uint32_t* ibufB = reinterpret_cast<uint32_t*>(kbufB + kbuf + ibuf);
-
-  {
-    KernelTimer kt("batch_histogram", s);
-    segmented_histogram_kernel<KeyT, HIST_THREADS, HIST_ITEMS><<<uint32_t(items), HIST_THREADS, 0, s>>>(
-        d_segs, d_items, G, SEG_HIST_ROWS, st);
-    AM_CUDA(cudaGetLastError());
-  }
-  {
-    KernelTimer kt("batch_plan", s);
-    segmented_plan_kernel<<<G, 256, 0, s>>>(d_segs, S, st, kp, pd, sum);
-    AM_CUDA(cudaGetLastError());
-  }
-  // Every array's counts fit 30 bits below 2^30 rows: 32-bit look-back words, zeroed per pass.
-  const bool narrow = max_n < (uint64_t(1) << 30);
-  StreamScratch& sc = stream_scratch(s, size_t(tiles) * NBINS);
-  for (int sl = 0; sl < S; sl++) {
-    if (narrow) {
-      AM_CUDA(cudaMemsetAsync(sc.status, 0, size_t(tiles) * NBINS * sizeof(uint32_t), s));
-    } else if (sc.epoch >= (1u << 30) - 1) {
-      AM_CUDA(cudaMemsetAsync(sc.status, 0, sc.status_words * sizeof(uint64_t), s));
-      sc.epoch = 0;
+  GroupLayout(const std::vector<SortKey>& keys, const std::vector<void*>& outs, const std::vector<size_t>& group) {
+    G = uint32_t(group.size());
+    std::vector<SegDesc> segs(G);
+    std::vector<uint32_t> tile_start(G + 1), item_start(G + 1);
+    lens.resize(G);
+    for (uint32_t g = 0; g < G; g++) {
+      const SortKey& k = keys[group[g]];
+      const uint64_t n = uint64_t(k.col->length);
+      segs[g].col = make_view(k);
+      segs[g].row_off = rows;
+      segs[g].out = outs[group[g]];
+      segs[g].n = uint32_t(n);
+      lens[g] = uint32_t(n);
+      tile_start[g] = uint32_t(tiles);
+      item_start[g] = uint32_t(items);
+      rows += n;
+      tiles += (n + TILE - 1) / TILE;
+      items += (n + SEG_HIST_ROWS - 1) / SEG_HIST_ROWS;
+      max_n = std::max(max_n, n);
     }
+    tile_start[G] = uint32_t(tiles);
+    item_start[G] = uint32_t(items);
+    if (tiles >= (uint64_t(1) << 32) || items >= (uint64_t(1) << 31))
+      throw invalid("a batch of " + std::to_string(rows) + " rows is too large for one segmented sort");
+    auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
+    off_tiles = up(sizeof(SegDesc) * G);
+    off_items = up(off_tiles + sizeof(uint32_t) * (G + 1));
+    tables = up(off_items + sizeof(uint32_t) * (G + 1));
+    off_stats = tables;
+    off_kplan = up(off_stats + sizeof(KeyStats) * G);
+    off_desc = up(off_kplan + sizeof(KeyPlan) * G);
+    off_sum = up(off_desc + sizeof(PassDesc) * G * S);
+    off_tick = up(off_sum + sizeof(SortSummary) * G);
+    header = up(off_tick + sizeof(uint32_t) * S);
+    kbuf = up(rows * sizeof(KeyT));
+    ibuf = up(rows * 4);
+    host.assign(tables, 0);
+    std::memcpy(host.data(), segs.data(), sizeof(SegDesc) * G);
+    std::memcpy(host.data() + off_tiles, tile_start.data(), sizeof(uint32_t) * (G + 1));
+    std::memcpy(host.data() + off_items, item_start.data(), sizeof(uint32_t) * (G + 1));
+  }
+};
+
+// The launches of one group, with its scratch at `base` and its tables already there or copied from
+// `pinned_tables` (a graph's first node) when that is given. `timed`: a KernelTimer per launch (not
+// inside a graph capture).
+template <typename KeyT>
+void enqueue_group(const GroupLayout<KeyT>& L, char* base, void* status, uint32_t* err, const void* pinned_tables,
+                   bool timed, cudaStream_t s) {
+  using C = PassConfig<KeyT>;
+  constexpr int S = GroupLayout<KeyT>::S;
+  if (pinned_tables) AM_CUDA(cudaMemcpyAsync(base, pinned_tables, L.tables, cudaMemcpyHostToDevice, s));
+  AM_CUDA(cudaMemsetAsync(base + L.tables, 0, L.header - L.tables, s));
+  const SegDesc* d_segs = reinterpret_cast<const SegDesc*>(base);
+  const uint32_t* d_tiles = reinterpret_cast<const uint32_t*>(base + L.off_tiles);
+  const uint32_t* d_items = reinterpret_cast<const uint32_t*>(base + L.off_items);
+  KeyStats* st = reinterpret_cast<KeyStats*>(base + L.off_stats);
+  KeyPlan* kp = reinterpret_cast<KeyPlan*>(base + L.off_kplan);
+  PassDesc* pd = reinterpret_cast<PassDesc*>(base + L.off_desc);
+  SortSummary* sum = reinterpret_cast<SortSummary*>(base + L.off_sum);
+  uint32_t* tick = reinterpret_cast<uint32_t*>(base + L.off_tick);
+  char* kbufA = base + L.header;
+  char* kbufB = kbufA + L.kbuf;
+  uint32_t* ibufA = reinterpret_cast<uint32_t*>(kbufB + L.kbuf);
+  uint32_t* ibufB = reinterpret_cast<uint32_t*>(kbufB + L.kbuf + L.ibuf);
+  {
+    std::unique_ptr<KernelTimer> kt(timed ? new KernelTimer("batch_histogram", s) : nullptr);
+    segmented_histogram_kernel<KeyT, HIST_THREADS, HIST_ITEMS><<<uint32_t(L.items), HIST_THREADS, 0, s>>>(
+        d_segs, d_items, L.G, SEG_HIST_ROWS, st);
+    AM_CUDA(cudaGetLastError());
+  }
+  {
+    std::unique_ptr<KernelTimer> kt(timed ? new KernelTimer("batch_plan", s) : nullptr);
+    segmented_plan_kernel<<<L.G, 256, 0, s>>>(d_segs, S, st, kp, pd, sum);
+    AM_CUDA(cudaGetLastError());
+  }
+  // Every array's counts fit 30 bits below 2^30 rows: 32-bit look-back words, zeroed per pass. Above,
+  // 64-bit words whose pass epochs (1..S) start over from a zeroed array in every call.
+  const bool narrow = L.narrow();
+  if (!narrow) AM_CUDA(cudaMemsetAsync(status, 0, size_t(L.tiles) * NBINS * sizeof(uint64_t), s));
+  const int bps = narrow ? pass_blocks_per_sm<KeyT, uint32_t, true>() : pass_blocks_per_sm<KeyT, uint64_t, true>();
+  const int grid = int(std::min<uint64_t>(L.tiles, uint64_t(device().sm_count) * bps));
+  for (int sl = 0; sl < S; sl++) {
+    if (narrow) AM_CUDA(cudaMemsetAsync(status, 0, size_t(L.tiles) * NBINS * sizeof(uint32_t), s));
     PassArgs a{};
     a.desc = pd;
     a.kplan = kp;
@@ -1358,30 +1376,154 @@ void sort_segment_group(const std::vector<SortKey>& keys, const std::vector<void
     a.ids[0] = ibufA;
     a.ids[1] = ibufB;
     a.final_out = nullptr;
-    a.status = sc.status;
-    a.epoch = ++sc.epoch;
+    a.status = status;
+    a.epoch = uint32_t(sl + 1);
     a.tile_counter = tick + sl;
-    a.err = sc.err;
+    a.err = err;
     a.carry_ids = 1;
     a.segs = d_segs;
     a.tile_start = d_tiles;
-    a.nsegs = G;
-    a.total_tiles = uint32_t(tiles);
+    a.nsegs = L.G;
+    a.total_tiles = uint32_t(L.tiles);
     a.slot = uint32_t(sl);
     a.nslots = uint32_t(S);
     const ColView none{};
-    KernelTimer kt("batch_pass", s);
-    if (narrow) {
-      auto fn = onesweep_pass_kernel<KeyT, uint32_t, C::THREADS, C::ITEMS, true>;
-      const int grid = int(std::min<uint64_t>(tiles, uint64_t(device().sm_count) * pass_blocks_per_sm<KeyT, uint32_t, true>()));
-      fn<<<std::max(grid, 1), C::THREADS, pass_smem<KeyT>(), s>>>(a, none);
-    } else {
-      auto fn = onesweep_pass_kernel<KeyT, uint64_t, C::THREADS, C::ITEMS, true>;
-      const int grid = int(std::min<uint64_t>(tiles, uint64_t(device().sm_count) * pass_blocks_per_sm<KeyT, uint64_t, true>()));
-      fn<<<std::max(grid, 1), C::THREADS, pass_smem<KeyT>(), s>>>(a, none);
-    }
+    std::unique_ptr<KernelTimer> kt(timed ? new KernelTimer("batch_pass", s) : nullptr);
+    if (narrow)
+      onesweep_pass_kernel<KeyT, uint32_t, C::THREADS, C::ITEMS, true><<<std::max(grid, 1), C::THREADS, pass_smem<KeyT>(), s>>>(a, none);
+    else
+      onesweep_pass_kernel<KeyT, uint64_t, C::THREADS, C::ITEMS, true><<<std::max(grid, 1), C::THREADS, pass_smem<KeyT>(), s>>>(a, none);
     AM_CUDA(cudaGetLastError());
   }
+}
+
+// ---- CUDA graphs for repeated batch shapes.
+//
+// A batch's launches depend on its key width and its arrays' lengths only: the columns, options and
+// output arrays reach the kernels through the segment table. The second time a thread sorts a batch of
+// the same shape on the same stream, the launches are captured into a graph whose first node copies the
+// table from a pinned host buffer; later batches of that shape write their table there and launch the
+// graph: one launch instead of 2 + 2 x digits, and no scratch allocation. Two graph instances with
+// their own pinned tables alternate, so a batch never waits for the one just before it.
+struct BatchGraph {
+  int width = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<uint32_t> lens;
+  char* base = nullptr;                 // scratch (device)
+  void* status = nullptr;               // look-back words (device)
+  size_t tables = 0;
+  struct Slot {
+    void* host = nullptr;               // pinned segment table
+    cudaGraphExec_t exec = nullptr;
+    cudaEvent_t done = nullptr;
+    bool launched = false;
+  } slot[2];
+  int next = 0;
+  ~BatchGraph() {
+    for (auto& sl : slot) {
+      if (sl.launched) (void)cudaEventSynchronize(sl.done);
+      if (sl.exec) (void)cudaGraphExecDestroy(sl.exec);
+      if (sl.done) (void)cudaEventDestroy(sl.done);
+      pinned_free(sl.host);
+    }
+    if (base) (void)cudaFree(base);
+    if (status) (void)cudaFree(status);
+  }
+};
+
+constexpr size_t kGraphCacheEntries = 4;
+constexpr size_t kGraphMaxScratch = size_t(16) << 30;    // larger batches run without a graph
+
+struct GraphCache {
+  std::list<std::unique_ptr<BatchGraph>> graphs;          // most recently used first
+  std::list<std::pair<int, std::vector<uint32_t>>> seen;  // shapes seen once
+};
+GraphCache& graph_cache() {
+  static thread_local GraphCache c;
+  return c;
+}
+
+bool graphs_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("ARROWMETAL_BATCH_GRAPHS");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+template <typename KeyT>
+BatchGraph* find_or_capture(const GroupLayout<KeyT>& L, uint32_t* err, cudaStream_t s) {
+  GraphCache& c = graph_cache();
+  const int width = int(sizeof(KeyT));
+  for (auto it = c.graphs.begin(); it != c.graphs.end(); ++it) {
+    if ((*it)->width == width && (*it)->stream == s && (*it)->lens == L.lens) {
+      c.graphs.splice(c.graphs.begin(), c.graphs, it);
+      return c.graphs.front().get();
+    }
+  }
+  bool seen = false;
+  for (auto& sh : c.seen) if (sh.first == width && sh.second == L.lens) seen = true;
+  if (!seen) {
+    c.seen.emplace_front(width, L.lens);
+    if (c.seen.size() > 16) c.seen.pop_back();
+    return nullptr;
+  }
+  if (L.bytes() > kGraphMaxScratch) return nullptr;
+  auto g = std::make_unique<BatchGraph>();
+  g->width = width;
+  g->stream = s;
+  g->lens = L.lens;
+  g->tables = L.tables;
+  AM_CUDA(cudaMalloc(reinterpret_cast<void**>(&g->base), L.bytes()));
+  const size_t status_bytes = size_t(L.tiles) * NBINS * (L.narrow() ? sizeof(uint32_t) : sizeof(uint64_t));
+  AM_CUDA(cudaMalloc(&g->status, std::max<size_t>(status_bytes, 16)));
+  // Launch attributes and occupancy are looked up before the capture.
+  (void)pass_blocks_per_sm<KeyT, uint32_t, true>();
+  (void)pass_blocks_per_sm<KeyT, uint64_t, true>();
+  for (auto& sl : g->slot) {
+    sl.host = pinned_alloc(L.tables);
+    AM_CUDA(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
+    cudaGraph_t graph = nullptr;
+    AM_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    try {
+      enqueue_group<KeyT>(L, g->base, g->status, err, sl.host, false, s);
+    } catch (...) {
+      cudaGraph_t discard = nullptr;
+      (void)cudaStreamEndCapture(s, &discard);
+      if (discard) (void)cudaGraphDestroy(discard);
+      throw;
+    }
+    AM_CUDA(cudaStreamEndCapture(s, &graph));
+    const cudaError_t e = cudaGraphInstantiate(&sl.exec, graph, 0);
+    (void)cudaGraphDestroy(graph);
+    AM_CUDA(e);
+  }
+  c.graphs.push_front(std::move(g));
+  if (c.graphs.size() > kGraphCacheEntries) c.graphs.pop_back();
+  return c.graphs.front().get();
+}
+
+template <typename KeyT>
+void sort_segment_group(const std::vector<SortKey>& keys, const std::vector<void*>& outs,
+                        const std::vector<size_t>& group, cudaStream_t s) {
+  GroupLayout<KeyT> L(keys, outs, group);
+  StreamScratch& sc = stream_scratch(s, L.narrow() ? (size_t(L.tiles) * NBINS + 1) / 2 : size_t(L.tiles) * NBINS);
+  if (graphs_enabled()) {
+    if (BatchGraph* g = find_or_capture<KeyT>(L, sc.err, s)) {
+      BatchGraph::Slot& sl = g->slot[g->next];
+      g->next ^= 1;
+      if (sl.launched) AM_CUDA(cudaEventSynchronize(sl.done));
+      std::memcpy(sl.host, L.host.data(), L.tables);
+      KernelTimer kt("batch_graph", s);
+      AM_CUDA(cudaGraphLaunch(sl.exec, s));
+      AM_CUDA(cudaEventRecord(sl.done, s));
+      sl.launched = true;
+      return;
+    }
+  }
+  char* base = static_cast<char*>(dmalloc(L.bytes(), s));
+  copy_h2d(base, L.host.data(), L.tables, s);
+  enqueue_group<KeyT>(L, base, sc.status, sc.err, nullptr, true, s);
   dfree(base, s);
 }
 

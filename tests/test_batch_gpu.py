@@ -120,3 +120,28 @@ def test_all_null_and_constant_arrays(am):
 
 def test_empty_batch(am):
     assert am.argsort_batch([]) == []
+
+
+def test_repeated_shapes_replay_a_graph(am):
+    # The second batch of a shape (same key widths and lengths) is captured into a CUDA graph and
+    # later ones replay it with their own columns, options and outputs: every call must still match
+    # am_argsort_ex2. Two shapes alternate, so both graphs stay in use.
+    # Each position keeps its key width (8 or 4 bytes) from call to call; its type within that width,
+    # its values and its options change.
+    rng = np.random.default_rng(77)
+    wide, narrow = ["int64", "uint64", "float64"], ["int32", "float32", "uint16", "int8", "bool", "float16"]
+    shape_a = [(5000, wide), (1, narrow), (70_000, narrow), (4096, wide), (300_001, narrow)]
+    shape_b = [(123, narrow), (45_678, wide)]
+    for call in range(4):
+        for shape in (shape_a, shape_b):
+            arrays, opts = [], []
+            for n, kinds in shape:
+                arrays.append(random_array(rng, kinds[int(rng.integers(len(kinds)))], n))
+                opts.append((bool(rng.integers(2)), PLACEMENTS[rng.integers(2)], ORDERS[rng.integers(3)]))
+            check_batch(am, arrays, opts)
+    am.profile(True)
+    am.profile_reset()
+    check_batch(am, [random_array(rng, "int64", n) if k is wide else random_array(rng, "int32", n)
+                     for n, k in shape_a], [(False, "at_end", "ieee")] * len(shape_a))
+    assert "batch_graph" in am.profile_entries()
+    am.profile(False)
