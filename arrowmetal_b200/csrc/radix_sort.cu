@@ -1006,22 +1006,22 @@ template <> struct PassConfig<uint64_t> { static constexpr int THREADS = 512, IT
 
 constexpr int HIST_THREADS = 256, HIST_ITEMS = 8;
 
-template <typename KeyT>
+template <typename KeyT, int ITEMS = PassConfig<KeyT>::ITEMS>
 static size_t pass_smem() {
   using C = PassConfig<KeyT>;
-  return sizeof(PassShared<KeyT, C::THREADS, C::ITEMS>);
+  return sizeof(PassShared<KeyT, C::THREADS, ITEMS>);
 }
 
-template <typename KeyT, typename StatusT, bool SEG = false>
+template <typename KeyT, typename StatusT, bool SEG = false, int ITEMS = PassConfig<KeyT>::ITEMS>
 static int pass_blocks_per_sm() {
   using C = PassConfig<KeyT>;
   static int cached = -1;
   static std::once_flag once;
   std::call_once(once, [] {
-    auto fn = onesweep_pass_kernel<KeyT, StatusT, C::THREADS, C::ITEMS, SEG>;
-    AM_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(pass_smem<KeyT>())));
+    auto fn = onesweep_pass_kernel<KeyT, StatusT, C::THREADS, ITEMS, SEG>;
+    AM_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(pass_smem<KeyT, ITEMS>())));
     int b = 0;
-    AM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, C::THREADS, pass_smem<KeyT>()));
+    AM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, C::THREADS, pass_smem<KeyT, ITEMS>()));
     cached = std::max(1, b);
   });
   return cached;
@@ -1270,9 +1270,9 @@ constexpr uint32_t SEG_HIST_ROWS = 32768;   // rows per histogram block
 
 // One key width's arrays of a batch: the tables the kernels read and where everything sits in the
 // group's scratch.
-template <typename KeyT>
+template <typename KeyT, int ITEMS>
 struct GroupLayout {
-  static constexpr uint64_t TILE = uint64_t(PassConfig<KeyT>::THREADS) * PassConfig<KeyT>::ITEMS;
+  static constexpr uint64_t TILE = uint64_t(PassConfig<KeyT>::THREADS) * ITEMS;
   static constexpr int S = int(sizeof(KeyT));
   uint32_t G = 0;
   uint64_t rows = 0, tiles = 0, items = 0, max_n = 0;
@@ -1330,11 +1330,11 @@ struct GroupLayout {
 // The launches of one group, with its scratch at `base` and its tables already there or copied from
 // `pinned_tables` (a graph's first node) when that is given. `timed`: a KernelTimer per launch (not
 // inside a graph capture).
-template <typename KeyT>
-void enqueue_group(const GroupLayout<KeyT>& L, char* base, void* status, uint32_t* err, const void* pinned_tables,
-                   bool timed, cudaStream_t s) {
+template <typename KeyT, int ITEMS>
+void enqueue_group(const GroupLayout<KeyT, ITEMS>& L, char* base, void* status, uint32_t* err,
+                   const void* pinned_tables, bool timed, cudaStream_t s) {
   using C = PassConfig<KeyT>;
-  constexpr int S = GroupLayout<KeyT>::S;
+  constexpr int S = GroupLayout<KeyT, ITEMS>::S;
   if (pinned_tables) AM_CUDA(cudaMemcpyAsync(base, pinned_tables, L.tables, cudaMemcpyHostToDevice, s));
   AM_CUDA(cudaMemsetAsync(base + L.tables, 0, L.header - L.tables, s));
   const SegDesc* d_segs = reinterpret_cast<const SegDesc*>(base);
@@ -1364,7 +1364,7 @@ void enqueue_group(const GroupLayout<KeyT>& L, char* base, void* status, uint32_
   // 64-bit words whose pass epochs (1..S) start over from a zeroed array in every call.
   const bool narrow = L.narrow();
   if (!narrow) AM_CUDA(cudaMemsetAsync(status, 0, size_t(L.tiles) * NBINS * sizeof(uint64_t), s));
-  const int bps = narrow ? pass_blocks_per_sm<KeyT, uint32_t, true>() : pass_blocks_per_sm<KeyT, uint64_t, true>();
+  const int bps = narrow ? pass_blocks_per_sm<KeyT, uint32_t, true, ITEMS>() : pass_blocks_per_sm<KeyT, uint64_t, true, ITEMS>();
   const int grid = int(std::min<uint64_t>(L.tiles, uint64_t(device().sm_count) * bps));
   for (int sl = 0; sl < S; sl++) {
     if (narrow) AM_CUDA(cudaMemsetAsync(status, 0, size_t(L.tiles) * NBINS * sizeof(uint32_t), s));
@@ -1390,9 +1390,9 @@ void enqueue_group(const GroupLayout<KeyT>& L, char* base, void* status, uint32_
     const ColView none{};
     std::unique_ptr<KernelTimer> kt(timed ? new KernelTimer("batch_pass", s) : nullptr);
     if (narrow)
-      onesweep_pass_kernel<KeyT, uint32_t, C::THREADS, C::ITEMS, true><<<std::max(grid, 1), C::THREADS, pass_smem<KeyT>(), s>>>(a, none);
+      onesweep_pass_kernel<KeyT, uint32_t, C::THREADS, ITEMS, true><<<std::max(grid, 1), C::THREADS, pass_smem<KeyT, ITEMS>(), s>>>(a, none);
     else
-      onesweep_pass_kernel<KeyT, uint64_t, C::THREADS, C::ITEMS, true><<<std::max(grid, 1), C::THREADS, pass_smem<KeyT>(), s>>>(a, none);
+      onesweep_pass_kernel<KeyT, uint64_t, C::THREADS, ITEMS, true><<<std::max(grid, 1), C::THREADS, pass_smem<KeyT, ITEMS>(), s>>>(a, none);
     AM_CUDA(cudaGetLastError());
   }
 }
@@ -1407,6 +1407,7 @@ void enqueue_group(const GroupLayout<KeyT>& L, char* base, void* status, uint32_
 // their own pinned tables alternate, so a batch never waits for the one just before it.
 struct BatchGraph {
   int width = 0;
+  int items = 0;
   cudaStream_t stream = nullptr;
   std::vector<uint32_t> lens;
   char* base = nullptr;                 // scratch (device)
@@ -1451,10 +1452,10 @@ bool graphs_enabled() {
   return on;
 }
 
-template <typename KeyT>
-BatchGraph* find_or_capture(const GroupLayout<KeyT>& L, uint32_t* err, cudaStream_t s) {
+template <typename KeyT, int ITEMS>
+BatchGraph* find_or_capture(const GroupLayout<KeyT, ITEMS>& L, uint32_t* err, cudaStream_t s) {
   GraphCache& c = graph_cache();
-  const int width = int(sizeof(KeyT));
+  const int width = int(sizeof(KeyT)) * 100 + ITEMS;    // key width and tile shape
   for (auto it = c.graphs.begin(); it != c.graphs.end(); ++it) {
     if ((*it)->width == width && (*it)->stream == s && (*it)->lens == L.lens) {
       c.graphs.splice(c.graphs.begin(), c.graphs, it);
@@ -1478,15 +1479,15 @@ BatchGraph* find_or_capture(const GroupLayout<KeyT>& L, uint32_t* err, cudaStrea
   const size_t status_bytes = size_t(L.tiles) * NBINS * (L.narrow() ? sizeof(uint32_t) : sizeof(uint64_t));
   AM_CUDA(cudaMalloc(&g->status, std::max<size_t>(status_bytes, 16)));
   // Launch attributes and occupancy are looked up before the capture.
-  (void)pass_blocks_per_sm<KeyT, uint32_t, true>();
-  (void)pass_blocks_per_sm<KeyT, uint64_t, true>();
+  (void)pass_blocks_per_sm<KeyT, uint32_t, true, ITEMS>();
+  (void)pass_blocks_per_sm<KeyT, uint64_t, true, ITEMS>();
   for (auto& sl : g->slot) {
     sl.host = pinned_alloc(L.tables);
     AM_CUDA(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
     cudaGraph_t graph = nullptr;
     AM_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     try {
-      enqueue_group<KeyT>(L, g->base, g->status, err, sl.host, false, s);
+      enqueue_group<KeyT, ITEMS>(L, g->base, g->status, err, sl.host, false, s);
     } catch (...) {
       cudaGraph_t discard = nullptr;
       (void)cudaStreamEndCapture(s, &discard);
@@ -1503,13 +1504,13 @@ BatchGraph* find_or_capture(const GroupLayout<KeyT>& L, uint32_t* err, cudaStrea
   return c.graphs.front().get();
 }
 
-template <typename KeyT>
-void sort_segment_group(const std::vector<SortKey>& keys, const std::vector<void*>& outs,
-                        const std::vector<size_t>& group, cudaStream_t s) {
-  GroupLayout<KeyT> L(keys, outs, group);
+template <typename KeyT, int ITEMS>
+void sort_segment_class(const std::vector<SortKey>& keys, const std::vector<void*>& outs,
+                        const std::vector<size_t>& group, bool allow_graph, cudaStream_t s) {
+  GroupLayout<KeyT, ITEMS> L(keys, outs, group);
   StreamScratch& sc = stream_scratch(s, L.narrow() ? (size_t(L.tiles) * NBINS + 1) / 2 : size_t(L.tiles) * NBINS);
-  if (graphs_enabled()) {
-    if (BatchGraph* g = find_or_capture<KeyT>(L, sc.err, s)) {
+  if (allow_graph && graphs_enabled()) {
+    if (BatchGraph* g = find_or_capture<KeyT, ITEMS>(L, sc.err, s)) {
       BatchGraph::Slot& sl = g->slot[g->next];
       g->next ^= 1;
       if (sl.launched) AM_CUDA(cudaEventSynchronize(sl.done));
@@ -1523,8 +1524,77 @@ void sort_segment_group(const std::vector<SortKey>& keys, const std::vector<void
   }
   char* base = static_cast<char*>(dmalloc(L.bytes(), s));
   copy_h2d(base, L.host.data(), L.tables, s);
-  enqueue_group<KeyT>(L, base, sc.status, sc.err, nullptr, true, s);
+  enqueue_group<KeyT, ITEMS>(L, base, sc.status, sc.err, nullptr, true, s);
   dfree(base, s);
+}
+
+// ---- Tile shape per size class, chosen by measurement.
+//
+// Arrays of a key width are sorted in two size classes (up to SMALL_ARRAY_ROWS rows, and above), each
+// with its own launches and tile shape: 512 threads x 8 rows (4096-row tiles) or x 4 rows (2048). The
+// first batch whose class holds at least TUNE_MIN_ROWS rows runs that class with both shapes, timed by
+// CUDA events, and the faster shape serves the class from then on (its second run leaves the same,
+// final output). ARROWMETAL_SEG_ITEMS=4 or 8 fixes the shape instead.
+constexpr uint32_t SMALL_ARRAY_ROWS = 16384;
+constexpr uint64_t TUNE_MIN_ROWS = uint64_t(2) << 20;
+
+std::mutex g_tune_mu;
+int g_tuned_items[2][2] = {{0, 0}, {0, 0}};   // [key width 4 / 8][size class]: 0 = not yet measured
+
+int forced_items() {
+  static const int v = [] {
+    const char* e = std::getenv("ARROWMETAL_SEG_ITEMS");
+    const int x = e ? std::atoi(e) : 0;
+    return (x == 4 || x == 8) ? x : 0;
+  }();
+  return v;
+}
+
+int tuned_items(int width, int cls) {
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  return g_tuned_items[width == 8][cls];
+}
+
+template <typename KeyT>
+void sort_segment_group(const std::vector<SortKey>& keys, const std::vector<void*>& outs,
+                        const std::vector<size_t>& group, cudaStream_t s) {
+  std::vector<size_t> cls[2];
+  uint64_t cls_rows[2] = {0, 0};
+  for (size_t i : group) {
+    const int c = uint64_t(keys[i].col->length) <= SMALL_ARRAY_ROWS ? 0 : 1;
+    cls[c].push_back(i);
+    cls_rows[c] += uint64_t(keys[i].col->length);
+  }
+  const int width = int(sizeof(KeyT));
+  for (int c = 0; c < 2; c++) {
+    if (cls[c].empty()) continue;
+    int items = forced_items();
+    if (!items) items = tuned_items(width, c);
+    if (!items && cls_rows[c] >= TUNE_MIN_ROWS) {
+      // Measure both shapes on this batch; the second run's output is the result.
+      float ms[2] = {0, 0};
+      const int shapes[2] = {4, 8};
+      cudaEvent_t e0, e1;
+      AM_CUDA(cudaEventCreate(&e0));
+      AM_CUDA(cudaEventCreate(&e1));
+      for (int k = 0; k < 2; k++) {
+        AM_CUDA(cudaEventRecord(e0, s));
+        if (shapes[k] == 4) sort_segment_class<KeyT, 4>(keys, outs, cls[c], false, s);
+        else sort_segment_class<KeyT, 8>(keys, outs, cls[c], false, s);
+        AM_CUDA(cudaEventRecord(e1, s));
+        AM_CUDA(cudaEventSynchronize(e1));
+        AM_CUDA(cudaEventElapsedTime(&ms[k], e0, e1));
+      }
+      (void)cudaEventDestroy(e0);
+      (void)cudaEventDestroy(e1);
+      std::lock_guard<std::mutex> g(g_tune_mu);
+      g_tuned_items[width == 8][c] = ms[0] < ms[1] ? 4 : 8;
+      continue;
+    }
+    if (!items) items = 8;
+    if (items == 4) sort_segment_class<KeyT, 4>(keys, outs, cls[c], true, s);
+    else sort_segment_class<KeyT, 8>(keys, outs, cls[c], true, s);
+  }
 }
 
 }  // namespace
