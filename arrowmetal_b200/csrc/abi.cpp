@@ -667,6 +667,18 @@ int am_top_k_ex(am_array* a, int64_t k, int largest, int null_placement, int flo
       *out = make_index_array(0, 4, stream());
       return 0;
     }
+    // k below the rows: radix selection, unless it would take most of the value rows anyway.
+    if (k < a->length) {
+      float_order_ok(float_order);
+      check_index_rows(a->length, "top_k");
+      cudaStream_t s = stream();
+      use_on(a, s);
+      if (am_array* r = radix_top_k(key[0], k, s)) {
+        checkpoint(s);
+        *out = r;
+        return 0;
+      }
+    }
     am_array* idx = argsort_keys(key, 4, "top_k");
     const int64_t m = std::min<int64_t>(k, idx->length);
     if (m == idx->length) {

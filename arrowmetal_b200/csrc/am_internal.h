@@ -217,6 +217,14 @@ struct SortKey {
 void radix_argsort(const std::vector<SortKey>& keys, int64_t n, void* out, int index_width,
                    cudaStream_t s, am_sort_stats* stats);
 
+namespace rs { struct KeyStats; struct ColView; ColView make_view(const SortKey& k); }
+// The key column's statistics (all digit histograms of its value keys, null / NaN / value counts)
+// into `st` on the device.
+void key_statistics(const SortKey& k, rs::KeyStats* st, cudaStream_t s);
+// The first min(k, rows) indices of the stable argsort of `key`, by radix selection; NULL when a full
+// sort is the better way (k close to the number of value rows).
+am_array* radix_top_k(const SortKey& key, int64_t k, cudaStream_t s);
+
 // True when the key column can be rebuilt from its sorted keys (the key map is a bijection).
 bool key_invertible(const SortKey& k);
 // The sort engine. `out` (may be NULL) receives the index array; `key_dst` (may be NULL; one
