@@ -1,21 +1,27 @@
 // Top-k by radix selection: the first k indices of the stable argsort without sorting every row.
 //
 // am_top_k_ex answers with the first k indices am_argsort_ex2 gives with the same options
-// (include/arrowmetal.h:1345-1350; the reference's TopK.swift / RadixSelect.swift select on the same
-// key maps). In the argsort's arrangement the value rows come in key order and the NaN-block and null
-// rows in row order ([values][NaN][nulls] with nulls at the end, [nulls][NaN][values] at the start),
-// so the answer is some leading category rows in row order plus the kv smallest value keys, ties in
-// row order. On the order-preserving unsigned keys of the sort:
-//   1. the key statistics (one read) give the category counts and the most significant digit's
-//      histogram;
-//   2. one histogram per lower digit over the value rows that share the digits chosen so far narrows
-//      the threshold key T down to the digit at which the kv-th smallest key sits;
-//   3. a stable two-phase compaction (per-block counts, one scan, ordered writes) takes every value row
-//      with key < T and the first `need` rows with key == T, in row order: exactly kv candidates;
-//   4. those kv (key, row) pairs are argsorted by the radix sort and their rows written out;
-//   5. the category rows needed before or after them are compacted in row order the same way.
+// (include/arrowmetal.h:1345-1350; the reference selects on the same key maps in TopK.swift and
+// RadixSelect.swift). In the argsort's arrangement the value rows come in key order and the NaN-block
+// and null rows in row order ([values][NaN][nulls] with nulls at the end, [nulls][NaN][values] at the
+// start), so the answer is some category rows in row order plus the kv smallest value keys, ties in
+// row order. On the order-preserving unsigned keys of the sort, reading the column twice:
+//   1. the key statistics give the category counts and every digit's histogram; on the host, the
+//      digits that are constant over the value keys and the first one that is not (digit dv, whose
+//      histogram is then exact for the rows that share the constant ones) fix the threshold's leading
+//      digits and the rank k_rem of the wanted key within its bucket;
+//   2. one ordered compaction of the column extracts every value row whose leading digits (down to dv)
+//      are at most the threshold's -- all rows below the bucket and the bucket itself -- as
+//      (key, row) pairs in row order;
+//   3. on that buffer, a histogram per lower digit over the pairs that share the digits chosen so far
+//      narrows the threshold key T to its last digit;
+//   4. an ordered compaction of the buffer takes every pair with key < T and the first `need` pairs
+//      with key == T: exactly kv candidates, in row order;
+//   5. the candidates are argsorted by the radix sort (stable, so equal keys stay in row order) and
+//      their rows written out, beside the category rows, compacted in row order the same way.
 // The output is bit-identical to the prefix of the full argsort.
 #include <algorithm>
+#include <vector>
 
 #include "am_internal.h"
 #include "key_encode.cuh"
@@ -26,16 +32,46 @@ namespace rs {
 namespace {
 
 constexpr int SEL_THREADS = 256, SEL_ITEMS = 8;
-constexpr uint64_t SEL_CHUNK = uint64_t(SEL_THREADS) * SEL_ITEMS;   // rows per block in the compaction
+constexpr uint64_t SEL_CHUNK = uint64_t(SEL_THREADS) * SEL_ITEMS;   // rows per block in a compaction
 
 struct SelState {
   unsigned long long prefix;    // the threshold key's digits chosen so far
-  unsigned long long k_rem;     // rank of the wanted key among the rows that share them (1-based)
+  unsigned long long k_rem;     // rank of the wanted key among the keys that share them (1-based)
 };
+
+// Where a selection step reads: the key column itself (each key encoded on the fly), or a buffer of
+// encoded value keys with their row numbers.
+template <typename KeyT>
+struct Source {
+  ColView col;
+  const KeyT* keys;       // NULL: the column
+  const uint32_t* rows;
+  uint64_t n;
+};
+
+// Positions pos[i] of the source: keys, categories (0 value, 1 NaN block, 2 null) and row numbers.
+template <typename KeyT>
+__device__ __forceinline__ void load_source(const Source<KeyT>& s, const uint32_t (&pos)[SEL_ITEMS], uint32_t ok,
+                                            KeyT (&key)[SEL_ITEMS], int (&cat)[SEL_ITEMS],
+                                            uint32_t (&row)[SEL_ITEMS]) {
+  if (s.keys) {
+#pragma unroll
+    for (int i = 0; i < SEL_ITEMS; i++) {
+      const bool live = (ok >> i) & 1u;
+      key[i] = live ? s.keys[pos[i]] : KeyT(0);
+      row[i] = live ? s.rows[pos[i]] : 0u;
+      cat[i] = 0;
+    }
+  } else {
+    encode_rows<KeyT, SEL_ITEMS>(s.col, pos, ok, key, cat);
+#pragma unroll
+    for (int i = 0; i < SEL_ITEMS; i++) row[i] = pos[i];
+  }
+}
 
 // Digit `shift` of the value keys whose digits above it equal the state's prefix.
 template <typename KeyT>
-__global__ void __launch_bounds__(SEL_THREADS) select_histogram_kernel(const __grid_constant__ ColView col, uint64_t n,
+__global__ void __launch_bounds__(SEL_THREADS) select_histogram_kernel(const __grid_constant__ Source<KeyT> src,
                                                                        int shift, const SelState* __restrict__ st,
                                                                        uint32_t* __restrict__ hist) {
   __shared__ uint32_t sh[256];
@@ -43,23 +79,23 @@ __global__ void __launch_bounds__(SEL_THREADS) select_histogram_kernel(const __g
   __syncthreads();
   const KeyT want = KeyT(st->prefix >> (shift + 8));
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (uint64_t base = uint64_t(blockIdx.x) * SEL_CHUNK; base < n; base += uint64_t(gridDim.x) * SEL_CHUNK) {
-    uint32_t row[SEL_ITEMS];
+  for (uint64_t base = uint64_t(blockIdx.x) * SEL_CHUNK; base < src.n; base += uint64_t(gridDim.x) * SEL_CHUNK) {
+    uint32_t pos[SEL_ITEMS];
     uint32_t ok = 0;
 #pragma unroll
     for (int i = 0; i < SEL_ITEMS; i++) {
       const uint64_t g = base + uint64_t(warp) * (SEL_ITEMS * 32) + uint64_t(i) * 32 + lane;
-      row[i] = uint32_t(g);
-      if (g < n) ok |= 1u << i;
+      pos[i] = uint32_t(g);
+      if (g < src.n) ok |= 1u << i;
     }
     KeyT key[SEL_ITEMS];
     int cat[SEL_ITEMS];
-    encode_rows<KeyT, SEL_ITEMS>(col, row, ok, key, cat);
+    uint32_t row[SEL_ITEMS];
+    load_source<KeyT>(src, pos, ok, key, cat, row);
 #pragma unroll
     for (int i = 0; i < SEL_ITEMS; i++) {
       if (!((ok >> i) & 1u) || cat[i] != 0) continue;
-      const KeyT hi = (shift + 8 >= int(8 * sizeof(KeyT))) ? KeyT(0) : KeyT(key[i] >> (shift + 8));
-      if (hi == want) atomicAdd(&sh[uint32_t(key[i] >> shift) & 255u], 1u);
+      if (KeyT(key[i] >> (shift + 8)) == want) atomicAdd(&sh[uint32_t(key[i] >> shift) & 255u], 1u);
     }
   }
   __syncthreads();
@@ -71,11 +107,10 @@ __global__ void __launch_bounds__(SEL_THREADS) select_histogram_kernel(const __g
 // among the keys with that digit.
 __global__ void __launch_bounds__(256) select_step_kernel(const uint32_t* __restrict__ hist, int shift,
                                                           SelState* __restrict__ st) {
-  __shared__ uint32_t incl[256];
-  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   __shared__ uint32_t wsum[8];
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const unsigned long long k = st->k_rem;     // read by every thread before the one writer below
-  uint32_t v = hist[t];
+  const uint32_t v = hist[t];
   uint32_t x = v;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
@@ -86,10 +121,8 @@ __global__ void __launch_bounds__(256) select_step_kernel(const uint32_t* __rest
   __syncthreads();
   uint32_t add = 0;
   for (int w = 0; w < warp; w++) add += wsum[w];
-  incl[t] = x + add;
-  __syncthreads();
-  const uint32_t before = incl[t] - v;
-  if (v > 0 && before < k && k <= incl[t]) {
+  const uint32_t incl = x + add, before = incl - v;
+  if (v > 0 && before < k && k <= incl) {
     st->prefix |= (unsigned long long)t << shift;
     st->k_rem = k - before;
   }
@@ -118,34 +151,44 @@ __device__ __forceinline__ uint32_t block_scan(uint32_t v, uint32_t* s_warp, uin
   return x - v + add;
 }
 
-// The rows a compaction takes: every row of class A, and class-B rows up to `limit` in row order.
-//   mode 0: A = value rows with key < T, B = value rows with key == T (T = the state's prefix);
-//   mode 1: A = none, B = rows of category `cat` (1 NaN block, 2 null).
+// The entries a compaction takes, in source order: every entry of class A, and class-B entries up to
+// `limit`.
+//   PRED_PREFIX: A = value keys with (key >> shift) < p, B = those with (key >> shift) == p, no limit;
+//   PRED_THRESHOLD: A = keys < T, B = keys == T, limit k_rem (T, k_rem: the selection state);
+//   PRED_CATEGORY: B = rows of category `cat` (1 NaN block, 2 null), up to `limit`.
+constexpr int PRED_PREFIX = 0, PRED_THRESHOLD = 1, PRED_CATEGORY = 2;
 struct Compact {
   int mode;
   int cat;
-  unsigned long long limit;     // mode 1; mode 0 reads the state's k_rem
+  int shift;
+  unsigned long long p;
+  unsigned long long limit;
   const SelState* st;
 };
 
 template <typename KeyT>
-__device__ __forceinline__ void classify(const ColView& col, const Compact& c, uint64_t base, uint64_t n,
-                                         uint32_t (&a)[SEL_ITEMS], uint32_t (&b)[SEL_ITEMS], KeyT (&key)[SEL_ITEMS]) {
-  uint32_t row[SEL_ITEMS];
+__device__ __forceinline__ void classify(const Source<KeyT>& src, const Compact& c, uint64_t base,
+                                         uint32_t (&a)[SEL_ITEMS], uint32_t (&b)[SEL_ITEMS], KeyT (&key)[SEL_ITEMS],
+                                         uint32_t (&row)[SEL_ITEMS]) {
+  uint32_t pos[SEL_ITEMS];
   uint32_t ok = 0;
 #pragma unroll
   for (int i = 0; i < SEL_ITEMS; i++) {
-    const uint64_t g = base + uint64_t(threadIdx.x) * SEL_ITEMS + i;   // consecutive rows per thread
-    row[i] = uint32_t(g);
-    if (g < n) ok |= 1u << i;
+    const uint64_t g = base + uint64_t(threadIdx.x) * SEL_ITEMS + i;   // consecutive entries per thread
+    pos[i] = uint32_t(g);
+    if (g < src.n) ok |= 1u << i;
   }
   int cat[SEL_ITEMS];
-  encode_rows<KeyT, SEL_ITEMS>(col, row, ok, key, cat);
-  const KeyT T = KeyT(c.st ? c.st->prefix : 0);
+  load_source<KeyT>(src, pos, ok, key, cat, row);
+  const KeyT T = KeyT(c.mode == PRED_THRESHOLD ? c.st->prefix : 0);
 #pragma unroll
   for (int i = 0; i < SEL_ITEMS; i++) {
     const bool live = (ok >> i) & 1u;
-    if (c.mode == 0) {
+    if (c.mode == PRED_PREFIX) {
+      const KeyT hi = KeyT(key[i] >> c.shift);
+      a[i] = live && cat[i] == 0 && hi < KeyT(c.p);
+      b[i] = live && cat[i] == 0 && hi == KeyT(c.p);
+    } else if (c.mode == PRED_THRESHOLD) {
       a[i] = live && cat[i] == 0 && key[i] < T;
       b[i] = live && cat[i] == 0 && key[i] == T;
     } else {
@@ -156,14 +199,14 @@ __device__ __forceinline__ void classify(const ColView& col, const Compact& c, u
 }
 
 template <typename KeyT>
-__global__ void __launch_bounds__(SEL_THREADS) compact_count_kernel(const __grid_constant__ ColView col, uint64_t n,
+__global__ void __launch_bounds__(SEL_THREADS) compact_count_kernel(const __grid_constant__ Source<KeyT> src,
                                                                     const __grid_constant__ Compact c,
                                                                     uint32_t* __restrict__ count_a,
                                                                     uint32_t* __restrict__ count_b) {
   __shared__ uint32_t s_warp[SEL_THREADS / 32];
-  uint32_t a[SEL_ITEMS], b[SEL_ITEMS];
+  uint32_t a[SEL_ITEMS], b[SEL_ITEMS], row[SEL_ITEMS];
   KeyT key[SEL_ITEMS];
-  classify<KeyT>(col, c, uint64_t(blockIdx.x) * SEL_CHUNK, n, a, b, key);
+  classify<KeyT>(src, c, uint64_t(blockIdx.x) * SEL_CHUNK, a, b, key, row);
   uint32_t ca = 0, cb = 0;
 #pragma unroll
   for (int i = 0; i < SEL_ITEMS; i++) {
@@ -222,9 +265,9 @@ __global__ void __launch_bounds__(1024) compact_scan_kernel(uint32_t* __restrict
   }
 }
 
-// The ordered writes: row ids (and, in mode 0, keys) of the taken rows at their places.
+// The ordered writes: row numbers (and keys, when asked) of the taken entries at their places.
 template <typename KeyT>
-__global__ void __launch_bounds__(SEL_THREADS) compact_write_kernel(const __grid_constant__ ColView col, uint64_t n,
+__global__ void __launch_bounds__(SEL_THREADS) compact_write_kernel(const __grid_constant__ Source<KeyT> src,
                                                                     const __grid_constant__ Compact c,
                                                                     const uint32_t* __restrict__ off_a,
                                                                     const uint32_t* __restrict__ off_b,
@@ -232,15 +275,14 @@ __global__ void __launch_bounds__(SEL_THREADS) compact_write_kernel(const __grid
                                                                     uint32_t* __restrict__ out_rows, uint64_t out_cap,
                                                                     uint32_t* __restrict__ err) {
   __shared__ uint32_t s_warp[SEL_THREADS / 32];
-  uint32_t a[SEL_ITEMS], b[SEL_ITEMS];
+  uint32_t a[SEL_ITEMS], b[SEL_ITEMS], row[SEL_ITEMS];
   KeyT key[SEL_ITEMS];
-  const uint64_t base = uint64_t(blockIdx.x) * SEL_CHUNK;
-  classify<KeyT>(col, c, base, n, a, b, key);
-  const unsigned long long limit = c.mode == 0 ? c.st->k_rem : c.limit;
+  classify<KeyT>(src, c, uint64_t(blockIdx.x) * SEL_CHUNK, a, b, key, row);
+  const unsigned long long limit = c.mode == PRED_THRESHOLD ? c.st->k_rem : c.limit;
   uint32_t cb = 0;
 #pragma unroll
   for (int i = 0; i < SEL_ITEMS; i++) cb += b[i];
-  const uint32_t eb = block_scan(cb, s_warp, nullptr);    // B rows before this thread's, in the block
+  const uint32_t eb = block_scan(cb, s_warp, nullptr);    // B entries before this thread's, in the block
   const unsigned long long b_before = off_b[blockIdx.x];
   uint32_t take[SEL_ITEMS];
   uint32_t cp = 0, rb = 0;
@@ -261,7 +303,7 @@ __global__ void __launch_bounds__(SEL_THREADS) compact_write_kernel(const __grid
       atomicOr(err, ERR_BOUNDS);
       continue;
     }
-    out_rows[d] = uint32_t(base + uint64_t(threadIdx.x) * SEL_ITEMS + i);
+    out_rows[d] = row[i];
     if (out_keys) out_keys[d] = key[i];
   }
 }
@@ -274,30 +316,29 @@ __global__ void __launch_bounds__(256) gather_rows_kernel(const uint32_t* __rest
 }
 
 template <typename KeyT>
-void compact(const ColView& cv, uint64_t n, const Compact& c, KeyT* out_keys, uint32_t* out_rows, uint64_t cap,
+void compact(const Source<KeyT>& src, const Compact& c, KeyT* out_keys, uint32_t* out_rows, uint64_t cap,
              uint32_t* counts, uint32_t* err, cudaStream_t s) {
-  const uint32_t blocks = uint32_t((n + SEL_CHUNK - 1) / SEL_CHUNK);
+  const uint32_t blocks = uint32_t((src.n + SEL_CHUNK - 1) / SEL_CHUNK);
+  if (blocks == 0) return;
   uint32_t* count_a = counts;
   uint32_t* count_b = counts + blocks;
-  {
-    KernelTimer kt("topk_compact", s);
-    compact_count_kernel<KeyT><<<blocks, SEL_THREADS, 0, s>>>(cv, n, c, count_a, count_b);
-    AM_CUDA(cudaGetLastError());
-    compact_scan_kernel<<<1, 1024, 0, s>>>(count_a, count_b, blocks);
-    AM_CUDA(cudaGetLastError());
-    compact_write_kernel<KeyT><<<blocks, SEL_THREADS, 0, s>>>(cv, n, c, count_a, count_b, out_keys, out_rows, cap, err);
-    AM_CUDA(cudaGetLastError());
-  }
+  KernelTimer kt("topk_compact", s);
+  compact_count_kernel<KeyT><<<blocks, SEL_THREADS, 0, s>>>(src, c, count_a, count_b);
+  AM_CUDA(cudaGetLastError());
+  compact_scan_kernel<<<1, 1024, 0, s>>>(count_a, count_b, blocks);
+  AM_CUDA(cudaGetLastError());
+  compact_write_kernel<KeyT><<<blocks, SEL_THREADS, 0, s>>>(src, c, count_a, count_b, out_keys, out_rows, cap, err);
+  AM_CUDA(cudaGetLastError());
 }
 
 template <typename KeyT>
 am_array* top_k_of(const SortKey& key, int64_t k, cudaStream_t s) {
   const uint64_t n = uint64_t(key.col->length);
   constexpr int D = int(sizeof(KeyT));
-  const ColView cv = make_view(key);
+  const Source<KeyT> column{make_view(key), nullptr, nullptr, n};
   const uint32_t blocks = uint32_t((n + SEL_CHUNK - 1) / SEL_CHUNK);
 
-  // Scratch: statistics, state, per-digit histograms, compaction counts.
+  // Scratch: statistics, selection state, per-digit histograms, compaction counts.
   auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
   const size_t off_state = up(sizeof(KeyStats));
   const size_t off_hist = up(off_state + sizeof(SelState));
@@ -311,12 +352,13 @@ am_array* top_k_of(const SortKey& key, int64_t k, cudaStream_t s) {
   uint32_t* counts = reinterpret_cast<uint32_t*>(base + off_counts);
   key_statistics(key, st, s);
 
-  // The category counts decide the shape of the answer.
-  static thread_local uint32_t* host = nullptr;
-  if (!host) host = static_cast<uint32_t*>(pinned_alloc(16));
-  AM_CUDA(cudaMemcpyAsync(host, &st->n_value, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  // The statistics on the host: the category counts shape the answer, the digit histograms fix the
+  // threshold's leading digits.
+  static thread_local KeyStats* host = nullptr;
+  if (!host) host = static_cast<KeyStats*>(pinned_alloc(sizeof(KeyStats)));
+  AM_CUDA(cudaMemcpyAsync(host, st, sizeof(KeyStats), cudaMemcpyDeviceToHost, s));
   AM_CUDA(cudaStreamSynchronize(s));
-  const uint64_t n_value = host[0], n_null = host[1], n_nan = host[2];
+  const uint64_t n_value = host->n_value, n_null = host->n_null, n_nan = host->n_nan;
   const uint64_t m = std::min<uint64_t>(uint64_t(k), n);
   uint64_t kv, k_nan, k_null;
   if (!key.nulls_first) {
@@ -342,34 +384,78 @@ am_array* top_k_of(const SortKey& key, int64_t k, cudaStream_t s) {
     const uint64_t v_at = key.nulls_first ? k_null + k_nan : 0;
     const uint64_t nan_at = key.nulls_first ? k_null : kv;
     const uint64_t null_at = key.nulls_first ? 0 : kv + k_nan;
-    if (k_null) compact<KeyT>(cv, n, Compact{1, 2, k_null, nullptr}, nullptr, res + null_at, k_null, counts, err, s);
-    if (k_nan) compact<KeyT>(cv, n, Compact{1, 1, k_nan, nullptr}, nullptr, res + nan_at, k_nan, counts, err, s);
+    if (k_null) compact<KeyT>(column, Compact{PRED_CATEGORY, 2, 0, 0, k_null, nullptr}, nullptr, res + null_at, k_null,
+                              counts, err, s);
+    if (k_nan) compact<KeyT>(column, Compact{PRED_CATEGORY, 1, 0, 0, k_nan, nullptr}, nullptr, res + nan_at, k_nan,
+                             counts, err, s);
     if (kv) {
-      // Threshold: digit by digit from the most significant (whose histogram the statistics hold).
-      const SelState init{0ull, (unsigned long long)kv};
-      AM_CUDA(cudaMemcpyAsync(state, &init, sizeof(SelState), cudaMemcpyHostToDevice, s));
-      AM_CUDA(cudaMemsetAsync(hist, 0, sizeof(uint32_t) * 256 * D, s));
-      {
-        KernelTimer kt("topk_select", s);
-        for (int d = D - 1; d >= 0; d--) {
-          const uint32_t* h = st->hist[d];
-          if (d < D - 1) {
-            uint32_t* hd = hist + 256 * d;
-            const int grid = int(std::min<uint64_t>((n + SEL_CHUNK - 1) / SEL_CHUNK, uint64_t(device().sm_count) * 8));
-            select_histogram_kernel<KeyT><<<std::max(grid, 1), SEL_THREADS, 0, s>>>(cv, n, 8 * d, state, hd);
-            AM_CUDA(cudaGetLastError());
-            h = hd;
-          }
-          select_step_kernel<<<1, 256, 0, s>>>(h, 8 * d, state);
-          AM_CUDA(cudaGetLastError());
+      // 1. Leading digits on the host: constant ones, then the first that varies (digit dv).
+      unsigned long long prefix = 0, k_rem = kv;
+      int dv = -1;
+      uint64_t below = 0, bucket = 0;
+      for (int d = D - 1; d >= 0; d--) {
+        const uint32_t* h = host->hist[d];
+        int only = -1, nonzero = 0;
+        for (int b = 0; b < 256; b++)
+          if (h[b]) { nonzero++; only = b; }
+        if (nonzero == 1) {
+          prefix |= (unsigned long long)only << (8 * d);
+          continue;
         }
+        uint64_t run = 0;
+        for (int b = 0; b < 256; b++) {
+          if (h[b] && run < k_rem && k_rem <= run + h[b]) {
+            prefix |= (unsigned long long)b << (8 * d);
+            k_rem -= run;
+            below = run;
+            bucket = h[b];
+            break;
+          }
+          run += h[b];
+        }
+        dv = d;
+        break;
       }
-      // The kv candidates in row order, then their stable argsort.
+      const SelState init{prefix, k_rem};
+      AM_CUDA(cudaMemcpyAsync(state, &init, sizeof(SelState), cudaMemcpyHostToDevice, s));
       BufPtr cand_keys = DevBuffer::alloc(size_t(kv) * sizeof(KeyT) + 16, s);
       BufPtr cand_rows = DevBuffer::alloc(size_t(kv) * 4 + 16, s);
       BufPtr order = DevBuffer::alloc(size_t(kv) * 4 + 16, s);
-      compact<KeyT>(cv, n, Compact{0, 0, 0, state}, static_cast<KeyT*>(cand_keys->ptr),
-                    static_cast<uint32_t*>(cand_rows->ptr), kv, counts, err, s);
+      if (dv < 0) {
+        // Every value key is the same: the first kv value rows, in row order.
+        compact<KeyT>(column, Compact{PRED_THRESHOLD, 0, 0, 0, 0, state}, static_cast<KeyT*>(cand_keys->ptr),
+                      static_cast<uint32_t*>(cand_rows->ptr), kv, counts, err, s);
+      } else {
+        // 2. The rows at or below the threshold's bucket of digit dv, as (key, row) pairs in row order.
+        const uint64_t n1 = below + bucket;
+        BufPtr keys1 = DevBuffer::alloc(size_t(n1) * sizeof(KeyT) + 16, s);
+        BufPtr rows1 = DevBuffer::alloc(size_t(n1) * 4 + 16, s);
+        compact<KeyT>(column, Compact{PRED_PREFIX, 0, 8 * dv, prefix >> (8 * dv), ~0ull, nullptr},
+                      static_cast<KeyT*>(keys1->ptr), static_cast<uint32_t*>(rows1->ptr), n1, counts, err, s);
+        const Source<KeyT> cand{column.col, static_cast<const KeyT*>(keys1->ptr),
+                                static_cast<const uint32_t*>(rows1->ptr), n1};
+        // 3. The lower digits on the pairs.
+        if (dv > 0) {
+          AM_CUDA(cudaMemsetAsync(hist, 0, sizeof(uint32_t) * 256 * D, s));
+          KernelTimer kt("topk_select", s);
+          const int grid = int(std::min<uint64_t>((n1 + SEL_CHUNK - 1) / SEL_CHUNK, uint64_t(device().sm_count) * 8));
+          for (int d = dv - 1; d >= 0; d--) {
+            uint32_t* hd = hist + 256 * d;
+            select_histogram_kernel<KeyT><<<std::max(grid, 1), SEL_THREADS, 0, s>>>(cand, 8 * d, state, hd);
+            AM_CUDA(cudaGetLastError());
+            select_step_kernel<<<1, 256, 0, s>>>(hd, 8 * d, state);
+            AM_CUDA(cudaGetLastError());
+          }
+        }
+        // 4. Keys below the threshold and the first `need` equal to it: the kv candidates.
+        const uint32_t blocks1 = uint32_t((n1 + SEL_CHUNK - 1) / SEL_CHUNK);
+        if (blocks1 > blocks) throw Error("top_k: candidate buffer larger than its column");
+        compact<KeyT>(cand, Compact{PRED_THRESHOLD, 0, 0, 0, 0, state}, static_cast<KeyT*>(cand_keys->ptr),
+                      static_cast<uint32_t*>(cand_rows->ptr), kv, counts, err, s);
+        keys1->stream = s;
+        rows1->stream = s;
+      }
+      // 5. The candidates in key order (stable: equal keys stay in row order).
       am_array* tmp = new_array(D == 8 ? PT_U64 : PT_U32, D == 8 ? "L" : "I", int64_t(kv));
       tmp->values = cand_keys;
       tmp->null_count = 0;

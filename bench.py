@@ -379,6 +379,39 @@ def run_single(args, am, torch, stream, local):
         "clocks": clocks.summary()}))
 
 
+def run_topk(args, am, torch, stream, local):
+    """--workload topk: ORDER BY key LIMIT k on the 50M-row key column (int64 in [0, 2^40), 10% nulls):
+    am_top_k_ex (radix selection) for several k against the full argsort, CUDA events per call."""
+    import pyarrow as pa
+    key, valid, _, _ = make_table(N_ROWS)
+    col = am.MetalArray.from_arrow(pa.array(key, mask=~valid))
+
+    def timed(fn, reps):
+        for _ in range(3):
+            fn()
+        am.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(reps):
+            fn()
+        ev1.record(stream)
+        ev1.synchronize()
+        am.synchronize()
+        return ev0.elapsed_time(ev1) / reps
+
+    with ClockSampler(local) as clocks:
+        full_ms = timed(lambda: col.argsort(False, "at_end"), 20)
+        per_k = {str(k): timed(lambda: col.top_k(k, False, "at_end"), 20) for k in (10, 1000, 100_000, 1_000_000)}
+    k_head = "1000"
+    print(json.dumps({
+        "metric": METRIC, "value": N_ROWS / (per_k[k_head] / 1e3), "unit": "rows/s", "n_gpus": 1, "steps": 20,
+        "warmup": 3, "ms_per_step": per_k[k_head], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "int64", "data": "synthetic",
+        "config": {"workload": "ORDER BY key LIMIT 1000 (am_top_k_ex) on 50,000,000 int64 keys in [0, 2^40) with "
+                               "10% nulls, uint32 indices", "rows": N_ROWS},
+        "top_k_ms": per_k, "full_argsort_ms": full_ms, "clocks": clocks.summary()}))
+
+
 def plain_run(am, table, offset, n):
     """One request through am_plan_run on the calling thread (the plain per-call path)."""
     src, keys = table
@@ -561,10 +594,10 @@ def main():
     ap.add_argument("--impl", default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="order_by",
-                    choices=["order_by", "segmented", "serving", "full_range", "multikey"],
+                    choices=["order_by", "segmented", "serving", "full_range", "multikey", "topk"],
                     help="order_by: the 50M-row ORDER BY (the headline); segmented: 2,048 arrays in one call; "
                          "serving: the served request stream; full_range: 1M full-range int64 keys; multikey: "
-                         "the 50M-row two-key sort")
+                         "the 50M-row two-key sort; topk: ORDER BY ... LIMIT k by radix selection")
     ap.add_argument("--rate", type=float, default=200.0, help="serving: requests per second")
     ap.add_argument("--serve-seconds", type=float, default=30.0, help="serving: length of the open-loop stream")
     ap.add_argument("--sat-requests", type=int, default=400, help="serving: requests of the saturation run")
@@ -597,6 +630,12 @@ def main():
     if args.workload == "serving":
         if rank == 0:
             run_serving(args, am, torch, local)
+        return
+    if args.workload == "topk":
+        stream = torch.cuda.Stream()
+        am.set_stream(stream.cuda_stream)
+        if rank == 0:
+            run_topk(args, am, torch, stream, local)
         return
     if args.workload in ("full_range", "multikey"):
         stream = torch.cuda.Stream()
