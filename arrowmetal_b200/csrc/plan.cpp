@@ -146,6 +146,93 @@ std::vector<am_array*> materialize(Frame& f, const std::vector<int>& which) {
 
 Frame eval(const json::Value& node, am_plan_source** sources, int64_t nsrc, std::ostringstream* explain, int depth);
 
+// The sort of a frame by `keys`.
+Frame sort_frame(Frame f, const std::vector<KeySpec>& keys) {
+  std::vector<int> which;
+  for (auto& k : keys) {
+    const int i = f.find(k.col);
+    if (i < 0) throw invalid("plan: unknown sort column \"" + k.col + "\"");
+    which.push_back(i);
+  }
+  // One integer (or totalOrder float) key over an unpermuted frame: the last pass rebuilds the sorted
+  // key column from the sorted keys while it writes the permutation, and the other columns come
+  // through one fused gather. The key column is never gathered.
+  if (keys.size() == 1 && !f.perm && f.rows > 0) {
+    SortKey key{f.cols[size_t(which[0])], keys[0].desc, keys[0].nulls_first, keys[0].float_order};
+    if (key.float_order < 0 || key.float_order > 2) throw invalid("unknown float_order " + std::to_string(key.float_order));
+    if (key_invertible(key)) {
+      check_index_rows(f.rows, "sort");
+      cudaStream_t s = stream();
+      use_on(key.col, s);
+      am_array* sorted_key = new_array(key.col->pt, key.col->format, f.rows);
+      am_array* idx = new_array(PT_U32, "I", f.rows);
+      std::vector<am_array*> src, taken;
+      try {
+        idx->values = DevBuffer::alloc(size_t(f.rows) * 4 + 16, s);
+        idx->null_count = 0;
+        idx->perm_of = f.rows;
+        idx->last_stream = s;
+        radix_sort({key}, f.rows, idx->values->ptr, 4, sorted_key, s, &tls().last_stats);
+        for (size_t c = 0; c < f.cols.size(); c++)
+          if (int(c) != which[0]) src.push_back(f.cols[c]);
+        taken.assign(src.size(), nullptr);
+        if (!src.empty() && am_take_columns(src.data(), int64_t(src.size()), idx, taken.data()) != 0)
+          throw Error(am_last_error());
+      } catch (...) {
+        am::release(sorted_key);
+        am::release(idx);
+        throw;
+      }
+      am::release(idx);
+      size_t t = 0;
+      for (size_t c = 0; c < f.cols.size(); c++) {
+        am::release(f.cols[c]);
+        f.cols[c] = int(c) == which[0] ? sorted_key : taken[t++];
+      }
+      return f;
+    }
+  }
+  std::vector<am_array*> kc = materialize(f, which);
+  std::vector<am_array*> handles = kc;
+  std::vector<int> desc, np, fo;
+  for (auto& k : keys) {
+    desc.push_back(k.desc ? 1 : 0);
+    np.push_back(k.nulls_first ? 1 : 0);
+    fo.push_back(k.float_order);
+  }
+  am_array* idx = nullptr;
+  int rc = f.rows == 0 ? 0 : am_lexsort_ex2(handles.data(), desc.data(), np.data(), fo.data(), int64_t(keys.size()), &idx);
+  for (am_array* c : kc) am::release(c);
+  if (rc != 0) throw Error(am_last_error());
+  if (f.rows == 0) return f;
+  if (f.perm) {
+    am_array* composed = gather_index(f.perm, idx);
+    am::release(idx);
+    am::release(f.perm);
+    f.perm = composed;
+  } else {
+    f.perm = idx;
+  }
+  return f;
+}
+
+// Rows [off, off + count) of a frame.
+Frame limit_frame(Frame f, int64_t off, int64_t count) {
+  const int64_t start = std::min(off, f.rows);
+  const int64_t len = std::min<int64_t>(count, f.rows - start);
+  auto cut = [&](am_array*& a) {
+    am_array* s = nullptr;
+    if (am_slice(a, start, len, &s) != 0) throw Error(am_last_error());
+    am::release(a);
+    a = s;
+  };
+  if (f.perm) cut(f.perm);
+  else for (am_array*& col : f.cols) cut(col);
+  f.rows = len;
+  return f;
+}
+
+
 Frame eval(const json::Value& node, am_plan_source** sources, int64_t nsrc, std::ostringstream* explain, int depth) {
   if (node.kind != json::Value::Object) throw invalid("plan: a node must be an object");
   const std::string op = str_of(node.get("op"), "\"op\"");
@@ -226,72 +313,7 @@ Frame eval(const json::Value& node, am_plan_source** sources, int64_t nsrc, std:
       *explain << " (GPU radix argsort, one fused take)\n";
     }
     Frame f = eval(*in, sources, nsrc, explain, depth + 1);
-    std::vector<int> which;
-    for (auto& k : keys) {
-      const int i = f.find(k.col);
-      if (i < 0) throw invalid("plan: unknown sort column \"" + k.col + "\"");
-      which.push_back(i);
-    }
-    // One integer (or totalOrder float) key over an unpermuted frame: the last pass rebuilds the sorted
-    // key column from the sorted keys while it writes the permutation, and the other columns come
-    // through one fused gather. The key column is never gathered.
-    if (keys.size() == 1 && !f.perm && f.rows > 0) {
-      SortKey key{f.cols[size_t(which[0])], keys[0].desc, keys[0].nulls_first, keys[0].float_order};
-      if (key.float_order < 0 || key.float_order > 2) throw invalid("unknown float_order " + std::to_string(key.float_order));
-      if (key_invertible(key)) {
-        check_index_rows(f.rows, "sort");
-        cudaStream_t s = stream();
-        use_on(key.col, s);
-        am_array* sorted_key = new_array(key.col->pt, key.col->format, f.rows);
-        am_array* idx = new_array(PT_U32, "I", f.rows);
-        std::vector<am_array*> src, taken;
-        try {
-          idx->values = DevBuffer::alloc(size_t(f.rows) * 4 + 16, s);
-          idx->null_count = 0;
-          idx->perm_of = f.rows;
-          idx->last_stream = s;
-          radix_sort({key}, f.rows, idx->values->ptr, 4, sorted_key, s, &tls().last_stats);
-          for (size_t c = 0; c < f.cols.size(); c++)
-            if (int(c) != which[0]) src.push_back(f.cols[c]);
-          taken.assign(src.size(), nullptr);
-          if (!src.empty() && am_take_columns(src.data(), int64_t(src.size()), idx, taken.data()) != 0)
-            throw Error(am_last_error());
-        } catch (...) {
-          am::release(sorted_key);
-          am::release(idx);
-          throw;
-        }
-        am::release(idx);
-        size_t t = 0;
-        for (size_t c = 0; c < f.cols.size(); c++) {
-          am::release(f.cols[c]);
-          f.cols[c] = int(c) == which[0] ? sorted_key : taken[t++];
-        }
-        return f;
-      }
-    }
-    std::vector<am_array*> kc = materialize(f, which);
-    std::vector<am_array*> handles = kc;
-    std::vector<int> desc, np, fo;
-    for (auto& k : keys) {
-      desc.push_back(k.desc ? 1 : 0);
-      np.push_back(k.nulls_first ? 1 : 0);
-      fo.push_back(k.float_order);
-    }
-    am_array* idx = nullptr;
-    int rc = f.rows == 0 ? 0 : am_lexsort_ex2(handles.data(), desc.data(), np.data(), fo.data(), int64_t(keys.size()), &idx);
-    for (am_array* c : kc) am::release(c);
-    if (rc != 0) throw Error(am_last_error());
-    if (f.rows == 0) return f;
-    if (f.perm) {
-      am_array* composed = gather_index(f.perm, idx);
-      am::release(idx);
-      am::release(f.perm);
-      f.perm = composed;
-    } else {
-      f.perm = idx;
-    }
-    return f;
+    return sort_frame(std::move(f), keys);
   }
   if (op == "limit") {
     const json::Value* c = node.get("count");
@@ -300,19 +322,41 @@ Frame eval(const json::Value& node, am_plan_source** sources, int64_t nsrc, std:
     const int64_t off = (o && o->kind == json::Value::Number) ? int64_t(o->num) : 0;
     if (off < 0) throw invalid("plan: limit \"offset\" must be non-negative");
     if (explain) *explain << pad << "limit " << int64_t(c->num) << " offset " << off << "\n";
+    // LIMIT over a one-key sort of an unpermuted frame (ORDER BY ... LIMIT): the sort's first
+    // offset + count rows by radix selection, identical to the full sort's prefix; only those rows
+    // are gathered.
+    if (!explain && in->kind == json::Value::Object && in->get("op") && in->get("op")->kind == json::Value::String &&
+        in->get("op")->str == "sort" && in->get("input")) {
+      std::vector<KeySpec> keys = sort_keys(*in);
+      if (keys.size() == 1) {
+        Frame f = eval(*in->get("input"), sources, nsrc, nullptr, depth + 2);
+        const int ki = f.find(keys[0].col);
+        if (ki < 0) throw invalid("plan: unknown sort column \"" + keys[0].col + "\"");
+        const int64_t want = std::min<int64_t>(off + int64_t(c->num), f.rows);
+        if (!f.perm && f.rows > 0 && want < f.rows) {
+          SortKey key{f.cols[size_t(ki)], keys[0].desc, keys[0].nulls_first, keys[0].float_order};
+          if (key.float_order < 0 || key.float_order > 2) throw invalid("unknown float_order " + std::to_string(key.float_order));
+          check_index_rows(f.rows, "sort");
+          cudaStream_t st = stream();
+          use_on(key.col, st);
+          if (am_array* top = radix_top_k(key, want, st)) {
+            const int64_t start = std::min(off, want);
+            am_array* cut = nullptr;
+            const int rc = am_slice(top, start, want - start, &cut);
+            am::release(top);
+            if (rc != 0) throw Error(am_last_error());
+            f.perm = cut;
+            f.rows = want - start;
+            return f;
+          }
+        }
+        // Otherwise the full sort, then the slice.
+        f = sort_frame(std::move(f), keys);
+        return limit_frame(std::move(f), off, int64_t(c->num));
+      }
+    }
     Frame f = eval(*in, sources, nsrc, explain, depth + 1);
-    const int64_t start = std::min(off, f.rows);
-    const int64_t len = std::min<int64_t>(int64_t(c->num), f.rows - start);
-    auto cut = [&](am_array*& a) {
-      am_array* s = nullptr;
-      if (am_slice(a, start, len, &s) != 0) throw Error(am_last_error());
-      am::release(a);
-      a = s;
-    };
-    if (f.perm) cut(f.perm);
-    else for (am_array*& col : f.cols) cut(col);
-    f.rows = len;
-    return f;
+    return limit_frame(std::move(f), off, int64_t(c->num));
   }
   throw invalid("plan: op \"" + op + "\" is not supported by this build (scan, select, with_columns, sort and limit are)");
 }

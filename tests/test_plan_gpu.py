@@ -153,3 +153,30 @@ def test_sorted_copy_total_order_floats(am):
     key = np.where(bits >> np.uint64(63), ~bits, bits | np.uint64(1 << 63))
     want = bits[np.argsort(key, kind="stable")]
     assert np.array_equal(got.to_numpy(zero_copy_only=False).view(np.uint64), want)
+
+
+@pytest.mark.parametrize("key_kind", ["int64", "float64_ieee", "float64_total", "float32_nan_largest", "int32"])
+@pytest.mark.parametrize("desc,nulls", [(False, "last"), (True, "first")])
+def test_order_by_limit_is_the_sorted_prefix(am, key_kind, desc, nulls):
+    # LIMIT over a one-key sort goes through radix selection: the rows must be those of the full sort.
+    rng = np.random.default_rng(len(key_kind) * 3 + desc)
+    n = 400_003
+    fo = "ieee"
+    if key_kind == "int64":
+        key = pa.array(rng.integers(-2**50, 2**50, n), mask=rng.random(n) < 0.1)
+    elif key_kind == "int32":
+        key = pa.array(rng.integers(0, 1000, n).astype(np.int32), mask=rng.random(n) < 0.1)
+    else:
+        v = rng.standard_normal(n).astype(np.float32 if key_kind.startswith("float32") else np.float64)
+        v[rng.random(n) < 0.05] = np.nan
+        key = pa.array(v, mask=rng.random(n) < 0.1)
+        fo = key_kind.split("_", 1)[1]
+    t = {"k": key, "p": pa.array(rng.standard_normal(n)), "q": pa.array(rng.integers(0, 9, n).astype(np.int16))}
+    src = am.PlanSource("t", t)
+    sort = {"op": "sort", "by": [["k", desc, {"nulls": nulls, "float_order": fo}]], "input": {"op": "scan", "source": "t"}}
+    full = am.run_plan(sort, [src])
+    for off, count in [(0, 1), (0, 100), (17, 5000), (0, 20_000), (3, n), (n - 2, 10)]:
+        out = am.run_plan({"op": "limit", "count": count, "offset": off, "input": sort}, [src])
+        for name in t:
+            want = full[name].to_arrow().slice(off, count)
+            assert same_bits(out[name].to_arrow(), want), (name, off, count)
