@@ -514,9 +514,9 @@ def algorithmic_bytes(n, m, passes):
 
 
 # DRAM bytes (read + write) per row of the workload, per kernel and step, from an ncu capture of this
-# benchmark at 20,000,000 rows (dram__bytes_read.sum + dram__bytes_write.sum summed over the kernel's
-# launches in one step, profiles/order_by_int64_20M_dram_traffic.md), scaled by rows.
-TRAFFIC_PER_ROW = {"radix_histogram": 8.17, "radix_onesweep_pass": 94.70, "take_gather": 173.47}
+# benchmark at 25,000,000 rows (dram__bytes_read.sum + dram__bytes_write.sum summed over the kernel's
+# launches in one step, profiles/order_by_int64_25M_dram_traffic.md), scaled by rows.
+TRAFFIC_PER_ROW = {"radix_histogram": 8.17, "radix_onesweep_pass": 97.30, "take_gather": 146.13}
 
 
 def traffic_per_step(kernel, n):
