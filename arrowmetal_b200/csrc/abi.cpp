@@ -125,6 +125,43 @@ void import_host(am_array* a, const ArrowArray* arr, cudaStream_t s) {
   a->last_stream = s;
 }
 
+// A primitive array whose buffers are pinned host memory: its copies are enqueued on the calling
+// thread's copy stream and the import returns at once; the array records that stream, so its first use
+// on another stream waits for the copies, and the producer's buffers are released once they are done.
+// The ArrowArray is moved into the pending release. Returns false (nothing done) for other arrays.
+bool import_pinned_async(am_array* a, ArrowArray* arr) {
+  const int64_t n = arr->length, off = arr->offset;
+  const int w = pt_bytes(a->pt);
+  const uint8_t* vbits = static_cast<const uint8_t*>(arr->buffers[0]);
+  const void* vals = arr->buffers[1];
+  if (w == 0 || n <= 0 || !vals || !is_pinned(vals)) return false;
+  int64_t nulls = 0;
+  if (vbits) nulls = arr->null_count >= 0 ? arr->null_count : host_null_count(vbits, off, n);
+  if (nulls > 0 && ((off & 7) != 0 || !is_pinned(vbits))) return false;
+  cudaStream_t cs = copy_stream();
+  const size_t bytes = size_t(n) * w;
+  a->values = DevBuffer::alloc(bytes + 16, cs);
+  AM_CUDA(cudaMemcpyAsync(a->values->ptr, static_cast<const char*>(vals) + size_t(off) * w, bytes,
+                          cudaMemcpyHostToDevice, cs));
+  a->null_count = nulls;
+  if (nulls > 0) {
+    const size_t vb = size_t((n + 7) / 8);
+    a->validity = DevBuffer::alloc(vb + 16, cs);
+    AM_CUDA(cudaMemcpyAsync(a->validity->ptr, vbits + (off >> 3), vb, cudaMemcpyHostToDevice, cs));
+  }
+  a->last_stream = cs;
+  cudaEvent_t ev;
+  AM_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  AM_CUDA(cudaEventRecord(ev, cs));
+  auto* moved = new ArrowArray(*arr);
+  arr->release = nullptr;
+  release_after(ev, [moved] {
+    if (moved->release) moved->release(moved);
+    delete moved;
+  });
+  return true;
+}
+
 void move_release(ArrowArray* arr) {
   if (arr->release) arr->release(arr);
   arr->release = nullptr;
@@ -275,6 +312,10 @@ int am_import(const ArrowSchema* schema, ArrowArray* array, am_array** out) {
     cudaStream_t s = stream();
     am_array* a = new_array(pt, schema->format, array->length);
     try {
+      if (import_pinned_async(a, array)) {
+        *out = a;
+        return 0;
+      }
       import_host(a, array, s);
     } catch (...) {
       am::release(a);

@@ -56,6 +56,10 @@ struct Device {
 };
 Device& device();                       // initialises on first use; throws when no CUDA device
 cudaStream_t stream();                  // the calling thread's stream (override or its own)
+cudaStream_t copy_stream();             // the calling thread's stream for asynchronous host copies
+// Runs `fn` on a library thread once `ev` (recorded by the caller) has completed, then destroys `ev`:
+// a producer's buffers are released as soon as the copies reading them are done.
+void release_after(cudaEvent_t ev, std::function<void()> fn);
 void set_stream_override(cudaStream_t s);
 cudaStream_t stream_override();
 
@@ -92,6 +96,7 @@ void set_import_threads(int n);
 // ring of pinned staging slots filled by `import_threads()` host threads. copy_h2d returns true when
 // the copy may still read `src` after it returns (a pinned source): the caller keeps it alive.
 bool copy_h2d(void* dst, const void* src, size_t bytes, cudaStream_t s);
+bool is_pinned(const void* p);          // page-locked host memory the GPU reads directly
 void copy_d2h(void* dst, const void* src, size_t bytes, cudaStream_t s);
 
 // Per-thread state.
@@ -100,6 +105,7 @@ struct ThreadState {
   int batch_depth = 0;
   cudaStream_t override_stream = nullptr;
   cudaStream_t own_stream = nullptr;
+  cudaStream_t copy_stream = nullptr;                    // asynchronous imports from pinned memory
   am_sort_stats last_stats{};
   cudaStream_t stats_stream = nullptr;                   // the last sort's counters are copied here
   std::vector<std::function<void()>> deferred_checks;   // run at the batch's end

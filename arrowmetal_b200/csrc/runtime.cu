@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <condition_variable>
+#include <deque>
 #include <cstdlib>
 #include <cstring>
 #include <map>
@@ -70,6 +71,54 @@ Device& device() {
   });
   if (!g_dev_error.empty()) throw Error(g_dev_error);
   return g_dev;
+}
+
+cudaStream_t copy_stream() {
+  Device& d = device();
+  ThreadState& t = tls();
+  if (!t.copy_stream) {
+    AM_CUDA(cudaSetDevice(d.ordinal));
+    AM_CUDA(cudaStreamCreateWithFlags(&t.copy_stream, cudaStreamNonBlocking));
+  }
+  return t.copy_stream;
+}
+
+namespace {
+// The releaser: one library thread that waits for copy events and then runs their releases, in order.
+struct Releaser {
+  std::mutex mu;
+  std::condition_variable cv;
+  std::deque<std::pair<cudaEvent_t, std::function<void()>>> q;
+  Releaser() {
+    std::thread([this] {
+      for (;;) {
+        std::pair<cudaEvent_t, std::function<void()>> job;
+        {
+          std::unique_lock<std::mutex> lk(mu);
+          cv.wait(lk, [&] { return !q.empty(); });
+          job = std::move(q.front());
+          q.pop_front();
+        }
+        (void)cudaEventSynchronize(job.first);
+        (void)cudaEventDestroy(job.first);
+        job.second();
+      }
+    }).detach();
+  }
+};
+Releaser& releaser() {
+  static Releaser* r = new Releaser();   // lives for the process: its thread never exits
+  return *r;
+}
+}  // namespace
+
+void release_after(cudaEvent_t ev, std::function<void()> fn) {
+  Releaser& r = releaser();
+  {
+    std::lock_guard<std::mutex> lk(r.mu);
+    r.q.emplace_back(ev, std::move(fn));
+  }
+  r.cv.notify_one();
 }
 
 cudaStream_t stream() {
@@ -279,14 +328,6 @@ struct Staging {
 };
 Staging g_stage;
 
-bool is_pinned(const void* p) {
-  cudaPointerAttributes at{};
-  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
-    (void)cudaGetLastError();
-    return false;
-  }
-  return at.type == cudaMemoryTypeHost;
-}
 bool staged_copies() {
   const char* e = std::getenv("ARROWMETAL_STAGED_COPY");
   return !(e && e[0] == '0');
@@ -302,6 +343,15 @@ void parallel_memcpy(void* dst, const void* src, size_t bytes) {
   });
 }
 }  // namespace
+
+bool is_pinned(const void* p) {
+  cudaPointerAttributes at{};
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeHost;
+}
 
 int import_threads() { return g_import_threads.load(); }
 void set_import_threads(int n) { g_import_threads.store(n); }
