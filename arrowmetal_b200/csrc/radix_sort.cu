@@ -845,27 +845,30 @@ __global__ void __launch_bounds__(256) key_validity_kernel(const SortSummary* __
 
 template <typename KeyT>
 struct PassConfig;
-template <> struct PassConfig<uint32_t> { static constexpr int THREADS = 512, ITEMS = 8; };
-template <> struct PassConfig<uint64_t> { static constexpr int THREADS = 512, ITEMS = 8; };
+// Tile shape of a single sort's digit passes: 384 threads x 14 rows (5,376-row tiles), measured best
+// on B200 among 320-512 threads x 8-16 rows (two blocks per SM).
+template <> struct PassConfig<uint32_t> { static constexpr int THREADS = 384, ITEMS = 14; };
+template <> struct PassConfig<uint64_t> { static constexpr int THREADS = 384, ITEMS = 14; };
+// The segmented sort's tiles: 512 threads x 8 or 4 rows, chosen per size class.
+constexpr int SEG_THREADS = 512;
 
 constexpr int HIST_THREADS = 256, HIST_ITEMS = 8;
 
-template <typename KeyT, int ITEMS = PassConfig<KeyT>::ITEMS>
+template <typename KeyT, int ITEMS = PassConfig<KeyT>::ITEMS, int THREADS = PassConfig<KeyT>::THREADS>
 static size_t pass_smem() {
-  using C = PassConfig<KeyT>;
-  return sizeof(PassShared<KeyT, C::THREADS, ITEMS>);
+  return sizeof(PassShared<KeyT, THREADS, ITEMS>);
 }
 
-template <typename KeyT, typename StatusT, bool SEG = false, int ITEMS = PassConfig<KeyT>::ITEMS>
+template <typename KeyT, typename StatusT, bool SEG = false, int ITEMS = PassConfig<KeyT>::ITEMS,
+          int THREADS = PassConfig<KeyT>::THREADS>
 static int pass_blocks_per_sm() {
-  using C = PassConfig<KeyT>;
   static int cached = -1;
   static std::once_flag once;
   std::call_once(once, [] {
-    auto fn = onesweep_pass_kernel<KeyT, StatusT, C::THREADS, ITEMS, SEG>;
-    AM_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(pass_smem<KeyT, ITEMS>())));
+    auto fn = onesweep_pass_kernel<KeyT, StatusT, THREADS, ITEMS, SEG>;
+    AM_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(pass_smem<KeyT, ITEMS, THREADS>())));
     int b = 0;
-    AM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, C::THREADS, pass_smem<KeyT, ITEMS>()));
+    AM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, THREADS, pass_smem<KeyT, ITEMS, THREADS>()));
     cached = std::max(1, b);
   });
   return cached;
@@ -1123,7 +1126,7 @@ constexpr uint32_t SEG_HIST_ROWS = 32768;   // rows per histogram block
 // group's scratch.
 template <typename KeyT, int ITEMS>
 struct GroupLayout {
-  static constexpr uint64_t TILE = uint64_t(PassConfig<KeyT>::THREADS) * ITEMS;
+  static constexpr uint64_t TILE = uint64_t(SEG_THREADS) * ITEMS;
   static constexpr int S = int(sizeof(KeyT));
   uint32_t G = 0;
   uint64_t rows = 0, tiles = 0, items = 0, max_n = 0;
@@ -1184,7 +1187,6 @@ struct GroupLayout {
 template <typename KeyT, int ITEMS>
 void enqueue_group(const GroupLayout<KeyT, ITEMS>& L, char* base, void* status, uint32_t* err,
                    const void* pinned_tables, bool timed, cudaStream_t s) {
-  using C = PassConfig<KeyT>;
   constexpr int S = GroupLayout<KeyT, ITEMS>::S;
   if (pinned_tables) AM_CUDA(cudaMemcpyAsync(base, pinned_tables, L.tables, cudaMemcpyHostToDevice, s));
   AM_CUDA(cudaMemsetAsync(base + L.tables, 0, L.header - L.tables, s));
@@ -1215,7 +1217,8 @@ void enqueue_group(const GroupLayout<KeyT, ITEMS>& L, char* base, void* status, 
   // 64-bit words whose pass epochs (1..S) start over from a zeroed array in every call.
   const bool narrow = L.narrow();
   if (!narrow) AM_CUDA(cudaMemsetAsync(status, 0, size_t(L.tiles) * NBINS * sizeof(uint64_t), s));
-  const int bps = narrow ? pass_blocks_per_sm<KeyT, uint32_t, true, ITEMS>() : pass_blocks_per_sm<KeyT, uint64_t, true, ITEMS>();
+  const int bps = narrow ? pass_blocks_per_sm<KeyT, uint32_t, true, ITEMS, SEG_THREADS>()
+                         : pass_blocks_per_sm<KeyT, uint64_t, true, ITEMS, SEG_THREADS>();
   const int grid = int(std::min<uint64_t>(L.tiles, uint64_t(device().sm_count) * bps));
   for (int sl = 0; sl < S; sl++) {
     if (narrow) AM_CUDA(cudaMemsetAsync(status, 0, size_t(L.tiles) * NBINS * sizeof(uint32_t), s));
@@ -1240,10 +1243,11 @@ void enqueue_group(const GroupLayout<KeyT, ITEMS>& L, char* base, void* status, 
     a.nslots = uint32_t(S);
     const ColView none{};
     std::unique_ptr<KernelTimer> kt(timed ? new KernelTimer("batch_pass", s) : nullptr);
+    constexpr size_t smem = sizeof(PassShared<KeyT, SEG_THREADS, ITEMS>);
     if (narrow)
-      onesweep_pass_kernel<KeyT, uint32_t, C::THREADS, ITEMS, true><<<std::max(grid, 1), C::THREADS, pass_smem<KeyT, ITEMS>(), s>>>(a, none);
+      onesweep_pass_kernel<KeyT, uint32_t, SEG_THREADS, ITEMS, true><<<std::max(grid, 1), SEG_THREADS, smem, s>>>(a, none);
     else
-      onesweep_pass_kernel<KeyT, uint64_t, C::THREADS, ITEMS, true><<<std::max(grid, 1), C::THREADS, pass_smem<KeyT, ITEMS>(), s>>>(a, none);
+      onesweep_pass_kernel<KeyT, uint64_t, SEG_THREADS, ITEMS, true><<<std::max(grid, 1), SEG_THREADS, smem, s>>>(a, none);
     AM_CUDA(cudaGetLastError());
   }
 }
@@ -1330,8 +1334,8 @@ BatchGraph* find_or_capture(const GroupLayout<KeyT, ITEMS>& L, uint32_t* err, cu
   const size_t status_bytes = size_t(L.tiles) * NBINS * (L.narrow() ? sizeof(uint32_t) : sizeof(uint64_t));
   AM_CUDA(cudaMalloc(&g->status, std::max<size_t>(status_bytes, 16)));
   // Launch attributes and occupancy are looked up before the capture.
-  (void)pass_blocks_per_sm<KeyT, uint32_t, true, ITEMS>();
-  (void)pass_blocks_per_sm<KeyT, uint64_t, true, ITEMS>();
+  (void)pass_blocks_per_sm<KeyT, uint32_t, true, ITEMS, SEG_THREADS>();
+  (void)pass_blocks_per_sm<KeyT, uint64_t, true, ITEMS, SEG_THREADS>();
   for (auto& sl : g->slot) {
     sl.host = pinned_alloc(L.tables);
     AM_CUDA(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
