@@ -150,6 +150,7 @@ bool import_pinned_async(am_array* a, ArrowArray* arr) {
     AM_CUDA(cudaMemcpyAsync(a->validity->ptr, vbits + (off >> 3), vb, cudaMemcpyHostToDevice, cs));
   }
   a->last_stream = cs;
+  a->ready = std::make_shared<ReadyEvent>(cs);      // readers wait for these copies, not later ones
   cudaEvent_t ev;
   AM_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
   AM_CUDA(cudaEventRecord(ev, cs));
@@ -263,6 +264,7 @@ am_array* slice_of(am_array* a, int64_t offset, int64_t length) {
   o->validity_offset = a->validity_offset + offset;
   o->last_stream = a->last_stream;
   o->shared_read = a->shared_read;
+  o->ready = a->ready;
   if (a->perm_of >= 0) o->perm_of = a->perm_of;
   if (a->null_count == 0 || !a->validity) {
     o->null_count = 0;
@@ -470,6 +472,12 @@ int am_export(am_array* a, ArrowSchema* schema, ArrowArray* array) {
   return guard([&] {
     cudaStream_t s = a->last_stream ? a->last_stream : stream();
     const int64_t nulls = resolve_null_count(a);
+    if (a->ready) {
+      // The contents are complete at the ready event: copy on the export stream after it, without
+      // waiting for the work enqueued since on the producing stream.
+      s = d2h_stream();
+      AM_CUDA(cudaStreamWaitEvent(s, a->ready->ev, 0));
+    }
     const int64_t n = a->length;
     auto* h = new ExportHold();
     try {

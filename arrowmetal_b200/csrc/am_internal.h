@@ -57,6 +57,13 @@ struct Device {
 Device& device();                       // initialises on first use; throws when no CUDA device
 cudaStream_t stream();                  // the calling thread's stream (override or its own)
 cudaStream_t copy_stream();             // the calling thread's stream for asynchronous host copies
+cudaStream_t d2h_stream();              // the calling thread's stream for exports that need not wait
+// An event recorded when an array's contents were complete; copies of the array wait for it alone.
+struct ReadyEvent {
+  cudaEvent_t ev = nullptr;
+  explicit ReadyEvent(cudaStream_t s);
+  ~ReadyEvent();
+};
 // Runs `fn` on a library thread once `ev` (recorded by the caller) has completed, then destroys `ev`:
 // a producer's buffers are released as soon as the copies reading them are done.
 void release_after(cudaEvent_t ev, std::function<void()> fn);
@@ -106,6 +113,7 @@ struct ThreadState {
   cudaStream_t override_stream = nullptr;
   cudaStream_t own_stream = nullptr;
   cudaStream_t copy_stream = nullptr;                    // asynchronous imports from pinned memory
+  cudaStream_t d2h_stream = nullptr;                     // exports of arrays that carry a ready event
   am_sort_stats last_stats{};
   cudaStream_t stats_stream = nullptr;                   // the last sort's counters are copied here
   std::vector<std::function<void()>> deferred_checks;   // run at the batch's end
@@ -185,6 +193,9 @@ struct am_array {
   // so readers neither wait for nor record a stream; its buffers outlive every reader, which holds
   // them through its own slices.
   bool shared_read = false;
+  // Recorded on last_stream when the contents were complete (optional): an export waits for it alone,
+  // not for later work on that stream.
+  std::shared_ptr<am::ReadyEvent> ready;
 
   const void* data() const {
     if (!values) return nullptr;

@@ -1030,7 +1030,8 @@ void radix_sort(const std::vector<SortKey>& keys, int64_t n64, void* out, int in
     if (keys[0].col->null_count != 0) {
       key_dst->validity = DevBuffer::alloc(words * 4, s);
       key_dst->null_count_dev = DevBuffer::alloc(sizeof(unsigned long long), s);
-      key_dst->null_count = -1;
+      // The sorted column has the input's null rows: a known count needs no device round trip.
+      key_dst->null_count = keys[0].col->null_count > 0 ? keys[0].col->null_count : -1;
     } else {
       key_dst->null_count = 0;
     }
@@ -1104,6 +1105,7 @@ void radix_sort(const std::vector<SortKey>& keys, int64_t n64, void* out, int in
                                                             static_cast<unsigned long long*>(key_dst->null_count_dev->ptr));
     AM_CUDA(cudaGetLastError());
   }
+  if (key_dst) key_dst->ready = std::make_shared<ReadyEvent>(s);
   if (stats) {
     // Counters arrive asynchronously; am_last_sort_stats waits for them.
     stats->rows = int64_t(n);

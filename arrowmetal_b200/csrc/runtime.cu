@@ -83,6 +83,24 @@ cudaStream_t copy_stream() {
   return t.copy_stream;
 }
 
+cudaStream_t d2h_stream() {
+  Device& d = device();
+  ThreadState& t = tls();
+  if (!t.d2h_stream) {
+    AM_CUDA(cudaSetDevice(d.ordinal));
+    AM_CUDA(cudaStreamCreateWithFlags(&t.d2h_stream, cudaStreamNonBlocking));
+  }
+  return t.d2h_stream;
+}
+
+ReadyEvent::ReadyEvent(cudaStream_t s) {
+  AM_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  AM_CUDA(cudaEventRecord(ev, s));
+}
+ReadyEvent::~ReadyEvent() {
+  if (ev) (void)cudaEventDestroy(ev);
+}
+
 namespace {
 // The releaser: one library thread that waits for copy events and then runs their releases, in order.
 struct Releaser {
@@ -577,7 +595,10 @@ void release(am_array* a) {
 
 void use_on(am_array* a, cudaStream_t s) {
   if (!a || a->shared_read) return;
-  if (a->last_stream && a->last_stream != s) {
+  if (a->ready && a->last_stream != s) {
+    // Contents complete at the ready event: wait for it alone, not for later work on its stream.
+    AM_CUDA(cudaStreamWaitEvent(s, a->ready->ev, 0));
+  } else if (a->last_stream && a->last_stream != s) {
     cudaEvent_t e;
     AM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     AM_CUDA(cudaEventRecord(e, a->last_stream));
