@@ -95,7 +95,10 @@ void check_array_struct(const ArrowSchema* schema, const ArrowArray* array) {
   if (schema->dictionary || array->dictionary) throw unsupported("dictionary arrays are not carried by this build");
   if (schema->n_children != 0 || array->n_children != 0) throw unsupported("nested arrays are not carried by this build");
   if (array->length < 0 || array->offset < 0) throw invalid("negative length or offset");
-  if (array->n_buffers != 2) throw invalid("a primitive array has 2 buffers, got " + std::to_string(array->n_buffers));
+  const int want = pt_var(parse_format(schema->format)) ? 3 : 2;
+  if (array->n_buffers != want)
+    throw invalid(std::string(want == 3 ? "a string or binary" : "a primitive") + " array has " + std::to_string(want) +
+                  " buffers, got " + std::to_string(array->n_buffers));
 }
 
 // Fills `a` from a host ArrowArray (the caller still owns the struct).
@@ -109,7 +112,29 @@ void import_host(am_array* a, const ArrowArray* arr, cudaStream_t s) {
   if (nulls > 0) a->validity = upload_bits(vbits, off, n, s);
   const int w = pt_bytes(a->pt);
   bool reads_later = false;
-  if (w == 0) {
+  if (pt_var(a->pt)) {
+    // Offsets rebased to the first row's start, and exactly the bytes the rows span.
+    const bool large = a->pt == PT_LSTR;
+    std::vector<char> offs(size_t(n + 1) * w);
+    int64_t first = 0, last = 0;
+    for (int64_t i = 0; i <= n; i++) {
+      const int64_t o = large ? static_cast<const int64_t*>(vals)[off + i] : static_cast<const int32_t*>(vals)[off + i];
+      if (i == 0) first = o;
+      if (i == n) last = o;
+      if (large) reinterpret_cast<int64_t*>(offs.data())[i] = o - first;
+      else reinterpret_cast<int32_t*>(offs.data())[i] = int32_t(o - first);
+    }
+    if (last < first) throw invalid("string offsets decrease");
+    a->values = DevBuffer::alloc(offs.size() + 16, s);
+    copy_h2d(a->values->ptr, offs.data(), offs.size(), s);
+    a->bytes = DevBuffer::alloc(size_t(last - first) + 16, s);
+    if (last > first) {
+      const void* bytes = arr->buffers[2];
+      if (!bytes) throw invalid("string array without a data buffer");
+      reads_later = copy_h2d(a->bytes->ptr, static_cast<const char*>(bytes) + first, size_t(last - first), s);
+    }
+    AM_CUDA(cudaStreamSynchronize(s));   // the rebased offsets are a temporary
+  } else if (w == 0) {
     if (n > 0 && !vals) throw invalid("boolean array without a values buffer");
     a->values = n > 0 ? upload_bits(static_cast<const uint8_t*>(vals), off, n, s) : DevBuffer::alloc(16, s);
   } else {
@@ -134,7 +159,7 @@ bool import_pinned_async(am_array* a, ArrowArray* arr) {
   const int w = pt_bytes(a->pt);
   const uint8_t* vbits = static_cast<const uint8_t*>(arr->buffers[0]);
   const void* vals = arr->buffers[1];
-  if (w == 0 || n <= 0 || !vals || !is_pinned(vals)) return false;
+  if (w == 0 || pt_var(a->pt) || n <= 0 || !vals || !is_pinned(vals)) return false;
   int64_t nulls = 0;
   if (vbits) nulls = arr->null_count >= 0 ? arr->null_count : host_null_count(vbits, off, n);
   if (nulls > 0 && ((off & 7) != 0 || !is_pinned(vbits))) return false;
@@ -173,7 +198,7 @@ void move_release(ArrowArray* arr) {
 struct ExportHold {
   std::vector<void*> pinned;      // am_export: pinned host buffers
   am_array* keep = nullptr;       // am_export_device: the array whose HBM the buffers point into
-  const void* buffers[2] = {nullptr, nullptr};
+  const void* buffers[3] = {nullptr, nullptr, nullptr};
   std::string format, name;
 };
 
@@ -232,12 +257,27 @@ am_array* argsort_keys(std::vector<SortKey>& keys, int width, const char* op) {
   cudaStream_t s = stream();
   for (auto& k : keys) use_on(k.col, s);
   am_array* out = make_index_array(n, width, s);
+  std::vector<am_array*> derived;
   try {
-    radix_argsort(keys, n, out->values->ptr, width, s, &tls().last_stats);
+    // String keys sort as their derived chunk and length keys.
+    std::vector<SortKey> sort_keys;
+    for (auto& k : keys) {
+      if (!pt_var(k.col->pt) || n == 0) {
+        sort_keys.push_back(k);
+        continue;
+      }
+      for (am_array* c : string_key_columns(k.col, s)) {
+        derived.push_back(c);
+        sort_keys.push_back(SortKey{c, k.descending, k.nulls_first, 0});
+      }
+    }
+    radix_argsort(sort_keys, n, out->values->ptr, width, s, &tls().last_stats);
   } catch (...) {
+    for (am_array* c : derived) am::release(c);
     am::release(out);
     throw;
   }
+  for (am_array* c : derived) am::release(c);
   if (!in_batch() && std::getenv("ARROWMETAL_SYNC_EVERY_CALL")) check_device_errors(s);
   return out;
 }
@@ -247,7 +287,7 @@ am_array* take_one(am_array* a, am_array* idx) {
   am_array* out = new_array(a->pt, a->format, idx->length);
   const bool trusted = idx->perm_of >= 0 && idx->perm_of <= a->length;
   try {
-    take_columns(&a, 1, idx, &out, !trusted, s);
+    take_columns(&a, 1, idx, &out, !trusted, s);   // string columns go through take_strings
     if (!trusted) checkpoint(s);
   } catch (...) {
     am::release(out);
@@ -259,6 +299,7 @@ am_array* take_one(am_array* a, am_array* idx) {
 am_array* slice_of(am_array* a, int64_t offset, int64_t length) {
   am_array* o = new_array(a->pt, a->format, length);
   o->values = a->values;
+  o->bytes = a->bytes;
   o->value_offset = a->value_offset + offset;
   o->validity = a->validity;
   o->validity_offset = a->validity_offset + offset;
@@ -334,6 +375,8 @@ int am_import_device(const ArrowSchema* schema, ArrowDeviceArray* darr, am_array
   return guard([&] {
     ArrowArray* array = &darr->array;
     const int pt = parse_format(schema->format);
+    const int dt0 = darr->device_type;
+    if (pt_var(pt) && dt0 == ARROW_DEVICE_CUDA) throw unsupported("am_import_device takes fixed-width CUDA arrays; import string arrays from host memory");
     check_array_struct(schema, array);
     const int dt = darr->device_type;
     if (dt == ARROW_DEVICE_CPU || dt == ARROW_DEVICE_CUDA_HOST) return am_import(schema, array, out);
@@ -387,8 +430,7 @@ int am_import_device(const ArrowSchema* schema, ArrowDeviceArray* darr, am_array
 int am_import_chunks_supported(const ArrowSchema* schema) {
   if (!schema || !schema->format || schema->dictionary || schema->n_children) return 0;
   try {
-    parse_format(schema->format);
-    return 1;
+    return pt_var(parse_format(schema->format)) ? 0 : 1;
   } catch (...) {
     return 0;
   }
@@ -496,7 +538,24 @@ int am_export(am_array* a, ArrowSchema* schema, ArrowArray* array) {
         }
         return p;
       };
-      if (w == 0) {
+      if (pt_var(a->pt)) {
+        // Offsets rebased to 0 and the bytes they span.
+        const bool large = a->pt == PT_LSTR;
+        const size_t ob = size_t(n + 1) * w;
+        vals = pinned_alloc(ob);
+        h->pinned.push_back(vals);
+        copy_d2h(vals, static_cast<const char*>(a->values->ptr) + size_t(a->value_offset) * w, ob, s);
+        const int64_t first = large ? static_cast<int64_t*>(vals)[0] : static_cast<int32_t*>(vals)[0];
+        const int64_t last = large ? static_cast<int64_t*>(vals)[n] : static_cast<int32_t*>(vals)[n];
+        for (int64_t i = 0; i <= n; i++) {
+          if (large) static_cast<int64_t*>(vals)[i] -= first;
+          else static_cast<int32_t*>(vals)[i] -= int32_t(first);
+        }
+        void* bytes = pinned_alloc(size_t(std::max<int64_t>(last - first, 1)));
+        h->pinned.push_back(bytes);
+        if (last > first) copy_d2h(bytes, static_cast<const char*>(a->bytes->ptr) + first, size_t(last - first), s);
+        h->buffers[2] = bytes;
+      } else if (w == 0) {
         vals = bits_down(a->values, a->value_offset);
       } else {
         const size_t bytes = size_t(n) * w;
@@ -518,7 +577,7 @@ int am_export(am_array* a, ArrowSchema* schema, ArrowArray* array) {
     array->length = n;
     array->null_count = nulls;
     array->offset = 0;
-    array->n_buffers = 2;
+    array->n_buffers = pt_var(a->pt) ? 3 : 2;
     array->n_children = 0;
     array->buffers = h->buffers;
     array->children = nullptr;
@@ -532,6 +591,7 @@ int am_export(am_array* a, ArrowSchema* schema, ArrowArray* array) {
 int am_export_device(am_array* a, ArrowSchema* schema, ArrowDeviceArray* darr) {
   if (!a || !darr) return 2;
   return guard([&] {
+    if (pt_var(a->pt)) throw unsupported("am_export_device takes fixed-width arrays; export string arrays with am_export");
     const int64_t nulls = resolve_null_count(a);
     if (a->validity && a->validity_offset != a->value_offset)
       throw invalid("export_device: the validity and value offsets differ");

@@ -154,16 +154,20 @@ void profile_reset();
 
 enum PhysType : int32_t {
   PT_BOOL = 0, PT_I8, PT_U8, PT_I16, PT_U16, PT_I32, PT_U32, PT_I64, PT_U64, PT_F16, PT_F32, PT_F64,
+  PT_STR,    // variable-size bytes (utf8 "u", binary "z") with int32 offsets
+  PT_LSTR,   // the same with int64 offsets (large_utf8 "U", large_binary "Z")
 };
+// Bytes per value; for the variable-size types, bytes per offset.
 AM_HD inline int pt_bytes(int pt) {
   switch (pt) {
     case PT_BOOL: return 0;   // bit-packed
     case PT_I8: case PT_U8: return 1;
     case PT_I16: case PT_U16: case PT_F16: return 2;
-    case PT_I32: case PT_U32: case PT_F32: return 4;
+    case PT_I32: case PT_U32: case PT_F32: case PT_STR: return 4;
     default: return 8;
   }
 }
+AM_HD inline bool pt_var(int pt) { return pt == PT_STR || pt == PT_LSTR; }
 AM_HD inline bool pt_float(int pt) { return pt == PT_F16 || pt == PT_F32 || pt == PT_F64; }
 AM_HD inline int pt_key_bytes(int pt) { return pt_bytes(pt) == 8 ? 8 : 4; }
 // Parses an Arrow C Data Interface format string; throws unsupported for the types this build does
@@ -181,7 +185,8 @@ struct am_array {
   std::string format;
   int64_t length = 0;
   int64_t null_count = 0;             // -1: being counted on the device (null_count_dev)
-  am::BufPtr values;                  // element 0 sits at values->ptr + value_offset * width
+  am::BufPtr values;                  // element 0 sits at values->ptr + value_offset * width (strings: offsets)
+  am::BufPtr bytes;                   // strings: the bytes the offsets point into
   int64_t value_offset = 0;           // elements (bits for bool)
   am::BufPtr validity;                // may be null: no nulls
   int64_t validity_offset = 0;        // bits
@@ -257,6 +262,11 @@ void radix_argsort_batch(const std::vector<SortKey>& keys, const std::vector<voi
 uint64_t noalloc_max_rows();
 void argsort_noalloc(int pt, const void* values, const uint8_t* validity, int64_t offset, int64_t length,
                      bool descending, bool nulls_first, int float_order, uint32_t* indices, cudaStream_t s);
+
+// String and binary columns: the derived unsigned keys that sort like the strings (big-endian 8-byte
+// chunks, then the length; the first carries the nulls), and the take of one string column.
+std::vector<am_array*> string_key_columns(const am_array* a, cudaStream_t s);
+void take_strings(am_array* src, am_array* idx, am_array* out, bool check_range, cudaStream_t s);
 
 // Gathers `count` columns through one index array. outs[i] must be new arrays of indices' length.
 // `check_range` asks the kernel to flag an index outside [0, src length) in the stream's error word.

@@ -964,7 +964,9 @@ void radix_sort(const std::vector<SortKey>& keys, int64_t n64, void* out, int in
                 cudaStream_t s, am_sort_stats* stats) {
   using namespace rs;
   const int K = int(keys.size());
-  if (K < 1 || K > MAX_KEYS) throw invalid("sort takes 1 to " + std::to_string(MAX_KEYS) + " key columns");
+  if (K < 1 || K > MAX_KEYS) throw invalid("sort takes 1 to " + std::to_string(MAX_KEYS) + " key columns (a string key counts as its 8-byte chunks plus one)");
+  for (auto& k : keys)
+    if (pt_var(k.col->pt)) throw Error("radix_sort: string keys must be expanded to their chunk keys first");
   if (n64 <= 0) return;
   const uint64_t n = uint64_t(n64);
   if (key_dst && (K != 1 || !key_invertible(keys[0])))
@@ -1461,6 +1463,20 @@ void radix_argsort_batch(const std::vector<SortKey>& keys, const std::vector<voi
   std::vector<size_t> g4, g8;
   for (size_t i = 0; i < keys.size(); i++) {
     if (keys[i].col->length <= 0) continue;
+    if (pt_var(keys[i].col->pt)) {
+      // A string array: its derived chunk and length keys, sorted on their own.
+      std::vector<am_array*> derived = string_key_columns(keys[i].col, s);
+      std::vector<SortKey> ks;
+      for (am_array* c : derived) ks.push_back(SortKey{c, keys[i].descending, keys[i].nulls_first, 0});
+      try {
+        radix_argsort(ks, keys[i].col->length, outs[i], 4, s, nullptr);
+      } catch (...) {
+        for (am_array* c : derived) release(c);
+        throw;
+      }
+      for (am_array* c : derived) release(c);
+      continue;
+    }
     (pt_key_bytes(keys[i].col->pt) == 8 ? g8 : g4).push_back(i);
   }
   if (!g4.empty()) rs::sort_segment_group<uint32_t>(keys, outs, g4, s);
@@ -1589,6 +1605,7 @@ uint64_t noalloc_max_rows() { return rs::NOALLOC_MAX_ROWS; }
 void argsort_noalloc(int pt, const void* values, const uint8_t* validity, int64_t offset, int64_t length,
                      bool descending, bool nulls_first, int float_order, uint32_t* indices, cudaStream_t s) {
   using namespace rs;
+  if (pt_var(pt)) throw unsupported("argsort without allocation takes fixed-width columns");
   if (length < 0) throw invalid("negative length " + std::to_string(length));
   if (offset < 0) throw invalid("negative offset " + std::to_string(offset));
   if (uint64_t(length) > NOALLOC_MAX_ROWS)

@@ -561,15 +561,17 @@ int parse_format(const char* f) {
   if (s == "f") return PT_F32;
   if (s == "g") return PT_F64;
   // Temporal types sort and move as their integer storage (MultiSort.swift:96-99).
+  if (s == "u" || s == "z") return PT_STR;
+  if (s == "U" || s == "Z") return PT_LSTR;
   if (s == "tdD" || s == "tts" || s == "ttm") return PT_I32;
   if (s == "tdm" || s == "ttu" || s == "ttn") return PT_I64;
   if (s.size() >= 4 && s[0] == 't' && s[1] == 's' && s[3] == ':' && std::strchr("smun", s[2])) return PT_I64;
   if (s.size() == 3 && s[0] == 't' && s[1] == 'D' && std::strchr("smun", s[2])) return PT_I64;
-  throw unsupported(s + " is not carried by this build (primitive numeric, boolean and temporal types are)");
+  throw unsupported(s + " is not carried by this build (primitive numeric, boolean, temporal, string and binary types are)");
 }
 
 std::string format_of(int pt) {
-  static const char* names[] = {"b", "c", "C", "s", "S", "i", "I", "l", "L", "e", "f", "g"};
+  static const char* names[] = {"b", "c", "C", "s", "S", "i", "I", "l", "L", "e", "f", "g", "u", "U"};
   return names[pt];
 }
 
@@ -586,7 +588,7 @@ void release(am_array* a) {
   if (a->refs.fetch_sub(1) == 1) {
     cudaStream_t s = a->last_stream;
     if (s) {
-      for (BufPtr* b : {&a->values, &a->validity, &a->null_count_dev})
+      for (BufPtr* b : {&a->values, &a->bytes, &a->validity, &a->null_count_dev})
         if (*b && b->use_count() == 1) (*b)->stream = s;
     }
     delete a;

@@ -455,9 +455,22 @@ static void take_through_records(const tk::TakeArgs& a, am_array* const* cols, i
   dfree(r.rec, s);
 }
 
-void take_columns(am_array* const* cols, int count, am_array* indices, am_array** outs, bool check_range,
+void take_columns(am_array* const* cols_in, int count_in, am_array* indices, am_array** outs_in, bool check_range,
                   cudaStream_t s) {
   using namespace tk;
+  // String columns have their own gather; the fixed-width ones share the launches below.
+  std::vector<am_array*> fixed_cols, fixed_outs;
+  for (int c = 0; c < count_in; c++) {
+    if (pt_var(cols_in[c]->pt)) {
+      take_strings(cols_in[c], indices, outs_in[c], check_range, s);
+    } else {
+      fixed_cols.push_back(cols_in[c]);
+      fixed_outs.push_back(outs_in[c]);
+    }
+  }
+  am_array* const* cols = fixed_cols.data();
+  am_array** outs = fixed_outs.data();
+  const int count = int(fixed_cols.size());
   const int64_t n = indices->length;
   int kind;
   switch (indices->pt) {

@@ -487,7 +487,7 @@ am_array* top_k_of(const SortKey& key, int64_t k, cudaStream_t s) {
 }  // namespace rs
 
 am_array* radix_top_k(const SortKey& key, int64_t k, cudaStream_t s) {
-  if (key.col->length <= 0 || k <= 0) return nullptr;
+  if (key.col->length <= 0 || k <= 0 || pt_var(key.col->pt)) return nullptr;
   return pt_key_bytes(key.col->pt) == 8 ? rs::top_k_of<uint64_t>(key, k, s) : rs::top_k_of<uint32_t>(key, k, s);
 }
 
