@@ -413,6 +413,64 @@ def run_topk(args, am, torch, stream, local):
         "top_k_ms": per_k, "full_argsort_ms": full_ms, "clocks": clocks.summary()}))
 
 
+def make_strings(n, seed=SEED + 8):
+    """n utf8 strings of 0-24 lowercase letters (uniform length), 5% nulls, built from numpy buffers."""
+    import pyarrow as pa
+    rng = np.random.default_rng(seed)
+    lens = rng.integers(0, 25, n).astype(np.int32)
+    offs = np.zeros(n + 1, dtype=np.int32)
+    np.cumsum(lens, out=offs[1:])
+    data = rng.integers(ord("a"), ord("z") + 1, int(offs[-1]), dtype=np.uint8)
+    valid = rng.random(n) >= 0.05
+    return pa.Array.from_buffers(pa.utf8(), n, [pa.py_buffer(np.packbits(valid, bitorder="little")),
+                                                pa.py_buffer(offs), pa.py_buffer(data)], null_count=-1)
+
+
+def run_strings(args, am, torch, stream, local):
+    """--workload strings: ORDER BY a utf8 key (10M rows, 0-24 lowercase letters, 5% nulls) + take of a
+    float64 payload through am_plan_run; pyarrow's sort_indices + take on the host timed beside it."""
+    import pyarrow as pa
+    import pyarrow.compute as pc
+    n = 10_000_000
+    key = make_strings(n)
+    pay = pa.array(np.random.default_rng(SEED + 9).standard_normal(n))
+    src = am.PlanSource("t", {"s": key, "v": pay})
+    plan = {"op": "sort", "by": [["s", False, {"nulls": "last"}]], "input": {"op": "scan", "source": "t"}}
+    for _ in range(3):
+        am.run_plan(plan, [src])
+    am.synchronize()
+    am.profile(True)
+    am.profile_reset()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    steps = max(3, min(args.steps, 20))
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(steps):
+            out = am.run_plan(plan, [src])
+            del out
+        ev1.record(stream)
+        ev1.synchronize()
+        am.synchronize()
+    ms = ev0.elapsed_time(ev1) / steps
+    prof = am.profile_entries()
+    am.profile(False)
+    t0 = time.perf_counter()
+    idx = pc.sort_indices(pa.table({"s": key}), [("s", "ascending")], null_placement="at_end")
+    key.take(idx), pay.take(idx)
+    cpu_s = time.perf_counter() - t0
+    print(json.dumps({
+        "metric": METRIC, "value": n / (ms / 1e3), "unit": "rows/s", "n_gpus": 1, "steps": steps, "warmup": 3,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "utf8",
+        "data": "synthetic",
+        "config": {"workload": "ORDER BY utf8 key (0-24 lowercase letters, 5% nulls) + take of the key and a float64 "
+                               "payload, 10,000,000 rows", "rows": n},
+        "per_kernel_ms_per_step": {k: t / steps for k, (l, t) in prof.items()},
+        "cpu_baseline": {"value": n / cpu_s, "unit": "rows/s", "cores": 1, "kind": "pyarrow",
+                         "sample": "pyarrow sort_indices + take of the same 10M rows, once"},
+        "clocks": clocks.summary()}))
+
+
 def plain_run(am, table, offset, n):
     """One request through am_plan_run on the calling thread (the plain per-call path)."""
     src, keys = table
@@ -595,10 +653,10 @@ def main():
     ap.add_argument("--impl", default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="order_by",
-                    choices=["order_by", "segmented", "serving", "full_range", "multikey", "topk"],
+                    choices=["order_by", "segmented", "serving", "full_range", "multikey", "topk", "strings"],
                     help="order_by: the 50M-row ORDER BY (the headline); segmented: 2,048 arrays in one call; "
                          "serving: the served request stream; full_range: 1M full-range int64 keys; multikey: "
-                         "the 50M-row two-key sort; topk: ORDER BY ... LIMIT k by radix selection")
+                         "the 50M-row two-key sort; topk: ORDER BY ... LIMIT k by radix selection; strings: ORDER BY a utf8 key")
     ap.add_argument("--rate", type=float, default=200.0, help="serving: requests per second")
     ap.add_argument("--serve-seconds", type=float, default=30.0, help="serving: length of the open-loop stream")
     ap.add_argument("--sat-requests", type=int, default=400, help="serving: requests of the saturation run")
@@ -631,6 +689,12 @@ def main():
     if args.workload == "serving":
         if rank == 0:
             run_serving(args, am, torch, local)
+        return
+    if args.workload == "strings":
+        stream = torch.cuda.Stream()
+        am.set_stream(stream.cuda_stream)
+        if rank == 0:
+            run_strings(args, am, torch, stream, local)
         return
     if args.workload == "topk":
         stream = torch.cuda.Stream()
