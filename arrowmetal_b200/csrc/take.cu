@@ -168,62 +168,15 @@ __global__ void __launch_bounds__(256) take_kernel(const __grid_constant__ TakeA
 
 // ---- row records
 
-// Column c's value of row j, zero-extended (booleans as 0/1).
-__device__ __forceinline__ uint64_t record_value(const RecArgs& r, int c, uint64_t j) {
-  switch (r.width[c]) {
-    case 8: return static_cast<const uint64_t*>(r.src[c])[j];
-    case 4: return static_cast<const uint32_t*>(r.src[c])[j];
-    case 2: return static_cast<const uint16_t*>(r.src[c])[j];
-    case 1: return static_cast<const uint8_t*>(r.src[c])[j];
-    default: return bit_at(static_cast<const uint8_t*>(r.src[c]), r.src_bit_off[c] + int64_t(j)) ? 1u : 0u;
-  }
-}
-
-// Each thread packs two rows (a block's two halves of 2 x 256 consecutive rows) into W-byte records:
-// every column's two loads are issued before any is used.
+// Each thread packs four rows of a block's 4 x 256 consecutive rows, their loads in flight together.
 template <int W>
 __global__ void __launch_bounds__(256) pack_records_kernel(const __grid_constant__ RecArgs r) {
-  constexpr int WORDS = W / 8;
-  const uint64_t step = uint64_t(gridDim.x) * 512;
-  for (uint64_t base = uint64_t(blockIdx.x) * 512; base < r.n; base += step) {
-    const uint64_t row[2] = {base + threadIdx.x, base + 256 + threadIdx.x};
-    uint64_t w[2][WORDS];
-    uint32_t valid[2] = {0, 0};
+  const uint64_t step = uint64_t(gridDim.x) * 1024;
+  for (uint64_t base = uint64_t(blockIdx.x) * 1024; base < r.n; base += step) {
 #pragma unroll
-    for (int h = 0; h < 2; h++)
-#pragma unroll
-      for (int k = 0; k < WORDS; k++) w[h][k] = 0;
-#pragma unroll
-    for (int c = 0; c < kMaxTakeCols; c++) {
-      if (c >= r.ncols) break;
-      const int o = r.rec_off[c];
-      uint64_t v[2];
-#pragma unroll
-      for (int h = 0; h < 2; h++) v[h] = row[h] < r.n ? record_value(r, c, row[h]) : 0;
-#pragma unroll
-      for (int h = 0; h < 2; h++) {
-#pragma unroll
-        for (int k = 0; k < WORDS; k++)
-          if ((o >> 3) == k) w[h][k] |= v[h] << (8 * (o & 7));
-        if (row[h] < r.n && (!r.src_valid[c] || bit_at(r.src_valid[c], r.src_voff[c] + int64_t(row[h]))))
-          valid[h] |= 1u << c;
-      }
-    }
-#pragma unroll
-    for (int h = 0; h < 2; h++) {
-      if (row[h] >= r.n) continue;
-      if (r.valid_off >= 0) {
-#pragma unroll
-        for (int k = 0; k < WORDS; k++)
-          if ((r.valid_off >> 3) == k) w[h][k] |= uint64_t(valid[h]) << (8 * (r.valid_off & 7));
-      }
-      uint64_t* dst = static_cast<uint64_t*>(r.rec) + row[h] * WORDS;
-      if constexpr (WORDS == 1) {
-        dst[0] = w[h][0];
-      } else {
-#pragma unroll
-        for (int k = 0; k < WORDS; k += 2) reinterpret_cast<ulonglong2*>(dst)[k / 2] = make_ulonglong2(w[h][k], w[h][k + 1]);
-      }
+    for (int h = 0; h < 4; h++) {
+      const uint64_t j = base + uint64_t(h) * 256 + threadIdx.x;
+      if (j < r.n) pack_record<W>(r, j);
     }
   }
 }
@@ -395,12 +348,12 @@ static int record_bytes(am_array* const* cols, int m, bool checked, int64_t n) {
   return bytes <= 8 ? 8 : bytes <= 16 ? 16 : bytes <= 32 ? 32 : 0;
 }
 
-static void take_through_records(const tk::TakeArgs& a, am_array* const* cols, int rec_w, cudaStream_t s) {
+// The record layout of a TakeArgs' columns: widest first, so every field sits at a multiple of its
+// width; the validity byte last when any column has nulls.
+static void layout_records(const tk::TakeArgs& a, tk::RecArgs& r) {
   using namespace tk;
-  RecArgs r{};
   r.ncols = a.ncols;
   r.n = a.src_len;
-  // Widest first, so every field sits at a multiple of its width.
   int order[kMaxTakeCols];
   for (int c = 0; c < a.ncols; c++) order[c] = c;
   std::stable_sort(order, order + a.ncols, [&](int x, int y) { return a.col[x].width > a.col[y].width; });
@@ -418,11 +371,16 @@ static void take_through_records(const tk::TakeArgs& a, am_array* const* cols, i
     r.src_bit_off[c] = a.col[c].src_bit_off;
     r.width[c] = a.col[c].width;
     if (a.col[c].src_valid) nullable = true;
-    (void)cols;
   }
   r.valid_off = nullable ? off : -1;
+}
+
+static void take_through_records(const tk::TakeArgs& a, int rec_w, cudaStream_t s) {
+  using namespace tk;
+  RecArgs r{};
+  layout_records(a, r);
   r.rec = dmalloc(size_t(a.src_len) * size_t(rec_w), s);
-  const int pack_grid = int(std::min<uint64_t>((a.src_len + 511) / 512, uint64_t(device().sm_count) * 16));
+  const int pack_grid = int(std::min<uint64_t>((a.src_len + 1023) / 1024, uint64_t(device().sm_count) * 16));
   const uint64_t chunks = (a.n + 127) / 128;
   const int grid = int(std::min<uint64_t>((chunks + 7) / 8, uint64_t(device().sm_count) * 8));
   {
@@ -528,7 +486,7 @@ void take_columns(am_array* const* cols_in, int count_in, am_array* indices, am_
       o->last_stream = s;
     }
     const int rec_w = record_bytes(cols + base, m, check_range || a.idx_valid != nullptr, n);
-    if (rec_w) take_through_records(a, cols + base, rec_w, s);
+    if (rec_w) take_through_records(a, rec_w, s);
     else launch_take(a, s);
   }
 }

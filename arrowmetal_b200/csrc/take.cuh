@@ -51,6 +51,53 @@ struct RecArgs {
   void* rec;
 };
 
+#ifdef __CUDACC__
+__device__ __forceinline__ bool rec_bit(const uint8_t* p, int64_t i) { return (p[i >> 3] >> (i & 7)) & 1; }
+
+// Column c's value of row j, zero-extended (booleans as 0/1).
+__device__ __forceinline__ uint64_t record_value(const RecArgs& r, int c, uint64_t j) {
+  switch (r.width[c]) {
+    case 8: return static_cast<const uint64_t*>(r.src[c])[j];
+    case 4: return static_cast<const uint32_t*>(r.src[c])[j];
+    case 2: return static_cast<const uint16_t*>(r.src[c])[j];
+    case 1: return static_cast<const uint8_t*>(r.src[c])[j];
+    default: return rec_bit(static_cast<const uint8_t*>(r.src[c]), r.src_bit_off[c] + int64_t(j)) ? 1u : 0u;
+  }
+}
+
+// Row j's W-byte record: every column's value at its offset and the validity byte.
+template <int W>
+__device__ __forceinline__ void pack_record(const RecArgs& r, uint64_t j) {
+  constexpr int WORDS = W / 8;
+  uint64_t w[WORDS];
+#pragma unroll
+  for (int k = 0; k < WORDS; k++) w[k] = 0;
+  uint32_t valid = 0;
+#pragma unroll
+  for (int c = 0; c < kMaxTakeCols; c++) {
+    if (c >= r.ncols) break;
+    const uint64_t v = record_value(r, c, j);
+    const int o = r.rec_off[c];
+#pragma unroll
+    for (int k = 0; k < WORDS; k++)
+      if ((o >> 3) == k) w[k] |= v << (8 * (o & 7));
+    if (!r.src_valid[c] || rec_bit(r.src_valid[c], r.src_voff[c] + int64_t(j))) valid |= 1u << c;
+  }
+  if (r.valid_off >= 0) {
+#pragma unroll
+    for (int k = 0; k < WORDS; k++)
+      if ((r.valid_off >> 3) == k) w[k] |= uint64_t(valid) << (8 * (r.valid_off & 7));
+  }
+  uint64_t* dst = static_cast<uint64_t*>(r.rec) + j * WORDS;
+  if constexpr (WORDS == 1) {
+    dst[0] = w[0];
+  } else {
+#pragma unroll
+    for (int k = 0; k < WORDS; k += 2) reinterpret_cast<ulonglong2*>(dst)[k / 2] = make_ulonglong2(w[k], w[k + 1]);
+  }
+}
+#endif
+
 }  // namespace tk
 
 void launch_take(const tk::TakeArgs& a, cudaStream_t s);
