@@ -26,6 +26,9 @@ LIB_PATH = os.path.join(_HERE, "lib", "libArrowMetalC.so")
 
 NULL_PLACEMENT = ("at_end", "at_start")
 FLOAT_ORDERS = ("ieee", "total", "nan_largest")
+TIEBREAKERS = ("min", "max", "first", "dense")       # Arrow's rank tiebreakers, in the C ABI's numbering
+VALUE_ORDERS = ("first_appearance", "sorted")        # unique / value_counts
+WINDOW_OPS = ("row_number", "rank", "dense_rank", "percent_rank", "cume_dist")   # am_window ops 0-4
 
 
 def _find_library():
@@ -124,6 +127,11 @@ for _name, _res, _args in [
     ("am_server_wait", _I, [_P, _I64, _PP, ctypes.POINTER(ctypes.c_double)]),
     ("am_server_get_stats", _I, [_P, ctypes.POINTER(ServerStats)]),
     ("am_server_release", _I, [_P]),
+    ("am_partition_nth_indices", _I, [_P, _I64, _PP]), ("am_partition_nth_ex", _I, [_P, _I64, _I, _PP]),
+    ("am_rank_ex", _I, [_P, _I, _I, _I, _PP]), ("am_rank_quantile_ex", _I, [_P, _I, _I, _I, _PP]),
+    ("am_rank", _I, [_P, _I, _PP]), ("am_window", _I, [_P, _I, _I64, _I64, _P, _PP]),
+    ("am_unique", _I, [_P, _PP]), ("am_unique_ex", _I, [_P, _I, _PP]),
+    ("am_value_counts", _I, [_P, _PP]), ("am_value_counts_ex", _I, [_P, _I, _PP]),
 ]:
     _sig(_name, _res, _args)
 
@@ -287,6 +295,63 @@ class MetalArray:
         return _call(_lib.am_top_k_ex, self._h, int(k), 1 if largest else 0,
                      _index_of(NULL_PLACEMENT, null_placement, "null_placement"),
                      _index_of(FLOAT_ORDERS, float_order, "float_order"))
+
+
+    # ---- sort consumers (one argsort, then run marks, a scan and scatters)
+    def partition_nth_indices(self, pivot, null_placement="at_end"):
+        """Arrow `partition_nth_indices`: uint32 indices with, at position `pivot`, the row a stable
+        ascending sort puts there; no row before it orders after it and none after it before it. Each
+        of the three blocks (before, equal, after) keeps row order. A radix select, not a sort."""
+        return _call(_lib.am_partition_nth_ex, self._h, int(pivot),
+                     _index_of(NULL_PLACEMENT, null_placement, "null_placement"))
+
+    def rank(self, sort_keys="ascending", null_placement="at_end", tiebreaker="min"):
+        """Arrow `rank` (uint32; pyarrow returns uint64 with the same values). Nulls and NaN rows are one
+        tie group at the `null_placement` end, as in pyarrow."""
+        return _call(_lib.am_rank_ex, self._h, _index_of(TIEBREAKERS, tiebreaker, "tiebreaker"),
+                     _direction(sort_keys), _index_of(NULL_PLACEMENT, null_placement, "null_placement"))
+
+    def rank_quantile(self, sort_keys="ascending", null_placement="at_end"):
+        """Arrow `rank_quantile`: (average 1-based rank of the row's tie group - 0.5) / n, float64."""
+        return _call(_lib.am_rank_quantile_ex, self._h, 0, _direction(sort_keys),
+                     _index_of(NULL_PLACEMENT, null_placement, "null_placement"))
+
+    def rank_normal(self, sort_keys="ascending", null_placement="at_end", float32=False):
+        """Arrow `rank_normal`: the standard normal quantile of `rank_quantile()` (float64, or float32)."""
+        return _call(_lib.am_rank_quantile_ex, self._h, 2 if float32 else 1, _direction(sort_keys),
+                     _index_of(NULL_PLACEMENT, null_placement, "null_placement"))
+
+    def window(self, op):
+        """One of the SQL ranking window functions by name (ascending, nulls last and tied)."""
+        return _call(_lib.am_window, self._h, _index_of(WINDOW_OPS, op, "op"), 0, 0, None)
+
+    def row_number(self):
+        return self.window("row_number")
+
+    def dense_rank(self):
+        return self.window("dense_rank")
+
+    def percent_rank(self):
+        return self.window("percent_rank")
+
+    def cume_dist(self):
+        return self.window("cume_dist")
+
+    def unique(self, order="first_appearance"):
+        """Arrow `unique`. "first_appearance" keeps Arrow's order and its one null entry (not for string
+        columns); "sorted" is ascending with the nulls dropped. -0.0 matches 0.0 and every NaN is one
+        value; the representative is the earliest row."""
+        return _call(_lib.am_unique_ex, self._h, _index_of(VALUE_ORDERS, order, "order"))
+
+    def value_counts(self, order="first_appearance"):
+        """Arrow `value_counts`: a struct array of `values` and their int64 `counts`, in `unique`'s order."""
+        return _call(_lib.am_value_counts_ex, self._h, _index_of(VALUE_ORDERS, order, "order"))
+
+
+def _direction(sort_keys):
+    if sort_keys not in ("ascending", "descending"):
+        raise ArrowMetalError('sort_keys must be "ascending" or "descending"')
+    return 1 if sort_keys == "descending" else 0
 
 
 class _DeviceHolder:

@@ -232,6 +232,38 @@ void fill_schema(am_array* a, ArrowSchema* schema) {
   schema->private_data = h;
 }
 
+// A struct array (value_counts' result): one child array and schema per field, exported the way
+// am_export exports a flat array, and no buffer of its own but an absent validity bitmap.
+struct StructArrayHold {
+  std::vector<ArrowArray> arrays;
+  std::vector<ArrowArray*> ptrs;
+  const void* buffers[1] = {nullptr};
+};
+struct StructSchemaHold {
+  std::vector<ArrowSchema> schemas;
+  std::vector<ArrowSchema*> ptrs;
+  std::vector<std::string> names;
+  std::string format = "+s", name;
+};
+void release_struct_array(ArrowArray* a) {
+  if (!a || !a->release) return;
+  auto* h = static_cast<StructArrayHold*>(a->private_data);
+  for (ArrowArray& c : h->arrays)
+    if (c.release) c.release(&c);
+  delete h;
+  a->release = nullptr;
+  a->private_data = nullptr;
+}
+void release_struct_schema(ArrowSchema* s) {
+  if (!s || !s->release) return;
+  auto* h = static_cast<StructSchemaHold*>(s->private_data);
+  for (ArrowSchema& c : h->schemas)
+    if (c.release) c.release(&c);
+  delete h;
+  s->release = nullptr;
+  s->private_data = nullptr;
+}
+
 am_array* make_index_array(int64_t n, int width, cudaStream_t s) {
   am_array* o = new_array(width == 8 ? PT_U64 : PT_U32, width == 8 ? "L" : "I", n);
   o->values = DevBuffer::alloc(size_t(std::max<int64_t>(n, 1)) * width + 16, s);
@@ -297,6 +329,7 @@ am_array* take_one(am_array* a, am_array* idx) {
 }
 
 am_array* slice_of(am_array* a, int64_t offset, int64_t length) {
+  if (a->pt == PT_STRUCT) throw unsupported("+s: a struct result is exported, not computed on");
   am_array* o = new_array(a->pt, a->format, length);
   o->values = a->values;
   o->bytes = a->bytes;
@@ -511,6 +544,62 @@ int am_get_import_threads(void) { return import_threads(); }
 
 int am_export(am_array* a, ArrowSchema* schema, ArrowArray* array) {
   if (!a || !array) return 2;
+  if (a->pt == PT_STRUCT) {
+    auto* ah = new StructArrayHold();
+    auto* sh = schema ? new StructSchemaHold() : nullptr;
+    const size_t k = a->children.size();
+    ah->arrays.resize(k);
+    if (sh) {
+      sh->schemas.resize(k);
+      sh->names = a->child_names;
+    }
+    for (size_t i = 0; i < k; i++) {
+      std::memset(&ah->arrays[i], 0, sizeof(ArrowArray));
+      if (sh) std::memset(&sh->schemas[i], 0, sizeof(ArrowSchema));
+    }
+    int rc = 0;
+    for (size_t i = 0; i < k && rc == 0; i++) {
+      rc = am_export(a->children[i], sh ? &sh->schemas[i] : nullptr, &ah->arrays[i]);
+      if (rc == 0 && sh) sh->schemas[i].name = sh->names[i].c_str();
+    }
+    ArrowArray tmp_a{};
+    tmp_a.release = release_struct_array;
+    tmp_a.private_data = ah;
+    if (rc != 0) {
+      release_struct_array(&tmp_a);
+      if (sh) {
+        ArrowSchema tmp_s{};
+        tmp_s.release = release_struct_schema;
+        tmp_s.private_data = sh;
+        release_struct_schema(&tmp_s);
+      }
+      return rc;
+    }
+    for (ArrowArray& c : ah->arrays) ah->ptrs.push_back(&c);
+    array->length = a->length;
+    array->null_count = 0;
+    array->offset = 0;
+    array->n_buffers = 1;
+    array->n_children = int64_t(k);
+    array->buffers = ah->buffers;
+    array->children = ah->ptrs.data();
+    array->dictionary = nullptr;
+    array->release = release_struct_array;
+    array->private_data = ah;
+    if (sh) {
+      for (ArrowSchema& c : sh->schemas) sh->ptrs.push_back(&c);
+      schema->format = sh->format.c_str();
+      schema->name = sh->name.c_str();
+      schema->metadata = nullptr;
+      schema->flags = 0;
+      schema->n_children = int64_t(k);
+      schema->children = sh->ptrs.data();
+      schema->dictionary = nullptr;
+      schema->release = release_struct_schema;
+      schema->private_data = sh;
+    }
+    return 0;
+  }
   return guard([&] {
     cudaStream_t s = a->last_stream ? a->last_stream : stream();
     const int64_t nulls = resolve_null_count(a);
@@ -591,6 +680,7 @@ int am_export(am_array* a, ArrowSchema* schema, ArrowArray* array) {
 int am_export_device(am_array* a, ArrowSchema* schema, ArrowDeviceArray* darr) {
   if (!a || !darr) return 2;
   return guard([&] {
+    if (a->pt == PT_STRUCT) throw unsupported("am_export_device takes flat arrays; export a struct result with am_export");
     if (pt_var(a->pt)) throw unsupported("am_export_device takes fixed-width arrays; export string arrays with am_export");
     const int64_t nulls = resolve_null_count(a);
     if (a->validity && a->validity_offset != a->value_offset)
@@ -801,6 +891,99 @@ int am_top_k_ex(am_array* a, int64_t k, int largest, int null_placement, int flo
   });
 }
 int am_top_k(am_array* a, int64_t k, int largest, am_array** out) { return am_top_k_ex(a, k, largest, 0, 0, out); }
+
+// ---- sort consumers (Sources/ArrowMetalC/ArrowMetalC_Options.swift:134-143, :228-320)
+
+int am_partition_nth_ex(am_array* a, int64_t pivot, int null_placement, am_array** out) {
+  if (!a || !out) return 2;
+  return guard([&] {
+    if (a->pt == PT_STRUCT) throw unsupported("+s: a struct result is exported, not computed on");
+    if (pivot < 0 || pivot > a->length)
+      throw invalid("partition index " + std::to_string(pivot) + " is outside 0..." + std::to_string(a->length));
+    check_index_rows(a->length, "partition_nth_indices");
+    SortKey key{a, false, null_placement == 1, 0};
+    if (a->length == 0) {
+      *out = make_index_array(0, 4, stream());
+      return 0;
+    }
+    cudaStream_t s = stream();
+    use_on(a, s);
+    if (am_array* r = radix_partition_nth(key, pivot, s)) {
+      checkpoint(s);
+      *out = r;
+      return 0;
+    }
+    // A string column: the stable argsort is itself such a partition.
+    std::vector<SortKey> k{key};
+    *out = argsort_keys(k, 4, "partition_nth_indices");
+    return 0;
+  });
+}
+int am_partition_nth_indices(am_array* a, int64_t n, am_array** out) { return am_partition_nth_ex(a, n, 0, out); }
+
+int am_rank_ex(am_array* a, int tiebreaker, int descending, int null_placement, am_array** out) {
+  if (!a || !out) return 2;
+  return guard([&] {
+    if (tiebreaker < 0 || tiebreaker > 3) throw invalid("unknown rank tiebreaker " + std::to_string(tiebreaker));
+    check_index_rows(a->length, "rank");
+    *out = rank_of(a, tiebreaker, descending != 0, null_placement == 1, true, stream());
+    return 0;
+  });
+}
+
+int am_rank_quantile_ex(am_array* a, int op, int descending, int null_placement, am_array** out) {
+  if (!a || !out) return 2;
+  return guard([&] {
+    if (op < 0 || op > 2) throw invalid("unknown rank op " + std::to_string(op));
+    check_index_rows(a->length, "rank");
+    *out = rank_of(a, RANK_QUANTILE + op, descending != 0, null_placement == 1, true, stream());
+    return 0;
+  });
+}
+int am_rank(am_array* a, int op, am_array** out) { return am_rank_quantile_ex(a, op, 0, 0, out); }
+
+// The ranking ops of am_window (0 row_number, 1 rank, 2 dense_rank, 3 percent_rank, 4 cume_dist):
+// ascending, nulls last and one tie group, every NaN one value after +inf.
+int am_window(am_array* a, int op, int64_t p1, int64_t p2, const void* scalar_or_null, am_array** out) {
+  (void)p1;
+  (void)p2;
+  (void)scalar_or_null;
+  if (!a || !out) return 2;
+  return guard([&] {
+    static const int fn[] = {RANK_FIRST, RANK_MIN, RANK_DENSE, RANK_PERCENT, RANK_CUME};
+    if (op < 0 || op > 12) throw invalid("unknown window op " + std::to_string(op));
+    if (op > 4) throw unsupported("window op " + std::to_string(op) + " (shifts, differences, running and rolling windows are not on the sort path)");
+    check_index_rows(a->length, "window");
+    *out = rank_of(a, fn[op], false, false, false, stream());
+    return 0;
+  });
+}
+
+int am_unique_ex(am_array* a, int order, am_array** out) {
+  if (!a || !out) return 2;
+  return guard([&] {
+    check_index_rows(a->length, "unique");
+    *out = unique_of(a, order != 1, nullptr, stream());
+    return 0;
+  });
+}
+int am_unique(am_array* a, am_array** out) { return am_unique_ex(a, 1, out); }
+
+int am_value_counts_ex(am_array* a, int order, am_array** out) {
+  if (!a || !out) return 2;
+  return guard([&] {
+    check_index_rows(a->length, "value_counts");
+    am_array* counts = nullptr;
+    am_array* values = unique_of(a, order != 1, &counts, stream());
+    am_array* st = new_array(PT_STRUCT, "+s", values->length);
+    st->null_count = 0;
+    st->children = {values, counts};
+    st->child_names = {"values", "counts"};
+    *out = st;
+    return 0;
+  });
+}
+int am_value_counts(am_array* a, am_array** out) { return am_value_counts_ex(a, 1, out); }
 
 int am_lexsort_ex2(am_array** columns, const int* descending, const int* null_placement, const int* float_order,
                    int64_t count, am_array** out) {

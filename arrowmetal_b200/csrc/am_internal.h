@@ -156,6 +156,7 @@ enum PhysType : int32_t {
   PT_BOOL = 0, PT_I8, PT_U8, PT_I16, PT_U16, PT_I32, PT_U32, PT_I64, PT_U64, PT_F16, PT_F32, PT_F64,
   PT_STR,    // variable-size bytes (utf8 "u", binary "z") with int32 offsets
   PT_LSTR,   // the same with int64 offsets (large_utf8 "U", large_binary "Z")
+  PT_STRUCT, // a struct of child arrays ("+s"): value_counts' result, exported only
 };
 // Bytes per value; for the variable-size types, bytes per offset.
 AM_HD inline int pt_bytes(int pt) {
@@ -201,6 +202,9 @@ struct am_array {
   // Recorded on last_stream when the contents were complete (optional): an export waits for it alone,
   // not for later work on that stream.
   std::shared_ptr<am::ReadyEvent> ready;
+  // PT_STRUCT: the fields, owned (one reference each), and their names.
+  std::vector<am_array*> children;
+  std::vector<std::string> child_names;
 
   const void* data() const {
     if (!values) return nullptr;
@@ -262,6 +266,21 @@ void radix_argsort_batch(const std::vector<SortKey>& keys, const std::vector<voi
 uint64_t noalloc_max_rows();
 void argsort_noalloc(int pt, const void* values, const uint8_t* validity, int64_t offset, int64_t length,
                      bool descending, bool nulls_first, int float_order, uint32_t* indices, cudaStream_t s);
+
+// Partition around position `pivot` of the ascending stable argsort (Arrow partition_nth_indices), by
+// radix selection; NULL for a string column (the caller sorts instead).
+am_array* radix_partition_nth(const SortKey& key, int64_t pivot, cudaStream_t s);
+
+// Sort consumers (consumers.cu). rank_of's functions: Arrow's rank tiebreakers in the C ABI's numbering
+// (0 min, 1 max, 2 first, 3 dense), then rank_quantile, rank_normal in float64 and float32, and the SQL
+// percent_rank and cume_dist. `merge_nan`: the NaN rows tie with the nulls (Arrow's rank functions).
+enum RankFn {
+  RANK_MIN = 0, RANK_MAX, RANK_FIRST, RANK_DENSE, RANK_QUANTILE, RANK_NORMAL64, RANK_NORMAL32, RANK_PERCENT, RANK_CUME
+};
+am_array* rank_of(am_array* a, int fn, bool desc, bool nulls_first, bool merge_nan, cudaStream_t s);
+// The distinct values, ascending or in order of first appearance; `counts_out` (may be NULL) receives
+// each one's row count (int64).
+am_array* unique_of(am_array* a, bool first_appearance, am_array** counts_out, cudaStream_t s);
 
 // String and binary columns: the derived unsigned keys that sort like the strings (big-endian 8-byte
 // chunks, then the length; the first carries the nulls), and the take of one string column.

@@ -1,0 +1,503 @@
+// Sort consumers: Arrow's rank with its four tiebreakers, rank_quantile / rank_normal, the SQL window
+// ranking functions (row_number, rank, dense_rank, percent_rank, cume_dist), unique and value_counts.
+// Each is one stable argsort of the column and a few passes over its sorted order (the reference builds
+// them the same way: Sources/ArrowMetal/Kernels/Window.swift:106-200 for the rankings,
+// Kernels/Unique.swift:46-65 and Kernels/UniqueOrder.swift:88-140 for the distinct values):
+//   1. run marks: sorted position i starts a run when its row is not equal to the row at i - 1, with
+//      the sort's value equality (-0.0 ties +0.0, every NaN is one value, the nulls are one run; Arrow's
+//      rank functions also put the NaN rows and the nulls in one run, as pyarrow ranks them). One byte
+//      per position, and a count of marks per block;
+//   2. an exclusive scan of the block counts (one block; the total run count lands after them);
+//   3. every position's run number (its block's offset plus a block scan of the marks), scattered to
+//      its original row; a run's first position is recorded as the run's start, and its row as the
+//      run's representative (the earliest row of the run: the sort is stable);
+//   4. one pass over the original rows turns run numbers into the answer (the run's first or last
+//      position, its quantile), or one over the runs gives their lengths.
+#include <algorithm>
+#include <vector>
+
+#include "am_internal.h"
+#include "key_encode.cuh"
+#include "radix_sort.cuh"
+
+namespace am {
+namespace rs {
+namespace {
+
+constexpr int RUN_THREADS = 256, RUN_ITEMS = 16;
+constexpr uint64_t RUN_CHUNK = uint64_t(RUN_THREADS) * RUN_ITEMS;
+
+// A string column as the run marks read it.
+struct StrView {
+  const void* offsets;        // row 0's offset
+  const uint8_t* bytes;
+  const uint8_t* valid;       // NULL: no nulls
+  int64_t valid_off;
+};
+
+// The equality class of a fixed-width row: its sort key and category (0 value, 1 NaN, 2 null).
+template <typename KeyT>
+__device__ __forceinline__ void run_key(const ColView& c, uint32_t row, bool merge_nan, KeyT& key, int& cat) {
+  const KeyT raw = load_raw<KeyT>(c, row);
+  const bool valid = !c.valid || bit_at(c.valid, c.valid_off + int64_t(row));
+  key = key_from_raw<KeyT>(c, raw, valid, cat);
+  if (merge_nan && cat == 1) cat = 2;
+}
+
+template <typename OffT>
+__device__ __forceinline__ bool same_string(const StrView& v, uint32_t a, uint32_t b) {
+  const bool va = !v.valid || bit_at(v.valid, v.valid_off + int64_t(a));
+  const bool vb = !v.valid || bit_at(v.valid, v.valid_off + int64_t(b));
+  if (va != vb) return false;
+  if (!va) return true;
+  const OffT* off = static_cast<const OffT*>(v.offsets);
+  const uint64_t sa = uint64_t(off[a]), sb = uint64_t(off[b]);
+  const uint64_t la = uint64_t(off[a + 1]) - sa, lb = uint64_t(off[b + 1]) - sb;
+  if (la != lb) return false;
+  for (uint64_t j = 0; j < la; j++)
+    if (v.bytes[sa + j] != v.bytes[sb + j]) return false;
+  return true;
+}
+
+__device__ __forceinline__ uint32_t block_sum(uint32_t v, uint32_t* s_warp) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  v = __reduce_add_sync(0xffffffffu, v);
+  if (lane == 0) s_warp[warp] = v;
+  __syncthreads();
+  uint32_t all = 0;
+#pragma unroll
+  for (int w = 0; w < RUN_THREADS / 32; w++) all += s_warp[w];
+  return all;
+}
+
+// Block-wide exclusive scan of one value per thread.
+__device__ __forceinline__ uint32_t block_exclusive(uint32_t v, uint32_t* s_warp) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) s_warp[warp] = x;
+  __syncthreads();
+  uint32_t add = 0;
+#pragma unroll
+  for (int w = 0; w < RUN_THREADS / 32; w++)
+    if (w < warp) add += s_warp[w];
+  return x - v + add;
+}
+
+// Writes one thread's RUN_ITEMS marks at position `base` (a multiple of RUN_ITEMS), 16 bytes at once
+// when all of them exist.
+__device__ __forceinline__ void store_marks(uint8_t* marks, uint64_t base, uint64_t m, const uint8_t (&mk)[RUN_ITEMS]) {
+  if (base + RUN_ITEMS <= m) {
+    uint32_t w[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+      w[q] = uint32_t(mk[4 * q]) | (uint32_t(mk[4 * q + 1]) << 8) | (uint32_t(mk[4 * q + 2]) << 16) |
+             (uint32_t(mk[4 * q + 3]) << 24);
+    *reinterpret_cast<uint4*>(marks + base) = make_uint4(w[0], w[1], w[2], w[3]);
+  } else {
+    for (int i = 0; i < RUN_ITEMS && base + i < m; i++) marks[base + i] = mk[i];
+  }
+}
+
+// 1. Run marks of sorted positions [0, m) of a fixed-width column, and their count per block.
+template <typename KeyT>
+__global__ void __launch_bounds__(RUN_THREADS) run_marks_kernel(const __grid_constant__ ColView c, int merge_nan,
+                                                                const uint32_t* __restrict__ perm, uint64_t m,
+                                                                uint8_t* __restrict__ marks,
+                                                                uint32_t* __restrict__ block_counts) {
+  __shared__ uint32_t s_warp[RUN_THREADS / 32];
+  const uint64_t base = uint64_t(blockIdx.x) * RUN_CHUNK + uint64_t(threadIdx.x) * RUN_ITEMS;
+  uint8_t mk[RUN_ITEMS];
+  uint32_t cnt = 0;
+  if (base < m) {
+    // Rows of positions base - 1 .. base + RUN_ITEMS - 1: all the index loads, then the value loads.
+    uint32_t row[RUN_ITEMS + 1];
+#pragma unroll
+    for (int i = 0; i <= RUN_ITEMS; i++) {
+      const uint64_t pos = base + i - 1;
+      row[i] = (i == 0 && base == 0) || pos >= m ? 0u : perm[pos];
+    }
+    KeyT key[RUN_ITEMS + 1];
+    int cat[RUN_ITEMS + 1];
+#pragma unroll
+    for (int i = 0; i <= RUN_ITEMS; i++) run_key<KeyT>(c, row[i], merge_nan != 0, key[i], cat[i]);
+#pragma unroll
+    for (int i = 0; i < RUN_ITEMS; i++) {
+      const uint64_t pos = base + i;
+      const bool start = pos == 0 || cat[i] != cat[i + 1] || (cat[i + 1] == 0 && key[i] != key[i + 1]);
+      mk[i] = (pos < m && start) ? 1 : 0;
+      cnt += mk[i];
+    }
+    store_marks(marks, base, m, mk);
+  }
+  const uint32_t total = block_sum(cnt, s_warp);
+  if (threadIdx.x == 0) block_counts[blockIdx.x] = total;
+}
+
+// 1'. The same for a string column (bytes compared, lengths first).
+template <typename OffT>
+__global__ void __launch_bounds__(RUN_THREADS) run_marks_str_kernel(const __grid_constant__ StrView v,
+                                                                    const uint32_t* __restrict__ perm, uint64_t m,
+                                                                    uint8_t* __restrict__ marks,
+                                                                    uint32_t* __restrict__ block_counts) {
+  __shared__ uint32_t s_warp[RUN_THREADS / 32];
+  const uint64_t base = uint64_t(blockIdx.x) * RUN_CHUNK + uint64_t(threadIdx.x) * RUN_ITEMS;
+  uint8_t mk[RUN_ITEMS];
+  uint32_t cnt = 0;
+  if (base < m) {
+    uint32_t prev = base == 0 ? 0u : perm[base - 1];
+    for (int i = 0; i < RUN_ITEMS; i++) {
+      const uint64_t pos = base + i;
+      mk[i] = 0;
+      if (pos >= m) continue;
+      const uint32_t r = perm[pos];
+      mk[i] = (pos == 0 || !same_string<OffT>(v, prev, r)) ? 1 : 0;
+      cnt += mk[i];
+      prev = r;
+    }
+    store_marks(marks, base, m, mk);
+  }
+  const uint32_t total = block_sum(cnt, s_warp);
+  if (threadIdx.x == 0) block_counts[blockIdx.x] = total;
+}
+
+// 2. One block: exclusive scan of the block counts in place; the total run count lands at [blocks].
+__global__ void __launch_bounds__(1024) run_scan_kernel(uint32_t* __restrict__ counts, uint32_t blocks) {
+  __shared__ uint32_t s[32];
+  __shared__ uint32_t carry;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  if (t == 0) carry = 0;
+  __syncthreads();
+  for (uint32_t base = 0; base < blocks; base += 1024) {
+    const uint32_t i = base + uint32_t(t);
+    const uint32_t v = i < blocks ? counts[i] : 0u;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) s[warp] = x;
+    __syncthreads();
+    uint32_t add = carry, all = 0;
+    for (int w = 0; w < 32; w++) {
+      if (w < warp) add += s[w];
+      all += s[w];
+    }
+    if (i < blocks) counts[i] = x - v + add;
+    __syncthreads();
+    if (t == 0) carry += all;
+    __syncthreads();
+  }
+  if (t == 0) counts[blocks] = carry;
+}
+
+// 3. Run numbers (1-based) of positions [0, m): run_of_row[perm[i]] (when wanted), and for each run's
+// first position its start and its row.
+__global__ void __launch_bounds__(RUN_THREADS) run_ids_kernel(const uint8_t* __restrict__ marks,
+                                                              const uint32_t* __restrict__ block_off,
+                                                              const uint32_t* __restrict__ perm, uint64_t m,
+                                                              uint32_t* __restrict__ run_of_row,
+                                                              uint32_t* __restrict__ starts,
+                                                              uint32_t* __restrict__ heads) {
+  __shared__ uint32_t s_warp[RUN_THREADS / 32];
+  const uint64_t base = uint64_t(blockIdx.x) * RUN_CHUNK + uint64_t(threadIdx.x) * RUN_ITEMS;
+  uint8_t mk[RUN_ITEMS];
+  if (base + RUN_ITEMS <= m) {
+    const uint4 w = *reinterpret_cast<const uint4*>(marks + base);
+    const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+    for (int i = 0; i < RUN_ITEMS; i++) mk[i] = uint8_t(ws[i >> 2] >> (8 * (i & 3)));
+  } else {
+#pragma unroll
+    for (int i = 0; i < RUN_ITEMS; i++) mk[i] = base + i < m ? marks[base + i] : 0;
+  }
+  uint32_t cnt = 0;
+#pragma unroll
+  for (int i = 0; i < RUN_ITEMS; i++) cnt += mk[i];
+  uint32_t run = block_off[blockIdx.x] + block_exclusive(cnt, s_warp);
+#pragma unroll
+  for (int i = 0; i < RUN_ITEMS; i++) {
+    const uint64_t pos = base + i;
+    if (pos >= m) break;
+    run += mk[i];
+    const uint32_t r = perm[pos];
+    if (run_of_row) run_of_row[r] = run;
+    if (mk[i]) {
+      if (starts) starts[run - 1] = uint32_t(pos);
+      if (heads) heads[run - 1] = r;
+    }
+  }
+}
+
+// row_number: the 1-based sorted position, at the original row.
+__global__ void __launch_bounds__(256) position_kernel(const uint32_t* __restrict__ perm, uint64_t n,
+                                                       uint32_t* __restrict__ out) {
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x)
+    out[perm[i]] = uint32_t(i + 1);
+}
+
+// 4. Run numbers into the answer, per original row. A run [s, e) of sorted positions:
+//   FIN_MIN s + 1; FIN_MAX e; FIN_QUANTILE (s + e) / 2n, the run's average 1-based rank minus one
+//   half over n; FIN_NORMAL64 / FIN_NORMAL32 the standard normal quantile of that; FIN_PERCENT
+//   s / (n - 1) (0 for one row); FIN_CUME e / n.
+enum Finish { FIN_MIN = 0, FIN_MAX, FIN_QUANTILE, FIN_NORMAL64, FIN_NORMAL32, FIN_PERCENT, FIN_CUME };
+
+__global__ void __launch_bounds__(256) rank_finish_kernel(uint32_t* __restrict__ run_of_row,
+                                                          const uint32_t* __restrict__ starts,
+                                                          const uint32_t* __restrict__ total_runs, uint64_t n,
+                                                          int mode, void* __restrict__ out) {
+  const uint32_t runs = *total_runs;
+  for (uint64_t r = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; r < n; r += uint64_t(gridDim.x) * blockDim.x) {
+    const uint32_t g = run_of_row[r];
+    const uint64_t s = starts[g - 1];
+    const uint64_t e = g < runs ? uint64_t(starts[g]) : n;
+    switch (mode) {
+      case FIN_MIN: static_cast<uint32_t*>(out)[r] = uint32_t(s + 1); break;
+      case FIN_MAX: static_cast<uint32_t*>(out)[r] = uint32_t(e); break;
+      case FIN_QUANTILE: static_cast<double*>(out)[r] = double(s + e) / double(2 * n); break;
+      case FIN_NORMAL64: static_cast<double*>(out)[r] = normcdfinv(double(s + e) / double(2 * n)); break;
+      case FIN_NORMAL32: static_cast<float*>(out)[r] = float(normcdfinv(double(s + e) / double(2 * n))); break;
+      case FIN_PERCENT: static_cast<double*>(out)[r] = n > 1 ? double(s) / double(n - 1) : 0.0; break;
+      default: static_cast<double*>(out)[r] = double(e) / double(n); break;
+    }
+  }
+}
+
+// Run lengths: counts[g] = start of run g + 1 (or m) - start of run g.
+__global__ void __launch_bounds__(256) run_lengths_kernel(const uint32_t* __restrict__ starts, const uint32_t* __restrict__ total_runs,
+                                                          uint64_t m, int64_t* __restrict__ counts) {
+  const uint32_t runs = *total_runs;
+  for (uint64_t g = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < runs; g += uint64_t(gridDim.x) * blockDim.x) {
+    const uint64_t e = g + 1 < runs ? uint64_t(starts[g + 1]) : m;
+    counts[g] = int64_t(e - starts[g]);
+  }
+}
+
+// rows_out[i] = heads[order[i]], counts_out[i] = counts[order[i]] (when counts are wanted).
+__global__ void __launch_bounds__(256) runs_in_order_kernel(const uint32_t* __restrict__ order, const uint32_t* __restrict__ heads,
+                                                            const int64_t* __restrict__ counts, uint64_t runs,
+                                                            uint32_t* __restrict__ rows_out, int64_t* __restrict__ counts_out) {
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < runs; i += uint64_t(gridDim.x) * blockDim.x) {
+    const uint32_t g = order[i];
+    rows_out[i] = heads[g];
+    if (counts) counts_out[i] = counts[g];
+  }
+}
+
+int grid_for(uint64_t n) {
+  return int(std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, uint64_t(device().sm_count) * 8)));
+}
+
+}  // namespace
+}  // namespace rs
+
+namespace {
+
+using namespace rs;
+
+// The stable argsort (uint32) of one column: a string column through its derived chunk keys.
+BufPtr sorted_order(am_array* a, bool desc, bool nulls_first, cudaStream_t s) {
+  const int64_t n = a->length;
+  BufPtr perm = DevBuffer::alloc(size_t(n) * 4 + 16, s);
+  std::vector<am_array*> derived;
+  std::vector<SortKey> keys;
+  if (pt_var(a->pt)) {
+    derived = string_key_columns(a, s);
+    for (am_array* c : derived) keys.push_back(SortKey{c, desc, nulls_first, 0});
+  } else {
+    keys.push_back(SortKey{a, desc, nulls_first, FO_IEEE});
+  }
+  try {
+    radix_argsort(keys, n, perm->ptr, 4, s, nullptr);
+  } catch (...) {
+    for (am_array* c : derived) release(c);
+    throw;
+  }
+  for (am_array* c : derived) release(c);
+  return perm;
+}
+
+// Steps 1 and 2 over sorted positions [0, m): marks and scanned block counts (blocks + 1 words).
+struct Runs {
+  BufPtr marks, counts;
+  uint32_t blocks = 0;
+  const uint32_t* total() const { return static_cast<const uint32_t*>(counts->ptr) + blocks; }
+};
+
+Runs mark_runs(am_array* a, const uint32_t* perm, uint64_t m, bool merge_nan, cudaStream_t s) {
+  Runs r;
+  r.blocks = uint32_t((m + RUN_CHUNK - 1) / RUN_CHUNK);
+  r.marks = DevBuffer::alloc(size_t(m) + 16, s);
+  r.counts = DevBuffer::alloc(size_t(r.blocks + 1) * 4, s);
+  uint8_t* marks = static_cast<uint8_t*>(r.marks->ptr);
+  uint32_t* counts = static_cast<uint32_t*>(r.counts->ptr);
+  KernelTimer kt("run_marks", s);
+  if (pt_var(a->pt)) {
+    const StrView v{a->data(), static_cast<const uint8_t*>(a->bytes->ptr), a->null_count != 0 ? a->valid_bits() : nullptr,
+                    a->validity_offset};
+    if (a->pt == PT_LSTR) run_marks_str_kernel<int64_t><<<r.blocks, RUN_THREADS, 0, s>>>(v, perm, m, marks, counts);
+    else run_marks_str_kernel<int32_t><<<r.blocks, RUN_THREADS, 0, s>>>(v, perm, m, marks, counts);
+  } else {
+    const ColView c = make_view(SortKey{a, false, false, FO_IEEE});
+    if (pt_key_bytes(a->pt) == 8)
+      run_marks_kernel<uint64_t><<<r.blocks, RUN_THREADS, 0, s>>>(c, merge_nan ? 1 : 0, perm, m, marks, counts);
+    else run_marks_kernel<uint32_t><<<r.blocks, RUN_THREADS, 0, s>>>(c, merge_nan ? 1 : 0, perm, m, marks, counts);
+  }
+  AM_CUDA(cudaGetLastError());
+  run_scan_kernel<<<1, 1024, 0, s>>>(counts, r.blocks);
+  AM_CUDA(cudaGetLastError());
+  return r;
+}
+
+void run_ids(const Runs& r, const uint32_t* perm, uint64_t m, uint32_t* run_of_row, uint32_t* starts, uint32_t* heads,
+             cudaStream_t s) {
+  KernelTimer kt("run_ids", s);
+  run_ids_kernel<<<r.blocks, RUN_THREADS, 0, s>>>(static_cast<const uint8_t*>(r.marks->ptr),
+                                                  static_cast<const uint32_t*>(r.counts->ptr), perm, m, run_of_row,
+                                                  starts, heads);
+  AM_CUDA(cudaGetLastError());
+}
+
+am_array* new_filled(int pt, const char* format, int64_t n, cudaStream_t s) {
+  am_array* o = new_array(pt, format, n);
+  o->values = DevBuffer::alloc(size_t(std::max<int64_t>(n, 1)) * std::max(pt_bytes(pt), 1) + 16, s);
+  o->null_count = 0;
+  o->last_stream = s;
+  return o;
+}
+
+}  // namespace
+
+am_array* rank_of(am_array* a, int fn, bool desc, bool nulls_first, bool merge_nan, cudaStream_t s) {
+  const int64_t n = a->length;
+  const bool f32 = fn == RANK_NORMAL32;
+  const bool f64 = fn == RANK_QUANTILE || fn == RANK_NORMAL64 || fn == RANK_PERCENT || fn == RANK_CUME;
+  am_array* out = f32 ? new_filled(PT_F32, "f", n, s) : f64 ? new_filled(PT_F64, "g", n, s) : new_filled(PT_U32, "I", n, s);
+  if (n == 0) return out;
+  try {
+    use_on(a, s);
+    BufPtr perm = sorted_order(a, desc, nulls_first, s);
+    const uint32_t* p = static_cast<const uint32_t*>(perm->ptr);
+    if (fn == RANK_FIRST) {
+      KernelTimer kt("rank_scatter", s);
+      position_kernel<<<grid_for(uint64_t(n)), 256, 0, s>>>(p, uint64_t(n), static_cast<uint32_t*>(out->values->ptr));
+      AM_CUDA(cudaGetLastError());
+      return out;
+    }
+    const Runs r = mark_runs(a, p, uint64_t(n), merge_nan, s);
+    // Run numbers go straight into a uint32 answer; the float answers read them from scratch.
+    BufPtr scratch = (f32 || f64) ? DevBuffer::alloc(size_t(n) * 4 + 16, s) : nullptr;
+    uint32_t* run_of_row = scratch ? static_cast<uint32_t*>(scratch->ptr) : static_cast<uint32_t*>(out->values->ptr);
+    BufPtr starts = fn == RANK_DENSE ? nullptr : DevBuffer::alloc(size_t(n) * 4 + 16, s);
+    run_ids(r, p, uint64_t(n), run_of_row, starts ? static_cast<uint32_t*>(starts->ptr) : nullptr, nullptr, s);
+    if (fn != RANK_DENSE) {
+      static const int finish[] = {FIN_MIN, FIN_MAX, -1, -1, FIN_QUANTILE, FIN_NORMAL64, FIN_NORMAL32, FIN_PERCENT, FIN_CUME};
+      KernelTimer kt("rank_finish", s);
+      rank_finish_kernel<<<grid_for(uint64_t(n)), 256, 0, s>>>(run_of_row, static_cast<const uint32_t*>(starts->ptr),
+                                                               r.total(), uint64_t(n), finish[fn], out->values->ptr);
+      AM_CUDA(cudaGetLastError());
+    }
+    // The scratch buffers are freed in stream order after the kernels that read them.
+  } catch (...) {
+    release(out);
+    throw;
+  }
+  return out;
+}
+
+am_array* unique_of(am_array* a, bool first_appearance, am_array** counts_out, cudaStream_t s) {
+  const int64_t n = a->length;
+  const int64_t nulls = resolve_null_count(a);
+  // The nulls sort last and are one run; a fixed-width column keeps it in first-appearance order, as
+  // Arrow does, and a string column drops it in both orders (the reference's string dictionary has no
+  // slot for it, Kernels/UniqueOrder.swift:165-200).
+  const bool keep_null = first_appearance && !pt_var(a->pt);
+  const uint64_t m = uint64_t(keep_null ? n : n - nulls);
+  am_array* values = nullptr;
+  am_array* counts = nullptr;
+  auto empty = [&]() {
+    values = new_array(a->pt, a->format, 0);
+    values->null_count = 0;
+    if (pt_var(a->pt)) {
+      values->values = DevBuffer::alloc(16, s);
+      AM_CUDA(cudaMemsetAsync(values->values->ptr, 0, 16, s));
+      values->bytes = DevBuffer::alloc(16, s);
+    } else {
+      values->values = DevBuffer::alloc(16, s);
+    }
+    values->last_stream = s;
+    if (counts_out) *counts_out = new_filled(PT_I64, "l", 0, s);
+    return values;
+  };
+  if (m == 0) return empty();
+  use_on(a, s);
+  BufPtr perm = sorted_order(a, false, false, s);
+  const uint32_t* p = static_cast<const uint32_t*>(perm->ptr);
+  const Runs r = mark_runs(a, p, m, false, s);
+  BufPtr starts = DevBuffer::alloc(size_t(m) * 4 + 16, s);
+  BufPtr heads = DevBuffer::alloc(size_t(m) * 4 + 16, s);
+  run_ids(r, p, m, nullptr, static_cast<uint32_t*>(starts->ptr), static_cast<uint32_t*>(heads->ptr), s);
+  uint32_t runs = 0;
+  AM_CUDA(cudaMemcpyAsync(&runs, r.total(), 4, cudaMemcpyDeviceToHost, s));
+  AM_CUDA(cudaStreamSynchronize(s));
+  if (runs == 0) return empty();
+
+  BufPtr run_counts;
+  if (counts_out) {
+    run_counts = DevBuffer::alloc(size_t(runs) * 8 + 16, s);
+    KernelTimer kt("run_lengths", s);
+    run_lengths_kernel<<<grid_for(runs), 256, 0, s>>>(static_cast<const uint32_t*>(starts->ptr), r.total(), m,
+                                                      static_cast<int64_t*>(run_counts->ptr));
+    AM_CUDA(cudaGetLastError());
+  }
+  // The representatives' rows: ascending order as they are; first-appearance order by a sort of the
+  // runs' earliest rows (distinct, so the order is total).
+  am_array* rows = new_filled(PT_U32, "I", int64_t(runs), s);
+  rows->perm_of = n;
+  try {
+    if (!first_appearance) {
+      AM_CUDA(cudaMemcpyAsync(rows->values->ptr, heads->ptr, size_t(runs) * 4, cudaMemcpyDeviceToDevice, s));
+      if (counts_out) {
+        counts = new_filled(PT_I64, "l", int64_t(runs), s);
+        AM_CUDA(cudaMemcpyAsync(counts->values->ptr, run_counts->ptr, size_t(runs) * 8, cudaMemcpyDeviceToDevice, s));
+      }
+    } else {
+      am_array* head_col = new_array(PT_U32, "I", int64_t(runs));
+      head_col->values = heads;
+      head_col->null_count = 0;
+      head_col->last_stream = s;
+      BufPtr order = DevBuffer::alloc(size_t(runs) * 4 + 16, s);
+      try {
+        radix_argsort({SortKey{head_col, false, false, 0}}, int64_t(runs), order->ptr, 4, s, nullptr);
+      } catch (...) {
+        release(head_col);
+        throw;
+      }
+      release(head_col);
+      if (counts_out) counts = new_filled(PT_I64, "l", int64_t(runs), s);
+      KernelTimer kt("runs_in_order", s);
+      runs_in_order_kernel<<<grid_for(runs), 256, 0, s>>>(
+          static_cast<const uint32_t*>(order->ptr), static_cast<const uint32_t*>(heads->ptr),
+          counts_out ? static_cast<const int64_t*>(run_counts->ptr) : nullptr, runs,
+          static_cast<uint32_t*>(rows->values->ptr), counts ? static_cast<int64_t*>(counts->values->ptr) : nullptr);
+      AM_CUDA(cudaGetLastError());
+    }
+    values = new_array(a->pt, a->format, int64_t(runs));
+    take_columns(&a, 1, rows, &values, false, s);
+  } catch (...) {
+    release(rows);
+    if (values) release(values);
+    if (counts) release(counts);
+    throw;
+  }
+  release(rows);
+  if (counts_out) *counts_out = counts;
+  return values;
+}
+
+}  // namespace am

@@ -905,6 +905,7 @@ static uint64_t min_super() {
 ColView make_view(const SortKey& k) {
   ColView v{};
   const am_array* a = k.col;
+  if (a->pt == PT_STRUCT) throw unsupported("+s: a struct result is exported, not computed on");
   v.values = a->data();
   v.valid = (a->null_count != 0) ? a->valid_bits() : nullptr;
   v.valid_off = a->validity_offset;

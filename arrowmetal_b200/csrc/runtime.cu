@@ -571,7 +571,7 @@ int parse_format(const char* f) {
 }
 
 std::string format_of(int pt) {
-  static const char* names[] = {"b", "c", "C", "s", "S", "i", "I", "l", "L", "e", "f", "g", "u", "U"};
+  static const char* names[] = {"b", "c", "C", "s", "S", "i", "I", "l", "L", "e", "f", "g", "u", "U", "+s"};
   return names[pt];
 }
 
@@ -591,11 +591,13 @@ void release(am_array* a) {
       for (BufPtr* b : {&a->values, &a->bytes, &a->validity, &a->null_count_dev})
         if (*b && b->use_count() == 1) (*b)->stream = s;
     }
+    for (am_array* c : a->children) release(c);
     delete a;
   }
 }
 
 void use_on(am_array* a, cudaStream_t s) {
+  if (a && a->pt == PT_STRUCT) throw unsupported("+s: a struct result is exported, not computed on");
   if (!a || a->shared_read) return;
   if (a->ready && a->last_stream != s) {
     // Contents complete at the ready event: wait for it alone, not for later work on its stream.

@@ -155,8 +155,10 @@ __device__ __forceinline__ uint32_t block_scan(uint32_t v, uint32_t* s_warp, uin
 // `limit`.
 //   PRED_PREFIX: A = value keys with (key >> shift) < p, B = those with (key >> shift) == p, no limit;
 //   PRED_THRESHOLD: A = keys < T, B = keys == T, limit k_rem (T, k_rem: the selection state);
-//   PRED_CATEGORY: B = rows of category `cat` (1 NaN block, 2 null), up to `limit`.
-constexpr int PRED_PREFIX = 0, PRED_THRESHOLD = 1, PRED_CATEGORY = 2;
+//   PRED_CATEGORY: B = rows of category `cat` (1 NaN block, 2 null), up to `limit`;
+//   PRED_PARTITION: against the pivot (category place `cat` in the sorted arrangement, key T when that
+//     is the value block): A = rows before it, B = rows equal to it; every row is written.
+constexpr int PRED_PREFIX = 0, PRED_THRESHOLD = 1, PRED_CATEGORY = 2, PRED_PARTITION = 3;
 struct Compact {
   int mode;
   int cat;
@@ -164,6 +166,7 @@ struct Compact {
   unsigned long long p;
   unsigned long long limit;
   const SelState* st;
+  int nulls_first;            // PRED_PARTITION: the arrangement is [nulls][NaN][values]
 };
 
 template <typename KeyT>
@@ -180,7 +183,7 @@ __device__ __forceinline__ void classify(const Source<KeyT>& src, const Compact&
   }
   int cat[SEL_ITEMS];
   load_source<KeyT>(src, pos, ok, key, cat, row);
-  const KeyT T = KeyT(c.mode == PRED_THRESHOLD ? c.st->prefix : 0);
+  const KeyT T = KeyT((c.mode == PRED_THRESHOLD || c.mode == PRED_PARTITION) ? c.st->prefix : 0);
 #pragma unroll
   for (int i = 0; i < SEL_ITEMS; i++) {
     const bool live = (ok >> i) & 1u;
@@ -191,6 +194,11 @@ __device__ __forceinline__ void classify(const Source<KeyT>& src, const Compact&
     } else if (c.mode == PRED_THRESHOLD) {
       a[i] = live && cat[i] == 0 && key[i] < T;
       b[i] = live && cat[i] == 0 && key[i] == T;
+    } else if (c.mode == PRED_PARTITION) {
+      const int place = c.nulls_first ? 2 - cat[i] : cat[i];   // the category's block in the arrangement
+      const bool same = place == c.cat;
+      a[i] = live && (place < c.cat || (same && cat[i] == 0 && key[i] < T));
+      b[i] = live && same && (cat[i] != 0 || key[i] == T);
     } else {
       a[i] = 0;
       b[i] = live && cat[i] == c.cat;
@@ -222,7 +230,7 @@ __global__ void __launch_bounds__(SEL_THREADS) compact_count_kernel(const __grid
   }
 }
 
-// One block: exclusive scans of the per-block counts, in place.
+// One block: exclusive scans of the per-block counts, in place; the totals land at [blocks].
 __global__ void __launch_bounds__(1024) compact_scan_kernel(uint32_t* __restrict__ count_a, uint32_t* __restrict__ count_b,
                                                             uint32_t blocks) {
   __shared__ unsigned long long s[2][32];
@@ -262,6 +270,10 @@ __global__ void __launch_bounds__(1024) compact_scan_kernel(uint32_t* __restrict
       carry[1] += all[1];
     }
     __syncthreads();
+  }
+  if (t == 0) {
+    count_a[blocks] = uint32_t(carry[0]);
+    count_b[blocks] = uint32_t(carry[1]);
   }
 }
 
@@ -315,13 +327,57 @@ __global__ void __launch_bounds__(256) gather_rows_kernel(const uint32_t* __rest
     out[i] = rows[order[i]];
 }
 
+// Every row at its place: class A rows (in row order) first, then class B rows, then the rest.
+template <typename KeyT>
+__global__ void __launch_bounds__(SEL_THREADS) partition_write_kernel(const __grid_constant__ Source<KeyT> src,
+                                                                      const __grid_constant__ Compact c,
+                                                                      const uint32_t* __restrict__ off_a,
+                                                                      const uint32_t* __restrict__ off_b,
+                                                                      uint32_t blocks, uint32_t* __restrict__ out,
+                                                                      uint32_t* __restrict__ err) {
+  __shared__ uint32_t s_warp[SEL_THREADS / 32];
+  uint32_t a[SEL_ITEMS], b[SEL_ITEMS], row[SEL_ITEMS];
+  KeyT key[SEL_ITEMS];
+  const uint64_t base = uint64_t(blockIdx.x) * SEL_CHUNK;
+  classify<KeyT>(src, c, base, a, b, key, row);
+  uint32_t ca = 0, cb = 0;
+#pragma unroll
+  for (int i = 0; i < SEL_ITEMS; i++) {
+    ca += a[i];
+    cb += b[i];
+  }
+  const uint32_t ea = block_scan(ca, s_warp, nullptr);
+  const uint32_t eb = block_scan(cb, s_warp, nullptr);
+  const uint64_t total_a = off_a[blocks], total_b = off_b[blocks];
+  uint64_t a_before = uint64_t(off_a[blockIdx.x]) + ea, b_before = uint64_t(off_b[blockIdx.x]) + eb;
+#pragma unroll
+  for (int i = 0; i < SEL_ITEMS; i++) {
+    const uint64_t g = base + uint64_t(threadIdx.x) * SEL_ITEMS + i;
+    if (g >= src.n) break;
+    uint64_t d;
+    if (a[i]) d = a_before;
+    else if (b[i]) d = total_a + b_before;
+    else d = total_a + total_b + (g - a_before - b_before);
+    a_before += a[i];
+    b_before += b[i];
+    if (d >= src.n) {
+      atomicOr(err, ERR_BOUNDS);
+      continue;
+    }
+    out[d] = row[i];
+  }
+}
+
+// Per-block counts of a compaction's two classes: blocks + 1 words each (the totals at [blocks]).
+inline size_t compact_count_words(uint64_t n) { return 2 * (size_t((n + SEL_CHUNK - 1) / SEL_CHUNK) + 1); }
+
 template <typename KeyT>
 void compact(const Source<KeyT>& src, const Compact& c, KeyT* out_keys, uint32_t* out_rows, uint64_t cap,
              uint32_t* counts, uint32_t* err, cudaStream_t s) {
   const uint32_t blocks = uint32_t((src.n + SEL_CHUNK - 1) / SEL_CHUNK);
   if (blocks == 0) return;
   uint32_t* count_a = counts;
-  uint32_t* count_b = counts + blocks;
+  uint32_t* count_b = counts + blocks + 1;
   KernelTimer kt("topk_compact", s);
   compact_count_kernel<KeyT><<<blocks, SEL_THREADS, 0, s>>>(src, c, count_a, count_b);
   AM_CUDA(cudaGetLastError());
@@ -329,6 +385,45 @@ void compact(const Source<KeyT>& src, const Compact& c, KeyT* out_keys, uint32_t
   AM_CUDA(cudaGetLastError());
   compact_write_kernel<KeyT><<<blocks, SEL_THREADS, 0, s>>>(src, c, count_a, count_b, out_keys, out_rows, cap, err);
   AM_CUDA(cudaGetLastError());
+}
+
+// The leading digits of the k-th smallest value key (1-based), read off the key statistics' digit
+// histograms: the digits that are constant over the value keys, then the first digit that is not
+// (dv; -1 when every value key is the same), whose histogram is exact for the rows that share the
+// constant ones. k_rem is the wanted key's rank among the keys with those digits; below and bucket
+// count the keys under the chosen digit dv and on it.
+struct Leading {
+  unsigned long long prefix = 0, k_rem = 0;
+  int dv = -1;
+  uint64_t below = 0, bucket = 0;
+};
+Leading leading_digits(const KeyStats& st, int D, uint64_t k) {
+  Leading r;
+  r.k_rem = k;
+  for (int d = D - 1; d >= 0; d--) {
+    const uint32_t* h = st.hist[d];
+    int only = -1, nonzero = 0;
+    for (int b = 0; b < 256; b++)
+      if (h[b]) { nonzero++; only = b; }
+    if (nonzero == 1) {
+      r.prefix |= (unsigned long long)only << (8 * d);
+      continue;
+    }
+    uint64_t run = 0;
+    for (int b = 0; b < 256; b++) {
+      if (h[b] && run < r.k_rem && r.k_rem <= run + h[b]) {
+        r.prefix |= (unsigned long long)b << (8 * d);
+        r.k_rem -= run;
+        r.below = run;
+        r.bucket = h[b];
+        break;
+      }
+      run += h[b];
+    }
+    r.dv = d;
+    break;
+  }
+  return r;
 }
 
 template <typename KeyT>
@@ -343,7 +438,7 @@ am_array* top_k_of(const SortKey& key, int64_t k, cudaStream_t s) {
   const size_t off_state = up(sizeof(KeyStats));
   const size_t off_hist = up(off_state + sizeof(SelState));
   const size_t off_counts = up(off_hist + sizeof(uint32_t) * 256 * D);
-  const size_t bytes = up(off_counts + sizeof(uint32_t) * 2 * size_t(blocks));
+  const size_t bytes = up(off_counts + sizeof(uint32_t) * compact_count_words(n));
   char* base = static_cast<char*>(dmalloc(bytes, s));
   struct Free { char* p; cudaStream_t s; ~Free() { dfree(p, s); } } guard{base, s};
   KeyStats* st = reinterpret_cast<KeyStats*>(base);
@@ -390,33 +485,11 @@ am_array* top_k_of(const SortKey& key, int64_t k, cudaStream_t s) {
                              counts, err, s);
     if (kv) {
       // 1. Leading digits on the host: constant ones, then the first that varies (digit dv).
-      unsigned long long prefix = 0, k_rem = kv;
-      int dv = -1;
-      uint64_t below = 0, bucket = 0;
-      for (int d = D - 1; d >= 0; d--) {
-        const uint32_t* h = host->hist[d];
-        int only = -1, nonzero = 0;
-        for (int b = 0; b < 256; b++)
-          if (h[b]) { nonzero++; only = b; }
-        if (nonzero == 1) {
-          prefix |= (unsigned long long)only << (8 * d);
-          continue;
-        }
-        uint64_t run = 0;
-        for (int b = 0; b < 256; b++) {
-          if (h[b] && run < k_rem && k_rem <= run + h[b]) {
-            prefix |= (unsigned long long)b << (8 * d);
-            k_rem -= run;
-            below = run;
-            bucket = h[b];
-            break;
-          }
-          run += h[b];
-        }
-        dv = d;
-        break;
-      }
-      const SelState init{prefix, k_rem};
+      const Leading lead = leading_digits(*host, D, kv);
+      const int dv = lead.dv;
+      const unsigned long long prefix = lead.prefix;
+      const uint64_t below = lead.below, bucket = lead.bucket;
+      const SelState init{prefix, lead.k_rem};
       AM_CUDA(cudaMemcpyAsync(state, &init, sizeof(SelState), cudaMemcpyHostToDevice, s));
       BufPtr cand_keys = DevBuffer::alloc(size_t(kv) * sizeof(KeyT) + 16, s);
       BufPtr cand_rows = DevBuffer::alloc(size_t(kv) * 4 + 16, s);
@@ -483,8 +556,105 @@ am_array* top_k_of(const SortKey& key, int64_t k, cudaStream_t s) {
   return out;
 }
 
+// Arrow partition_nth_indices (include/arrowmetal.h:1060-1069, :1335; the reference selects the pivot by
+// radix select and compacts, Kernels/PartitionNth.swift:229): a permutation whose position `pivot`
+// holds the row the stable argsort (ascending, the given null placement) puts there, with no row
+// after it ordered before it and none before it ordered after it. By radix selection, reading the
+// column a few times and sorting nothing:
+//   1. the key statistics give the category counts, so the pivot's block ([values][NaN][nulls], or
+//      [nulls][NaN][values]), and for the value block the leading digits of the pivot key T;
+//   2. the lower digits of T, one histogram pass over the column per digit (only the keys that share
+//      the digits chosen so far count);
+//   3. one ordered three-way partition: the rows before the pivot's in the arrangement, in row order,
+//      then the rows equal to it, then the rest.
+template <typename KeyT>
+am_array* partition_of(const SortKey& key, int64_t pivot, cudaStream_t s) {
+  const uint64_t n = uint64_t(key.col->length);
+  constexpr int D = int(sizeof(KeyT));
+  const Source<KeyT> column{make_view(key), nullptr, nullptr, n};
+
+  auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
+  const size_t off_state = up(sizeof(KeyStats));
+  const size_t off_hist = up(off_state + sizeof(SelState));
+  const size_t off_counts = up(off_hist + sizeof(uint32_t) * 256 * D);
+  const size_t bytes = up(off_counts + sizeof(uint32_t) * compact_count_words(n));
+  char* base = static_cast<char*>(dmalloc(bytes, s));
+  struct Free { char* p; cudaStream_t s; ~Free() { dfree(p, s); } } guard{base, s};
+  KeyStats* st = reinterpret_cast<KeyStats*>(base);
+  SelState* state = reinterpret_cast<SelState*>(base + off_state);
+  uint32_t* hist = reinterpret_cast<uint32_t*>(base + off_hist);
+  uint32_t* counts = reinterpret_cast<uint32_t*>(base + off_counts);
+  key_statistics(key, st, s);
+  static thread_local KeyStats* host = nullptr;
+  if (!host) host = static_cast<KeyStats*>(pinned_alloc(sizeof(KeyStats)));
+  AM_CUDA(cudaMemcpyAsync(host, st, sizeof(KeyStats), cudaMemcpyDeviceToHost, s));
+  AM_CUDA(cudaStreamSynchronize(s));
+
+  // 1. The pivot's block: sizes of the arrangement's three blocks in order.
+  const uint64_t p = std::min<uint64_t>(uint64_t(pivot), n - 1);   // pivot == n: any permutation will do
+  const uint64_t sizes[3] = {key.nulls_first ? host->n_null : host->n_value, host->n_nan,
+                             key.nulls_first ? host->n_value : host->n_null};
+  const int value_place = key.nulls_first ? 2 : 0;
+  int place = 0;
+  uint64_t before = 0;
+  while (place < 2 && p >= before + sizes[place]) before += sizes[place++];
+  SelState init{0, 0};
+  int dv = -1;
+  if (place == value_place) {
+    const Leading lead = leading_digits(*host, D, p - before + 1);
+    init = SelState{lead.prefix, lead.k_rem};
+    dv = lead.dv;
+  }
+  AM_CUDA(cudaMemcpyAsync(state, &init, sizeof(SelState), cudaMemcpyHostToDevice, s));
+
+  am_array* out = new_array(PT_U32, "I", int64_t(n));
+  try {
+    out->values = DevBuffer::alloc(size_t(n) * 4 + 16, s);
+    out->null_count = 0;
+    out->perm_of = int64_t(n);
+    out->last_stream = s;
+    // 2. The lower digits of T.
+    if (dv > 0) {
+      AM_CUDA(cudaMemsetAsync(hist, 0, sizeof(uint32_t) * 256 * D, s));
+      KernelTimer kt("partition_select", s);
+      const int grid = int(std::min<uint64_t>((n + SEL_CHUNK - 1) / SEL_CHUNK, uint64_t(device().sm_count) * 8));
+      for (int d = dv - 1; d >= 0; d--) {
+        uint32_t* hd = hist + 256 * d;
+        select_histogram_kernel<KeyT><<<std::max(grid, 1), SEL_THREADS, 0, s>>>(column, 8 * d, state, hd);
+        AM_CUDA(cudaGetLastError());
+        select_step_kernel<<<1, 256, 0, s>>>(hd, 8 * d, state);
+        AM_CUDA(cudaGetLastError());
+      }
+    }
+    // 3. The three-way partition.
+    const uint32_t blocks = uint32_t((n + SEL_CHUNK - 1) / SEL_CHUNK);
+    const Compact c{PRED_PARTITION, place, 0, 0, 0, state, key.nulls_first ? 1 : 0};
+    uint32_t* count_a = counts;
+    uint32_t* count_b = counts + blocks + 1;
+    KernelTimer kt("partition_write", s);
+    compact_count_kernel<KeyT><<<blocks, SEL_THREADS, 0, s>>>(column, c, count_a, count_b);
+    AM_CUDA(cudaGetLastError());
+    compact_scan_kernel<<<1, 1024, 0, s>>>(count_a, count_b, blocks);
+    AM_CUDA(cudaGetLastError());
+    partition_write_kernel<KeyT><<<blocks, SEL_THREADS, 0, s>>>(column, c, count_a, count_b, blocks,
+                                                                static_cast<uint32_t*>(out->values->ptr),
+                                                                stream_scratch(s, 0).err);
+    AM_CUDA(cudaGetLastError());
+  } catch (...) {
+    release(out);
+    throw;
+  }
+  return out;
+}
+
 }  // namespace
 }  // namespace rs
+
+am_array* radix_partition_nth(const SortKey& key, int64_t pivot, cudaStream_t s) {
+  if (key.col->length <= 0 || pt_var(key.col->pt)) return nullptr;
+  return pt_key_bytes(key.col->pt) == 8 ? rs::partition_of<uint64_t>(key, pivot, s)
+                                        : rs::partition_of<uint32_t>(key, pivot, s);
+}
 
 am_array* radix_top_k(const SortKey& key, int64_t k, cudaStream_t s) {
   if (key.col->length <= 0 || k <= 0 || pt_var(key.col->pt)) return nullptr;

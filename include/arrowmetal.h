@@ -96,6 +96,39 @@ int  am_lexsort_ex2(am_array** columns, const int* descending, const int* null_p
 /* Multi-column sort, first column most significant. include/arrowmetal.h:458 */
 int  am_lexsort(am_array** columns, const int* descending, int64_t count, am_array** out);
 
+/* ---- sort consumers --------------------------------------------------------------------------- */
+/* partition_nth_indices: uint32 indices whose position `pivot` holds the row the ascending stable sort
+ * (null_placement as above) puts there; no row before it orders after it, none after it before it, and
+ * each of the three blocks keeps row order. 0 <= pivot <= length, else 1 ("partition index P is outside
+ * 0...N"). A radix select and one three-way partition, not a sort. include/arrowmetal.h:1069, :1335 */
+int  am_partition_nth_indices(am_array* a, int64_t n, am_array** out);                       /* :1069 */
+int  am_partition_nth_ex(am_array* a, int64_t pivot, int null_placement, am_array** out);    /* :1335 */
+/* Arrow rank, uint32 (pyarrow returns uint64 with the same values). tiebreaker: 0 min, 1 max, 2 first,
+ * 3 dense. The nulls and the NaN rows are one tie group at the null_placement end; -0.0 ties +0.0.
+ * include/arrowmetal.h:1306, :1355 */
+int  am_rank_ex(am_array* a, int tiebreaker, int descending, int null_placement, am_array** out);
+/* op 0 rank_quantile (float64: (s + e) / 2n over the row's tie group [s, e) of sorted positions),
+ * op 1 rank_normal (float64: the standard normal quantile of that), op 2 rank_normal in float32.
+ * am_rank is ascending with nulls at the end. include/arrowmetal.h:1001-1014, :1356 */
+int  am_rank(am_array* a, int op, am_array** out);                                           /* :1014 */
+int  am_rank_quantile_ex(am_array* a, int op, int descending, int null_placement, am_array** out);
+/* The ranking ops of am_window: 0 row_number, 1 rank, 2 dense_rank (uint32), 3 percent_rank
+ * ((rank - 1) / (n - 1)), 4 cume_dist (rows at or before the value / n) (float64); ascending, nulls last
+ * and one tie group, every NaN one value after +inf. p1, p2 and scalar_or_null are unused by these ops;
+ * ops 5-12 (shifts, differences, running and rolling windows) return 1, unsupported.
+ * include/arrowmetal.h:415-452 */
+int  am_window(am_array* a, int op, int64_t p1, int64_t p2, const void* scalar_or_null, am_array** out);
+/* Distinct values. order 0 first_appearance (Arrow's order; a fixed-width column keeps one null entry
+ * at the first null's place), 1 sorted (ascending, nulls dropped). String columns drop the null in
+ * both orders. -0.0 matches 0.0 and every NaN is one value; the representative is the earliest row.
+ * am_unique and am_value_counts are the sorted order. value_counts returns a struct array ("+s") of
+ * `values` and int64 `counts`, exported with am_export (it takes part in no other call).
+ * include/arrowmetal.h:1060-1068, :1359-1360 */
+int  am_unique(am_array* a, am_array** out);                                                 /* :1067 */
+int  am_value_counts(am_array* a, am_array** out);                                           /* :1068 */
+int  am_unique_ex(am_array* a, int order, am_array** out);                                   /* :1359 */
+int  am_value_counts_ex(am_array* a, int order, am_array** out);                             /* :1360 */
+
 /* ---- batching --------------------------------------------------------------------------------- */
 /* Between begin and end the calls of this thread do not wait for the GPU; deferred errors (a take
  * out of range) surface from am_batch_end. include/arrowmetal.h:184-185 */

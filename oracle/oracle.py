@@ -236,3 +236,141 @@ def np_lexsort(arrays, descending=None, null_placement="at_end", float_order="ie
     if n == 0:
         return np.empty(0, np.uint32)
     return np.lexsort(seq).astype(np.uint32)
+
+
+# ---- sort consumers (numpy, on the orders above) ----------------------------------------------------
+#
+# Rank, the window rankings, unique / value_counts and partition_nth_indices restated from their
+# definitions over np_argsort's order: a run is a maximal block of sorted positions whose rows are equal
+# under the sort's value equality (same category; same key for a value row -- so -0.0 ties +0.0 and
+# every NaN is one value). The reference builds these on its argsort the same way
+# (Sources/ArrowMetal/Kernels/Window.swift:65-200, Kernels/Unique.swift:46-65,
+# Kernels/UniqueOrder.swift:88-140, Kernels/PartitionNth.swift:215-235).
+
+def _run_starts(arr, order, merge_nan):
+    """True at each sorted position that starts a run. merge_nan: NaN rows and nulls are one run."""
+    key, cat = _keys_and_categories(arr, False, "ieee")
+    k = key[order]
+    c = cat[order].copy()
+    if merge_nan:
+        c[c == 1] = 2
+    start = np.ones(len(order), bool)
+    start[1:] = (c[1:] != c[:-1]) | ((c[1:] == 0) & (k[1:] != k[:-1]))
+    return start
+
+
+def _rank_positions(arr, descending, null_placement, merge_nan):
+    """(sorted order, run number per sorted position (1-based), first and one-past-last position of
+    each position's run)."""
+    order = np_argsort(arr, descending, null_placement).astype(np.int64)
+    n = len(order)
+    start = _run_starts(arr, order, merge_nan)
+    run = np.cumsum(start)
+    starts = np.nonzero(start)[0]
+    ends = np.append(starts[1:], n)
+    return order, run, starts[run - 1], ends[run - 1]
+
+
+def rank(arr, tiebreaker="min", descending=False, null_placement="at_end"):
+    """Arrow rank (pyarrow.compute.rank; the reference's am_rank_ex): 1-based ranks at the original rows,
+    the nulls and NaN rows one tie group at the null_placement end; uint32."""
+    arr = _as_array(arr)
+    n = len(arr)
+    if n == 0:
+        return np.empty(0, np.uint32)
+    order, run, s, e = _rank_positions(arr, descending, null_placement, True)
+    val = {"min": s + 1, "max": e, "first": np.arange(1, n + 1), "dense": run}[tiebreaker]
+    out = np.empty(n, np.uint32)
+    out[order] = val
+    return out
+
+
+def rank_quantile(arr, descending=False, null_placement="at_end"):
+    """Arrow rank_quantile: (s + e) / 2n over the row's run [s, e) of sorted positions, float64 (the
+    run's average 1-based rank minus one half, over n)."""
+    arr = _as_array(arr)
+    n = len(arr)
+    if n == 0:
+        return np.empty(0, np.float64)
+    order, run, s, e = _rank_positions(arr, descending, null_placement, True)
+    out = np.empty(n, np.float64)
+    out[order] = (s + e).astype(np.float64) / np.float64(2 * n)
+    return out
+
+
+def window(arr, op):
+    """The SQL ranking window functions of am_window (ops 0-4): ascending, nulls last and one tie group,
+    every NaN one value after +inf (include/arrowmetal.h:415-434 of the reference)."""
+    arr = _as_array(arr)
+    n = len(arr)
+    if n == 0:
+        return np.empty(0, np.float64 if op in ("percent_rank", "cume_dist") else np.uint32)
+    order, run, s, e = _rank_positions(arr, False, "at_end", False)
+    if op == "row_number":
+        val, dt = np.arange(1, n + 1), np.uint32
+    elif op == "rank":
+        val, dt = s + 1, np.uint32
+    elif op == "dense_rank":
+        val, dt = run, np.uint32
+    elif op == "percent_rank":
+        val, dt = (s.astype(np.float64) / np.float64(n - 1)) if n > 1 else np.zeros(n), np.float64
+    else:
+        val, dt = e.astype(np.float64) / np.float64(n), np.float64
+    out = np.empty(n, dt)
+    out[order] = val
+    return out
+
+
+def unique_rows(arr, order="first_appearance"):
+    """(representative rows, counts) of Arrow unique / value_counts: one row per distinct value, the
+    earliest row carrying it. "sorted": ascending, nulls dropped; "first_appearance": in order of the
+    representatives, with one null entry when there are nulls (not for string columns)."""
+    arr = _as_array(arr)
+    n = len(arr)
+    is_str = pa.types.is_string(arr.type) or pa.types.is_binary(arr.type) or \
+        pa.types.is_large_string(arr.type) or pa.types.is_large_binary(arr.type)
+    if is_str:
+        vals = arr.to_pylist()
+        ordered = sorted((v, i) for i, v in enumerate(vals) if v is not None)
+        heads, counts = [], []
+        for v, i in ordered:
+            if heads and vals[heads[-1]] == v:
+                counts[-1] += 1
+            else:
+                heads.append(i)
+                counts.append(1)
+        heads, counts = np.array(heads, np.int64), np.array(counts, np.int64)
+    else:
+        srt = np_argsort(arr, False, "at_end").astype(np.int64)
+        m = n if order == "first_appearance" else n - arr.null_count
+        srt = srt[:m]
+        if m == 0:
+            return np.empty(0, np.int64), np.empty(0, np.int64)
+        start = _run_starts(arr, srt, False)
+        starts = np.nonzero(start)[0]
+        heads = srt[starts]
+        counts = np.diff(np.append(starts, m))
+    if order == "first_appearance":
+        o = np.argsort(heads, kind="stable")
+        heads, counts = heads[o], counts[o]
+    return heads, counts
+
+
+def partition_nth(arr, pivot, null_placement="at_end"):
+    """Arrow partition_nth_indices as the reference arranges it (Kernels/PartitionNth.swift:215-235):
+    the rows ordered before the pivot row of the ascending stable argsort, then the rows equal to it,
+    then the rest, each block in row order; uint32."""
+    arr = _as_array(arr)
+    n = len(arr)
+    if n == 0:
+        return np.empty(0, np.uint32)
+    key, cat = _keys_and_categories(arr, False, "ieee")
+    place = (2 - cat) if null_placement == "at_start" else cat.astype(np.int64)
+    order = np_argsort(arr, False, null_placement)
+    p = order[min(pivot, n - 1)]
+    P, K = place[p], key[p]
+    value = cat == 0
+    before = (place < P) | ((place == P) & value & (key < K))
+    equal = (place == P) & (~value | (key == K))
+    rows = np.arange(n)
+    return np.concatenate([rows[before], rows[equal], rows[~before & ~equal]]).astype(np.uint32)

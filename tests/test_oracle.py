@@ -1,6 +1,7 @@
 """The CPU oracle, pinned before it is trusted: the reference's known-answer vectors, and every golden
 fixture pyarrow produced (tests/golden/make_golden.py), through both restatements (C and numpy)."""
 import math
+import zlib
 
 import numpy as np
 import pyarrow as pa
@@ -127,3 +128,43 @@ def test_oracle_threads_agree(oracle):
     assert np.array_equal(one, many)
     want = pc.array_sort_indices(a).to_numpy()
     assert np.array_equal(one, want)
+
+
+@pytest.mark.parametrize("t", ["int64", "double", "float", "uint8"])
+def test_consumer_oracles_pinned_to_pyarrow(oracle, t):
+    """The consumers' restatements agree with pyarrow's rank, rank_quantile, unique and value_counts on
+    the same inputs (pyarrow is the reference's oracle for them: python/tests/test_options.py:125-405);
+    the partition has the reference's block arrangement and its row at the pivot ties the sorted one."""
+    import pyarrow.compute as pc
+    rng = np.random.default_rng(zlib.crc32(t.encode()))
+    n = 20_000
+    valid = rng.random(n) > 0.1
+    if t in ("double", "float"):
+        v = np.round(rng.standard_normal(n), 1).astype(np.float64 if t == "double" else np.float32)
+        v[rng.random(n) < 0.05] = np.nan
+        v[rng.random(n) < 0.05] = 0.0
+        v[rng.random(n) < 0.05] = -0.0
+    elif t == "uint8":
+        v = rng.integers(0, 256, n).astype(np.uint8)
+    else:
+        v = rng.integers(-40, 40, n).astype(np.int64)
+    arr = build_array(t, v, valid)
+    for desc in (False, True):
+        sk = "descending" if desc else "ascending"
+        for place in ("at_end", "at_start"):
+            for tb in ("min", "max", "first", "dense"):
+                want = pc.rank(arr, sort_keys=sk, null_placement=place, tiebreaker=tb).to_numpy()
+                assert np.array_equal(oracle.rank(arr, tb, desc, place), want), (desc, place, tb)
+            want_q = pc.rank_quantile(arr, sort_keys=sk, null_placement=place).to_numpy()
+            assert np.allclose(oracle.rank_quantile(arr, desc, place), want_q, rtol=0, atol=1e-15)
+    rows, counts = oracle.unique_rows(arr, "first_appearance")
+    if t not in ("double", "float"):   # pyarrow keeps -0.0 and 0.0 apart; the sort's equality ties them
+        assert arr.take(pa.array(rows, type=pa.int64())).equals(pc.unique(arr))
+        assert np.array_equal(counts, pc.value_counts(arr).field("counts").to_numpy())
+    full = oracle.np_argsort(arr)
+    key, cat = oracle._keys_and_categories(arr, False, "ieee")
+    for pivot in (0, n // 2, n - 1):
+        got = oracle.partition_nth(arr, pivot)
+        assert sorted(got) == list(range(n))
+        a, b = got[pivot], full[pivot]
+        assert cat[a] == cat[b] and (cat[a] != 0 or key[a] == key[b])
