@@ -413,6 +413,54 @@ def run_topk(args, am, torch, stream, local):
         "top_k_ms": per_k, "full_argsort_ms": full_ms, "clocks": clocks.summary()}))
 
 
+def run_consumers(args, am, torch, stream, local):
+    """--workload consumers: the sort consumers on the 50M-row key column (int64 in [0, 2^40), 10% nulls)
+    and on a 50M-row low-cardinality column (1,000 distinct int64 values, 10% nulls): partition_nth_indices
+    at the median, rank, rank_quantile, row_number, unique and value_counts, against the full argsort;
+    CUDA events per call."""
+    import pyarrow as pa
+    key, valid, _, _ = make_table(N_ROWS)
+    col = am.MetalArray.from_arrow(pa.array(key, mask=~valid))
+    rng = np.random.default_rng(SEED + 9)
+    low = am.MetalArray.from_arrow(pa.array(rng.integers(0, 1000, N_ROWS, dtype=np.int64),
+                                            mask=rng.random(N_ROWS) < 0.10))
+
+    def timed(fn, reps):
+        for _ in range(3):
+            fn()
+        am.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(reps):
+            fn()
+        ev1.record(stream)
+        ev1.synchronize()
+        am.synchronize()
+        return ev0.elapsed_time(ev1) / reps
+
+    reps = max(args.steps, 3)
+    with ClockSampler(local) as clocks:
+        ms = {
+            "argsort": timed(lambda: col.argsort(False, "at_end"), reps),
+            "partition_nth_median": timed(lambda: col.partition_nth_indices(N_ROWS // 2), reps),
+            "rank_min": timed(lambda: col.rank(), reps),
+            "rank_dense_low_cardinality": timed(lambda: low.rank(tiebreaker="dense"), reps),
+            "rank_quantile": timed(lambda: col.rank_quantile(), reps),
+            "row_number": timed(lambda: col.row_number(), reps),
+            "unique_sorted": timed(lambda: col.unique("sorted"), reps),
+            "value_counts_low_cardinality": timed(lambda: low.value_counts(), reps),
+        }
+    head = ms["partition_nth_median"]
+    print(json.dumps({
+        "metric": METRIC, "value": N_ROWS / (head / 1e3), "unit": "rows/s", "n_gpus": 1, "steps": reps,
+        "warmup": 3, "ms_per_step": head, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "int64", "data": "synthetic",
+        "config": {"workload": "partition_nth_indices at the median (am_partition_nth_ex) on 50,000,000 int64 keys "
+                               "in [0, 2^40) with 10% nulls, uint32 indices; the other sort consumers beside it",
+                   "rows": N_ROWS},
+        "consumer_ms": ms, "clocks": clocks.summary()}))
+
+
 def make_strings(n, seed=SEED + 8):
     """n utf8 strings of 0-24 lowercase letters (uniform length), 5% nulls, built from numpy buffers."""
     import pyarrow as pa
@@ -653,10 +701,12 @@ def main():
     ap.add_argument("--impl", default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="order_by",
-                    choices=["order_by", "segmented", "serving", "full_range", "multikey", "topk", "strings"],
+                    choices=["order_by", "segmented", "serving", "full_range", "multikey", "topk", "strings",
+                             "consumers"],
                     help="order_by: the 50M-row ORDER BY (the headline); segmented: 2,048 arrays in one call; "
                          "serving: the served request stream; full_range: 1M full-range int64 keys; multikey: "
-                         "the 50M-row two-key sort; topk: ORDER BY ... LIMIT k by radix selection; strings: ORDER BY a utf8 key")
+                         "the 50M-row two-key sort; topk: ORDER BY ... LIMIT k by radix selection; strings: ORDER BY a utf8 key; "
+                         "consumers: partition_nth, rank, unique and value_counts on 50M rows")
     ap.add_argument("--rate", type=float, default=200.0, help="serving: requests per second")
     ap.add_argument("--serve-seconds", type=float, default=30.0, help="serving: length of the open-loop stream")
     ap.add_argument("--sat-requests", type=int, default=400, help="serving: requests of the saturation run")
@@ -701,6 +751,12 @@ def main():
         am.set_stream(stream.cuda_stream)
         if rank == 0:
             run_topk(args, am, torch, stream, local)
+        return
+    if args.workload == "consumers":
+        stream = torch.cuda.Stream()
+        am.set_stream(stream.cuda_stream)
+        if rank == 0:
+            run_consumers(args, am, torch, stream, local)
         return
     if args.workload in ("full_range", "multikey"):
         stream = torch.cuda.Stream()
