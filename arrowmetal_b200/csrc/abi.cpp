@@ -91,8 +91,23 @@ BufPtr upload_bits(const uint8_t* src, int64_t off, int64_t n, cudaStream_t s) {
   return b;
 }
 
+bool is_index_format(const char* f) {
+  static const char* idx[] = {"c", "C", "s", "S", "i", "I", "l", "L"};
+  for (const char* x : idx)
+    if (std::strcmp(f, x) == 0) return true;
+  return false;
+}
+
 void check_array_struct(const ArrowSchema* schema, const ArrowArray* array) {
-  if (schema->dictionary || array->dictionary) throw unsupported("dictionary arrays are not carried by this build");
+  if (!schema->dictionary != !array->dictionary) throw invalid("the schema and the array disagree on a dictionary");
+  if (schema->dictionary) {
+    // A dictionary array: integer codes, and a flat dictionary (not itself dictionary-encoded).
+    if (!is_index_format(schema->format))
+      throw invalid(std::string("dictionary codes of type ") + schema->format + " (an integer type is required)");
+    if (schema->dictionary->dictionary || array->dictionary->dictionary)
+      throw unsupported("a dictionary whose values are themselves dictionary-encoded");
+    parse_format(schema->dictionary->format);
+  }
   if (schema->n_children != 0 || array->n_children != 0) throw unsupported("nested arrays are not carried by this build");
   if (array->length < 0 || array->offset < 0) throw invalid("negative length or offset");
   const int want = pt_var(parse_format(schema->format)) ? 3 : 2;
@@ -200,11 +215,18 @@ struct ExportHold {
   am_array* keep = nullptr;       // am_export_device: the array whose HBM the buffers point into
   const void* buffers[3] = {nullptr, nullptr, nullptr};
   std::string format, name;
+  ArrowArray* dict_array = nullptr;     // a dictionary array's exported dictionary (owned)
+  ArrowSchema* dict_schema = nullptr;
 };
 
 void release_schema(ArrowSchema* s) {
   if (!s || !s->release) return;
-  delete static_cast<ExportHold*>(s->private_data);
+  auto* h = static_cast<ExportHold*>(s->private_data);
+  if (h->dict_schema) {
+    if (h->dict_schema->release) h->dict_schema->release(h->dict_schema);
+    delete h->dict_schema;
+  }
+  delete h;
   s->release = nullptr;
   s->private_data = nullptr;
 }
@@ -213,6 +235,10 @@ void release_array(ArrowArray* a) {
   auto* h = static_cast<ExportHold*>(a->private_data);
   for (void* p : h->pinned) pinned_free(p);
   if (h->keep) am::release(h->keep);
+  if (h->dict_array) {
+    if (h->dict_array->release) h->dict_array->release(h->dict_array);
+    delete h->dict_array;
+  }
   delete h;
   a->release = nullptr;
   a->private_data = nullptr;
@@ -291,17 +317,11 @@ am_array* argsort_keys(std::vector<SortKey>& keys, int width, const char* op) {
   am_array* out = make_index_array(n, width, s);
   std::vector<am_array*> derived;
   try {
-    // String keys sort as their derived chunk and length keys.
+    // String keys sort as their derived chunk and length keys, dictionary keys as their rank columns.
     std::vector<SortKey> sort_keys;
     for (auto& k : keys) {
-      if (!pt_var(k.col->pt) || n == 0) {
-        sort_keys.push_back(k);
-        continue;
-      }
-      for (am_array* c : string_key_columns(k.col, s)) {
-        derived.push_back(c);
-        sort_keys.push_back(SortKey{c, k.descending, k.nulls_first, 0});
-      }
+      if (n == 0) sort_keys.push_back(k);
+      else expand_sort_key(k, sort_keys, derived, s);
     }
     radix_argsort(sort_keys, n, out->values->ptr, width, s, &tls().last_stats);
   } catch (...) {
@@ -331,6 +351,10 @@ am_array* take_one(am_array* a, am_array* idx) {
 am_array* slice_of(am_array* a, int64_t offset, int64_t length) {
   if (a->pt == PT_STRUCT) throw unsupported("+s: a struct result is exported, not computed on");
   am_array* o = new_array(a->pt, a->format, length);
+  if (a->dictionary) {
+    retain(a->dictionary);
+    o->dictionary = a->dictionary;
+  }
   o->values = a->values;
   o->bytes = a->bytes;
   o->value_offset = a->value_offset + offset;
@@ -388,6 +412,17 @@ int am_import(const ArrowSchema* schema, ArrowArray* array, am_array** out) {
     cudaStream_t s = stream();
     am_array* a = new_array(pt, schema->format, array->length);
     try {
+      if (schema->dictionary) {
+        // The codes, then the dictionary (both copied before the producer's release).
+        import_host(a, array, s);
+        am_array* d = new_array(parse_format(schema->dictionary->format), schema->dictionary->format,
+                                array->dictionary->length);
+        a->dictionary = d;
+        import_host(d, array->dictionary, s);
+        move_release(array);
+        *out = a;
+        return 0;
+      }
       if (import_pinned_async(a, array)) {
         *out = a;
         return 0;
@@ -409,7 +444,8 @@ int am_import_device(const ArrowSchema* schema, ArrowDeviceArray* darr, am_array
     ArrowArray* array = &darr->array;
     const int pt = parse_format(schema->format);
     const int dt0 = darr->device_type;
-    if (pt_var(pt) && dt0 == ARROW_DEVICE_CUDA) throw unsupported("am_import_device takes fixed-width CUDA arrays; import string arrays from host memory");
+    if ((pt_var(pt) || schema->dictionary) && dt0 == ARROW_DEVICE_CUDA)
+      throw unsupported("am_import_device takes fixed-width CUDA arrays; import string and dictionary arrays from host memory");
     check_array_struct(schema, array);
     const int dt = darr->device_type;
     if (dt == ARROW_DEVICE_CPU || dt == ARROW_DEVICE_CUDA_HOST) return am_import(schema, array, out);
@@ -662,7 +698,28 @@ int am_export(am_array* a, ArrowSchema* schema, ArrowArray* array) {
       delete h;
       throw;
     }
-    if (schema) fill_schema(a, schema);
+    ArrowSchema* dict_schema = nullptr;
+    if (a->dictionary) {
+      // A dictionary array: the codes above, and the dictionary exported beside them.
+      h->dict_array = new ArrowArray{};
+      dict_schema = schema ? new ArrowSchema{} : nullptr;
+      const int rc = am_export(a->dictionary, dict_schema, h->dict_array);
+      if (rc != 0) {
+        const std::string why = am_last_error();
+        delete dict_schema;
+        delete h->dict_array;
+        for (void* p : h->pinned) pinned_free(p);
+        delete h;
+        throw Error(why, rc);
+      }
+    }
+    if (schema) {
+      fill_schema(a, schema);
+      if (dict_schema) {
+        static_cast<ExportHold*>(schema->private_data)->dict_schema = dict_schema;
+        schema->dictionary = dict_schema;
+      }
+    }
     array->length = n;
     array->null_count = nulls;
     array->offset = 0;
@@ -670,7 +727,7 @@ int am_export(am_array* a, ArrowSchema* schema, ArrowArray* array) {
     array->n_children = 0;
     array->buffers = h->buffers;
     array->children = nullptr;
-    array->dictionary = nullptr;
+    array->dictionary = h->dict_array;
     array->release = release_array;
     array->private_data = h;
     return 0;
@@ -680,7 +737,8 @@ int am_export(am_array* a, ArrowSchema* schema, ArrowArray* array) {
 int am_export_device(am_array* a, ArrowSchema* schema, ArrowDeviceArray* darr) {
   if (!a || !darr) return 2;
   return guard([&] {
-    if (a->pt == PT_STRUCT) throw unsupported("am_export_device takes flat arrays; export a struct result with am_export");
+    if (a->pt == PT_STRUCT || a->dictionary)
+      throw unsupported("am_export_device takes flat arrays; export struct and dictionary arrays with am_export");
     if (pt_var(a->pt)) throw unsupported("am_export_device takes fixed-width arrays; export string arrays with am_export");
     const int64_t nulls = resolve_null_count(a);
     if (a->validity && a->validity_offset != a->value_offset)

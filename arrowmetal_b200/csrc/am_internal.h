@@ -202,6 +202,10 @@ struct am_array {
   // Recorded on last_stream when the contents were complete (optional): an export waits for it alone,
   // not for later work on that stream.
   std::shared_ptr<am::ReadyEvent> ready;
+  // A dictionary-encoded array: `pt` / `format` / `values` are its integer codes and this is the
+  // dictionary they index (a flat array, one reference owned). Sorts order by the values; takes and
+  // slices move the codes and share the dictionary.
+  am_array* dictionary = nullptr;
   // PT_STRUCT: the fields, owned (one reference each), and their names.
   std::vector<am_array*> children;
   std::vector<std::string> child_names;
@@ -274,13 +278,21 @@ am_array* radix_partition_nth(const SortKey& key, int64_t pivot, cudaStream_t s)
 // Sort consumers (consumers.cu). rank_of's functions: Arrow's rank tiebreakers in the C ABI's numbering
 // (0 min, 1 max, 2 first, 3 dense), then rank_quantile, rank_normal in float64 and float32, and the SQL
 // percent_rank and cume_dist. `merge_nan`: the NaN rows tie with the nulls (Arrow's rank functions).
-enum RankFn {
+enum RankFn : int {
   RANK_MIN = 0, RANK_MAX, RANK_FIRST, RANK_DENSE, RANK_QUANTILE, RANK_NORMAL64, RANK_NORMAL32, RANK_PERCENT, RANK_CUME
 };
-am_array* rank_of(am_array* a, int fn, bool desc, bool nulls_first, bool merge_nan, cudaStream_t s);
+am_array* rank_of(am_array* a, int fn, bool desc, bool nulls_first, bool merge_nan, cudaStream_t s,
+                  int float_order = 0);
 // The distinct values, ascending or in order of first appearance; `counts_out` (may be NULL) receives
 // each one's row count (int64).
 am_array* unique_of(am_array* a, bool first_appearance, am_array** counts_out, cudaStream_t s);
+// The sort key of a dictionary column: per row the rank of its value among the dictionary's distinct
+// values under `k`'s float order (a float, so a NaN value stays NaN), null where the code or the value
+// is null. Sorting it with k's direction and null placement (float order ieee) sorts the column.
+am_array* dictionary_key_column(const SortKey& k, cudaStream_t s);
+// The radix sort's keys for one sort key: the key itself, a string key's chunk and length keys, or a
+// dictionary key's rank column. Derived columns are appended to `derived` (the caller releases them).
+void expand_sort_key(const SortKey& k, std::vector<SortKey>& keys, std::vector<am_array*>& derived, cudaStream_t s);
 
 // String and binary columns: the derived unsigned keys that sort like the strings (big-endian 8-byte
 // chunks, then the length; the first carries the nulls), and the take of one string column.

@@ -289,6 +289,79 @@ __global__ void __launch_bounds__(256) runs_in_order_kernel(const uint32_t* __re
   }
 }
 
+// A dictionary column's values as the key builder reads them: validity, and (ieee float values) the
+// bits that tell a NaN.
+struct DictView {
+  const void* values;
+  const uint8_t* valid;       // NULL: no null entries
+  int64_t valid_off;
+  int32_t pt;
+  int32_t nan_cat;            // a NaN value is its own block (ieee order)
+};
+
+__device__ __forceinline__ int64_t load_code(const void* codes, int pt, uint64_t r) {
+  switch (pt) {
+    case PT_I8: return static_cast<const int8_t*>(codes)[r];
+    case PT_U8: return static_cast<const uint8_t*>(codes)[r];
+    case PT_I16: return static_cast<const int16_t*>(codes)[r];
+    case PT_U16: return static_cast<const uint16_t*>(codes)[r];
+    case PT_I32: return static_cast<const int32_t*>(codes)[r];
+    case PT_U32: return static_cast<const uint32_t*>(codes)[r];
+    case PT_U64: {
+      const uint64_t v = static_cast<const uint64_t*>(codes)[r];
+      return v > uint64_t(INT64_MAX) ? -1 : int64_t(v);
+    }
+    default: return static_cast<const int64_t*>(codes)[r];
+  }
+}
+
+__device__ __forceinline__ bool entry_is_nan(const DictView& d, uint64_t c) {
+  switch (d.pt) {
+    case PT_F16: return (static_cast<const uint16_t*>(d.values)[c] & 0x7FFFu) > 0x7C00u;
+    case PT_F32: return (static_cast<const uint32_t*>(d.values)[c] & 0x7FFFFFFFu) > 0x7F800000u;
+    case PT_F64: return (static_cast<const uint64_t*>(d.values)[c] & 0x7FFFFFFFFFFFFFFFull) > 0x7FF0000000000000ull;
+    default: return false;
+  }
+}
+
+// Row keys of a dictionary column: the dense rank (1-based) of the row's value among the dictionary's
+// distinct values, minus one, as a float; NaN for a NaN value in the ieee order; null where the code or
+// the value is null. A warp handles 32 consecutive rows and writes their validity word.
+template <typename OutT>
+__global__ void __launch_bounds__(256) dict_row_keys_kernel(const void* __restrict__ codes, int code_pt,
+                                                            const uint8_t* __restrict__ code_valid, int64_t code_voff,
+                                                            uint64_t n, const __grid_constant__ DictView dict,
+                                                            const uint32_t* __restrict__ dense, uint64_t d,
+                                                            OutT* __restrict__ key, uint32_t* __restrict__ valid_words,
+                                                            unsigned long long* __restrict__ null_count,
+                                                            uint32_t* __restrict__ err) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t warps = uint64_t(gridDim.x) * (blockDim.x >> 5);
+  unsigned long long nulls = 0;
+  for (uint64_t w = uint64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); w * 32 < n; w += warps) {
+    const uint64_t r = w * 32 + lane;
+    bool valid = false;
+    OutT k = OutT(0);
+    if (r < n && (!code_valid || bit_at(code_valid, code_voff + int64_t(r)))) {
+      const int64_t c = load_code(codes, code_pt, r);
+      if (c < 0 || uint64_t(c) >= d) {
+        atomicOr(err, ERR_DICT_CODE);
+      } else if (!dict.valid || bit_at(dict.valid, dict.valid_off + c)) {
+        valid = true;
+        k = (dict.nan_cat && entry_is_nan(dict, uint64_t(c))) ? OutT(NAN) : OutT(dense[c] - 1u);
+      }
+    }
+    const uint32_t word = __ballot_sync(0xffffffffu, valid);
+    if (r < n) key[r] = k;
+    if (lane == 0) {
+      valid_words[w] = word;
+      const uint64_t live = n - w * 32 < 32 ? n - w * 32 : 32;
+      nulls += live - uint64_t(__popc(word));
+    }
+  }
+  if (lane == 0 && nulls) atomicAdd(null_count, nulls);
+}
+
 int grid_for(uint64_t n) {
   return int(std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, uint64_t(device().sm_count) * 8)));
 }
@@ -301,7 +374,7 @@ namespace {
 using namespace rs;
 
 // The stable argsort (uint32) of one column: a string column through its derived chunk keys.
-BufPtr sorted_order(am_array* a, bool desc, bool nulls_first, cudaStream_t s) {
+BufPtr sorted_order(am_array* a, bool desc, bool nulls_first, int float_order, cudaStream_t s) {
   const int64_t n = a->length;
   BufPtr perm = DevBuffer::alloc(size_t(n) * 4 + 16, s);
   std::vector<am_array*> derived;
@@ -310,7 +383,7 @@ BufPtr sorted_order(am_array* a, bool desc, bool nulls_first, cudaStream_t s) {
     derived = string_key_columns(a, s);
     for (am_array* c : derived) keys.push_back(SortKey{c, desc, nulls_first, 0});
   } else {
-    keys.push_back(SortKey{a, desc, nulls_first, FO_IEEE});
+    keys.push_back(SortKey{a, desc, nulls_first, float_order});
   }
   try {
     radix_argsort(keys, n, perm->ptr, 4, s, nullptr);
@@ -329,7 +402,7 @@ struct Runs {
   const uint32_t* total() const { return static_cast<const uint32_t*>(counts->ptr) + blocks; }
 };
 
-Runs mark_runs(am_array* a, const uint32_t* perm, uint64_t m, bool merge_nan, cudaStream_t s) {
+Runs mark_runs(am_array* a, const uint32_t* perm, uint64_t m, bool merge_nan, int float_order, cudaStream_t s) {
   Runs r;
   r.blocks = uint32_t((m + RUN_CHUNK - 1) / RUN_CHUNK);
   r.marks = DevBuffer::alloc(size_t(m) + 16, s);
@@ -343,7 +416,7 @@ Runs mark_runs(am_array* a, const uint32_t* perm, uint64_t m, bool merge_nan, cu
     if (a->pt == PT_LSTR) run_marks_str_kernel<int64_t><<<r.blocks, RUN_THREADS, 0, s>>>(v, perm, m, marks, counts);
     else run_marks_str_kernel<int32_t><<<r.blocks, RUN_THREADS, 0, s>>>(v, perm, m, marks, counts);
   } else {
-    const ColView c = make_view(SortKey{a, false, false, FO_IEEE});
+    const ColView c = make_view(SortKey{a, false, false, float_order});
     if (pt_key_bytes(a->pt) == 8)
       run_marks_kernel<uint64_t><<<r.blocks, RUN_THREADS, 0, s>>>(c, merge_nan ? 1 : 0, perm, m, marks, counts);
     else run_marks_kernel<uint32_t><<<r.blocks, RUN_THREADS, 0, s>>>(c, merge_nan ? 1 : 0, perm, m, marks, counts);
@@ -373,15 +446,29 @@ am_array* new_filled(int pt, const char* format, int64_t n, cudaStream_t s) {
 
 }  // namespace
 
-am_array* rank_of(am_array* a, int fn, bool desc, bool nulls_first, bool merge_nan, cudaStream_t s) {
+am_array* rank_of(am_array* a, int fn, bool desc, bool nulls_first, bool merge_nan, cudaStream_t s, int float_order) {
   const int64_t n = a->length;
+  if (a->dictionary && n > 0) {
+    // A dictionary column ranks as its sort key, which orders and ties exactly as its values.
+    use_on(a, s);
+    am_array* key = dictionary_key_column(SortKey{a, desc, nulls_first, float_order}, s);
+    am_array* r = nullptr;
+    try {
+      r = rank_of(key, fn, desc, nulls_first, merge_nan, s, FO_IEEE);
+    } catch (...) {
+      release(key);
+      throw;
+    }
+    release(key);
+    return r;
+  }
   const bool f32 = fn == RANK_NORMAL32;
   const bool f64 = fn == RANK_QUANTILE || fn == RANK_NORMAL64 || fn == RANK_PERCENT || fn == RANK_CUME;
   am_array* out = f32 ? new_filled(PT_F32, "f", n, s) : f64 ? new_filled(PT_F64, "g", n, s) : new_filled(PT_U32, "I", n, s);
   if (n == 0) return out;
   try {
     use_on(a, s);
-    BufPtr perm = sorted_order(a, desc, nulls_first, s);
+    BufPtr perm = sorted_order(a, desc, nulls_first, float_order, s);
     const uint32_t* p = static_cast<const uint32_t*>(perm->ptr);
     if (fn == RANK_FIRST) {
       KernelTimer kt("rank_scatter", s);
@@ -389,7 +476,7 @@ am_array* rank_of(am_array* a, int fn, bool desc, bool nulls_first, bool merge_n
       AM_CUDA(cudaGetLastError());
       return out;
     }
-    const Runs r = mark_runs(a, p, uint64_t(n), merge_nan, s);
+    const Runs r = mark_runs(a, p, uint64_t(n), merge_nan, float_order, s);
     // Run numbers go straight into a uint32 answer; the float answers read them from scratch.
     BufPtr scratch = (f32 || f64) ? DevBuffer::alloc(size_t(n) * 4 + 16, s) : nullptr;
     uint32_t* run_of_row = scratch ? static_cast<uint32_t*>(scratch->ptr) : static_cast<uint32_t*>(out->values->ptr);
@@ -411,6 +498,7 @@ am_array* rank_of(am_array* a, int fn, bool desc, bool nulls_first, bool merge_n
 }
 
 am_array* unique_of(am_array* a, bool first_appearance, am_array** counts_out, cudaStream_t s) {
+  if (a->dictionary) throw unsupported("unique / value_counts of a dictionary column (its dictionary holds the distinct values)");
   const int64_t n = a->length;
   const int64_t nulls = resolve_null_count(a);
   // The nulls sort last and are one run; a fixed-width column keeps it in first-appearance order, as
@@ -436,9 +524,9 @@ am_array* unique_of(am_array* a, bool first_appearance, am_array** counts_out, c
   };
   if (m == 0) return empty();
   use_on(a, s);
-  BufPtr perm = sorted_order(a, false, false, s);
+  BufPtr perm = sorted_order(a, false, false, FO_IEEE, s);
   const uint32_t* p = static_cast<const uint32_t*>(perm->ptr);
-  const Runs r = mark_runs(a, p, m, false, s);
+  const Runs r = mark_runs(a, p, m, false, FO_IEEE, s);
   BufPtr starts = DevBuffer::alloc(size_t(m) * 4 + 16, s);
   BufPtr heads = DevBuffer::alloc(size_t(m) * 4 + 16, s);
   run_ids(r, p, m, nullptr, static_cast<uint32_t*>(starts->ptr), static_cast<uint32_t*>(heads->ptr), s);
@@ -498,6 +586,69 @@ am_array* unique_of(am_array* a, bool first_appearance, am_array** counts_out, c
   release(rows);
   if (counts_out) *counts_out = counts;
   return values;
+}
+
+void expand_sort_key(const SortKey& k, std::vector<SortKey>& keys, std::vector<am_array*>& derived, cudaStream_t s) {
+  if (k.col->dictionary) {
+    am_array* c = dictionary_key_column(k, s);
+    derived.push_back(c);
+    keys.push_back(SortKey{c, k.descending, k.nulls_first, FO_IEEE});
+  } else if (pt_var(k.col->pt)) {
+    for (am_array* c : string_key_columns(k.col, s)) {
+      derived.push_back(c);
+      keys.push_back(SortKey{c, k.descending, k.nulls_first, 0});
+    }
+  } else {
+    keys.push_back(k);
+  }
+}
+
+am_array* dictionary_key_column(const SortKey& k, cudaStream_t s) {
+  am_array* a = k.col;
+  am_array* dict = a->dictionary;
+  const int64_t n = a->length, d = dict->length;
+  if (dict->dictionary) throw unsupported("a dictionary whose values are themselves dictionary-encoded");
+  use_on(dict, s);
+  // Dense ranks of the dictionary's values (ascending, in the key's float order): equal values share one.
+  am_array* dense = d > 0 ? rank_of(dict, RANK_DENSE, false, false, false, s, k.float_order) : nullptr;
+  // A float32 key holds every rank exactly below 2^24 distinct values; a float64 one beyond.
+  const bool wide = d > (int64_t(1) << 24);
+  am_array* key = new_array(wide ? PT_F64 : PT_F32, wide ? "g" : "f", n);
+  try {
+    const uint64_t words = uint64_t(n + 31) / 32;
+    key->values = DevBuffer::alloc(size_t(std::max<int64_t>(n, 1)) * (wide ? 8 : 4) + 16, s);
+    key->validity = DevBuffer::alloc(size_t(words) * 4 + 16, s);
+    key->null_count_dev = DevBuffer::alloc(16, s);
+    key->null_count = -1;
+    key->last_stream = s;
+    AM_CUDA(cudaMemsetAsync(key->null_count_dev->ptr, 0, sizeof(unsigned long long), s));
+    const bool fl = pt_float(dict->pt);
+    const DictView dv{pt_var(dict->pt) ? nullptr : dict->data(), dict->null_count != 0 ? dict->valid_bits() : nullptr,
+                      dict->validity_offset, dict->pt, (fl && k.float_order == FO_IEEE) ? 1 : 0};
+    const uint32_t* dn = dense ? static_cast<const uint32_t*>(dense->values->ptr) : nullptr;
+    const int grid = int(std::max<uint64_t>(1, std::min<uint64_t>(words / 8 + 1, uint64_t(device().sm_count) * 8)));
+    uint32_t* err = stream_scratch(s, 0).err;
+    auto* nc = static_cast<unsigned long long*>(key->null_count_dev->ptr);
+    const uint8_t* cv = a->null_count != 0 ? a->valid_bits() : nullptr;
+    KernelTimer kt("dictionary_keys", s);
+    if (wide)
+      dict_row_keys_kernel<double><<<grid, 256, 0, s>>>(a->data(), a->pt, cv, a->validity_offset, uint64_t(n), dv, dn,
+                                                        uint64_t(d), static_cast<double*>(key->values->ptr),
+                                                        static_cast<uint32_t*>(key->validity->ptr), nc, err);
+    else
+      dict_row_keys_kernel<float><<<grid, 256, 0, s>>>(a->data(), a->pt, cv, a->validity_offset, uint64_t(n), dv, dn,
+                                                       uint64_t(d), static_cast<float*>(key->values->ptr),
+                                                       static_cast<uint32_t*>(key->validity->ptr), nc, err);
+    AM_CUDA(cudaGetLastError());
+    // A code outside the dictionary is an invalid array: report it here, not in a later call.
+    check_device_errors(s);
+  } catch (...) {
+    release(key);
+    if (dense) release(dense);
+    throw;
+  }
+  if (dense) release(dense);
+  return key;
 }
 
 }  // namespace am

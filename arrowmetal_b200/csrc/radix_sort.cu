@@ -906,6 +906,7 @@ ColView make_view(const SortKey& k) {
   ColView v{};
   const am_array* a = k.col;
   if (a->pt == PT_STRUCT) throw unsupported("+s: a struct result is exported, not computed on");
+  if (a->dictionary) throw Error("radix sort: a dictionary column must be sorted through its key column");
   v.values = a->data();
   v.valid = (a->null_count != 0) ? a->valid_bits() : nullptr;
   v.valid_off = a->validity_offset;
@@ -946,6 +947,7 @@ void key_statistics(const SortKey& k, rs::KeyStats* st, cudaStream_t s) {
 }
 
 bool key_invertible(const SortKey& k) {
+  if (k.col->dictionary) return false;   // the codes do not order the column
   switch (k.col->pt) {
     case PT_I8: case PT_U8: case PT_I16: case PT_U16: case PT_I32: case PT_U32: case PT_I64: case PT_U64:
       return true;
@@ -1464,12 +1466,12 @@ void radix_argsort_batch(const std::vector<SortKey>& keys, const std::vector<voi
   std::vector<size_t> g4, g8;
   for (size_t i = 0; i < keys.size(); i++) {
     if (keys[i].col->length <= 0) continue;
-    if (pt_var(keys[i].col->pt)) {
-      // A string array: its derived chunk and length keys, sorted on their own.
-      std::vector<am_array*> derived = string_key_columns(keys[i].col, s);
+    if (pt_var(keys[i].col->pt) || keys[i].col->dictionary) {
+      // A string or dictionary array: its derived keys, sorted on their own.
+      std::vector<am_array*> derived;
       std::vector<SortKey> ks;
-      for (am_array* c : derived) ks.push_back(SortKey{c, keys[i].descending, keys[i].nulls_first, 0});
       try {
+        expand_sort_key(keys[i], ks, derived, s);
         radix_argsort(ks, keys[i].col->length, outs[i], 4, s, nullptr);
       } catch (...) {
         for (am_array* c : derived) release(c);

@@ -31,6 +31,7 @@ constexpr uint64_t LOOKBACK_TIMEOUT_NS = 1000000000ull;   // 1 s, then the pass 
 constexpr uint32_t ERR_LOOKBACK_TIMEOUT = 1;
 constexpr uint32_t ERR_TAKE_RANGE = 2;
 constexpr uint32_t ERR_BOUNDS = 4;                        // a kernel computed a destination outside its array
+constexpr uint32_t ERR_DICT_CODE = 8;                     // a dictionary code outside its dictionary
 
 // One key column as the kernels read it.
 struct ColView {

@@ -467,6 +467,7 @@ void check_device_errors(cudaStream_t s) {
   if (e & rs::ERR_TAKE_RANGE) throw invalid("take: index out of range");
   if (e & rs::ERR_LOOKBACK_TIMEOUT) throw Error("radix sort: a look-back wait timed out on the device");
   if (e & rs::ERR_BOUNDS) throw Error("radix sort: a destination fell outside its array (write skipped)");
+  if (e & rs::ERR_DICT_CODE) throw invalid("dictionary code out of range of its dictionary");
   throw Error("device error word " + std::to_string(e));
 }
 
@@ -592,6 +593,7 @@ void release(am_array* a) {
         if (*b && b->use_count() == 1) (*b)->stream = s;
     }
     for (am_array* c : a->children) release(c);
+    if (a->dictionary) release(a->dictionary);
     delete a;
   }
 }

@@ -420,6 +420,11 @@ void take_columns(am_array* const* cols_in, int count_in, am_array* indices, am_
   std::vector<am_array*> fixed_cols, fixed_outs;
   for (int c = 0; c < count_in; c++) {
     if (cols_in[c]->pt == PT_STRUCT) throw unsupported("+s: a struct result is exported, not computed on");
+    if (cols_in[c]->dictionary && !outs_in[c]->dictionary) {
+      // The codes move; the dictionary is shared.
+      retain(cols_in[c]->dictionary);
+      outs_in[c]->dictionary = cols_in[c]->dictionary;
+    }
     if (pt_var(cols_in[c]->pt)) {
       take_strings(cols_in[c], indices, outs_in[c], check_range, s);
     } else {

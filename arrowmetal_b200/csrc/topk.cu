@@ -650,13 +650,32 @@ am_array* partition_of(const SortKey& key, int64_t pivot, cudaStream_t s) {
 }  // namespace
 }  // namespace rs
 
+// A dictionary column selects on its rank column, which orders and ties as its values.
+template <typename F>
+am_array* on_dictionary_key(const SortKey& key, cudaStream_t s, F&& f) {
+  am_array* c = dictionary_key_column(key, s);
+  am_array* r = nullptr;
+  try {
+    r = f(SortKey{c, key.descending, key.nulls_first, rs::FO_IEEE});
+  } catch (...) {
+    release(c);
+    throw;
+  }
+  release(c);
+  return r;
+}
+
 am_array* radix_partition_nth(const SortKey& key, int64_t pivot, cudaStream_t s) {
+  if (key.col->length > 0 && key.col->dictionary)
+    return on_dictionary_key(key, s, [&](const SortKey& k) { return radix_partition_nth(k, pivot, s); });
   if (key.col->length <= 0 || pt_var(key.col->pt)) return nullptr;
   return pt_key_bytes(key.col->pt) == 8 ? rs::partition_of<uint64_t>(key, pivot, s)
                                         : rs::partition_of<uint32_t>(key, pivot, s);
 }
 
 am_array* radix_top_k(const SortKey& key, int64_t k, cudaStream_t s) {
+  if (key.col->length > 0 && k > 0 && key.col->dictionary)
+    return on_dictionary_key(key, s, [&](const SortKey& kk) { return radix_top_k(kk, k, s); });
   if (key.col->length <= 0 || k <= 0 || pt_var(key.col->pt)) return nullptr;
   return pt_key_bytes(key.col->pt) == 8 ? rs::top_k_of<uint64_t>(key, k, s) : rs::top_k_of<uint32_t>(key, k, s);
 }

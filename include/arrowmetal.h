@@ -39,8 +39,10 @@ const char* am_device_name(void);                 /* include/arrowmetal.h:16 */
 const char* am_last_error(void);                  /* include/arrowmetal.h:17 */
 
 /* ---- lifecycle and interop -------------------------------------------------------------------- */
-/* Moves `array` (its release is NULL on success) and copies its buffers into HBM.
- * include/arrowmetal.h:20 */
+/* Moves `array` (its release is NULL on success) and copies its buffers into HBM. Primitive, boolean,
+ * temporal, utf8 / binary (and their large forms) arrays, and dictionary arrays of those with integer
+ * codes: am_format then reports the codes' format, every sort orders the column by its values, and
+ * take / slice / sorted copies keep the dictionary. include/arrowmetal.h:20, :124-130 */
 int  am_import(const struct ArrowSchema* schema, struct ArrowArray* array, am_array** out);
 /* ARROW_DEVICE_CUDA arrays on this library's device are wrapped without a copy (the producer's
  * release runs when the last handle goes); ARROW_DEVICE_CPU / CUDA_HOST arrays are copied.

@@ -75,8 +75,12 @@ def _physical(arr):
 
 
 def _as_array(a):
+    """A plain array: chunks combined, and a dictionary array decoded -- the reference orders a dictionary
+    column by its decoded values (Sources/ArrowMetal/Kernels/MultiSort.swift:124-133)."""
     if isinstance(a, pa.ChunkedArray):
         a = a.combine_chunks()
+    if pa.types.is_dictionary(a.type):
+        a = a.dictionary_decode()
     return a
 
 
@@ -206,6 +210,7 @@ def _keys_and_categories(arr, descending, float_order):
 
 
 def np_argsort(arr, descending=False, null_placement="at_end", float_order="ieee"):
+    arr = _as_array(arr)
     key, cat = _keys_and_categories(arr, descending, float_order)
     order = np.argsort(key, kind="stable")
     vals = order[cat[order] == 0]
@@ -224,7 +229,7 @@ def np_lexsort(arrays, descending=None, null_placement="at_end", float_order="ie
     order = [float_order] * K if isinstance(float_order, str) else list(float_order)
     cols = []
     for a, d, p, f in zip(arrays, desc, place, order):
-        key, cat = _keys_and_categories(a, d, f)
+        key, cat = _keys_and_categories(_as_array(a), d, f)
         rank = np.where(cat == 0, 2, np.where(cat == 1, 1, 0)) if p == "at_start" else cat
         key = np.where(cat == 0, key, np.uint64(0))
         cols.append((rank.astype(np.int64), key))
