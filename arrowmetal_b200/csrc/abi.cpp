@@ -315,21 +315,13 @@ am_array* argsort_keys(std::vector<SortKey>& keys, int width, const char* op) {
   cudaStream_t s = stream();
   for (auto& k : keys) use_on(k.col, s);
   am_array* out = make_index_array(n, width, s);
-  std::vector<am_array*> derived;
   try {
     // String keys sort as their derived chunk and length keys, dictionary keys as their rank columns.
-    std::vector<SortKey> sort_keys;
-    for (auto& k : keys) {
-      if (n == 0) sort_keys.push_back(k);
-      else expand_sort_key(k, sort_keys, derived, s);
-    }
-    radix_argsort(sort_keys, n, out->values->ptr, width, s, &tls().last_stats);
+    argsort_any(keys, n, out->values->ptr, width, s, &tls().last_stats);
   } catch (...) {
-    for (am_array* c : derived) am::release(c);
     am::release(out);
     throw;
   }
-  for (am_array* c : derived) am::release(c);
   if (!in_batch() && std::getenv("ARROWMETAL_SYNC_EVERY_CALL")) check_device_errors(s);
   return out;
 }

@@ -290,13 +290,19 @@ am_array* unique_of(am_array* a, bool first_appearance, am_array** counts_out, c
 // values under `k`'s float order (a float, so a NaN value stays NaN), null where the code or the value
 // is null. Sorting it with k's direction and null placement (float order ieee) sorts the column.
 am_array* dictionary_key_column(const SortKey& k, cudaStream_t s);
-// The radix sort's keys for one sort key: the key itself, a string key's chunk and length keys, or a
-// dictionary key's rank column. Derived columns are appended to `derived` (the caller releases them).
-void expand_sort_key(const SortKey& k, std::vector<SortKey>& keys, std::vector<am_array*>& derived, cudaStream_t s);
+// Stable argsort over any sort keys: string keys of any length (their chunk and length keys),
+// dictionary keys (their rank columns) and plain columns. Up to MAX_KEYS derived keys sort in one
+// radix sort; more are sorted in groups of MAX_KEYS, least significant group first, each group's
+// keys gathered through the order so far and the orders composed. `out` gets n indices of `width`.
+void argsort_any(const std::vector<SortKey>& keys, int64_t n, void* out, int width, cudaStream_t s,
+                 am_sort_stats* stats);
 
 // String and binary columns: the derived unsigned keys that sort like the strings (big-endian 8-byte
 // chunks, then the length; the first carries the nulls), and the take of one string column.
-std::vector<am_array*> string_key_columns(const am_array* a, cudaStream_t s);
+// A string key is the tuple (chunk 0, ..., chunk m-1, length) with m = string_chunk_count; a call
+// derives chunks [first, first + count) and, when asked, the length (chunk 0 carries the nulls).
+int string_chunk_count(const am_array* a, cudaStream_t s);
+std::vector<am_array*> string_key_columns(const am_array* a, int first, int count, bool with_length, cudaStream_t s);
 void take_strings(am_array* src, am_array* idx, am_array* out, bool check_range, cudaStream_t s);
 
 // Gathers `count` columns through one index array. outs[i] must be new arrays of indices' length.

@@ -373,25 +373,11 @@ namespace {
 
 using namespace rs;
 
-// The stable argsort (uint32) of one column: a string column through its derived chunk keys.
+// The stable argsort (uint32) of one column.
 BufPtr sorted_order(am_array* a, bool desc, bool nulls_first, int float_order, cudaStream_t s) {
   const int64_t n = a->length;
   BufPtr perm = DevBuffer::alloc(size_t(n) * 4 + 16, s);
-  std::vector<am_array*> derived;
-  std::vector<SortKey> keys;
-  if (pt_var(a->pt)) {
-    derived = string_key_columns(a, s);
-    for (am_array* c : derived) keys.push_back(SortKey{c, desc, nulls_first, 0});
-  } else {
-    keys.push_back(SortKey{a, desc, nulls_first, float_order});
-  }
-  try {
-    radix_argsort(keys, n, perm->ptr, 4, s, nullptr);
-  } catch (...) {
-    for (am_array* c : derived) release(c);
-    throw;
-  }
-  for (am_array* c : derived) release(c);
+  argsort_any({SortKey{a, desc, nulls_first, float_order}}, n, perm->ptr, 4, s, nullptr);
   return perm;
 }
 
@@ -588,19 +574,163 @@ am_array* unique_of(am_array* a, bool first_appearance, am_array** counts_out, c
   return values;
 }
 
-void expand_sort_key(const SortKey& k, std::vector<SortKey>& keys, std::vector<am_array*>& derived, cudaStream_t s) {
-  if (k.col->dictionary) {
-    am_array* c = dictionary_key_column(k, s);
-    derived.push_back(c);
-    keys.push_back(SortKey{c, k.descending, k.nulls_first, FO_IEEE});
-  } else if (pt_var(k.col->pt)) {
-    for (am_array* c : string_key_columns(k.col, s)) {
-      derived.push_back(c);
-      keys.push_back(SortKey{c, k.descending, k.nulls_first, 0});
+namespace {
+
+// One derived key of argsort_any: a column as it is (chunk == -2), or a string column's chunk `chunk`
+// or (chunk == -1) its length.
+struct Piece {
+  SortKey key;
+  int chunk;
+};
+
+__global__ void __launch_bounds__(256) compose_kernel(const uint32_t* __restrict__ perm, const uint32_t* __restrict__ order,
+                                                      uint64_t n, uint32_t* __restrict__ out) {
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x)
+    out[i] = perm[order[i]];
+}
+
+__global__ void __launch_bounds__(256) widen_kernel(const uint32_t* __restrict__ in, uint64_t n, uint64_t* __restrict__ out) {
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x)
+    out[i] = in[i];
+}
+
+// The columns of pieces [lo, hi), in row order: consecutive chunks of one string column are derived
+// in one pass over its bytes.
+std::vector<am_array*> materialize(const std::vector<Piece>& p, size_t lo, size_t hi, cudaStream_t s) {
+  std::vector<am_array*> cols;
+  try {
+    for (size_t i = lo; i < hi;) {
+      if (p[i].chunk == -2) {
+        retain(p[i].key.col);
+        cols.push_back(p[i].key.col);
+        i++;
+        continue;
+      }
+      if (p[i].chunk == -1) {
+        // A length piece on its own (its chunks sit in the group before).
+        std::vector<am_array*> c = string_key_columns(p[i].key.col, 0, 0, true, s);
+        cols.insert(cols.end(), c.begin(), c.end());
+        i++;
+        continue;
+      }
+      size_t j = i;
+      while (j + 1 < hi && p[j + 1].key.col == p[i].key.col && p[j + 1].chunk == p[j].chunk + 1) j++;
+      const bool with_length = j + 1 < hi && p[j + 1].key.col == p[i].key.col && p[j + 1].chunk == -1;
+      std::vector<am_array*> c = string_key_columns(p[i].key.col, p[i].chunk, int(j - i + 1), with_length, s);
+      cols.insert(cols.end(), c.begin(), c.end());
+      i = j + 1 + (with_length ? 1 : 0);
     }
-  } else {
-    keys.push_back(k);
+  } catch (...) {
+    for (am_array* c : cols) release(c);
+    throw;
   }
+  return cols;
+}
+
+}  // namespace
+
+void argsort_any(const std::vector<SortKey>& keys, int64_t n, void* out, int width, cudaStream_t s,
+                 am_sort_stats* stats) {
+  if (n <= 0) return;
+  std::vector<am_array*> owned;
+  std::vector<Piece> pieces;
+  auto release_all = [&](std::vector<am_array*>& v) {
+    for (am_array* c : v) release(c);
+    v.clear();
+  };
+  try {
+    for (const SortKey& k : keys) {
+      if (k.col->dictionary) {
+        am_array* c = dictionary_key_column(k, s);
+        owned.push_back(c);
+        pieces.push_back(Piece{SortKey{c, k.descending, k.nulls_first, FO_IEEE}, -2});
+      } else if (pt_var(k.col->pt)) {
+        const int m = string_chunk_count(k.col, s);
+        for (int j = 0; j < m; j++) pieces.push_back(Piece{SortKey{k.col, k.descending, k.nulls_first, 0}, j});
+        pieces.push_back(Piece{SortKey{k.col, k.descending, k.nulls_first, 0}, -1});
+      } else {
+        pieces.push_back(Piece{k, -2});
+      }
+    }
+    auto sort_keys_of = [&](const std::vector<am_array*>& cols, size_t lo) {
+      std::vector<SortKey> ks;
+      for (size_t c = 0; c < cols.size(); c++) {
+        const SortKey& pk = pieces[lo + c].key;
+        ks.push_back(SortKey{cols[c], pk.descending, pk.nulls_first, pieces[lo + c].chunk == -2 ? pk.float_order : 0});
+      }
+      return ks;
+    };
+    const size_t P = pieces.size(), G = size_t(MAX_KEYS);
+    if (P <= G) {
+      std::vector<am_array*> cols = materialize(pieces, 0, P, s);
+      try {
+        radix_sort(sort_keys_of(cols, 0), n, out, width, nullptr, s, stats);
+      } catch (...) {
+        release_all(cols);
+        throw;
+      }
+      release_all(cols);
+      release_all(owned);
+      return;
+    }
+    // Groups of MAX_KEYS derived keys, least significant first: each sorted stably in the order the
+    // groups after it left, so the composed order sorts by every key.
+    am_array* perm = nullptr;      // the order so far (uint32 row numbers), NULL: the identity
+    try {
+      for (size_t hi = P; hi > 0;) {
+        const size_t lo = hi > G ? hi - G : 0;
+        std::vector<am_array*> cols = materialize(pieces, lo, hi, s);
+        std::vector<am_array*> moved;
+        BufPtr order = DevBuffer::alloc(size_t(n) * 4 + 16, s);
+        try {
+          if (perm) {
+            // This group's keys in the current order.
+            moved.assign(cols.size(), nullptr);
+            for (size_t c = 0; c < cols.size(); c++) moved[c] = new_array(cols[c]->pt, cols[c]->format, n);
+            take_columns(cols.data(), int(cols.size()), perm, moved.data(), false, s);
+          }
+          radix_sort(sort_keys_of(perm ? moved : cols, lo), n, order->ptr, 4, nullptr, s, stats);
+        } catch (...) {
+          release_all(cols);
+          release_all(moved);
+          throw;
+        }
+        release_all(cols);
+        release_all(moved);
+        am_array* next = new_array(PT_U32, "I", n);
+        next->null_count = 0;
+        next->perm_of = n;
+        next->last_stream = s;
+        if (perm) {
+          next->values = DevBuffer::alloc(size_t(n) * 4 + 16, s);
+          compose_kernel<<<grid_for(uint64_t(n)), 256, 0, s>>>(static_cast<const uint32_t*>(perm->values->ptr),
+                                                               static_cast<const uint32_t*>(order->ptr), uint64_t(n),
+                                                               static_cast<uint32_t*>(next->values->ptr));
+          AM_CUDA(cudaGetLastError());
+          release(perm);
+        } else {
+          next->values = order;
+        }
+        perm = next;
+        hi = lo;
+      }
+      if (width == 8) {
+        widen_kernel<<<grid_for(uint64_t(n)), 256, 0, s>>>(static_cast<const uint32_t*>(perm->values->ptr), uint64_t(n),
+                                                          static_cast<uint64_t*>(out));
+        AM_CUDA(cudaGetLastError());
+      } else {
+        AM_CUDA(cudaMemcpyAsync(out, perm->values->ptr, size_t(n) * 4, cudaMemcpyDeviceToDevice, s));
+      }
+    } catch (...) {
+      if (perm) release(perm);
+      throw;
+    }
+    release(perm);
+  } catch (...) {
+    release_all(owned);
+    throw;
+  }
+  release_all(owned);
 }
 
 am_array* dictionary_key_column(const SortKey& k, cudaStream_t s) {

@@ -1467,17 +1467,8 @@ void radix_argsort_batch(const std::vector<SortKey>& keys, const std::vector<voi
   for (size_t i = 0; i < keys.size(); i++) {
     if (keys[i].col->length <= 0) continue;
     if (pt_var(keys[i].col->pt) || keys[i].col->dictionary) {
-      // A string or dictionary array: its derived keys, sorted on their own.
-      std::vector<am_array*> derived;
-      std::vector<SortKey> ks;
-      try {
-        expand_sort_key(keys[i], ks, derived, s);
-        radix_argsort(ks, keys[i].col->length, outs[i], 4, s, nullptr);
-      } catch (...) {
-        for (am_array* c : derived) release(c);
-        throw;
-      }
-      for (am_array* c : derived) release(c);
+      // A string or dictionary array: sorted on its own through its derived keys.
+      argsort_any({keys[i]}, keys[i].col->length, outs[i], 4, s, nullptr);
       continue;
     }
     (pt_key_bytes(keys[i].col->pt) == 8 ? g8 : g4).push_back(i);

@@ -47,24 +47,28 @@ __global__ void __launch_bounds__(256) max_length_kernel(const OffT* __restrict_
   if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
 }
 
-// chunk[j][r]: bytes [8j, 8j + 8) of row r, big-endian, zero-padded; length[r].
+// chunk[j][r]: bytes [8 (first + j), 8 (first + j) + 8) of row r, big-endian, zero-padded, for j < m;
+// length[r] (when asked). A null row is the empty string here, whatever its slot spans, so the null
+// rows tie on every derived key and keep their row order.
 template <typename OffT, typename LenT>
 __global__ void __launch_bounds__(256) chunk_kernel(const OffT* __restrict__ off, const uint8_t* __restrict__ bytes,
-                                                    uint64_t n, int m, uint64_t* const* __restrict__ chunks,
+                                                    const uint8_t* __restrict__ valid, int64_t voff, uint64_t n,
+                                                    int first, int m, uint64_t* const* __restrict__ chunks,
                                                     LenT* __restrict__ length) {
   for (uint64_t r = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; r < n; r += uint64_t(gridDim.x) * blockDim.x) {
     uint64_t s, l;
     row_span(off, int64_t(r), s, l);
+    if (valid && !bit_at(valid, voff + int64_t(r))) l = 0;
     for (int j = 0; j < m; j++) {
       uint64_t v = 0;
 #pragma unroll
       for (int b = 0; b < 8; b++) {
-        const uint64_t p = uint64_t(j) * 8 + b;
+        const uint64_t p = uint64_t(first + j) * 8 + b;
         v = (v << 8) | (p < l ? uint64_t(bytes[s + p]) : 0u);
       }
       chunks[j][r] = v;
     }
-    length[r] = LenT(l);
+    if (length) length[r] = LenT(l);
   }
 }
 
@@ -260,7 +264,7 @@ uint64_t max_length(const am_array* a, cudaStream_t s) {
 }
 
 template <typename OffT, typename LenT>
-std::vector<am_array*> key_columns(const am_array* a, int m, cudaStream_t s) {
+std::vector<am_array*> key_columns(const am_array* a, int first, int m, bool with_length, cudaStream_t s) {
   const uint64_t n = uint64_t(a->length);
   std::vector<am_array*> cols;
   std::vector<uint64_t*> ptrs;
@@ -274,25 +278,32 @@ std::vector<am_array*> key_columns(const am_array* a, int m, cudaStream_t s) {
       ptrs.push_back(static_cast<uint64_t*>(c->values->ptr));
     }
     const bool wide = sizeof(LenT) == 8;
-    am_array* len = new_array(wide ? PT_U64 : PT_U32, wide ? "L" : "I", int64_t(n));
-    cols.push_back(len);
-    len->values = DevBuffer::alloc(size_t(std::max<uint64_t>(n, 1)) * sizeof(LenT) + 16, s);
-    len->null_count = 0;
-    len->last_stream = s;
+    LenT* len_ptr = nullptr;
+    if (with_length) {
+      am_array* len = new_array(wide ? PT_U64 : PT_U32, wide ? "L" : "I", int64_t(n));
+      cols.push_back(len);
+      len->values = DevBuffer::alloc(size_t(std::max<uint64_t>(n, 1)) * sizeof(LenT) + 16, s);
+      len->null_count = 0;
+      len->last_stream = s;
+      len_ptr = static_cast<LenT*>(len->values->ptr);
+    }
     BufPtr table = DevBuffer::alloc(sizeof(uint64_t*) * std::max(m, 1), s);
     if (m > 0) AM_CUDA(cudaMemcpyAsync(table->ptr, ptrs.data(), sizeof(uint64_t*) * m, cudaMemcpyHostToDevice, s));
+    const uint8_t* valid = a->null_count != 0 ? a->valid_bits() : nullptr;
     chunk_kernel<OffT, LenT><<<grid_for(n, 256), 256, 0, s>>>(offsets_at_row0<OffT>(a),
-                                                             static_cast<const uint8_t*>(a->bytes->ptr), n, m,
-                                                             static_cast<uint64_t* const*>(table->ptr),
-                                                             static_cast<LenT*>(len->values->ptr));
+                                                             a->bytes ? static_cast<const uint8_t*>(a->bytes->ptr) : nullptr,
+                                                             valid, a->validity_offset, n, first, m,
+                                                             static_cast<uint64_t* const*>(table->ptr), len_ptr);
     AM_CUDA(cudaGetLastError());
-    // The first derived key carries the column's nulls (routed or folded by the sort).
-    am_array* first = cols.front();
-    first->validity = a->validity;
-    first->validity_offset = a->validity_offset;
-    first->null_count = a->null_count;
-    first->null_count_dev = a->null_count_dev;
-    if (a->null_count < 0) first->null_count = -1;
+    // Chunk 0 carries the column's nulls (routed or folded by the sort).
+    if (first == 0 && m > 0) {
+      am_array* c0 = cols.front();
+      c0->validity = a->validity;
+      c0->validity_offset = a->validity_offset;
+      c0->null_count = a->null_count;
+      c0->null_count_dev = a->null_count_dev;
+      if (a->null_count < 0) c0->null_count = -1;
+    }
   } catch (...) {
     for (am_array* c : cols) release(c);
     throw;
@@ -375,16 +386,20 @@ void take_strings_t(am_array* src, am_array* idx, am_array* out, bool check, cud
 
 }  // namespace
 
-std::vector<am_array*> string_key_columns(const am_array* a, cudaStream_t s) {
+int string_chunk_count(const am_array* a, cudaStream_t s) {
+  if (!pt_var(a->pt)) throw Error("string_chunk_count: not a string column");
+  if (a->length <= 0) return 1;
+  const uint64_t maxlen = a->pt == PT_LSTR ? max_length<int64_t>(a, s) : max_length<int32_t>(a, s);
+  const uint64_t m = std::max<uint64_t>(1, (maxlen + 7) / 8);
+  if (m > (uint64_t(1) << 24)) throw unsupported("string keys longer than 128 MiB");
+  return int(m);
+}
+
+std::vector<am_array*> string_key_columns(const am_array* a, int first, int count, bool with_length, cudaStream_t s) {
   if (!pt_var(a->pt)) throw Error("string_key_columns: not a string column");
   if (a->length <= 0) throw Error("string_key_columns: empty column");
-  const bool large = a->pt == PT_LSTR;
-  const uint64_t maxlen = large ? max_length<int64_t>(a, s) : max_length<int32_t>(a, s);
-  const int m = int(std::max<uint64_t>(1, (maxlen + 7) / 8));
-  if (m > rs::MAX_KEYS - 1)
-    throw unsupported("string keys longer than " + std::to_string(8 * (rs::MAX_KEYS - 1)) + " bytes (" +
-                      std::to_string(maxlen) + " here) are not sorted by this build");
-  return large ? key_columns<int64_t, uint64_t>(a, m, s) : key_columns<int32_t, uint32_t>(a, m, s);
+  return a->pt == PT_LSTR ? key_columns<int64_t, uint64_t>(a, first, count, with_length, s)
+                          : key_columns<int32_t, uint32_t>(a, first, count, with_length, s);
 }
 
 void take_strings(am_array* src, am_array* idx, am_array* out, bool check_range, cudaStream_t s) {

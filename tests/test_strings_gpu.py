@@ -1,6 +1,6 @@
 """String and binary columns (utf8 / binary, large_utf8 / large_binary): import and export, argsort in
-Arrow's byte order (a prefix before its extensions, ties in row order), take, lexsort with mixed keys,
-plan sorts, batches, top-k -- all against pyarrow on the same inputs."""
+Arrow's byte order (a prefix before its extensions, ties in row order) at any key length, take, lexsort
+with mixed keys, plan sorts, batches, top-k -- all against pyarrow on the same inputs."""
 import numpy as np
 import pyarrow as pa
 import pyarrow.compute as pc
@@ -136,7 +136,68 @@ def test_batch_top_k_and_sorted_copy(am):
     assert m.sort(True).to_arrow().equals(arr.take(pa.array(full)))
 
 
-def test_long_strings_are_refused(am):
-    arr = pa.array([b"x" * 200, b"y"], type=pa.binary())
-    with pytest.raises(am.ArrowMetalError, match="longer than 120 bytes"):
-        am.MetalArray.from_arrow(arr).argsort()
+def long_strings(rng, n, max_len=600, null_frac=0.05):
+    """Strings past 120 bytes that share long prefixes: a few long stems, then short random tails."""
+    stems = [bytes(rng.integers(97, 100, int(k)).astype(np.uint8)) for k in (0, 100, 119, 120, 121, 250, 500)]
+    out = []
+    for _ in range(n):
+        if rng.random() < null_frac:
+            out.append(None)
+            continue
+        stem = stems[int(rng.integers(len(stems)))]
+        tail = bytes(rng.integers(0, 3, int(rng.integers(0, 12))).astype(np.uint8))
+        out.append((stem + tail)[:max_len])
+    return out
+
+
+@pytest.mark.parametrize("typ", [pa.binary(), pa.large_utf8()])
+@pytest.mark.parametrize("desc", [False, True])
+@pytest.mark.parametrize("placement", PLACEMENTS)
+def test_keys_longer_than_sixteen_chunks(am, typ, desc, placement):
+    # More than 15 chunks: the key sorts in chained groups of 16 derived keys.
+    rng = np.random.default_rng(7 + desc)
+    vals = long_strings(rng, 60_000)
+    if typ == pa.large_utf8():
+        vals = [None if v is None else v.decode("latin-1") for v in vals]
+    arr = pa.array(vals, type=typ)
+    got = ids(am.MetalArray.from_arrow(arr).argsort(desc, placement))
+    want = pc.array_sort_indices(arr, order="descending" if desc else "ascending", null_placement=placement).to_numpy()
+    assert np.array_equal(got, want)
+
+
+def test_long_keys_in_lexsort_plans_and_batches(am):
+    rng = np.random.default_rng(8)
+    n = 40_000
+    s = pa.array(long_strings(rng, n, max_len=300), type=pa.binary())
+    k = pa.array(rng.integers(0, 4, n), mask=rng.random(n) < 0.1)
+    t = pa.table({"s": s, "k": k})
+    for keys in ([("s", "ascending"), ("k", "descending")], [("k", "ascending"), ("s", "descending")]):
+        cols = [t[c].combine_chunks() for c, _ in keys]
+        got = ids(am.lexsort_indices(cols, descending=[o == "descending" for _, o in keys], null_placement="at_start"))
+        want = pc.sort_indices(t, keys, null_placement="at_start").to_numpy()
+        assert np.array_equal(got, want), keys
+    outs = am.argsort_batch([am.MetalArray.from_arrow(s), am.MetalArray.from_arrow(k)])
+    assert np.array_equal(ids(outs[0]), pc.array_sort_indices(s).to_numpy())
+    src = am.PlanSource("t", {"s": s, "k": k})
+    out = am.run_plan({"op": "sort", "by": [["s", False, {"nulls": "last"}]], "input": {"op": "scan", "source": "t"}},
+                      [src])
+    assert out["s"].to_arrow().equals(s.take(pc.array_sort_indices(s)))
+    m = am.MetalArray.from_arrow(s)
+    assert np.array_equal(ids(m.top_k(100, False)), pc.array_sort_indices(s).to_numpy()[:100])
+    assert np.array_equal(ids(m.rank(tiebreaker="dense")), pc.rank(s, tiebreaker="dense").to_numpy())
+
+
+def test_null_slots_that_span_bytes_keep_row_order(am):
+    # Arrow lets a null row's slot cover bytes; the sort must still tie the null rows.
+    vals = [b"zz", b"b", b"a", b"q", b"c", b"aa"]
+    offsets = np.array([0, 2, 3, 4, 5, 6, 8], dtype=np.int32)
+    data = b"".join(vals)
+    valid = np.array([1, 0, 1, 0, 0, 1], dtype=np.uint8)
+    arr = pa.Array.from_buffers(pa.binary(), 6, [pa.py_buffer(np.packbits(valid, bitorder="little").tobytes()),
+                                                 pa.py_buffer(offsets.tobytes()), pa.py_buffer(data)], null_count=3)
+    for desc in (False, True):
+        for placement in PLACEMENTS:
+            got = ids(am.MetalArray.from_arrow(arr).argsort(desc, placement))
+            want = pc.array_sort_indices(arr, order="descending" if desc else "ascending",
+                                         null_placement=placement).to_numpy()
+            assert np.array_equal(got, want), (desc, placement)
