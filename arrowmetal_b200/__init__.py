@@ -130,6 +130,18 @@ for _name, _res, _args in [
     ("am_partition_nth_indices", _I, [_P, _I64, _PP]), ("am_partition_nth_ex", _I, [_P, _I64, _I, _PP]),
     ("am_rank_ex", _I, [_P, _I, _I, _I, _PP]), ("am_rank_quantile_ex", _I, [_P, _I, _I, _I, _PP]),
     ("am_rank", _I, [_P, _I, _PP]), ("am_window", _I, [_P, _I, _I64, _I64, _P, _PP]),
+    ("am_stream_last_error", ctypes.c_char_p, []), ("am_stream_from_c_stream", _P, [_P, _I]),
+    ("am_stream_open_ipc", _P, [ctypes.c_char_p, _I, _I]), ("am_stream_release", None, [_P]),
+    ("am_stream_select", _I, [_P, ctypes.POINTER(ctypes.c_char_p), _I64]),
+    ("am_stream_sort_ex", _I, [_P, ctypes.POINTER(ctypes.c_char_p), _IP, _IP, _IP, _I64, _I64, ctypes.c_char_p,
+                               ctypes.c_char_p, _PP]),
+    ("am_stream_sort", _I, [_P, ctypes.POINTER(ctypes.c_char_p), _IP, _I64, _I64, ctypes.c_char_p, ctypes.c_char_p,
+                            _PP]),
+    ("am_stream_result_column_count", _I64, [_P]), ("am_stream_result_column_name", ctypes.c_char_p, [_P, _I64]),
+    ("am_stream_result_column", _I, [_P, _I64, _PP]), ("am_stream_result_rows_out", _I64, [_P]),
+    ("am_stream_result_stats", _I, [_P] + [ctypes.POINTER(_I64)] * 3 + [ctypes.POINTER(ctypes.c_double)] * 5),
+    ("am_stream_result_stalls", _I, [_P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
+    ("am_stream_result_release", None, [_P]),
     ("am_unique", _I, [_P, _PP]), ("am_unique_ex", _I, [_P, _I, _PP]),
     ("am_value_counts", _I, [_P, _PP]), ("am_value_counts_ex", _I, [_P, _I, _PP]),
 ]:
@@ -582,6 +594,133 @@ class Server:
 
     def __del__(self):
         self.close()
+
+
+class _ArrowArrayStream(ctypes.Structure):
+    _fields_ = [("get_schema", _P), ("get_next", _P), ("get_last_error", _P), ("release", _P), ("private_data", _P)]
+
+
+def _stream_error(rc=None):
+    raise ArrowMetalError((_lib.am_stream_last_error() or b"unknown error").decode())
+
+
+def _as_reader(source):
+    if isinstance(source, pa.RecordBatchReader):
+        return source
+    if isinstance(source, pa.Table):
+        return source.to_reader()
+    if isinstance(source, pa.RecordBatch):
+        return pa.Table.from_batches([source]).to_reader()
+    if hasattr(source, "to_reader"):
+        return source.to_reader()
+    if hasattr(source, "__arrow_c_stream__"):
+        return pa.RecordBatchReader.from_stream(source)
+    raise ArrowMetalError(f"cannot stream record batches from {type(source).__name__}")
+
+
+def _sort_keys(by):
+    """Column names and descending flags from a name, a (name, descending) pair or a list of either."""
+    if isinstance(by, (str, tuple)):
+        by = [by]
+    names, desc = [], []
+    for k in by:
+        if isinstance(k, str):
+            names.append(k)
+            desc.append(False)
+        else:
+            name, d = k
+            names.append(name)
+            desc.append(d in (True, "descending") if not isinstance(d, bool) else d)
+    return names, desc
+
+
+class Stream:
+    """A source of Arrow record batches larger than HBM, consumed by one terminal call (`sort`,
+    `sort_to_ipc`). Anything that speaks the Arrow C Stream Interface: a pyarrow RecordBatchReader,
+    Table, dataset or scanner. `prefetch` batches are read ahead on a library thread."""
+
+    def __init__(self, source, prefetch=3):
+        reader = _as_reader(source)
+        c = _ArrowArrayStream()
+        reader._export_to_c(ctypes.addressof(c))
+        h = _lib.am_stream_from_c_stream(ctypes.addressof(c), int(prefetch))
+        if not h:
+            if c.release:
+                ctypes.CFUNCTYPE(None, _P)(c.release)(ctypes.addressof(c))
+            _stream_error()
+        self._h = h
+        self._consumed = False
+        self.stats = None
+        self.rows_out = None
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _lib is not None:
+            _lib.am_stream_release(h)
+            self._h = None
+
+    def select(self, names):
+        """Keep these columns, in this order, in the output."""
+        arr = (ctypes.c_char_p * len(names))(*[n.encode() for n in names])
+        if _lib.am_stream_select(self._h, arr, len(names)) != 0:
+            _stream_error()
+        return self
+
+    def _sort(self, by, limit, scratch, path, null_placement, float_order):
+        if self._consumed:
+            raise ArrowMetalError("this stream has already been consumed; open a new one")
+        self._consumed = True
+        names, desc = _sort_keys(by)
+        k = len(names)
+        places = _per_key(null_placement, k, "null_placement")
+        orders = _per_key(float_order, k, "float_order")
+        cn = (ctypes.c_char_p * k)(*[n.encode() for n in names])
+        cd = (ctypes.c_int * k)(*[1 if d else 0 for d in desc])
+        cp = (ctypes.c_int * k)(*[_index_of(NULL_PLACEMENT, p, "null_placement") for p in places])
+        cf = (ctypes.c_int * k)(*[_index_of(FLOAT_ORDERS, f, "float_order") for f in orders])
+        out = _P()
+        rc = _lib.am_stream_sort_ex(self._h, cn, cd, cp, cf, k, int(limit),
+                                    None if scratch is None else str(scratch).encode(),
+                                    None if path is None else str(path).encode(), ctypes.byref(out))
+        if rc != 0:
+            _stream_error()
+        try:
+            I64, D = ctypes.c_int64, ctypes.c_double
+            b, r, by_, wall, read, gpu, merge, overlap = I64(), I64(), I64(), D(), D(), D(), D(), D()
+            _lib.am_stream_result_stats(out, *[ctypes.byref(x) for x in (b, r, by_, wall, read, gpu, merge, overlap)])
+            rs, ms = D(), D()
+            _lib.am_stream_result_stalls(out, ctypes.byref(rs), ctypes.byref(ms))
+            self.rows_out = _lib.am_stream_result_rows_out(out)
+            self.stats = {"batches": b.value, "rows": r.value, "bytes_read": by_.value, "wall_s": wall.value,
+                          "read_s": read.value, "gpu_s": gpu.value, "merge_s": merge.value,
+                          "overlap": overlap.value, "read_stall_s": rs.value, "merge_stall_s": ms.value,
+                          "rows_out": self.rows_out}
+            n = _lib.am_stream_result_column_count(out)
+            cols, col_names = [], []
+            for i in range(n):
+                col_names.append(_lib.am_stream_result_column_name(out, i).decode())
+                h = _P()
+                _check(_lib.am_stream_result_column(out, i, ctypes.byref(h)))
+                cols.append(MetalArray(h).to_arrow())
+            return pa.table(cols, names=col_names) if n > 0 else None
+        finally:
+            _lib.am_stream_result_release(out)
+
+    def sort(self, by, limit=0, scratch=None, null_placement="at_end", float_order="ieee"):
+        """External sort, collected into a pyarrow.Table: sorted runs in HBM (spilled under `scratch`
+        when the stream does not fit one), merged on the GPU. `by` is a column name, a (name,
+        descending) pair or a list of either; `limit` 0 keeps every row. Ties keep stream order."""
+        return self._sort(by, limit, scratch, None, null_placement, float_order)
+
+    def sort_to_ipc(self, by, path, scratch=None, null_placement="at_end", float_order="ieee"):
+        """External sort written to `path` as an Arrow IPC stream; returns the run's statistics."""
+        self._sort(by, 0, scratch, path, null_placement, float_order)
+        return self.stats
+
+
+def scan_arrow(source, prefetch=3):
+    """A `Stream` over anything that speaks the Arrow C Stream Interface."""
+    return Stream(source, prefetch)
 
 
 def explain_plan(plan, sources):

@@ -379,6 +379,29 @@ am_array* slice_of(am_array* a, int64_t offset, int64_t length) {
 
 }  // namespace
 
+namespace am {
+// A host array (or a dictionary array) copied into HBM on stream `s`; the caller keeps the struct and
+// releases it (the copies are complete, or staged, when this returns).
+am_array* import_copy(const ArrowSchema* schema, const ArrowArray* array, cudaStream_t s) {
+  const int pt = parse_format(schema->format);
+  check_array_struct(schema, array);
+  am_array* a = new_array(pt, schema->format, array->length);
+  try {
+    import_host(a, array, s);
+    if (schema->dictionary) {
+      am_array* d = new_array(parse_format(schema->dictionary->format), schema->dictionary->format,
+                              array->dictionary->length);
+      a->dictionary = d;
+      import_host(d, array->dictionary, s);
+    }
+  } catch (...) {
+    am::release(a);
+    throw;
+  }
+  return a;
+}
+}  // namespace am
+
 extern "C" {
 
 const char* am_version(void) { return "0.6.1"; }

@@ -297,6 +297,10 @@ am_array* dictionary_key_column(const SortKey& k, cudaStream_t s);
 void argsort_any(const std::vector<SortKey>& keys, int64_t n, void* out, int width, cudaStream_t s,
                  am_sort_stats* stats);
 
+// Copies a host Arrow array (a dictionary array with its dictionary) into HBM on stream `s`; the caller
+// keeps and releases the struct.
+am_array* import_copy(const ArrowSchema* schema, const ArrowArray* array, cudaStream_t s);
+
 // String and binary columns: the derived unsigned keys that sort like the strings (big-endian 8-byte
 // chunks, then the length; the first carries the nulls), and the take of one string column.
 // A string key is the tuple (chunk 0, ..., chunk m-1, length) with m = string_chunk_count; a call

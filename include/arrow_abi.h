@@ -1,7 +1,7 @@
-/* Apache Arrow C Data Interface and C Device Data Interface.
+/* Apache Arrow C Data Interface, C Stream Interface and C Device Data Interface.
  *
  * The struct layouts are fixed by the Arrow specification
- * (https://arrow.apache.org/docs/format/CDataInterface.html and
+ * (https://arrow.apache.org/docs/format/CDataInterface.html, CStreamInterface.html and
  *  https://arrow.apache.org/docs/format/CDeviceDataInterface.html); every producer and consumer of
  * the interface, pyarrow and arrow-rs included, must agree on them byte for byte. The guard macros
  * are the specification's own, so this header coexists with any other copy of the definitions. */
@@ -47,6 +47,21 @@ struct ArrowArray {
 };
 
 #endif /* ARROW_C_DATA_INTERFACE */
+
+#ifndef ARROW_C_STREAM_INTERFACE
+#define ARROW_C_STREAM_INTERFACE
+
+/* The Arrow C Stream Interface (https://arrow.apache.org/docs/format/CStreamInterface.html): a
+ * producer of record batches, each a struct array whose children are the columns. */
+struct ArrowArrayStream {
+  int (*get_schema)(struct ArrowArrayStream*, struct ArrowSchema* out);
+  int (*get_next)(struct ArrowArrayStream*, struct ArrowArray* out);
+  const char* (*get_last_error)(struct ArrowArrayStream*);
+  void (*release)(struct ArrowArrayStream*);
+  void* private_data;
+};
+
+#endif /* ARROW_C_STREAM_INTERFACE */
 
 #ifndef ARROW_C_DEVICE_DATA_INTERFACE
 #define ARROW_C_DEVICE_DATA_INTERFACE

@@ -160,6 +160,53 @@ void        am_plan_result_release(am_plan_result* r);                          
 int  am_router_set_mode(int mode);
 int  am_router_get_mode(void);
 
+/* ---- out-of-core sort of a record-batch stream ------------------------------------------------ */
+/* A stream handle wraps a producer of Arrow record batches (the Arrow C Stream Interface: pyarrow's
+ * RecordBatchReader and dataset scanners, Polars, DuckDB) and is consumed by one terminal call.
+ * Errors: a NULL handle or a non-zero return, with the message in am_stream_last_error().
+ * include/arrowmetal.h:1515-1547 */
+typedef struct am_stream am_stream;                               /* :1528 */
+typedef struct am_stream_result am_stream_result;                 /* :1529 */
+const char* am_stream_last_error(void);                           /* :1538 */
+/* Takes ownership of `in` (its release is NULL afterwards); prefetch_depth batches are read ahead on
+ * a reader thread (0: read on the calling thread). include/arrowmetal.h:1546 */
+am_stream* am_stream_from_c_stream(struct ArrowArrayStream* in, int prefetch_depth);
+/* Arrow IPC files are not read by this build: returns NULL with the reason in am_stream_last_error
+ * (open the file with pyarrow and pass its RecordBatchReader). include/arrowmetal.h:1544 */
+am_stream* am_stream_open_ipc(const char* path, int prefetch_depth, int readers);
+void       am_stream_release(am_stream* s);                       /* :1547 */
+/* Keeps the named columns, in this order, in the terminal's output. include/arrowmetal.h:1551 */
+int am_stream_select(am_stream* s, const char** names, int64_t n);
+/* External sort: batches gather in HBM up to a run budget (a sixth of the free device memory, or
+ * ARROWMETAL_STREAM_RUN_BYTES), each run is sorted on the GPU and, when more than one is needed,
+ * spilled under scratch_dir (NULL: a new directory under the system's temporary directory) and
+ * merged on the GPU in windows. The output is in full sort order, ties in stream order (stable).
+ * limit 0 means all rows. sink_path NULL collects the rows into the result's columns; otherwise they
+ * are written to that path as an Arrow IPC stream. include/arrowmetal.h:1576-1584 */
+int am_stream_sort(am_stream* s, const char** columns, const int* descending, int64_t n_keys,
+                   int64_t limit, const char* scratch_dir, const char* sink_path, am_stream_result** out);
+int am_stream_sort_ex(am_stream* s, const char** columns, const int* descending,
+                      const int* null_placement, const int* float_order, int64_t n_keys,
+                      int64_t limit, const char* scratch_dir, const char* sink_path,
+                      am_stream_result** out);
+/* Results. A sort has columns and no scalars. include/arrowmetal.h:1597-1611 */
+int64_t     am_stream_result_column_count(am_stream_result* r);
+const char* am_stream_result_column_name(am_stream_result* r, int64_t i);
+int         am_stream_result_column(am_stream_result* r, int64_t i, am_array** out);
+int64_t     am_stream_result_scalar_count(am_stream_result* r);
+const char* am_stream_result_scalar_name(am_stream_result* r, int64_t i);
+int         am_stream_result_scalar(am_stream_result* r, int64_t i, int64_t* out_i64, double* out_f64,
+                                    int* out_kind, int* is_null);
+int64_t     am_stream_result_rows_out(am_stream_result* r);
+/* batches and rows read, bytes imported, wall time and the time each stage was busy (read: the
+ * producer's get_next; gpu: the run sorts; merge: the merge windows); overlap = (read + gpu + merge)
+ * / wall. */
+int         am_stream_result_stats(am_stream_result* r, int64_t* batches, int64_t* rows,
+                                   int64_t* bytes_read, double* wall_s, double* read_s,
+                                   double* gpu_s, double* merge_s, double* overlap);
+int         am_stream_result_stalls(am_stream_result* r, double* read_stall_s, double* merge_stall_s);
+void        am_stream_result_release(am_stream_result* r);
+
 /* ================================================================================================
  * Additions with no counterpart in the reference header. They stand beside the drop-in surface and
  * change nothing in it.

@@ -149,3 +149,20 @@ def _has_gpu():
         return torch.cuda.is_available()
     except Exception:
         return False
+
+
+def test_stream_handles_without_a_device():
+    """A record-batch stream is taken and its columns selected on the host; the sort itself needs the
+    device and fails loudly without one; IPC files are refused with the way round."""
+    import pyarrow as pa
+    import arrowmetal_b200 as am
+    s = am.scan_arrow(pa.table({"a": [3, 1, 2], "s": ["x", "y", "z"]}))
+    s.select(["s", "a"])
+    with pytest.raises(am.ArrowMetalError, match="no column named"):
+        s.select(["nope"])
+    with pytest.raises(am.ArrowMetalError, match="CUDA|device"):
+        s.sort("a")
+    with pytest.raises(am.ArrowMetalError, match="consumed"):
+        s.sort("a")
+    assert am._lib.am_stream_open_ipc(b"/nonexistent.arrow", 3, 1) is None
+    assert b"RecordBatchReader" in am._lib.am_stream_last_error()
