@@ -461,6 +461,44 @@ def run_consumers(args, am, torch, stream, local):
         "consumer_ms": ms, "clocks": clocks.summary()}))
 
 
+def run_external(args, am, torch, local):
+    """--workload external: the out-of-core sort of a record-batch stream (am_stream_sort_ex) over
+    100,000,000 rows in host memory (int64 key in [0, 2^40) with 10% nulls, float64 and int32 payload;
+    1M-row batches), collected back into host memory: once as one run in HBM, once with a 256 MiB run
+    budget, which spills 8+ sorted runs to the scratch directory and merges them on the GPU."""
+    import pyarrow as pa
+    n = 100_000_000
+    key, valid, p1, p2 = make_table(n, seed=SEED + 10)
+    table = pa.table({"key": pa.array(key, mask=~valid), "p1": pa.array(p1), "p2": pa.array(p2)})
+    batches = table.to_batches(max_chunksize=1_000_000)
+    res = {}
+    with ClockSampler(local) as clocks:
+        for name, budget in (("in_hbm", None), ("spilled_256MiB_runs", 256 << 20)):
+            if budget:
+                os.environ["ARROWMETAL_STREAM_RUN_BYTES"] = str(budget)
+            try:
+                with tempfile.TemporaryDirectory() as scratch:
+                    t0 = time.perf_counter()
+                    s = am.scan_arrow(pa.RecordBatchReader.from_batches(table.schema, batches))
+                    out = s.sort("key", scratch=scratch)
+                    wall = time.perf_counter() - t0
+            finally:
+                os.environ.pop("ARROWMETAL_STREAM_RUN_BYTES", None)
+            assert out.num_rows == n
+            res[name] = {"wall_s": wall, "rows_per_s": n / wall,
+                         **{k: s.stats[k] for k in ("read_s", "gpu_s", "merge_s", "bytes_read")}}
+            del out
+    head = res["in_hbm"]
+    print(json.dumps({
+        "metric": METRIC, "value": head["rows_per_s"], "unit": "rows/s", "n_gpus": 1, "steps": 1, "warmup": 0,
+        "ms_per_step": head["wall_s"] * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "int64", "data": "synthetic",
+        "config": {"workload": "external sort of a 100,000,000-row record-batch stream from host memory "
+                               "(am_stream_sort_ex, int64 key with 10% nulls + float64 + int32), collected to host",
+                   "rows": n, "batch_rows": 1_000_000},
+        "external": res, "clocks": clocks.summary()}))
+
+
 def make_strings(n, seed=SEED + 8):
     """n utf8 strings of 0-24 lowercase letters (uniform length), 5% nulls, built from numpy buffers."""
     import pyarrow as pa
@@ -702,11 +740,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="order_by",
                     choices=["order_by", "segmented", "serving", "full_range", "multikey", "topk", "strings",
-                             "consumers"],
+                             "consumers", "external"],
                     help="order_by: the 50M-row ORDER BY (the headline); segmented: 2,048 arrays in one call; "
                          "serving: the served request stream; full_range: 1M full-range int64 keys; multikey: "
                          "the 50M-row two-key sort; topk: ORDER BY ... LIMIT k by radix selection; strings: ORDER BY a utf8 key; "
-                         "consumers: partition_nth, rank, unique and value_counts on 50M rows")
+                         "consumers: partition_nth, rank, unique and value_counts on 50M rows; "
+                         "external: the out-of-core sort of a 100M-row batch stream")
     ap.add_argument("--rate", type=float, default=200.0, help="serving: requests per second")
     ap.add_argument("--serve-seconds", type=float, default=30.0, help="serving: length of the open-loop stream")
     ap.add_argument("--sat-requests", type=int, default=400, help="serving: requests of the saturation run")
@@ -751,6 +790,10 @@ def main():
         am.set_stream(stream.cuda_stream)
         if rank == 0:
             run_topk(args, am, torch, stream, local)
+        return
+    if args.workload == "external":
+        if rank == 0:
+            run_external(args, am, torch, local)
         return
     if args.workload == "consumers":
         stream = torch.cuda.Stream()
