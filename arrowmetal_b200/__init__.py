@@ -613,6 +613,8 @@ def _as_reader(source):
         return pa.Table.from_batches([source]).to_reader()
     if hasattr(source, "to_reader"):
         return source.to_reader()
+    if hasattr(source, "scanner"):                  # a pyarrow dataset
+        return source.scanner().to_reader()
     if hasattr(source, "__arrow_c_stream__"):
         return pa.RecordBatchReader.from_stream(source)
     raise ArrowMetalError(f"cannot stream record batches from {type(source).__name__}")
