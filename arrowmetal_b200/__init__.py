@@ -132,7 +132,7 @@ for _name, _res, _args in [
     ("am_rank", _I, [_P, _I, _PP]), ("am_window", _I, [_P, _I, _I64, _I64, _P, _PP]),
     ("am_stream_last_error", ctypes.c_char_p, []), ("am_stream_from_c_stream", _P, [_P, _I]),
     ("am_stream_open_ipc", _P, [ctypes.c_char_p, _I, _I]), ("am_stream_release", None, [_P]),
-    ("am_stream_select", _I, [_P, ctypes.POINTER(ctypes.c_char_p), _I64]),
+    ("am_stream_select", _I, [_P, ctypes.POINTER(ctypes.c_char_p), _I64]), ("am_stream_export_c", _I, [_P, _P]),
     ("am_stream_sort_ex", _I, [_P, ctypes.POINTER(ctypes.c_char_p), _IP, _IP, _IP, _I64, _I64, ctypes.c_char_p,
                                ctypes.c_char_p, _PP]),
     ("am_stream_sort", _I, [_P, ctypes.POINTER(ctypes.c_char_p), _IP, _I64, _I64, ctypes.c_char_p, ctypes.c_char_p,
@@ -641,16 +641,17 @@ class Stream:
     `sort_to_ipc`). Anything that speaks the Arrow C Stream Interface: a pyarrow RecordBatchReader,
     Table, dataset or scanner. `prefetch` batches are read ahead on a library thread."""
 
-    def __init__(self, source, prefetch=3):
-        reader = _as_reader(source)
-        c = _ArrowArrayStream()
-        reader._export_to_c(ctypes.addressof(c))
-        h = _lib.am_stream_from_c_stream(ctypes.addressof(c), int(prefetch))
-        if not h:
-            if c.release:
-                ctypes.CFUNCTYPE(None, _P)(c.release)(ctypes.addressof(c))
-            _stream_error()
-        self._h = h
+    def __init__(self, source, prefetch=3, _handle=None):
+        if _handle is None:
+            reader = _as_reader(source)
+            c = _ArrowArrayStream()
+            reader._export_to_c(ctypes.addressof(c))
+            _handle = _lib.am_stream_from_c_stream(ctypes.addressof(c), int(prefetch))
+            if not _handle:
+                if c.release:
+                    ctypes.CFUNCTYPE(None, _P)(c.release)(ctypes.addressof(c))
+                _stream_error()
+        self._h = _handle
         self._consumed = False
         self.stats = None
         self.rows_out = None
@@ -714,6 +715,16 @@ class Stream:
         descending) pair or a list of either; `limit` 0 keeps every row. Ties keep stream order."""
         return self._sort(by, limit, scratch, None, null_placement, float_order)
 
+    def to_reader(self):
+        """The stream's batches (the selected columns) as a pyarrow.RecordBatchReader; consumes the stream."""
+        if self._consumed:
+            raise ArrowMetalError("this stream has already been consumed; open a new one")
+        self._consumed = True
+        c = _ArrowArrayStream()
+        if _lib.am_stream_export_c(self._h, ctypes.addressof(c)) != 0:
+            _stream_error()
+        return pa.RecordBatchReader._import_from_c(ctypes.addressof(c))
+
     def sort_to_ipc(self, by, path, scratch=None, null_placement="at_end", float_order="ieee"):
         """External sort written to `path` as an Arrow IPC stream; returns the run's statistics."""
         self._sort(by, 0, scratch, path, null_placement, float_order)
@@ -723,6 +734,14 @@ class Stream:
 def scan_arrow(source, prefetch=3):
     """A `Stream` over anything that speaks the Arrow C Stream Interface."""
     return Stream(source, prefetch)
+
+
+def scan_ipc(path, prefetch=3, readers=1):
+    """A `Stream` over an Arrow IPC file (file or stream format) or a directory of them, memory-mapped."""
+    h = _lib.am_stream_open_ipc(str(path).encode(), int(prefetch), int(readers))
+    if not h:
+        _stream_error()
+    return Stream(None, _handle=h)
 
 
 def explain_plan(plan, sources):

@@ -17,6 +17,7 @@
 // cursor advances by its rows in that prefix (a prefix of its block, the sort being stable), and the
 // run that attains the bound has emitted its whole block, so every window makes progress.
 #include <cuda_runtime.h>
+#include <dirent.h>
 #include <fcntl.h>
 #include <sys/mman.h>
 #include <sys/stat.h>
@@ -684,6 +685,436 @@ struct IpcWriter {
   }
 };
 
+// ---- IPC input
+
+// Reading side of the flatbuffer format, bounds-checked against the message.
+struct FlatReader {
+  const uint8_t* p;
+  size_t n;
+  void need(size_t at, size_t len) const {
+    if (at > n || len > n - at) throw invalid("a malformed Arrow IPC message");
+  }
+  template <typename T>
+  T get(size_t at) const {
+    need(at, sizeof(T));
+    T v;
+    std::memcpy(&v, p + at, sizeof(T));
+    return v;
+  }
+  size_t deref(size_t at) const { return at + get<uint32_t>(at); }
+  size_t root() const { return deref(0); }
+  // The address of field `slot` of the table at `t`, or 0 when absent.
+  size_t field(size_t t, int slot) const {
+    const size_t vt = size_t(int64_t(t) - int64_t(get<int32_t>(t)));
+    const uint16_t vsize = get<uint16_t>(vt);
+    const size_t at = 4 + 2 * size_t(slot);
+    if (at + 2 > vsize) return 0;
+    const uint16_t off = get<uint16_t>(vt + at);
+    return off ? t + off : 0;
+  }
+  template <typename T>
+  T scalar(size_t t, int slot, T dflt) const {
+    const size_t a = field(t, slot);
+    return a ? get<T>(a) : dflt;
+  }
+  size_t table(size_t t, int slot) const {
+    const size_t a = field(t, slot);
+    return a ? deref(a) : 0;
+  }
+  std::string string(size_t t, int slot) const {
+    const size_t a = table(t, slot);
+    if (!a) return "";
+    const uint32_t len = get<uint32_t>(a);
+    need(a + 4, len);
+    return std::string(reinterpret_cast<const char*>(p + a + 4), len);
+  }
+  // (element address, count) of a vector field.
+  std::pair<size_t, uint32_t> vec(size_t t, int slot) const {
+    const size_t a = table(t, slot);
+    if (!a) return {0, 0};
+    return {a + 4, get<uint32_t>(a)};
+  }
+};
+
+// The C Data format string of an IPC Field's type.
+std::string ipc_format(const FlatReader& r, size_t field) {
+  const uint8_t code = r.scalar<uint8_t>(field, 2, 0);
+  const size_t t = r.table(field, 3);
+  static const char* units[] = {"s", "m", "u", "n"};
+  auto unit = [&](int slot, int16_t dflt) {
+    const int16_t u = t ? r.scalar<int16_t>(t, slot, dflt) : dflt;
+    if (u < 0 || u > 3) throw invalid("an IPC time unit out of range");
+    return std::string(units[u]);
+  };
+  switch (code) {
+    case 2: {
+      const int32_t bits = t ? r.scalar<int32_t>(t, 0, 0) : 0;
+      const bool sgn = t ? r.scalar<uint8_t>(t, 1, 0) != 0 : false;
+      if (bits == 8) return sgn ? "c" : "C";
+      if (bits == 16) return sgn ? "s" : "S";
+      if (bits == 32) return sgn ? "i" : "I";
+      if (bits == 64) return sgn ? "l" : "L";
+      break;
+    }
+    case 3: {
+      const int16_t prec = t ? r.scalar<int16_t>(t, 0, 0) : 0;
+      return prec == 0 ? "e" : prec == 1 ? "f" : "g";
+    }
+    case 4: return "z";
+    case 5: return "u";
+    case 6: return "b";
+    case 8: return (t ? r.scalar<int16_t>(t, 0, 1) : 1) == 0 ? "tdD" : "tdm";
+    case 9: return "tt" + unit(0, 1);
+    case 10: return "ts" + unit(0, 0) + ":" + (t ? r.string(t, 1) : "");
+    case 18: return "tD" + unit(0, 1);
+    case 19: return "Z";
+    case 20: return "U";
+    default: break;
+  }
+  throw unsupported("an Arrow IPC column of type code " + std::to_string(code) +
+                    " (primitive, boolean, temporal, string and binary columns are read)");
+}
+
+struct IpcMap {
+  const uint8_t* data = nullptr;
+  size_t size = 0;
+  ~IpcMap() {
+    if (data) munmap(const_cast<uint8_t*>(data), size);
+  }
+};
+
+// One record batch handed out by the IPC source: the struct array and its children, pointing into the
+// mapped file (held until the batch is released).
+struct IpcBatch {
+  std::shared_ptr<IpcMap> map;
+  std::vector<ArrowArray> children;
+  std::vector<ArrowArray*> child_ptrs;
+  std::vector<std::vector<const void*>> buffers;
+  const void* top_buffers[1] = {nullptr};
+};
+
+void release_ipc_batch(ArrowArray* a) {
+  if (!a || !a->release) return;
+  delete static_cast<IpcBatch*>(a->private_data);
+  a->release = nullptr;
+}
+
+struct IpcSource {
+  std::vector<std::string> files;
+  size_t file = 0;
+  std::shared_ptr<IpcMap> map;
+  size_t pos = 0, end = 0;
+  bool have_schema = false;
+  std::vector<std::string> names, formats;
+  std::vector<int> nbuf;          // buffers per column
+  std::string error;
+  std::vector<std::string> owned_strings;   // schema strings handed out
+
+  // Maps the next file, reads its schema (the first file's fixes the stream's; later ones must match).
+  bool open_next() {
+    map.reset();
+    while (file < files.size()) {
+      const std::string& path = files[file++];
+      const int fd = ::open(path.c_str(), O_RDONLY);
+      if (fd < 0) throw Error("cannot open " + path);
+      struct stat stt;
+      if (fstat(fd, &stt) != 0) {
+        close(fd);
+        throw Error("cannot stat " + path);
+      }
+      auto m = std::make_shared<IpcMap>();
+      m->size = size_t(stt.st_size);
+      if (m->size == 0) {
+        close(fd);
+        continue;
+      }
+      void* d = mmap(nullptr, m->size, PROT_READ, MAP_PRIVATE, fd, 0);
+      close(fd);
+      if (d == MAP_FAILED) throw Error("cannot map " + path);
+      m->data = static_cast<const uint8_t*>(d);
+      map = m;
+      pos = 0;
+      end = m->size;
+      if (m->size >= 8 && std::memcmp(m->data, "ARROW1", 6) == 0) {
+        // The file format: magic, the stream's messages, the footer, its length and the magic again.
+        pos = 8;
+        if (m->size >= 18) {
+          int32_t flen = 0;
+          std::memcpy(&flen, m->data + m->size - 10, 4);
+          if (flen > 0 && size_t(flen) + 18 <= m->size) end = m->size - 10 - size_t(flen);
+        }
+      }
+      // The schema message.
+      size_t body = 0, body_len = 0;
+      FlatReader r{};
+      if (!message(r, body, body_len)) continue;
+      const size_t msg = r.root();
+      if (r.scalar<uint8_t>(msg, 1, 0) != 1) throw invalid(path + ": an Arrow IPC stream starts with its schema");
+      schema_of(r, r.table(msg, 2), path);
+      return true;
+    }
+    return false;
+  }
+  // The next message of the current file: its flatbuffer, and its body's position and length.
+  bool message(FlatReader& r, size_t& body, size_t& body_len) {
+    for (;;) {
+      if (pos + 4 > end) return false;
+      int32_t len = 0;
+      std::memcpy(&len, map->data + pos, 4);
+      size_t at = pos + 4;
+      if (uint32_t(len) == 0xFFFFFFFFu) {
+        if (at + 4 > end) return false;
+        std::memcpy(&len, map->data + at, 4);
+        at += 4;
+      }
+      if (len == 0) return false;                       // end of stream
+      if (len < 0 || at + size_t(len) > end) throw invalid("a truncated Arrow IPC message");
+      r = FlatReader{map->data + at, size_t(len)};
+      const size_t msg = r.root();
+      const int64_t blen = r.scalar<int64_t>(msg, 3, 0);
+      body = at + size_t(len);
+      if (blen < 0 || body + size_t(blen) > map->size) throw invalid("a truncated Arrow IPC message body");
+      body_len = size_t(blen);
+      pos = body + body_len;
+      return true;
+    }
+  }
+  void schema_of(const FlatReader& r, size_t sch, const std::string& path) {
+    if (!sch) throw invalid(path + ": an Arrow IPC schema message without a schema");
+    const auto fv = r.vec(sch, 1);
+    std::vector<std::string> nm, fm;
+    std::vector<int> nb;
+    for (uint32_t i = 0; i < fv.second; i++) {
+      const size_t f = r.deref(fv.first + 4 * size_t(i));
+      if (r.field(f, 4)) throw unsupported("dictionary-encoded columns in an Arrow IPC file");
+      if (r.vec(f, 5).second != 0) throw unsupported("nested columns in an Arrow IPC file");
+      nm.push_back(r.string(f, 0));
+      fm.push_back(ipc_format(r, f));
+      nb.push_back(pt_var(parse_format(fm.back().c_str())) ? 3 : 2);
+    }
+    if (have_schema) {
+      if (nm != names || fm != formats) throw invalid(path + ": its schema differs from the first file's");
+      return;
+    }
+    names = nm;
+    formats = fm;
+    nbuf = nb;
+    have_schema = true;
+  }
+  // The next record batch, or false at the end of the last file.
+  bool next(ArrowArray* out) {
+    for (;;) {
+      if (!map && !open_next()) return false;
+      FlatReader r{};
+      size_t body = 0, body_len = 0;
+      if (!message(r, body, body_len)) {
+        map.reset();
+        continue;
+      }
+      const size_t msg = r.root();
+      const uint8_t type = r.scalar<uint8_t>(msg, 1, 0);
+      if (type == 2) throw unsupported("dictionary batches in an Arrow IPC file");
+      if (type != 3) continue;
+      const size_t rb = r.table(msg, 2);
+      if (!rb) throw invalid("a record batch message without its batch");
+      if (r.field(rb, 3)) throw unsupported("compressed Arrow IPC bodies (write them uncompressed)");
+      const int64_t length = r.scalar<int64_t>(rb, 0, 0);
+      const auto nodes = r.vec(rb, 1);
+      const auto bufs = r.vec(rb, 2);
+      if (nodes.second != names.size()) throw invalid("a record batch with the wrong number of columns");
+      auto* b = new IpcBatch();
+      b->map = map;
+      b->children.resize(names.size());
+      b->buffers.resize(names.size());
+      size_t bi = 0;
+      try {
+        for (size_t c = 0; c < names.size(); c++) {
+          ArrowArray& a = b->children[c];
+          a = ArrowArray{};
+          a.length = r.get<int64_t>(nodes.first + 16 * c);
+          a.null_count = r.get<int64_t>(nodes.first + 16 * c + 8);
+          a.n_buffers = nbuf[c];
+          for (int k = 0; k < nbuf[c]; k++, bi++) {
+            if (bi >= bufs.second) throw invalid("a record batch with too few buffers");
+            const int64_t off = r.get<int64_t>(bufs.first + 16 * bi);
+            const int64_t len = r.get<int64_t>(bufs.first + 16 * bi + 8);
+            if (off < 0 || len < 0 || size_t(off + len) > body_len) throw invalid("an IPC buffer outside its body");
+            b->buffers[c].push_back(len > 0 ? map->data + body + size_t(off) : nullptr);
+          }
+          a.buffers = b->buffers[c].data();
+          a.release = [](ArrowArray* x) { x->release = nullptr; };   // the parent owns the memory
+          b->child_ptrs.push_back(&a);
+        }
+      } catch (...) {
+        delete b;
+        throw;
+      }
+      *out = ArrowArray{};
+      out->length = length;
+      out->null_count = 0;
+      out->n_buffers = 1;
+      out->buffers = b->top_buffers;
+      out->n_children = int64_t(names.size());
+      out->children = b->child_ptrs.data();
+      out->release = release_ipc_batch;
+      out->private_data = b;
+      return true;
+    }
+  }
+};
+
+// The IPC source as an Arrow C stream, so the sort reads it like any other producer.
+struct IpcStreamState {
+  IpcSource src;
+};
+int ipc_get_schema(ArrowArrayStream* st, ArrowSchema* out) {
+  auto* s = static_cast<IpcStreamState*>(st->private_data);
+  struct Hold {
+    std::vector<ArrowSchema> kids;
+    std::vector<ArrowSchema*> ptrs;
+    std::vector<std::string> names, formats;
+  };
+  auto* h = new Hold();
+  h->names = s->src.names;
+  h->formats = s->src.formats;
+  h->kids.resize(h->names.size());
+  for (size_t i = 0; i < h->names.size(); i++) {
+    ArrowSchema& k = h->kids[i];
+    k = ArrowSchema{};
+    k.format = h->formats[i].c_str();
+    k.name = h->names[i].c_str();
+    k.flags = ARROW_FLAG_NULLABLE;
+    k.release = [](ArrowSchema* x) { x->release = nullptr; };
+    h->ptrs.push_back(&k);
+  }
+  *out = ArrowSchema{};
+  out->format = "+s";
+  out->name = "";
+  out->n_children = int64_t(h->names.size());
+  out->children = h->ptrs.data();
+  out->private_data = h;
+  out->release = [](ArrowSchema* x) {
+    delete static_cast<Hold*>(x->private_data);
+    x->release = nullptr;
+  };
+  return 0;
+}
+int ipc_get_next(ArrowArrayStream* st, ArrowArray* out) {
+  auto* s = static_cast<IpcStreamState*>(st->private_data);
+  try {
+    if (!s->src.next(out)) *out = ArrowArray{};
+    return 0;
+  } catch (const std::exception& e) {
+    s->src.error = e.what();
+    return 5;   // EIO
+  }
+}
+const char* ipc_last_error(ArrowArrayStream* st) {
+  return static_cast<IpcStreamState*>(st->private_data)->src.error.c_str();
+}
+void ipc_release(ArrowArrayStream* st) {
+  delete static_cast<IpcStreamState*>(st->private_data);
+  st->release = nullptr;
+}
+
+// ---- projection of a C stream (am_stream_export_c with selected columns)
+
+// The selected children are moved out of each schema / batch the inner stream gives (their structs
+// copied, the originals marked released), so the inner parent releases only what was not taken.
+struct ProjectState {
+  ArrowArrayStream inner{};
+  std::vector<int> select;
+  std::string error;
+};
+struct ProjectHold {
+  std::vector<ArrowSchema> schemas;
+  std::vector<ArrowArray> arrays;
+  std::vector<ArrowSchema*> sptrs;
+  std::vector<ArrowArray*> aptrs;
+  ArrowSchema parent_schema{};
+  ArrowArray parent_array{};
+  const void* top_buffers[1] = {nullptr};
+};
+int project_get_schema(ArrowArrayStream* st, ArrowSchema* out) {
+  auto* ps = static_cast<ProjectState*>(st->private_data);
+  auto* h = new ProjectHold();
+  int rc = ps->inner.get_schema(&ps->inner, &h->parent_schema);
+  if (rc != 0) {
+    delete h;
+    return rc;
+  }
+  for (int ci : ps->select) {
+    ArrowSchema* c = h->parent_schema.children[ci];
+    h->schemas.push_back(*c);
+    c->release = nullptr;
+  }
+  for (ArrowSchema& c : h->schemas) h->sptrs.push_back(&c);
+  *out = ArrowSchema{};
+  out->format = "+s";
+  out->name = "";
+  out->n_children = int64_t(h->sptrs.size());
+  out->children = h->sptrs.data();
+  out->private_data = h;
+  out->release = [](ArrowSchema* x) {
+    auto* hh = static_cast<ProjectHold*>(x->private_data);
+    for (ArrowSchema& c : hh->schemas)
+      if (c.release) c.release(&c);
+    if (hh->parent_schema.release) hh->parent_schema.release(&hh->parent_schema);
+    delete hh;
+    x->release = nullptr;
+  };
+  return 0;
+}
+int project_get_next(ArrowArrayStream* st, ArrowArray* out) {
+  auto* ps = static_cast<ProjectState*>(st->private_data);
+  auto* h = new ProjectHold();
+  int rc = ps->inner.get_next(&ps->inner, &h->parent_array);
+  if (rc != 0 || !h->parent_array.release) {
+    delete h;
+    *out = ArrowArray{};
+    return rc;
+  }
+  ArrowArray& p = h->parent_array;
+  for (int ci : ps->select) {
+    ArrowArray* c = p.children[ci];
+    h->arrays.push_back(*c);
+    c->release = nullptr;
+    if (p.offset != 0) {
+      h->arrays.back().offset += p.offset;
+      h->arrays.back().length = p.length;
+      h->arrays.back().null_count = -1;
+    }
+  }
+  for (ArrowArray& c : h->arrays) h->aptrs.push_back(&c);
+  *out = ArrowArray{};
+  out->length = p.length;
+  out->null_count = 0;
+  out->n_buffers = 1;
+  out->buffers = h->top_buffers;
+  out->n_children = int64_t(h->aptrs.size());
+  out->children = h->aptrs.data();
+  out->private_data = h;
+  out->release = [](ArrowArray* x) {
+    auto* hh = static_cast<ProjectHold*>(x->private_data);
+    for (ArrowArray& c : hh->arrays)
+      if (c.release) c.release(&c);
+    if (hh->parent_array.release) hh->parent_array.release(&hh->parent_array);
+    delete hh;
+    x->release = nullptr;
+  };
+  return 0;
+}
+const char* project_last_error(ArrowArrayStream* st) {
+  auto* ps = static_cast<ProjectState*>(st->private_data);
+  return ps->inner.get_last_error ? ps->inner.get_last_error(&ps->inner) : nullptr;
+}
+void project_release(ArrowArrayStream* st) {
+  auto* ps = static_cast<ProjectState*>(st->private_data);
+  if (ps->inner.release) ps->inner.release(&ps->inner);
+  delete ps;
+  st->release = nullptr;
+}
+
 // ---- the reader
 
 // Pulls record batches from the C stream, `depth` ahead on its own thread (depth 0: on the caller's).
@@ -1193,15 +1624,73 @@ am_stream* am_stream_from_c_stream(ArrowArrayStream* in, int prefetch_depth) {
 }
 
 am_stream* am_stream_open_ipc(const char* path, int prefetch_depth, int readers) {
-  (void)prefetch_depth;
-  (void)readers;
-  t_stream_error = std::string("Unsupported Arrow type: Arrow IPC files are not read by this build (") +
-                   (path ? path : "NULL") + "); open them with pyarrow and pass the RecordBatchReader to am_stream_from_c_stream";
-  set_last_error(t_stream_error);
-  return nullptr;
+  (void)readers;   // files are read one after another, so batch order is always the source's
+  if (!path) {
+    t_stream_error = "Invalid ArrowArray: a NULL path";
+    return nullptr;
+  }
+  try {
+    auto* state = new IpcStreamState();
+    std::unique_ptr<IpcStreamState> guard(state);
+    struct stat stt;
+    if (stat(path, &stt) != 0) throw Error(std::string("cannot open ") + path);
+    if (S_ISDIR(stt.st_mode)) {
+      // A directory: its Arrow IPC files in name order.
+      std::vector<std::string> names;
+      if (DIR* d = opendir(path)) {
+        while (dirent* e = readdir(d)) {
+          const std::string n = e->d_name;
+          auto ends = [&](const char* x) { return n.size() > std::strlen(x) && n.compare(n.size() - std::strlen(x), std::string::npos, x) == 0; };
+          if (ends(".arrow") || ends(".arrows") || ends(".ipc") || ends(".feather")) names.push_back(n);
+        }
+        closedir(d);
+      }
+      std::sort(names.begin(), names.end());
+      for (auto& n : names) state->src.files.push_back(std::string(path) + "/" + n);
+      if (state->src.files.empty()) throw Error(std::string("no Arrow IPC files (.arrow, .arrows, .ipc, .feather) in ") + path);
+    } else {
+      state->src.files.push_back(path);
+    }
+    if (!state->src.open_next()) throw invalid(std::string("no Arrow IPC schema in ") + path);
+    ArrowArrayStream in{};
+    in.get_schema = ipc_get_schema;
+    in.get_next = ipc_get_next;
+    in.get_last_error = ipc_last_error;
+    in.release = ipc_release;
+    in.private_data = guard.release();
+    return am_stream_from_c_stream(&in, prefetch_depth);
+  } catch (const std::exception& e) {
+    t_stream_error = e.what();
+    set_last_error(e.what());
+    return nullptr;
+  }
 }
 
 void am_stream_release(am_stream* s) { delete s; }
+
+int am_stream_export_c(am_stream* st, ArrowArrayStream* out) {
+  if (!st || !out) return 2;
+  return stream_guard([&] {
+    if (st->consumed) throw invalid("this stream has already been consumed");
+    st->consumed = true;
+    if (st->select.empty()) {
+      *out = st->in;
+      st->in.release = nullptr;
+      return 0;
+    }
+    auto* ps = new ProjectState();
+    ps->inner = st->in;
+    st->in.release = nullptr;
+    ps->select = st->select;
+    *out = ArrowArrayStream{};
+    out->get_schema = project_get_schema;
+    out->get_next = project_get_next;
+    out->get_last_error = project_last_error;
+    out->release = project_release;
+    out->private_data = ps;
+    return 0;
+  });
+}
 
 int am_stream_select(am_stream* st, const char** names, int64_t n) {
   if (!st || (!names && n > 0) || n < 0) return 2;

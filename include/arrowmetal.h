@@ -171,12 +171,17 @@ const char* am_stream_last_error(void);                           /* :1538 */
 /* Takes ownership of `in` (its release is NULL afterwards); prefetch_depth batches are read ahead on
  * a reader thread (0: read on the calling thread). include/arrowmetal.h:1546 */
 am_stream* am_stream_from_c_stream(struct ArrowArrayStream* in, int prefetch_depth);
-/* Arrow IPC files are not read by this build: returns NULL with the reason in am_stream_last_error
- * (open the file with pyarrow and pass its RecordBatchReader). include/arrowmetal.h:1544 */
+/* An Arrow IPC file (file or stream format) or a directory of them (.arrow, .arrows, .ipc, .feather, in
+ * name order), memory-mapped and read on the reader thread. Uncompressed bodies of flat columns;
+ * dictionary-encoded, nested and compressed IPC data return NULL with the reason. `readers` is
+ * accepted and the files are read in order. include/arrowmetal.h:1544 */
 am_stream* am_stream_open_ipc(const char* path, int prefetch_depth, int readers);
 void       am_stream_release(am_stream* s);                       /* :1547 */
 /* Keeps the named columns, in this order, in the terminal's output. include/arrowmetal.h:1551 */
 int am_stream_select(am_stream* s, const char** names, int64_t n);
+/* Hands the stream's batches (the selected columns) to a consumer as an Arrow C stream; a terminal,
+ * the handle is consumed. include/arrowmetal.h:1595 */
+int am_stream_export_c(am_stream* s, struct ArrowArrayStream* out);
 /* External sort: batches gather in HBM up to a run budget (a sixth of the free device memory, or
  * ARROWMETAL_STREAM_RUN_BYTES), each run is sorted on the GPU and, when more than one is needed,
  * spilled under scratch_dir (NULL: a new directory under the system's temporary directory) and

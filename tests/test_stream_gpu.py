@@ -143,3 +143,19 @@ def test_errors(am):
         s.sort("zz")
     with pytest.raises(am.ArrowMetalError, match="consumed"):
         s.sort("a")
+
+
+def test_sort_ipc_files_and_read_our_own_output(am, small_runs, tmp_path):
+    rng = np.random.default_rng(6)
+    t = table_of(rng, 150_000)
+    data = tmp_path / "in"
+    data.mkdir()
+    for i, b in enumerate(t.to_batches(max_chunksize=40_000)):
+        with pa.ipc.new_file(str(data / f"part-{i:03d}.arrow"), t.schema) as w:
+            w.write_batch(b)
+    keys = [("k2", "descending"), ("name", "ascending")]
+    got = am.scan_ipc(data).sort([("k2", True), ("name", False)])
+    same(got, expected(t, keys))
+    out = tmp_path / "sorted.arrows"
+    am.scan_ipc(data).sort_to_ipc([("k2", True), ("name", False)], out)
+    same(am.scan_ipc(out).to_reader().read_all(), expected(t, keys))
