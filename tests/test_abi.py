@@ -153,7 +153,7 @@ def _has_gpu():
 
 def test_stream_handles_without_a_device():
     """A record-batch stream is taken and its columns selected on the host; the sort itself needs the
-    device and fails loudly without one; IPC files are refused with the way round."""
+    device and fails loudly without one; a missing IPC file is an error with its path."""
     import pyarrow as pa
     import arrowmetal_b200 as am
     s = am.scan_arrow(pa.table({"a": [3, 1, 2], "s": ["x", "y", "z"]}))
@@ -165,4 +165,4 @@ def test_stream_handles_without_a_device():
     with pytest.raises(am.ArrowMetalError, match="consumed"):
         s.sort("a")
     assert am._lib.am_stream_open_ipc(b"/nonexistent.arrow", 3, 1) is None
-    assert b"RecordBatchReader" in am._lib.am_stream_last_error()
+    assert b"cannot open /nonexistent.arrow" in am._lib.am_stream_last_error()
