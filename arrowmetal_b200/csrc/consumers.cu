@@ -8,11 +8,14 @@
 //      rank functions also put the NaN rows and the nulls in one run, as pyarrow ranks them). One byte
 //      per position, and a count of marks per block;
 //   2. an exclusive scan of the block counts (one block; the total run count lands after them);
-//   3. every position's run number (its block's offset plus a block scan of the marks), scattered to
-//      its original row; a run's first position is recorded as the run's start, and its row as the
-//      run's representative (the earliest row of the run: the sort is stable);
-//   4. one pass over the original rows turns run numbers into the answer (the run's first or last
-//      position, its quantile), or one over the runs gives their lengths.
+//   3. every position's run number (its block's offset plus a block scan of the marks); a run's first
+//      position is recorded as the run's start, and its row as the run's representative (the earliest
+//      row of the run: the sort is stable);
+//   4. one pass over the positions turns run numbers into the answer (the run's first or last
+//      position, its quantile), or one over the runs gives their lengths;
+//   5. the answers go to their original rows by a scatter in two steps that keeps every random store
+//      inside L2: the (row, value) pairs are appended to the bucket of the row's high bits (a bucket's
+//      size is known, the order being a permutation), then drained bucket after bucket.
 #include <algorithm>
 #include <vector>
 
@@ -196,12 +199,12 @@ __global__ void __launch_bounds__(1024) run_scan_kernel(uint32_t* __restrict__ c
   if (t == 0) counts[blocks] = carry;
 }
 
-// 3. Run numbers (1-based) of positions [0, m): run_of_row[perm[i]] (when wanted), and for each run's
-// first position its start and its row.
+// 3. Run numbers (1-based) of positions [0, m): run_of_pos[i] (when wanted), and for each run's first
+// position its start and its row.
 __global__ void __launch_bounds__(RUN_THREADS) run_ids_kernel(const uint8_t* __restrict__ marks,
                                                               const uint32_t* __restrict__ block_off,
                                                               const uint32_t* __restrict__ perm, uint64_t m,
-                                                              uint32_t* __restrict__ run_of_row,
+                                                              uint32_t* __restrict__ run_of_pos,
                                                               uint32_t* __restrict__ starts,
                                                               uint32_t* __restrict__ heads) {
   __shared__ uint32_t s_warp[RUN_THREADS / 32];
@@ -225,35 +228,27 @@ __global__ void __launch_bounds__(RUN_THREADS) run_ids_kernel(const uint8_t* __r
     const uint64_t pos = base + i;
     if (pos >= m) break;
     run += mk[i];
-    const uint32_t r = perm[pos];
-    if (run_of_row) run_of_row[r] = run;
+    if (run_of_pos) run_of_pos[pos] = run;
     if (mk[i]) {
       if (starts) starts[run - 1] = uint32_t(pos);
-      if (heads) heads[run - 1] = r;
+      if (heads) heads[run - 1] = perm[pos];
     }
   }
 }
 
-// row_number: the 1-based sorted position, at the original row.
-__global__ void __launch_bounds__(256) position_kernel(const uint32_t* __restrict__ perm, uint64_t n,
-                                                       uint32_t* __restrict__ out) {
-  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x)
-    out[perm[i]] = uint32_t(i + 1);
-}
-
-// 4. Run numbers into the answer, per original row. A run [s, e) of sorted positions:
+// 4. Run numbers into the answer, per sorted position. A run [s, e) of sorted positions:
 //   FIN_MIN s + 1; FIN_MAX e; FIN_QUANTILE (s + e) / 2n, the run's average 1-based rank minus one
 //   half over n; FIN_NORMAL64 / FIN_NORMAL32 the standard normal quantile of that; FIN_PERCENT
 //   s / (n - 1) (0 for one row); FIN_CUME e / n.
 enum Finish { FIN_MIN = 0, FIN_MAX, FIN_QUANTILE, FIN_NORMAL64, FIN_NORMAL32, FIN_PERCENT, FIN_CUME };
 
-__global__ void __launch_bounds__(256) rank_finish_kernel(uint32_t* __restrict__ run_of_row,
+__global__ void __launch_bounds__(256) rank_finish_kernel(const uint32_t* run_of_pos,
                                                           const uint32_t* __restrict__ starts,
                                                           const uint32_t* __restrict__ total_runs, uint64_t n,
-                                                          int mode, void* __restrict__ out) {
+                                                          int mode, void* out) {
   const uint32_t runs = *total_runs;
   for (uint64_t r = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; r < n; r += uint64_t(gridDim.x) * blockDim.x) {
-    const uint32_t g = run_of_row[r];
+    const uint32_t g = run_of_pos[r];
     const uint64_t s = starts[g - 1];
     const uint64_t e = g < runs ? uint64_t(starts[g]) : n;
     switch (mode) {
@@ -265,6 +260,65 @@ __global__ void __launch_bounds__(256) rank_finish_kernel(uint32_t* __restrict__
       case FIN_PERCENT: static_cast<double*>(out)[r] = n > 1 ? double(s) / double(n - 1) : 0.0; break;
       default: static_cast<double*>(out)[r] = double(e) / double(n); break;
     }
+  }
+}
+
+// 5. The scatter to the original rows: out[perm[i]] = val[i] (val NULL: i + 1). perm is a permutation of
+// [0, n), so the pairs whose row lies in [b << shift, (b + 1) << shift) are exactly 2^shift (fewer in
+// the last bucket) and bucket b's pairs go to [b << shift, ...) of the pair arrays, each block reserving
+// its share of every bucket with one atomic. The drain then reads the pairs in order: the blocks in
+// flight work on a few neighbouring buckets, whose rows span a region L2 holds.
+constexpr int SC_THREADS = 512, SC_ITEMS = 8;
+constexpr uint64_t SC_CHUNK = uint64_t(SC_THREADS) * SC_ITEMS;
+
+template <typename V>
+__global__ void __launch_bounds__(SC_THREADS) bucket_pairs_kernel(const uint32_t* __restrict__ perm,
+                                                                  const V* __restrict__ val, uint64_t n, int shift,
+                                                                  int nb, uint32_t* __restrict__ cursor,
+                                                                  uint32_t* __restrict__ rows_out, V* __restrict__ vals_out,
+                                                                  uint32_t* __restrict__ err) {
+  extern __shared__ uint32_t sc_sh[];
+  uint32_t* cnt = sc_sh;
+  uint32_t* base = sc_sh + nb;
+  for (int b = threadIdx.x; b < nb; b += SC_THREADS) cnt[b] = 0;
+  __syncthreads();
+  const uint64_t start = uint64_t(blockIdx.x) * SC_CHUNK;
+  uint32_t row[SC_ITEMS], slot[SC_ITEMS];
+  V v[SC_ITEMS];
+#pragma unroll
+  for (int i = 0; i < SC_ITEMS; i++) {
+    const uint64_t pos = start + uint64_t(i) * SC_THREADS + threadIdx.x;
+    if (pos < n) {
+      row[i] = perm[pos];
+      v[i] = val ? val[pos] : V(pos + 1);
+      slot[i] = atomicAdd(&cnt[row[i] >> shift], 1u);
+    }
+  }
+  __syncthreads();
+  for (int b = threadIdx.x; b < nb; b += SC_THREADS)
+    if (cnt[b]) base[b] = (uint32_t(b) << shift) + atomicAdd(&cursor[b], cnt[b]);
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < SC_ITEMS; i++) {
+    const uint64_t pos = start + uint64_t(i) * SC_THREADS + threadIdx.x;
+    if (pos >= n) continue;
+    const uint64_t dst = uint64_t(base[row[i] >> shift]) + slot[i];
+    if (dst >= n) {
+      atomicOr(err, ERR_BOUNDS);
+      continue;
+    }
+    rows_out[dst] = row[i];
+    vals_out[dst] = v[i];
+  }
+}
+
+template <typename V>
+__global__ void __launch_bounds__(256) drain_pairs_kernel(const uint32_t* __restrict__ rows, const V* __restrict__ vals,
+                                                          uint64_t n, V* __restrict__ out, uint32_t* __restrict__ err) {
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
+    const uint32_t r = rows[i];
+    if (r < n) out[r] = vals[i];
+    else atomicOr(err, ERR_BOUNDS);
   }
 }
 
@@ -422,6 +476,32 @@ void run_ids(const Runs& r, const uint32_t* perm, uint64_t m, uint32_t* run_of_r
   AM_CUDA(cudaGetLastError());
 }
 
+// out[perm[i]] = vals[i] for i < n (vals NULL: i + 1), perm a permutation of [0, n).
+template <typename V>
+void scatter_to_rows(const uint32_t* perm, const V* vals, uint64_t n, V* out, cudaStream_t s) {
+  int bits = 0;
+  while ((uint64_t(1) << bits) < n) bits++;
+  // At most 64 buckets: a block's 4,096 pairs make runs of ~64 per bucket, and a bucket's rows (at
+  // most 2^26 of the 2^32 rows, 4-8 MB at 50M rows) still sit well inside L2 while they drain.
+  const int shift = std::max(12, bits - 6);
+  const int nb = int((n + (uint64_t(1) << shift) - 1) >> shift);
+  BufPtr cursor = DevBuffer::alloc(size_t(nb) * 4 + 16, s);
+  BufPtr rows = DevBuffer::alloc(size_t(n) * 4 + 16, s);
+  BufPtr pv = DevBuffer::alloc(size_t(n) * sizeof(V) + 16, s);
+  AM_CUDA(cudaMemsetAsync(cursor->ptr, 0, size_t(nb) * 4, s));
+  uint32_t* err = stream_scratch(s, 0).err;
+  KernelTimer kt("rank_scatter", s);
+  const uint32_t blocks = uint32_t((n + SC_CHUNK - 1) / SC_CHUNK);
+  bucket_pairs_kernel<V><<<blocks, SC_THREADS, size_t(nb) * 8, s>>>(perm, vals, n, shift, nb,
+                                                                    static_cast<uint32_t*>(cursor->ptr),
+                                                                    static_cast<uint32_t*>(rows->ptr),
+                                                                    static_cast<V*>(pv->ptr), err);
+  AM_CUDA(cudaGetLastError());
+  drain_pairs_kernel<V><<<grid_for(n), 256, 0, s>>>(static_cast<const uint32_t*>(rows->ptr),
+                                                    static_cast<const V*>(pv->ptr), n, out, err);
+  AM_CUDA(cudaGetLastError());
+}
+
 am_array* new_filled(int pt, const char* format, int64_t n, cudaStream_t s) {
   am_array* o = new_array(pt, format, n);
   o->values = DevBuffer::alloc(size_t(std::max<int64_t>(n, 1)) * std::max(pt_bytes(pt), 1) + 16, s);
@@ -457,24 +537,29 @@ am_array* rank_of(am_array* a, int fn, bool desc, bool nulls_first, bool merge_n
     BufPtr perm = sorted_order(a, desc, nulls_first, float_order, s);
     const uint32_t* p = static_cast<const uint32_t*>(perm->ptr);
     if (fn == RANK_FIRST) {
-      KernelTimer kt("rank_scatter", s);
-      position_kernel<<<grid_for(uint64_t(n)), 256, 0, s>>>(p, uint64_t(n), static_cast<uint32_t*>(out->values->ptr));
-      AM_CUDA(cudaGetLastError());
+      scatter_to_rows<uint32_t>(p, nullptr, uint64_t(n), static_cast<uint32_t*>(out->values->ptr), s);
       return out;
     }
     const Runs r = mark_runs(a, p, uint64_t(n), merge_nan, float_order, s);
-    // Run numbers go straight into a uint32 answer; the float answers read them from scratch.
-    BufPtr scratch = (f32 || f64) ? DevBuffer::alloc(size_t(n) * 4 + 16, s) : nullptr;
-    uint32_t* run_of_row = scratch ? static_cast<uint32_t*>(scratch->ptr) : static_cast<uint32_t*>(out->values->ptr);
+    // Run numbers by position; the uint32 answers are computed in place, the float ones beside them.
+    BufPtr run_of_pos = DevBuffer::alloc(size_t(n) * 4 + 16, s);
+    uint32_t* rp = static_cast<uint32_t*>(run_of_pos->ptr);
     BufPtr starts = fn == RANK_DENSE ? nullptr : DevBuffer::alloc(size_t(n) * 4 + 16, s);
-    run_ids(r, p, uint64_t(n), run_of_row, starts ? static_cast<uint32_t*>(starts->ptr) : nullptr, nullptr, s);
+    run_ids(r, p, uint64_t(n), rp, starts ? static_cast<uint32_t*>(starts->ptr) : nullptr, nullptr, s);
+    BufPtr val_pos = (f32 || f64) ? DevBuffer::alloc(size_t(n) * (f64 ? 8 : 4) + 16, s) : nullptr;
     if (fn != RANK_DENSE) {
       static const int finish[] = {FIN_MIN, FIN_MAX, -1, -1, FIN_QUANTILE, FIN_NORMAL64, FIN_NORMAL32, FIN_PERCENT, FIN_CUME};
       KernelTimer kt("rank_finish", s);
-      rank_finish_kernel<<<grid_for(uint64_t(n)), 256, 0, s>>>(run_of_row, static_cast<const uint32_t*>(starts->ptr),
-                                                               r.total(), uint64_t(n), finish[fn], out->values->ptr);
+      rank_finish_kernel<<<grid_for(uint64_t(n)), 256, 0, s>>>(rp, static_cast<const uint32_t*>(starts->ptr),
+                                                               r.total(), uint64_t(n), finish[fn],
+                                                               val_pos ? val_pos->ptr : static_cast<void*>(rp));
       AM_CUDA(cudaGetLastError());
     }
+    if (f64) scatter_to_rows<double>(p, static_cast<const double*>(val_pos->ptr), uint64_t(n),
+                                     static_cast<double*>(out->values->ptr), s);
+    else if (f32) scatter_to_rows<float>(p, static_cast<const float*>(val_pos->ptr), uint64_t(n),
+                                         static_cast<float*>(out->values->ptr), s);
+    else scatter_to_rows<uint32_t>(p, rp, uint64_t(n), static_cast<uint32_t*>(out->values->ptr), s);
     // The scratch buffers are freed in stream order after the kernels that read them.
   } catch (...) {
     release(out);
