@@ -1399,7 +1399,9 @@ void external_sort(am_stream* st, const SortSpec& spec_in, const std::vector<std
     return sorted;
   };
   auto spill_last = [&]() {
-    const std::string path = scratch() + "/run-" + std::to_string(runs.size()) + "-" + std::to_string(getpid()) + ".amrun";
+    // Unique within the machine: sorts of several threads or processes may share a scratch directory.
+    static std::atomic<uint64_t> seq{0};
+    const std::string path = scratch() + "/run-" + std::to_string(getpid()) + "-" + std::to_string(seq.fetch_add(1)) + ".amrun";
     runs.push_back(spill(last_run, path));
     release_all(last_run);
   };
