@@ -271,38 +271,74 @@ __global__ void __launch_bounds__(256) rank_finish_kernel(const uint32_t* run_of
 constexpr int SC_THREADS = 512, SC_ITEMS = 8;
 constexpr uint64_t SC_CHUNK = uint64_t(SC_THREADS) * SC_ITEMS;
 
+// Each warp ranks its pairs within their buckets by ballots on the bucket's bits (no shared atomics:
+// the warp's counters advance item by item, as in the sort's ranking); then one thread per bucket
+// reserves the block's share with one atomic and hands each warp its offset.
+constexpr int SC_WARPS = SC_THREADS / 32;
+constexpr int SC_MAX_BUCKETS = 64, SC_BUCKET_BITS = 6;
+
 template <typename V>
 __global__ void __launch_bounds__(SC_THREADS) bucket_pairs_kernel(const uint32_t* __restrict__ perm,
                                                                   const V* __restrict__ val, uint64_t n, int shift,
                                                                   int nb, uint32_t* __restrict__ cursor,
                                                                   uint32_t* __restrict__ rows_out, V* __restrict__ vals_out,
                                                                   uint32_t* __restrict__ err) {
-  extern __shared__ uint32_t sc_sh[];
-  uint32_t* cnt = sc_sh;
-  uint32_t* base = sc_sh + nb;
-  for (int b = threadIdx.x; b < nb; b += SC_THREADS) cnt[b] = 0;
-  __syncthreads();
-  const uint64_t start = uint64_t(blockIdx.x) * SC_CHUNK;
+  __shared__ uint32_t wcnt[SC_WARPS][SC_MAX_BUCKETS];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t lt = (1u << lane) - 1u;
+  for (int b = lane; b < SC_MAX_BUCKETS; b += 32) wcnt[warp][b] = 0;
+  __syncwarp();
+  // A warp's items: SC_ITEMS x 32 consecutive positions.
+  const uint64_t start = uint64_t(blockIdx.x) * SC_CHUNK + uint64_t(warp) * (SC_ITEMS * 32);
   uint32_t row[SC_ITEMS], slot[SC_ITEMS];
   V v[SC_ITEMS];
 #pragma unroll
   for (int i = 0; i < SC_ITEMS; i++) {
-    const uint64_t pos = start + uint64_t(i) * SC_THREADS + threadIdx.x;
-    if (pos < n) {
-      row[i] = perm[pos];
-      v[i] = val ? val[pos] : V(pos + 1);
-      slot[i] = atomicAdd(&cnt[row[i] >> shift], 1u);
+    const uint64_t pos = start + uint64_t(i) * 32 + lane;
+    const bool live = pos < n;
+    row[i] = live ? perm[pos] : 0u;
+    v[i] = live ? (val ? val[pos] : V(pos + 1)) : V(0);
+  }
+#pragma unroll
+  for (int i = 0; i < SC_ITEMS; i++) {
+    const uint64_t pos = start + uint64_t(i) * 32 + lane;
+    const bool live = pos < n;
+    const uint32_t b = live ? (row[i] >> shift) : 0u;
+    uint32_t peers = __ballot_sync(0xffffffffu, live);
+#pragma unroll
+    for (int k = 0; k < SC_BUCKET_BITS; k++) {
+      const uint32_t bit = (b >> k) & 1u;
+      const uint32_t bl = __ballot_sync(0xffffffffu, bit);
+      peers &= bit ? bl : ~bl;
+    }
+    const uint32_t base = live ? wcnt[warp][b] : 0u;
+    __syncwarp();
+    if (live) {
+      if (lane == __ffs(peers) - 1) wcnt[warp][b] = base + __popc(peers);
+      slot[i] = base + __popc(peers & lt);
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+  // Per bucket: the block's total, one reservation, and each warp's offset within it.
+  for (int b = threadIdx.x; b < nb; b += SC_THREADS) {
+    uint32_t total = 0;
+#pragma unroll
+    for (int w = 0; w < SC_WARPS; w++) total += wcnt[w][b];
+    uint32_t at = total ? (uint32_t(b) << shift) + atomicAdd(&cursor[b], total) : 0u;
+#pragma unroll
+    for (int w = 0; w < SC_WARPS; w++) {
+      const uint32_t c = wcnt[w][b];
+      wcnt[w][b] = at;
+      at += c;
     }
   }
   __syncthreads();
-  for (int b = threadIdx.x; b < nb; b += SC_THREADS)
-    if (cnt[b]) base[b] = (uint32_t(b) << shift) + atomicAdd(&cursor[b], cnt[b]);
-  __syncthreads();
 #pragma unroll
   for (int i = 0; i < SC_ITEMS; i++) {
-    const uint64_t pos = start + uint64_t(i) * SC_THREADS + threadIdx.x;
+    const uint64_t pos = start + uint64_t(i) * 32 + lane;
     if (pos >= n) continue;
-    const uint64_t dst = uint64_t(base[row[i] >> shift]) + slot[i];
+    const uint64_t dst = uint64_t(wcnt[warp][row[i] >> shift]) + slot[i];
     if (dst >= n) {
       atomicOr(err, ERR_BOUNDS);
       continue;
@@ -492,7 +528,8 @@ void scatter_to_rows(const uint32_t* perm, const V* vals, uint64_t n, V* out, cu
   uint32_t* err = stream_scratch(s, 0).err;
   KernelTimer kt("rank_scatter", s);
   const uint32_t blocks = uint32_t((n + SC_CHUNK - 1) / SC_CHUNK);
-  bucket_pairs_kernel<V><<<blocks, SC_THREADS, size_t(nb) * 8, s>>>(perm, vals, n, shift, nb,
+  if (nb > SC_MAX_BUCKETS) throw Error("rank scatter: more buckets than the kernel ranks");
+  bucket_pairs_kernel<V><<<blocks, SC_THREADS, 0, s>>>(perm, vals, n, shift, nb,
                                                                     static_cast<uint32_t*>(cursor->ptr),
                                                                     static_cast<uint32_t*>(rows->ptr),
                                                                     static_cast<V*>(pv->ptr), err);
