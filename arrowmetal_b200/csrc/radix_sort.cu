@@ -841,6 +841,429 @@ __global__ void __launch_bounds__(256) key_validity_kernel(const SortSummary* __
 }
 
 // ------------------------------------------------------------------------------------------------
+// The large single-key sort: two passes on the top digits, then local sorts in shared memory.
+//
+// One 8-byte key over at least 2^25 value rows with three or more active digits. Two onesweep passes
+// on the two highest active digits (the lower of them first: LSD order) leave the value rows grouped
+// by those digits -- at most 65,536 buckets, a few hundred rows each at the benchmark's size -- with
+// every bucket in row order. Each bucket is then sorted by the remaining active digits inside one
+// CTA's shared memory (the same warp-ballot ranking as the passes, no look-back), and written to its
+// final place: one read and one write of the rows instead of a global pass per remaining digit.
+// Buckets too large for every local shape make the sort run the remaining passes instead: the low
+// digits, then the two top digits again (a complete LSD sequence after the first two passes, so the
+// answer is the same). Every choice is made on the device, with no host round trip.
+
+constexpr uint64_t HYB_MIN_ROWS = uint64_t(1) << 25;
+constexpr int HYB_STEPS = 10;                 // two top-digit passes, then up to eight fallback passes
+constexpr int BND_THREADS = 256, BND_ITEMS = 16;
+constexpr uint64_t BND_CHUNK = uint64_t(BND_THREADS) * BND_ITEMS;
+constexpr int LOC_ITEMS = 7;
+constexpr int LOC_VARIANTS = 3;               // 128, 256 and 512 threads x 7 rows
+__host__ __device__ constexpr int loc_threads(int v) { return v == 0 ? 128 : v == 1 ? 256 : 512; }
+__host__ __device__ constexpr uint32_t loc_cap(int v) { return uint32_t(loc_threads(v) * LOC_ITEMS); }
+
+struct HybridState {
+  uint32_t mode;          // 1: the hybrid sort runs
+  uint32_t fallback;      // 1: a bucket exceeds every local shape; the remaining passes run
+  uint32_t variant;       // the local shape that runs
+  uint32_t buckets;       // non-empty buckets
+  uint32_t m;             // value rows
+  uint32_t value_base;    // the value rows' first output row
+  uint32_t nlocal;        // digits left to the local sorts, low to high
+  uint32_t nfall;         // fallback passes prepared
+  uint32_t hi_shift, lo_shift;   // the two bucket digits
+  uint32_t max_bucket;
+  uint32_t local_shift[8];
+};
+
+// One block: the hybrid's pass descriptors from the plan's (one descriptor per digit slot), or the
+// plan's own passes unchanged when the hybrid does not apply.
+__global__ void __launch_bounds__(256) hybrid_plan_kernel(PlanArgs a, const KeyStats* __restrict__ st,
+                                                          const PassDesc* __restrict__ normal,
+                                                          PassDesc* __restrict__ steps, HybridState* __restrict__ hs) {
+  __shared__ int s_src[HYB_STEPS];      // the normal slot each step copies (-1: none)
+  __shared__ int s_hyb, s_na, s_act[8];
+  if (threadIdx.x == 0) {
+    int na = 0;
+    for (int d = 0; d < a.nslots && d < 8; d++)
+      if (normal[d].active) s_act[na++] = d;
+    const bool hyb = a.nkeys == 1 && a.key_bytes[0] == 8 && uint64_t(st->n_value) >= HYB_MIN_ROWS && na >= 3;
+    s_hyb = hyb ? 1 : 0;
+    s_na = na;
+    for (int i = 0; i < HYB_STEPS; i++) s_src[i] = -1;
+    if (hyb) {
+      s_src[0] = s_act[na - 2];
+      s_src[1] = s_act[na - 1];
+      for (int i = 0; i < na; i++) s_src[2 + i] = s_act[i];   // low digits, then the top two again
+    } else {
+      for (int i = 0; i < a.nslots && i < 8; i++) s_src[2 + i] = i;
+    }
+  }
+  __syncthreads();
+  // The descriptors' words, copied by the whole block.
+  constexpr int W = int(sizeof(PassDesc) / 4);
+  for (int i = 0; i < HYB_STEPS; i++) {
+    uint32_t* dst = reinterpret_cast<uint32_t*>(steps + i);
+    if (s_src[i] < 0) {
+      for (int w = threadIdx.x; w < W; w += blockDim.x) dst[w] = 0;
+    } else {
+      const uint32_t* src = reinterpret_cast<const uint32_t*>(normal + s_src[i]);
+      for (int w = threadIdx.x; w < W; w += blockDim.x) dst[w] = src[w];
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  const uint32_t m = st->n_value;
+  hs->mode = uint32_t(s_hyb);
+  hs->fallback = 0;
+  hs->variant = 0;
+  hs->buckets = 0;
+  hs->m = m;
+  hs->value_base = a.nulls_first[0] ? st->n_null + st->n_nan : 0u;
+  hs->max_bucket = 0;
+  if (!s_hyb) {
+    hs->nlocal = 0;
+    hs->nfall = 0;
+    return;                              // steps 2.. are the plan's passes, as planned
+  }
+  const int na = s_na;
+  const uint32_t wide = a.index_wide ? PF_WIDE_OUT : 0u;
+  PassDesc& h0 = steps[0];
+  h0.active = 1;
+  h0.flags = PF_ENCODE | PF_ROUTE | wide;
+  h0.count = uint32_t(a.n);
+  h0.src_keys = -1;
+  h0.src_ids = -1;
+  h0.dst_keys = 0;
+  h0.dst_ids = 0;
+  PassDesc& h1 = steps[1];
+  h1.active = 1;
+  h1.flags = wide;
+  h1.count = m;
+  h1.src_keys = 0;
+  h1.src_ids = 0;
+  h1.dst_keys = 1;
+  h1.dst_ids = 1;
+  int cur = 1;
+  for (int i = 0; i < na; i++) {
+    PassDesc& f = steps[2 + i];
+    const bool last = i == na - 1;
+    f.active = 0;                        // activated by the decision when a bucket is too large
+    f.flags = wide | (last ? PF_LAST : 0u);
+    f.count = m;
+    f.src_keys = cur;
+    f.src_ids = cur;
+    if (last) {
+      f.dst_keys = -1;
+      f.dst_ids = -1;
+    } else {
+      f.dst_keys = 1 - cur;
+      f.dst_ids = 1 - cur;
+      cur = 1 - cur;
+    }
+  }
+  hs->nfall = uint32_t(na);
+  hs->nlocal = uint32_t(na - 2);
+  for (int i = 0; i < na - 2; i++) hs->local_shift[i] = uint32_t(8 * s_act[i]);
+  hs->hi_shift = uint32_t(8 * s_act[na - 1]);
+  hs->lo_shift = uint32_t(8 * s_act[na - 2]);
+}
+
+__device__ __forceinline__ uint32_t bucket_of(uint64_t k, uint32_t hi, uint32_t lo) {
+  return ((uint32_t(k >> hi) & 255u) << 8) | (uint32_t(k >> lo) & 255u);
+}
+
+// Bucket boundaries: position i of the value rows starts a bucket when its bucket differs from row
+// i - 1's. A block takes BND_CHUNK rows, thread t the rows t, t + BND_THREADS, ... of it (coalesced
+// loads, the row before each read from the neighbouring lane or the previous round).
+__device__ __forceinline__ uint32_t boundary_masks(const uint64_t* __restrict__ keys, uint64_t first, uint64_t m,
+                                                   uint32_t hi, uint32_t lo) {
+  // Bit k: row first + k * BND_THREADS + threadIdx.x starts a bucket.
+  uint32_t mask = 0;
+#pragma unroll
+  for (int k = 0; k < BND_ITEMS; k++) {
+    const uint64_t r = first + uint64_t(k) * BND_THREADS + threadIdx.x;
+    if (r >= m) continue;
+    const uint32_t b = bucket_of(keys[r], hi, lo);
+    const uint32_t p = r == 0 ? 0xFFFFFFFFu : bucket_of(keys[r - 1], hi, lo);
+    if (b != p) mask |= 1u << k;
+  }
+  return mask;
+}
+
+__global__ void __launch_bounds__(BND_THREADS) bounds_count_kernel(const uint64_t* __restrict__ keys,
+                                                                   const HybridState* __restrict__ hs,
+                                                                   uint32_t* __restrict__ counts) {
+  __shared__ uint32_t s_warp[BND_THREADS / 32];
+  if (!hs->mode) return;
+  const uint64_t first = uint64_t(blockIdx.x) * BND_CHUNK;
+  uint32_t c = __popc(boundary_masks(keys, first, hs->m, hs->hi_shift, hs->lo_shift));
+  c = __reduce_add_sync(0xffffffffu, c);
+  if ((threadIdx.x & 31) == 0) s_warp[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t t = 0;
+    for (int w = 0; w < BND_THREADS / 32; w++) t += s_warp[w];
+    counts[blockIdx.x] = t;
+  }
+}
+
+// One block: exclusive scan of the block counts in place; the bucket count and the end sentinel.
+__global__ void __launch_bounds__(1024) bounds_scan_kernel(uint32_t* __restrict__ counts, uint32_t blocks,
+                                                           HybridState* __restrict__ hs, uint32_t* __restrict__ pos) {
+  __shared__ uint32_t s[32];
+  __shared__ uint32_t carry;
+  if (!hs->mode) return;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  if (t == 0) carry = 0;
+  __syncthreads();
+  for (uint32_t b0 = 0; b0 < blocks; b0 += 1024) {
+    const uint32_t i = b0 + uint32_t(t);
+    const uint32_t v = i < blocks ? counts[i] : 0u;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) s[warp] = x;
+    __syncthreads();
+    uint32_t add = carry, all = 0;
+    for (int w = 0; w < 32; w++) {
+      if (w < warp) add += s[w];
+      all += s[w];
+    }
+    if (i < blocks) counts[i] = x - v + add;
+    __syncthreads();
+    if (t == 0) carry += all;
+    __syncthreads();
+  }
+  if (t == 0) {
+    hs->buckets = carry;
+    if (carry <= 65536u) pos[carry] = hs->m;   // pos holds 65,537 entries; more starts mean fallback
+  }
+}
+
+// The starts' positions, in row order: round k of the block before round k + 1, warp w before w + 1
+// within a round (rows first + k * BND_THREADS + 32 w + lane).
+__global__ void __launch_bounds__(BND_THREADS) bounds_write_kernel(const uint64_t* __restrict__ keys,
+                                                                   const HybridState* __restrict__ hs,
+                                                                   const uint32_t* __restrict__ offs,
+                                                                   uint32_t* __restrict__ pos,
+                                                                   uint32_t* __restrict__ err) {
+  constexpr int WARPS = BND_THREADS / 32;
+  __shared__ uint32_t s_cnt[BND_ITEMS][WARPS];
+  if (!hs->mode) return;
+  const uint64_t first = uint64_t(blockIdx.x) * BND_CHUNK;
+  const uint32_t mask = boundary_masks(keys, first, hs->m, hs->hi_shift, hs->lo_shift);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t lt = (1u << lane) - 1u;
+  uint32_t ball[BND_ITEMS];
+#pragma unroll
+  for (int k = 0; k < BND_ITEMS; k++) {
+    ball[k] = __ballot_sync(0xffffffffu, (mask >> k) & 1u);
+    if (lane == 0) s_cnt[k][warp] = __popc(ball[k]);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t run = offs[blockIdx.x];
+    for (int k = 0; k < BND_ITEMS; k++)
+      for (int w = 0; w < WARPS; w++) {
+        const uint32_t c = s_cnt[k][w];
+        s_cnt[k][w] = run;
+        run += c;
+      }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < BND_ITEMS; k++) {
+    if (!((mask >> k) & 1u)) continue;
+    const uint32_t at = s_cnt[k][warp] + __popc(ball[k] & lt);
+    if (at >= 65536u) {
+      atomicOr(err, ERR_BOUNDS);
+      continue;
+    }
+    pos[at] = uint32_t(first + uint64_t(k) * BND_THREADS + threadIdx.x);
+  }
+}
+
+// One block: the largest bucket picks the local shape, or the fallback passes.
+__global__ void __launch_bounds__(1024) bounds_decide_kernel(HybridState* __restrict__ hs, const uint32_t* __restrict__ pos,
+                                                             PassDesc* __restrict__ steps, SortSummary* __restrict__ sum) {
+  __shared__ uint32_t s_max;
+  if (!hs->mode) return;
+  if (threadIdx.x == 0) s_max = 0;
+  __syncthreads();
+  // The rows are grouped by a 16-bit bucket, so there are at most 65,536 starts; anything else takes
+  // the passes.
+  const uint32_t g = hs->buckets <= 65536u ? hs->buckets : 0u;
+  uint32_t mx = 0;
+  for (uint32_t j = threadIdx.x; j < g; j += blockDim.x) mx = max(mx, pos[j + 1] - pos[j]);
+  mx = __reduce_max_sync(0xffffffffu, mx);
+  if ((threadIdx.x & 31) == 0) atomicMax(&s_max, mx);
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  hs->max_bucket = s_max;
+  int v = -1;
+  for (int i = LOC_VARIANTS - 1; i >= 0; i--)
+    if (s_max <= loc_cap(i)) v = i;
+  if (hs->buckets > 65536u) v = -1;
+  if (v >= 0) {
+    hs->variant = uint32_t(v);
+    sum->passes_run = 2;                 // the local sorts stand in for the others
+  } else {
+    hs->fallback = 1;
+    for (uint32_t i = 0; i < hs->nfall; i++) steps[2 + i].active = 1;
+    sum->passes_run = 2 + hs->nfall;
+  }
+}
+
+// The local sorts: each bucket of the value rows, sorted by the digits below the bucket digits in
+// shared memory, then written to its final rows (ids, and the key column rebuilt when asked). A
+// persistent grid of CTAs walks the buckets; a shape that is not the chosen one returns at once.
+template <int THREADS, int VARIANT>
+__global__ void __launch_bounds__(THREADS) local_sort_kernel(const uint64_t* __restrict__ keys,
+                                                             const uint32_t* __restrict__ ids,
+                                                             const uint32_t* __restrict__ pos,
+                                                             const HybridState* __restrict__ hs,
+                                                             const __grid_constant__ PassArgs pa) {
+  constexpr int ITEMS = LOC_ITEMS, WARPS = THREADS / 32, CAP = THREADS * ITEMS;
+  extern __shared__ __align__(16) unsigned char loc_smem[];
+  uint64_t* skeys = reinterpret_cast<uint64_t*>(loc_smem);
+  uint32_t* sids = reinterpret_cast<uint32_t*>(skeys + CAP);
+  uint32_t* whist = sids + CAP;                       // [WARPS][256]
+  uint32_t* local = whist + WARPS * 256;              // [256]
+  uint32_t* wsum = local + 256;                       // [WARPS]
+  if (!hs->mode || hs->fallback || hs->variant != uint32_t(VARIANT)) return;
+  const uint32_t g = hs->buckets, nloc = hs->nlocal, vbase = hs->value_base;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t lt = (1u << lane) - 1u;
+  constexpr int DPT = THREADS >= 256 ? 1 : 256 / THREADS;
+  for (uint32_t j = blockIdx.x; j < g; j += gridDim.x) {
+    const uint32_t start = pos[j], size = pos[j + 1] - start;
+    if (size > uint32_t(CAP)) {            // the decision rules it out; never read past the tile
+      if (threadIdx.x == 0) atomicOr(pa.err, ERR_BOUNDS);
+      continue;
+    }
+    uint64_t key[ITEMS];
+    uint32_t id[ITEMS];
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++) {
+      const uint32_t r = uint32_t(warp) * (ITEMS * 32) + uint32_t(i) * 32 + lane;
+      key[i] = r < size ? keys[start + r] : 0ull;
+      id[i] = r < size ? ids[start + r] : 0u;
+    }
+    for (uint32_t dgi = 0; dgi < nloc; dgi++) {
+      const uint32_t shift = hs->local_shift[dgi];
+      uint32_t dg[ITEMS];
+#pragma unroll
+      for (int i = 0; i < ITEMS; i++) {
+        const uint32_t r = uint32_t(warp) * (ITEMS * 32) + uint32_t(i) * 32 + lane;
+        dg[i] = r < size ? (uint32_t(key[i] >> shift) & 255u) : INVALID_DIGIT;
+      }
+      for (int x = lane; x < 256; x += 32) whist[warp * 256 + x] = 0;
+      __syncwarp();
+#pragma unroll
+      for (int i = 0; i < ITEMS; i++)
+        if (dg[i] != INVALID_DIGIT) atomicAdd(&whist[warp * 256 + dg[i]], 1u);
+      __syncthreads();
+      // Per digit: the warps' exclusive starts, and the digit's total; then a scan over digits.
+      uint32_t tots[DPT];
+      uint32_t tot = 0;
+      if (threadIdx.x * DPT < 256) {
+#pragma unroll
+        for (int q = 0; q < DPT; q++) {
+          const int d = int(threadIdx.x) * DPT + q;
+          uint32_t run = 0;
+#pragma unroll
+          for (int w = 0; w < WARPS; w++) {
+            const uint32_t c = whist[w * 256 + d];
+            whist[w * 256 + d] = run;
+            run += c;
+          }
+          tots[q] = run;
+          tot += run;
+        }
+      }
+      uint32_t x = tot;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+      }
+      if (lane == 31) wsum[warp] = x;
+      __syncthreads();
+      uint32_t add = 0;
+      for (int w = 0; w < warp; w++) add += wsum[w];
+      if (threadIdx.x * DPT < 256) {
+        uint32_t at = x - tot + add;
+#pragma unroll
+        for (int q = 0; q < DPT; q++) {
+          local[int(threadIdx.x) * DPT + q] = at;
+          at += tots[q];
+        }
+      }
+      __syncthreads();
+      // Stable ranks: one ballot per digit bit; the warp's counters advance item by item.
+#pragma unroll
+      for (int i = 0; i < ITEMS; i++) {
+        const uint32_t d = dg[i];
+        uint32_t peers = __ballot_sync(0xffffffffu, d != INVALID_DIGIT);
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+          const uint32_t bit = (d >> k) & 1u;
+          const uint32_t bl = __ballot_sync(0xffffffffu, bit);
+          peers &= bit ? bl : ~bl;
+        }
+        uint32_t b0 = 0;
+        if (d != INVALID_DIGIT) b0 = whist[warp * 256 + d];
+        __syncwarp();
+        if (d != INVALID_DIGIT) {
+          if (lane == __ffs(peers) - 1) whist[warp * 256 + d] = b0 + __popc(peers);
+          const uint32_t p = local[d] + b0 + __popc(peers & lt);
+          skeys[p] = key[i];
+          sids[p] = id[i];
+        }
+        __syncwarp();
+      }
+      __syncthreads();
+      if (dgi + 1 < nloc) {
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++) {
+          const uint32_t r = uint32_t(warp) * (ITEMS * 32) + uint32_t(i) * 32 + lane;
+          if (r < size) {
+            key[i] = skeys[r];
+            id[i] = sids[r];
+          }
+        }
+        __syncthreads();
+      }
+    }
+    // The bucket's rows, in order, to their final places.
+    const uint64_t out0 = uint64_t(vbase) + start;
+    for (uint32_t r = threadIdx.x; r < size; r += THREADS) {
+      const uint64_t dst = out0 + r;
+      if (dst >= uint64_t(pa.desc->out_rows)) {
+        atomicOr(pa.err, ERR_BOUNDS);
+        continue;
+      }
+      if (pa.final_out) {
+        if (pa.desc->flags & PF_WIDE_OUT) static_cast<uint64_t*>(pa.final_out)[dst] = sids[r];
+        else static_cast<uint32_t*>(pa.final_out)[dst] = sids[r];
+      }
+      if (pa.key_out_mode == KEY_OUT_UNKEY)
+        store_width(pa.key_out, dst, pt_bytes(pa.key_out_pt), unkey_bits<uint64_t>(skeys[r], pa.key_out_pt, pa.key_desc));
+    }
+    __syncthreads();
+  }
+}
+
+template <int THREADS>
+constexpr size_t loc_smem_bytes() {
+  return size_t(THREADS) * LOC_ITEMS * 12 + size_t(THREADS / 32) * 256 * 4 + 256 * 4 + size_t(THREADS / 32) * 4;
+}
+
+// ------------------------------------------------------------------------------------------------
 // Host side.
 
 template <typename KeyT>
@@ -892,6 +1315,34 @@ static void launch_pass(const PassArgs& pa, const ColView& cv, uint64_t n, cudaS
   const int grid = int(std::min<uint64_t>(tiles, uint64_t(device().sm_count) * pass_blocks_per_sm<KeyT, StatusT>()));
   KernelTimer kt("radix_onesweep_pass", s);
   onesweep_pass_kernel<KeyT, StatusT, C::THREADS, C::ITEMS, false><<<std::max(grid, 1), C::THREADS, pass_smem<KeyT>(), s>>>(pa, cv);
+  AM_CUDA(cudaGetLastError());
+}
+
+// Zeroes a pass's look-back words, unless the pass is inactive (the hybrid's passes are decided on the
+// device, so a memset that always runs would clear the words for passes that never run).
+__global__ void __launch_bounds__(256) zero_status_kernel(const PassDesc* __restrict__ desc, uint4* __restrict__ words,
+                                                          uint64_t n16) {
+  if (!desc->active) return;
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n16; i += uint64_t(gridDim.x) * blockDim.x)
+    words[i] = make_uint4(0, 0, 0, 0);
+}
+
+// One local-sort shape as a persistent grid (it returns at once unless the decision chose it).
+template <int VARIANT>
+static void launch_local(const uint64_t* keys, const uint32_t* ids, const uint32_t* pos, const HybridState* hs,
+                         const PassArgs& a, cudaStream_t s) {
+  constexpr int THREADS = loc_threads(VARIANT);
+  constexpr size_t SMEM = loc_smem_bytes<THREADS>();
+  static int blocks = 0;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    auto fn = local_sort_kernel<THREADS, VARIANT>;
+    AM_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SMEM)));
+    int b = 0;
+    AM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, THREADS, SMEM));
+    blocks = std::max(1, b);
+  });
+  local_sort_kernel<THREADS, VARIANT><<<device().sm_count * blocks, THREADS, SMEM, s>>>(keys, ids, pos, hs, a);
   AM_CUDA(cudaGetLastError());
 }
 
@@ -1009,11 +1460,19 @@ void radix_sort(const std::vector<SortKey>& keys, int64_t n64, void* out, int in
 
   // Per-call scratch: stats, plans, pass descriptors, tickets, summary (one memset), then the
   // ping-pong key and id buffers.
+  // A single 8-byte key over at least 2^25 rows may take the two-level sort (the device decides).
+  const bool hybrid = K == 1 && pt_key_bytes(keys[0].col->pt) == 8 && n >= HYB_MIN_ROWS && n < (uint64_t(1) << 32);
+  const int NT = S + (hybrid ? HYB_STEPS : 0);          // tile counters: one per launched pass
+  const uint32_t bnd_blocks = uint32_t((n + BND_CHUNK - 1) / BND_CHUNK);
   const size_t off_stats = 0;
   const size_t off_kplan = off_stats + sizeof(KeyStats) * K;
   const size_t off_desc = (off_kplan + sizeof(KeyPlan) * K + 255) & ~size_t(255);
-  const size_t off_tick = off_desc + sizeof(PassDesc) * S;
-  const size_t off_sum = (off_tick + sizeof(uint32_t) * S + 15) & ~size_t(15);
+  const size_t off_steps = off_desc + sizeof(PassDesc) * S;
+  const size_t off_hs = (off_steps + (hybrid ? sizeof(PassDesc) * HYB_STEPS : 0) + 15) & ~size_t(15);
+  const size_t off_bcount = (off_hs + (hybrid ? sizeof(HybridState) : 0) + 15) & ~size_t(15);
+  const size_t off_bpos = off_bcount + (hybrid ? sizeof(uint32_t) * (bnd_blocks + 1) : 0);
+  const size_t off_tick = off_bpos + (hybrid ? sizeof(uint32_t) * 65537 : 0);
+  const size_t off_sum = (off_tick + sizeof(uint32_t) * NT + 15) & ~size_t(15);
   const size_t header = (off_sum + sizeof(SortSummary) + 255) & ~size_t(255);
   const size_t kbuf = ((n * max_kb) + 255) & ~size_t(255);
   const size_t ibuf = carry_ids ? ((n * 4) + 255) & ~size_t(255) : 0;
@@ -1024,6 +1483,10 @@ void radix_sort(const std::vector<SortKey>& keys, int64_t n64, void* out, int in
   PassDesc* pd = reinterpret_cast<PassDesc*>(base + off_desc);
   uint32_t* tick = reinterpret_cast<uint32_t*>(base + off_tick);
   SortSummary* sum = reinterpret_cast<SortSummary*>(base + off_sum);
+  PassDesc* steps = reinterpret_cast<PassDesc*>(base + off_steps);
+  HybridState* hs = reinterpret_cast<HybridState*>(base + off_hs);
+  uint32_t* bcount = reinterpret_cast<uint32_t*>(base + off_bcount);
+  uint32_t* bpos = reinterpret_cast<uint32_t*>(base + off_bpos);
   void* kbufA = base + header;
   void* kbufB = base + header + kbuf;
   uint32_t* ibufA = carry_ids ? reinterpret_cast<uint32_t*>(base + header + 2 * kbuf) : nullptr;
@@ -1044,8 +1507,8 @@ void radix_sort(const std::vector<SortKey>& keys, int64_t n64, void* out, int in
   if (debug_skip_first_tile()) {
     // Test hook: every pass's ticket starts at 1, so tile 0 is never processed and the look-back of
     // tile 1 runs into its time limit.
-    const std::vector<uint32_t> ones(size_t(S), 1u);
-    AM_CUDA(cudaMemcpyAsync(tick, ones.data(), sizeof(uint32_t) * S, cudaMemcpyHostToDevice, s));
+    const std::vector<uint32_t> ones(size_t(NT), 1u);
+    AM_CUDA(cudaMemcpyAsync(tick, ones.data(), sizeof(uint32_t) * NT, cudaMemcpyHostToDevice, s));
     AM_CUDA(cudaStreamSynchronize(s));
   }
 
@@ -1065,7 +1528,80 @@ void radix_sort(const std::vector<SortKey>& keys, int64_t n64, void* out, int in
   // Passes of fewer than 2^30 rows use 32-bit look-back words, zeroed before each pass.
   const bool narrow_status = n < (uint64_t(1) << 30);
   StreamScratch& sc = stream_scratch(s, size_t(max_tiles) * NBINS);
-  for (int sl = 0; sl < S; sl++) {
+  // The arguments every pass and the local sorts share.
+  auto args_for = [&](const PassDesc* desc, uint32_t* counter, const KeyPlan* plan) {
+    PassArgs a{};
+    a.desc = desc;
+    a.kplan = plan;
+    a.keys[0] = kbufA;
+    a.keys[1] = kbufB;
+    a.ids[0] = ibufA;
+    a.ids[1] = ibufB;
+    a.final_out = out;
+    a.status = sc.status;
+    a.tile_counter = counter;
+    a.err = sc.err;
+    a.carry_ids = carry_ids ? 1 : 0;
+    if (key_dst) {
+      a.key_out_mode = KEY_OUT_UNKEY;
+      a.key_out_pt = keys[0].col->pt;
+      a.key_desc = keys[0].descending ? 1 : 0;
+      a.key_float_order = keys[0].float_order;
+      a.key_out = key_dst->values->ptr;
+    }
+    return a;
+  };
+  auto launch_one = [&](const PassDesc* desc, uint32_t* counter, const KeyPlan* plan, const ColView& cv, int kb) {
+    if (narrow_status) {
+      const uint64_t bytes = uint64_t(max_tiles) * NBINS * sizeof(uint32_t);
+      const uint64_t n16 = (bytes + 15) / 16;
+      const int grid = int(std::min<uint64_t>((n16 + 255) / 256, uint64_t(device().sm_count) * 4));
+      zero_status_kernel<<<std::max(grid, 1), 256, 0, s>>>(desc, reinterpret_cast<uint4*>(sc.status), n16);
+      AM_CUDA(cudaGetLastError());
+    } else if (sc.epoch >= (1u << 30) - 1) {
+      AM_CUDA(cudaMemsetAsync(sc.status, 0, sc.status_words * sizeof(uint64_t), s));
+      sc.epoch = 0;
+    }
+    PassArgs a = args_for(desc, counter, plan);
+    a.epoch = ++sc.epoch;
+    if (kb == 8) {
+      if (narrow_status) launch_pass<uint64_t, uint32_t>(a, cv, n, s);
+      else launch_pass<uint64_t, uint64_t>(a, cv, n, s);
+    } else {
+      if (narrow_status) launch_pass<uint32_t, uint32_t>(a, cv, n, s);
+      else launch_pass<uint32_t, uint64_t>(a, cv, n, s);
+    }
+  };
+  if (hybrid) {
+    {
+      KernelTimer kt("radix_plan", s);
+      hybrid_plan_kernel<<<1, 256, 0, s>>>(pa, st, pd, steps, hs);
+      AM_CUDA(cudaGetLastError());
+    }
+    launch_one(steps + 0, tick + S + 0, kp, views[0], 8);
+    launch_one(steps + 1, tick + S + 1, kp, views[0], 8);
+    {
+      KernelTimer kt("radix_buckets", s);
+      const uint64_t* kb1 = static_cast<const uint64_t*>(kbufB);
+      bounds_count_kernel<<<bnd_blocks, BND_THREADS, 0, s>>>(kb1, hs, bcount);
+      AM_CUDA(cudaGetLastError());
+      bounds_scan_kernel<<<1, 1024, 0, s>>>(bcount, bnd_blocks, hs, bpos);
+      AM_CUDA(cudaGetLastError());
+      bounds_write_kernel<<<bnd_blocks, BND_THREADS, 0, s>>>(kb1, hs, bcount, bpos, sc.err);
+      AM_CUDA(cudaGetLastError());
+      bounds_decide_kernel<<<1, 1024, 0, s>>>(hs, bpos, steps, sum);
+      AM_CUDA(cudaGetLastError());
+    }
+    for (int i = 2; i < HYB_STEPS; i++) launch_one(steps + i, tick + S + i, kp, views[0], 8);
+    {
+      KernelTimer kt("radix_local_sort", s);
+      const PassArgs a = args_for(steps + 1, nullptr, kp);
+      launch_local<0>(static_cast<const uint64_t*>(kbufB), ibufB, bpos, hs, a, s);
+      launch_local<1>(static_cast<const uint64_t*>(kbufB), ibufB, bpos, hs, a, s);
+      launch_local<2>(static_cast<const uint64_t*>(kbufB), ibufB, bpos, hs, a, s);
+    }
+  }
+  for (int sl = 0; sl < S && !hybrid; sl++) {
     if (narrow_status) {
       AM_CUDA(cudaMemsetAsync(sc.status, 0, size_t(max_tiles) * NBINS * sizeof(uint32_t), s));
     } else if (sc.epoch >= (1u << 30) - 1) {

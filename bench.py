@@ -639,29 +639,37 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def algorithmic_bytes(n, m, passes):
+def algorithmic_bytes(n, m, passes, local_sort=False):
     """Bytes each kernel of one step must move once (the roofline's model, per step):
     - histogram: reads the key column (8 B a row) and its validity bitmap;
     - digit passes: the first reads the key column and bitmap again and writes the m value rows'
       (key, id) and the n - m null rows' id and zeroed key straight to their final places; a middle
       pass reads and writes m (key, id); the last reads m (key, id) and writes m ids and m rebuilt key
       values;
+    - local sorts (the two-level sort of one large key, after its two passes on the top digits): read
+      m (key, id) and write m ids and m rebuilt key values;
     - take: reads the n ids once and gathers and writes the two payload columns (8 + 4 B a row);
-    - sort_finish: writes the sorted key column's validity bitmap."""
+    - sort_finish: writes the sorted key column's validity bitmap.
+    The bucket-boundary kernels of the two-level sort move no compulsory bytes (like the plan)."""
     src = 8 * n + n / 8
     if passes <= 1:
         pass_bytes = src + 12 * n
     else:
         first = src + 12 * m + 12 * (n - m)
         pass_bytes = first + (passes - 2) * 24 * m + 24 * m
-    return {"radix_histogram": src, "radix_onesweep_pass": pass_bytes,
-            "take_gather": 4 * n + 2 * (8 + 4) * n, "sort_finish": n / 8}
+    out = {"radix_histogram": src, "radix_onesweep_pass": pass_bytes,
+           "take_gather": 4 * n + 2 * (8 + 4) * n, "sort_finish": n / 8}
+    if local_sort:
+        out["radix_local_sort"] = 24 * m
+    return out
 
 
 # DRAM bytes (read + write) per row of the workload, per kernel and step, from an ncu capture of this
-# benchmark at 25,000,000 rows (dram__bytes_read.sum + dram__bytes_write.sum summed over the kernel's
-# launches in one step, profiles/order_by_int64_25M_dram_traffic.md), scaled by rows.
-TRAFFIC_PER_ROW = {"radix_histogram": 8.17, "radix_onesweep_pass": 97.30, "take_gather": 146.13}
+# benchmark at 40,000,000 rows, where the two-level sort runs as at 50M (dram__bytes_read.sum +
+# dram__bytes_write.sum summed over the kernel's launches in one step,
+# profiles/order_by_int64_40M_dram_traffic.md), scaled by rows.
+TRAFFIC_PER_ROW = {"radix_histogram": 8.16, "radix_onesweep_pass": 41.67, "radix_local_sort": 19.32,
+                   "take_gather": 154.25}
 
 
 def traffic_per_step(kernel, n):
@@ -858,7 +866,9 @@ def main():
 
     # ---- roofline of the dominant kernel (the take's kernels count as one stage: their model bytes
     # are the take's, however the gather is organised)
-    model = algorithmic_bytes(n, m_rows, st["passes_run"])
+    # (the two-level sort: two passes, then the local sorts, when its timer ran and the stats count 2)
+    model = algorithmic_bytes(n, m_rows, st["passes_run"],
+                              local_sort=st["passes_run"] == 2 and "radix_local_sort" in prof)
     stages = {}
     for name, (launches, total_ms) in prof.items():
         stage = "take_gather" if name.startswith("take_") else name
