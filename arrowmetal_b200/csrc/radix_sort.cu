@@ -1153,19 +1153,23 @@ __global__ void __launch_bounds__(THREADS) local_sort_kernel(const uint64_t* __r
       key[i] = r < size ? keys[start + r] : 0ull;
       id[i] = r < size ? ids[start + r] : 0u;
     }
+    // The tile's empty slots (r >= size) are the last rows in order. They take digit 255 in the ballots
+    // but are neither counted nor stored: every row before them keeps its place in [0, size), and their
+    // own places come out at size or later.
+    uint32_t ok = 0;
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++)
+      if (uint32_t(warp) * (ITEMS * 32) + uint32_t(i) * 32 + lane < size) ok |= 1u << i;
     for (uint32_t dgi = 0; dgi < nloc; dgi++) {
       const uint32_t shift = hs->local_shift[dgi];
       uint32_t dg[ITEMS];
 #pragma unroll
-      for (int i = 0; i < ITEMS; i++) {
-        const uint32_t r = uint32_t(warp) * (ITEMS * 32) + uint32_t(i) * 32 + lane;
-        dg[i] = r < size ? (uint32_t(key[i] >> shift) & 255u) : INVALID_DIGIT;
-      }
+      for (int i = 0; i < ITEMS; i++) dg[i] = ((ok >> i) & 1u) ? (uint32_t(key[i] >> shift) & 255u) : 255u;
       for (int x = lane; x < 256; x += 32) whist[warp * 256 + x] = 0;
       __syncwarp();
 #pragma unroll
       for (int i = 0; i < ITEMS; i++)
-        if (dg[i] != INVALID_DIGIT) atomicAdd(&whist[warp * 256 + dg[i]], 1u);
+        if ((ok >> i) & 1u) atomicAdd(&whist[warp * 256 + dg[i]], 1u);
       __syncthreads();
       // Per digit: the warps' exclusive starts, and the digit's total; then a scan over digits.
       uint32_t tots[DPT];
@@ -1208,35 +1212,35 @@ __global__ void __launch_bounds__(THREADS) local_sort_kernel(const uint64_t* __r
 #pragma unroll
       for (int i = 0; i < ITEMS; i++) {
         const uint32_t d = dg[i];
-        uint32_t peers = __ballot_sync(0xffffffffu, d != INVALID_DIGIT);
+        uint32_t peers = 0xffffffffu;
 #pragma unroll
         for (int k = 0; k < 8; k++) {
           const uint32_t bit = (d >> k) & 1u;
           const uint32_t bl = __ballot_sync(0xffffffffu, bit);
           peers &= bit ? bl : ~bl;
         }
-        uint32_t b0 = 0;
-        if (d != INVALID_DIGIT) b0 = whist[warp * 256 + d];
+        const uint32_t b0 = whist[warp * 256 + d];
         __syncwarp();
-        if (d != INVALID_DIGIT) {
-          if (lane == __ffs(peers) - 1) whist[warp * 256 + d] = b0 + __popc(peers);
-          const uint32_t p = local[d] + b0 + __popc(peers & lt);
+        if (lane == __ffs(peers) - 1) whist[warp * 256 + d] = b0 + __popc(peers);
+        const uint32_t p = local[d] + b0 + __popc(peers & lt);
+        if (p < size) {
           skeys[p] = key[i];
           sids[p] = id[i];
         }
         __syncwarp();
       }
       __syncthreads();
+      // The next digit's rows, back from the tile. No barrier after: the tile is next written after
+      // the next digit's histogram barrier, which every warp reaches only once it has read its rows.
       if (dgi + 1 < nloc) {
 #pragma unroll
         for (int i = 0; i < ITEMS; i++) {
           const uint32_t r = uint32_t(warp) * (ITEMS * 32) + uint32_t(i) * 32 + lane;
-          if (r < size) {
+          if ((ok >> i) & 1u) {
             key[i] = skeys[r];
             id[i] = sids[r];
           }
         }
-        __syncthreads();
       }
     }
     // The bucket's rows, in order, to their final places.
@@ -1254,7 +1258,7 @@ __global__ void __launch_bounds__(THREADS) local_sort_kernel(const uint64_t* __r
       if (pa.key_out_mode == KEY_OUT_UNKEY)
         store_width(pa.key_out, dst, pt_bytes(pa.key_out_pt), unkey_bits<uint64_t>(skeys[r], pa.key_out_pt, pa.key_desc));
     }
-    __syncthreads();
+    // No barrier here either: the next bucket writes the tile only after its first histogram barrier.
   }
 }
 
