@@ -168,17 +168,13 @@ __global__ void __launch_bounds__(256) take_kernel(const __grid_constant__ TakeA
 
 // ---- row records
 
-// Each thread packs four rows of a block's 4 x 256 consecutive rows, their loads in flight together.
+// Each thread packs H rows of a block's H x 256 consecutive rows, their loads in flight together.
 template <int W>
 __global__ void __launch_bounds__(256) pack_records_kernel(const __grid_constant__ RecArgs r) {
-  const uint64_t step = uint64_t(gridDim.x) * 1024;
-  for (uint64_t base = uint64_t(blockIdx.x) * 1024; base < r.n; base += step) {
-#pragma unroll
-    for (int h = 0; h < 4; h++) {
-      const uint64_t j = base + uint64_t(h) * 256 + threadIdx.x;
-      if (j < r.n) pack_record<W>(r, j);
-    }
-  }
+  constexpr int H = pack_rows_per_thread(W);
+  const uint64_t step = uint64_t(gridDim.x) * (256 * H);
+  for (uint64_t base = uint64_t(blockIdx.x) * (256 * H); base < r.n; base += step)
+    pack_records_rows<W, H>(r, base + threadIdx.x);
 }
 
 template <int W>
@@ -380,7 +376,8 @@ static void take_through_records(const tk::TakeArgs& a, int rec_w, cudaStream_t 
   RecArgs r{};
   layout_records(a, r);
   r.rec = dmalloc(size_t(a.src_len) * size_t(rec_w), s);
-  const int pack_grid = int(std::min<uint64_t>((a.src_len + 1023) / 1024, uint64_t(device().sm_count) * 16));
+  const uint64_t pack_chunk = 256 * uint64_t(pack_rows_per_thread(rec_w));
+  const int pack_grid = int(std::min<uint64_t>((a.src_len + pack_chunk - 1) / pack_chunk, uint64_t(device().sm_count) * 16));
   const uint64_t chunks = (a.n + 127) / 128;
   const int grid = int(std::min<uint64_t>((chunks + 7) / 8, uint64_t(device().sm_count) * 8));
   {

@@ -54,46 +54,97 @@ struct RecArgs {
 #ifdef __CUDACC__
 __device__ __forceinline__ bool rec_bit(const uint8_t* p, int64_t i) { return (p[i >> 3] >> (i & 7)) & 1; }
 
-// Column c's value of row j, zero-extended (booleans as 0/1).
-__device__ __forceinline__ uint64_t record_value(const RecArgs& r, int c, uint64_t j) {
-  switch (r.width[c]) {
-    case 8: return static_cast<const uint64_t*>(r.src[c])[j];
-    case 4: return static_cast<const uint32_t*>(r.src[c])[j];
-    case 2: return static_cast<const uint16_t*>(r.src[c])[j];
-    case 1: return static_cast<const uint8_t*>(r.src[c])[j];
-    default: return rec_bit(static_cast<const uint8_t*>(r.src[c]), r.src_bit_off[c] + int64_t(j)) ? 1u : 0u;
-  }
-}
+// Rows a thread packs per grid-stride step, 256 rows apart: a W-byte record per row.
+__host__ __device__ constexpr int pack_rows_per_thread(int w) { return w == 8 ? 8 : 4; }
 
-// Row j's W-byte record: every column's value at its offset and the validity byte.
-template <int W>
-__device__ __forceinline__ void pack_record(const RecArgs& r, uint64_t j) {
+// Records of rows j0, j0 + 256, ..., j0 + 256 (H - 1): every column's value at its offset and the
+// validity byte. All H rows of a column are loaded before anything is stored, so each thread keeps H
+// loads in flight: a store between rows would order the next row's loads after it (the record buffer
+// is not known to be apart from the columns), one DRAM round trip per row.
+template <int W, int H>
+__device__ __forceinline__ void pack_records_rows(const RecArgs& r, uint64_t j0) {
   constexpr int WORDS = W / 8;
-  uint64_t w[WORDS];
+  uint64_t w[H][WORDS];
+  uint32_t valid[H];
+  bool in[H];
 #pragma unroll
-  for (int k = 0; k < WORDS; k++) w[k] = 0;
-  uint32_t valid = 0;
+  for (int h = 0; h < H; h++) {
+    in[h] = j0 + uint64_t(h) * 256 < r.n;
+    valid[h] = 0;
 #pragma unroll
+    for (int k = 0; k < WORDS; k++) w[h][k] = 0;
+  }
+#pragma unroll 1
   for (int c = 0; c < kMaxTakeCols; c++) {
     if (c >= r.ncols) break;
-    const uint64_t v = record_value(r, c, j);
-    const int o = r.rec_off[c];
+    uint64_t v[H];
+    switch (r.width[c]) {
+      case 8: {
+        const uint64_t* src = static_cast<const uint64_t*>(r.src[c]);
 #pragma unroll
-    for (int k = 0; k < WORDS; k++)
-      if ((o >> 3) == k) w[k] |= v << (8 * (o & 7));
-    if (!r.src_valid[c] || rec_bit(r.src_valid[c], r.src_voff[c] + int64_t(j))) valid |= 1u << c;
+        for (int h = 0; h < H; h++) v[h] = in[h] ? src[j0 + uint64_t(h) * 256] : 0;
+        break;
+      }
+      case 4: {
+        const uint32_t* src = static_cast<const uint32_t*>(r.src[c]);
+#pragma unroll
+        for (int h = 0; h < H; h++) v[h] = in[h] ? src[j0 + uint64_t(h) * 256] : 0;
+        break;
+      }
+      case 2: {
+        const uint16_t* src = static_cast<const uint16_t*>(r.src[c]);
+#pragma unroll
+        for (int h = 0; h < H; h++) v[h] = in[h] ? src[j0 + uint64_t(h) * 256] : 0;
+        break;
+      }
+      case 1: {
+        const uint8_t* src = static_cast<const uint8_t*>(r.src[c]);
+#pragma unroll
+        for (int h = 0; h < H; h++) v[h] = in[h] ? src[j0 + uint64_t(h) * 256] : 0;
+        break;
+      }
+      default: {   // boolean: bit-packed values, a 0/1 byte in the record
+        const uint8_t* src = static_cast<const uint8_t*>(r.src[c]);
+#pragma unroll
+        for (int h = 0; h < H; h++)
+          v[h] = (in[h] && rec_bit(src, r.src_bit_off[c] + int64_t(j0 + uint64_t(h) * 256))) ? 1u : 0u;
+        break;
+      }
+    }
+    const int o = r.rec_off[c];
+    const uint8_t* vb = r.src_valid[c];
+    // Word masks instead of a branch per word: the record stays in registers.
+    uint64_t wm[WORDS];
+#pragma unroll
+    for (int k = 0; k < WORDS; k++) wm[k] = uint64_t(0) - uint64_t((o >> 3) == k);
+#pragma unroll
+    for (int h = 0; h < H; h++) {
+      const uint64_t sh = v[h] << (8 * (o & 7));
+#pragma unroll
+      for (int k = 0; k < WORDS; k++) w[h][k] |= sh & wm[k];
+      if (!vb || (in[h] && rec_bit(vb, r.src_voff[c] + int64_t(j0 + uint64_t(h) * 256)))) valid[h] |= 1u << c;
+    }
   }
   if (r.valid_off >= 0) {
+    uint64_t wm[WORDS];
 #pragma unroll
-    for (int k = 0; k < WORDS; k++)
-      if ((r.valid_off >> 3) == k) w[k] |= uint64_t(valid) << (8 * (r.valid_off & 7));
+    for (int k = 0; k < WORDS; k++) wm[k] = uint64_t(0) - uint64_t((r.valid_off >> 3) == k);
+#pragma unroll
+    for (int h = 0; h < H; h++)
+#pragma unroll
+      for (int k = 0; k < WORDS; k++) w[h][k] |= (uint64_t(valid[h]) << (8 * (r.valid_off & 7))) & wm[k];
   }
-  uint64_t* dst = static_cast<uint64_t*>(r.rec) + j * WORDS;
-  if constexpr (WORDS == 1) {
-    dst[0] = w[0];
-  } else {
+  uint64_t* rec = static_cast<uint64_t*>(r.rec);
 #pragma unroll
-    for (int k = 0; k < WORDS; k += 2) reinterpret_cast<ulonglong2*>(dst)[k / 2] = make_ulonglong2(w[k], w[k + 1]);
+  for (int h = 0; h < H; h++) {
+    if (!in[h]) continue;
+    uint64_t* dst = rec + (j0 + uint64_t(h) * 256) * WORDS;
+    if constexpr (WORDS == 1) {
+      dst[0] = w[h][0];
+    } else {
+#pragma unroll
+      for (int k = 0; k < WORDS; k += 2) reinterpret_cast<ulonglong2*>(dst)[k / 2] = make_ulonglong2(w[h][k], w[h][k + 1]);
+    }
   }
 }
 #endif
