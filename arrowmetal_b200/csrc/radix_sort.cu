@@ -622,17 +622,28 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
         dg[i] = ((ok >> i) & 1u) ? ((is_null != bool(col.nulls_first)) ? 1u : 0u) : INVALID_DIGIT;
       }
     } else if (flags & PF_ENCODE) {
-      int cat[ITEMS];
-      encode_rows<KeyT, ITEMS>(col, id, ok, key, cat);
+      // Raw values and validity bytes loaded together; then each row's key, category and digit in one
+      // step, so only one row's category is live at a time.
+      KeyT raw[ITEMS];
+      uint32_t vb[ITEMS];
+      load_raw_rows<KeyT, ITEMS>(col, id, ok, raw);
+      if (col.valid) {
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++) vb[i] = ((ok >> i) & 1u) ? col.valid[(col.valid_off + int64_t(id[i])) >> 3] : 0u;
+      }
 #pragma unroll
       for (int i = 0; i < ITEMS; i++) {
-        if (cat[i] && (flags & PF_ROUTE)) {
-          dg[i] = (cat[i] == 1) ? uint32_t(NAN_BIN) : uint32_t(NULL_BIN);
+        const bool valid = !col.valid || ((vb[i] >> ((col.valid_off + int64_t(id[i])) & 7)) & 1u);
+        int cat;
+        KeyT k = key_from_raw<KeyT>(col, raw[i], valid, cat);
+        if (cat && (flags & PF_ROUTE)) {
+          dg[i] = (cat == 1) ? uint32_t(NAN_BIN) : uint32_t(NULL_BIN);
         } else {
-          if (cat[i]) key[i] = kplan.fold_mode ? KeyT(0) : KeyT(cat[i] == 1 ? kplan.fold_nan : kplan.fold_null);
-          dg[i] = uint32_t(key[i] >> shift) & 255u;
+          if (cat) k = kplan.fold_mode ? KeyT(0) : KeyT(cat == 1 ? kplan.fold_nan : kplan.fold_null);
+          dg[i] = uint32_t(k >> shift) & 255u;
         }
         if (!((ok >> i) & 1u)) dg[i] = INVALID_DIGIT;
+        key[i] = k;
       }
     } else {
 #pragma unroll
@@ -672,7 +683,6 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
     // independent, and only the warp's running digit counters advance item by item.
     {
       const int nbits = (flags & PF_ROUTE) ? 9 : 8;
-      uint32_t peers_of[ITEMS];
 #pragma unroll
       for (int i = 0; i < ITEMS; i++) {
         const uint32_t d = dg[i];
@@ -685,12 +695,6 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
             peers &= bit ? bl : ~bl;
           }
         }
-        peers_of[i] = peers;
-      }
-#pragma unroll
-      for (int i = 0; i < ITEMS; i++) {
-        const uint32_t d = dg[i];
-        const uint32_t peers = peers_of[i];
         uint32_t base = 0;
         if (d != INVALID_DIGIT) base = sm.whist[warp][d];
         __syncwarp();

@@ -181,3 +181,28 @@ def test_take_two_columns_through_16_byte_records(am):
     o1, o2 = am.take_columns(handles, idx)
     assert np.array_equal(o1.to_arrow().to_numpy().view(np.uint64), p1.view(np.uint64)[ii])
     assert np.array_equal(o2.to_arrow().to_numpy(), p2[ii])
+
+
+def test_take_columns_through_8_byte_records(am):
+    # int32 (nulls) + uint16 + boolean (nulls): 7 bytes and a validity byte, 8-byte row records. The
+    # row count is not a multiple of the pack's row groups, so the last group is partial.
+    rng = np.random.default_rng(17)
+    n = 40_000_003
+    cols = [pa.array(rng.integers(-2**31, 2**31 - 1, n, dtype=np.int32), mask=rng.random(n) < 0.2),
+            pa.array(rng.integers(0, 2**16, n).astype(np.uint16)),
+            pa.array(rng.random(n) < 0.5, mask=rng.random(n) < 0.05)]
+    handles = [am.MetalArray.from_arrow(c) for c in cols]
+    idx = am.MetalArray.from_arrow(pa.array(rng.integers(0, 2**40, n))).argsort()
+    ii = pa.array(idx.to_arrow().to_numpy())
+    am.profile(True)
+    am.profile_reset()
+    try:
+        outs = am.take_columns(handles, idx)
+        assert am.profile_entries()["take_pack_records"][0] == 1      # the row-record form ran
+    finally:
+        am.profile(False)
+    for c, o in zip(cols, outs):
+        got = o.to_arrow()
+        want = pc.take(c, ii)
+        assert got.null_count == want.null_count
+        assert got.equals(want)
