@@ -679,8 +679,9 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
     __syncthreads();
 
     // ---- warp ranking and staging: each row goes to its tile-local sorted slot. The rows of a lane's
-    // item that share its digit come from one ballot per digit bit; the ballots of different items are
-    // independent, and only the warp's running digit counters advance item by item.
+    // item that share its digit come from one ballot per digit bit, and the item is placed right after
+    // its ballots: holding every item's peer mask first overlaps more ballots but pushes the 8-byte
+    // key's pass past its 80 registers into spills, which measured slower.
     {
       const int nbits = (flags & PF_ROUTE) ? 9 : 8;
 #pragma unroll
