@@ -1127,7 +1127,7 @@ __global__ void __launch_bounds__(1024) bounds_decide_kernel(HybridState* __rest
 // shared memory, then written to its final rows (ids, and the key column rebuilt when asked). A
 // persistent grid of CTAs walks the buckets; a shape that is not the chosen one returns at once.
 template <int THREADS, int VARIANT>
-__global__ void __launch_bounds__(THREADS) local_sort_kernel(const uint64_t* __restrict__ keys,
+__global__ void __launch_bounds__(THREADS, THREADS == 128 ? 10 : THREADS == 256 ? 5 : 2) local_sort_kernel(const uint64_t* __restrict__ keys,
                                                              const uint32_t* __restrict__ ids,
                                                              const uint32_t* __restrict__ pos,
                                                              const HybridState* __restrict__ hs,
