@@ -664,11 +664,12 @@ def algorithmic_bytes(n, m, passes, local_sort=False):
     return out
 
 
-# DRAM bytes (read + write) per row of the workload, per kernel and step, from an ncu capture of this
+# DRAM bytes (read + write) per row of the workload, per kernel and step, from ncu captures of this
 # benchmark at 40,000,000 rows, where the two-level sort runs as at 50M (dram__bytes_read.sum +
 # dram__bytes_write.sum summed over the kernel's launches in one step,
-# profiles/order_by_int64_40M_dram_traffic.md), scaled by rows.
-TRAFFIC_PER_ROW = {"radix_histogram": 8.16, "radix_onesweep_pass": 41.67, "radix_local_sort": 19.32,
+# profiles/order_by_int64_40M_dram_traffic.md; the digit passes from
+# profiles/onesweep_pass_order_by_40M_full.md), scaled by rows.
+TRAFFIC_PER_ROW = {"radix_histogram": 8.16, "radix_onesweep_pass": 39.79, "radix_local_sort": 19.32,
                    "take_gather": 154.25}
 
 
