@@ -1016,16 +1016,24 @@ __global__ void __launch_bounds__(BND_THREADS) bounds_count_kernel(const uint64_
 // One block: exclusive scan of the block counts in place; the bucket count and the end sentinel.
 __global__ void __launch_bounds__(1024) bounds_scan_kernel(uint32_t* __restrict__ counts, uint32_t blocks,
                                                            HybridState* __restrict__ hs, uint32_t* __restrict__ pos) {
+  // Each thread scans K consecutive counts, all loaded before any is used (one round trip per 16K
+  // counts instead of one per 1,024).
+  constexpr int K = 16;
   __shared__ uint32_t s[32];
   __shared__ uint32_t carry;
   if (!hs->mode) return;
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   if (t == 0) carry = 0;
   __syncthreads();
-  for (uint32_t b0 = 0; b0 < blocks; b0 += 1024) {
-    const uint32_t i = b0 + uint32_t(t);
-    const uint32_t v = i < blocks ? counts[i] : 0u;
-    uint32_t x = v;
+  for (uint32_t b0 = 0; b0 < blocks; b0 += 1024u * K) {
+    const uint32_t i0 = b0 + uint32_t(t) * K;
+    uint32_t v[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) v[k] = i0 + k < blocks ? counts[i0 + k] : 0u;
+    uint32_t sum = 0;
+#pragma unroll
+    for (int k = 0; k < K; k++) sum += v[k];
+    uint32_t x = sum;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
@@ -1038,7 +1046,12 @@ __global__ void __launch_bounds__(1024) bounds_scan_kernel(uint32_t* __restrict_
       if (w < warp) add += s[w];
       all += s[w];
     }
-    if (i < blocks) counts[i] = x - v + add;
+    uint32_t run = x - sum + add;
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      if (i0 + k < blocks) counts[i0 + k] = run;
+      run += v[k];
+    }
     __syncthreads();
     if (t == 0) carry += all;
     __syncthreads();
@@ -1102,8 +1115,19 @@ __global__ void __launch_bounds__(1024) bounds_decide_kernel(HybridState* __rest
   // The rows are grouped by a 16-bit bucket, so there are at most 65,536 starts; anything else takes
   // the passes.
   const uint32_t g = hs->buckets <= 65536u ? hs->buckets : 0u;
+  // 16 bucket sizes a thread per round trip; j < g <= 65,536 keeps pos[j + 1] within its 65,537 entries.
   uint32_t mx = 0;
-  for (uint32_t j = threadIdx.x; j < g; j += blockDim.x) mx = max(mx, pos[j + 1] - pos[j]);
+  for (uint32_t j0 = 0; j0 < g; j0 += 16u * blockDim.x) {
+    uint32_t a[16], b[16];
+#pragma unroll
+    for (int u = 0; u < 16; u++) {
+      const uint32_t j = j0 + uint32_t(u) * blockDim.x + threadIdx.x;
+      a[u] = j < g ? pos[j] : 0u;
+      b[u] = j < g ? pos[j + 1] : 0u;
+    }
+#pragma unroll
+    for (int u = 0; u < 16; u++) mx = max(mx, b[u] - a[u]);
+  }
   mx = __reduce_max_sync(0xffffffffu, mx);
   if ((threadIdx.x & 31) == 0) atomicMax(&s_max, mx);
   __syncthreads();
