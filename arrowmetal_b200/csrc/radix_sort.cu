@@ -1189,6 +1189,10 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? 10 : THREADS == 256 
 #pragma unroll
     for (int i = 0; i < ITEMS; i++)
       if (uint32_t(warp) * (ITEMS * 32) + uint32_t(i) * 32 + lane < size) ok |= 1u << i;
+    // Items of this warp holding any row (the same for all its lanes): the ranking skips the others,
+    // whose slots are all empty and all after every row.
+    const uint32_t w_first = uint32_t(warp) * (ITEMS * 32);
+    const int nit = size > w_first ? int(min(uint32_t(ITEMS), (size - w_first + 31) / 32)) : 0;
     for (uint32_t dgi = 0; dgi < nloc; dgi++) {
       const uint32_t shift = hs->local_shift[dgi];
       uint32_t dg[ITEMS];
@@ -1240,6 +1244,7 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? 10 : THREADS == 256 
       // Stable ranks: one ballot per digit bit; the warp's counters advance item by item.
 #pragma unroll
       for (int i = 0; i < ITEMS; i++) {
+        if (i >= nit) break;
         const uint32_t d = dg[i];
         uint32_t peers = 0xffffffffu;
 #pragma unroll
