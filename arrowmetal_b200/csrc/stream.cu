@@ -799,6 +799,39 @@ void release_ipc_batch(ArrowArray* a) {
   a->release = nullptr;
 }
 
+// A column of an IPC record batch must fit its buffers before anything reads it (on the host, or on
+// the device after its import): the bitmap and the values cover `length` rows, and the offsets of a
+// string or binary column rise from 0 or more to at most the size of its data buffer.
+void check_ipc_buffers(int pt, int64_t length, int64_t null_count, const uint64_t (&lens)[3],
+                       const void* const* bufs) {
+  const uint64_t n = uint64_t(length);
+  if (n == 0) return;
+  const uint64_t bitmap = (n + 7) / 8;
+  if (lens[0] != 0 && lens[0] < bitmap) throw invalid("an IPC validity bitmap shorter than its column");
+  if (null_count > 0 && lens[0] == 0) throw invalid("an IPC column with nulls and no validity bitmap");
+  if (!pt_var(pt)) {
+    const uint64_t need = pt == PT_BOOL ? bitmap : n * uint64_t(pt_bytes(pt));
+    if (lens[1] < need) throw invalid("an IPC values buffer shorter than its column");
+    return;
+  }
+  const uint64_t ow = uint64_t(pt_bytes(pt));
+  if (lens[1] < (n + 1) * ow) throw invalid("an IPC offsets buffer shorter than its column");
+  int64_t prev = 0;
+  for (uint64_t i = 0; i <= n; i++) {
+    int64_t o;
+    if (ow == 4) {
+      int32_t v;
+      std::memcpy(&v, static_cast<const uint8_t*>(bufs[1]) + 4 * i, 4);
+      o = v;
+    } else {
+      std::memcpy(&o, static_cast<const uint8_t*>(bufs[1]) + 8 * i, 8);
+    }
+    if (o < (i == 0 ? 0 : prev)) throw invalid("IPC string offsets that are negative or decreasing");
+    prev = o;
+  }
+  if (uint64_t(prev) > lens[2]) throw invalid("IPC string offsets past the end of their data");
+}
+
 struct IpcSource {
   std::vector<std::string> files;
   size_t file = 0;
@@ -807,6 +840,7 @@ struct IpcSource {
   bool have_schema = false;
   std::vector<std::string> names, formats;
   std::vector<int> nbuf;          // buffers per column
+  std::vector<int> pts;           // physical type per column
   std::string error;
   std::vector<std::string> owned_strings;   // schema strings handed out
 
@@ -883,14 +917,15 @@ struct IpcSource {
     if (!sch) throw invalid(path + ": an Arrow IPC schema message without a schema");
     const auto fv = r.vec(sch, 1);
     std::vector<std::string> nm, fm;
-    std::vector<int> nb;
+    std::vector<int> nb, pt;
     for (uint32_t i = 0; i < fv.second; i++) {
       const size_t f = r.deref(fv.first + 4 * size_t(i));
       if (r.field(f, 4)) throw unsupported("dictionary-encoded columns in an Arrow IPC file");
       if (r.vec(f, 5).second != 0) throw unsupported("nested columns in an Arrow IPC file");
       nm.push_back(r.string(f, 0));
       fm.push_back(ipc_format(r, f));
-      nb.push_back(pt_var(parse_format(fm.back().c_str())) ? 3 : 2);
+      pt.push_back(parse_format(fm.back().c_str()));
+      nb.push_back(pt_var(pt.back()) ? 3 : 2);
     }
     if (have_schema) {
       if (nm != names || fm != formats) throw invalid(path + ": its schema differs from the first file's");
@@ -899,6 +934,7 @@ struct IpcSource {
     names = nm;
     formats = fm;
     nbuf = nb;
+    pts = pt;
     have_schema = true;
   }
   // The next record batch, or false at the end of the last file.
@@ -919,6 +955,7 @@ struct IpcSource {
       if (!rb) throw invalid("a record batch message without its batch");
       if (r.field(rb, 3)) throw unsupported("compressed Arrow IPC bodies (write them uncompressed)");
       const int64_t length = r.scalar<int64_t>(rb, 0, 0);
+      if (length < 0) throw invalid("an IPC record batch of negative length");
       const auto nodes = r.vec(rb, 1);
       const auto bufs = r.vec(rb, 2);
       if (nodes.second != names.size()) throw invalid("a record batch with the wrong number of columns");
@@ -934,13 +971,19 @@ struct IpcSource {
           a.length = r.get<int64_t>(nodes.first + 16 * c);
           a.null_count = r.get<int64_t>(nodes.first + 16 * c + 8);
           a.n_buffers = nbuf[c];
+          if (a.length != length || a.null_count < 0 || a.null_count > a.length)
+            throw invalid("an IPC column whose length or null count does not fit its record batch");
+          uint64_t lens[3] = {0, 0, 0};
           for (int k = 0; k < nbuf[c]; k++, bi++) {
             if (bi >= bufs.second) throw invalid("a record batch with too few buffers");
             const int64_t off = r.get<int64_t>(bufs.first + 16 * bi);
             const int64_t len = r.get<int64_t>(bufs.first + 16 * bi + 8);
-            if (off < 0 || len < 0 || size_t(off + len) > body_len) throw invalid("an IPC buffer outside its body");
+            if (off < 0 || len < 0 || uint64_t(off) > body_len || uint64_t(len) > body_len - uint64_t(off))
+              throw invalid("an IPC buffer outside its body");
+            lens[k] = uint64_t(len);
             b->buffers[c].push_back(len > 0 ? map->data + body + size_t(off) : nullptr);
           }
+          check_ipc_buffers(pts[c], a.length, a.null_count, lens, b->buffers[c].data());
           a.buffers = b->buffers[c].data();
           a.release = [](ArrowArray* x) { x->release = nullptr; };   // the parent owns the memory
           b->child_ptrs.push_back(&a);

@@ -80,3 +80,87 @@ def test_ipc_errors(tmp_path):
         w.write_table(pa.table({"x": np.arange(1000)}))
     with pytest.raises(Exception, match="compressed"):
         am.scan_ipc(c).to_reader().read_all()
+
+
+# ---- malformed files: every column must fit its buffers before anything reads it
+
+# A malformed batch surfaces as the stream's error: an ArrowMetalError, or pyarrow's OSError when
+# pyarrow reads the exported C stream.
+
+def messages_of(path):
+    """(metadata bytes, body bytes) of each message of an IPC stream file."""
+    reader = pa.ipc.MessageReader.open_stream(pa.OSFile(str(path)))
+    out = []
+    for m in reader:
+        out.append((bytearray(m.metadata.to_pybytes()), bytearray(m.body.to_pybytes() if m.body else b"")))
+    return out
+
+
+def write_messages(path, msgs):
+    import struct
+    with open(path, "wb") as f:
+        for meta, body in msgs:
+            f.write(b"\xff\xff\xff\xff" + struct.pack("<i", len(meta)) + bytes(meta) + bytes(body))
+        f.write(b"\xff\xff\xff\xff\x00\x00\x00\x00")
+
+
+def patch_int64(buf, old, new, count=None):
+    import struct
+    pat, rep = struct.pack("<q", old), struct.pack("<q", new)
+    hits = [i for i in range(len(buf) - 7) if buf[i:i + 8] == pat]
+    if count is not None:
+        assert len(hits) == count, hits
+    for i in hits:
+        buf[i:i + 8] = rep
+    return len(hits)
+
+
+def test_ipc_rows_past_their_buffers(tmp_path):
+    src = tmp_path / "ok.arrows"
+    write_stream(src, pa.table({"x": np.arange(1000, dtype=np.int64) * 7}), 1000)
+    msgs = messages_of(src)
+    assert patch_int64(msgs[1][0], 1000, 10**9) >= 2          # the batch's length and its column's
+    bad = tmp_path / "rows.arrows"
+    write_messages(bad, msgs)
+    with pytest.raises((am.ArrowMetalError, OSError), match="values buffer shorter"):
+        am.scan_ipc(bad).to_reader().read_all()
+
+
+def test_ipc_nulls_without_a_bitmap(tmp_path):
+    src = tmp_path / "ok.arrows"
+    write_stream(src, pa.table({"x": np.arange(1000, dtype=np.int64)}), 1000)
+    msgs = messages_of(src)
+    import struct
+    meta = msgs[1][0]
+    node = struct.pack("<qq", 1000, 0)
+    at = bytes(meta).find(node)
+    assert at >= 0
+    meta[at + 8:at + 16] = struct.pack("<q", 5)
+    bad = tmp_path / "nulls.arrows"
+    write_messages(bad, msgs)
+    with pytest.raises((am.ArrowMetalError, OSError), match="nulls and no validity bitmap"):
+        am.scan_ipc(bad).to_reader().read_all()
+
+
+@pytest.mark.parametrize("corrupt,message", [("past_end", "past the end"), ("decreasing", "negative or decreasing")])
+def test_ipc_string_offsets_checked(tmp_path, corrupt, message):
+    n = 100
+    vals = ["v%03d" % i for i in range(n)]                     # 4 bytes each, no nulls
+    src = tmp_path / "ok.arrows"
+    write_stream(src, pa.table({"s": pa.array(vals)}), n)
+    msgs = messages_of(src)
+    body = msgs[1][1]
+    offs = np.frombuffer(bytes(body[:4 * (n + 1)]), dtype=np.int32).copy()
+    assert offs[0] == 0 and offs[-1] == 4 * n                  # the offsets lead the body (no bitmap)
+    if corrupt == "past_end":
+        offs[-1] = 4 * n + 10_000
+    else:
+        offs[50] = offs[49] - 1
+    body[:4 * (n + 1)] = offs.tobytes()
+    bad = tmp_path / "offsets.arrows"
+    write_messages(bad, msgs)
+    with pytest.raises((am.ArrowMetalError, OSError), match=message):
+        am.scan_ipc(bad).to_reader().read_all()
+    # The same file unpatched still reads back.
+    write_messages(tmp_path / "again.arrows", messages_of(src))
+    assert am.scan_ipc(tmp_path / "again.arrows").to_reader().read_all().equals(pa.table({"s": pa.array(vals)}))
