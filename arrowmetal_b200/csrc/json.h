@@ -1,5 +1,7 @@
 // A small JSON reader for the plan engine: objects, arrays, strings (with escapes), numbers, true,
-// false and null. Throws am::Error with the byte offset of the first problem.
+// false and null. Throws am::Error with the byte offset of the first problem. Objects and arrays nest
+// at most kMaxDepth deep: the reader (and the plan walk after it) recurses once a level, and a deeper
+// input would overflow the calling thread's stack instead of failing.
 #pragma once
 
 #include <cstdlib>
@@ -29,6 +31,8 @@ struct Value {
   bool is_null() const { return kind == Null; }
 };
 
+constexpr int kMaxDepth = 512;
+
 class Parser {
  public:
   explicit Parser(const std::string& s) : s_(s) {}
@@ -42,6 +46,14 @@ class Parser {
  private:
   const std::string& s_;
   size_t i_ = 0;
+  int depth_ = 0;
+  struct Level {
+    Parser& p;
+    explicit Level(Parser& q) : p(q) {
+      if (++p.depth_ > kMaxDepth) p.fail("nested more than " + std::to_string(kMaxDepth) + " levels deep");
+    }
+    ~Level() { p.depth_--; }
+  };
   [[noreturn]] void fail(const std::string& m) {
     throw invalid("plan: JSON " + m + " at byte " + std::to_string(i_));
   }
@@ -59,6 +71,7 @@ class Parser {
     Value v;
     char c = s_[i_];
     if (c == '{') {
+      const Level level(*this);
       v.kind = Value::Object;
       i_++;
       ws();
@@ -78,6 +91,7 @@ class Parser {
       }
     }
     if (c == '[') {
+      const Level level(*this);
       v.kind = Value::Array;
       i_++;
       ws();

@@ -97,6 +97,36 @@ def test_plan_errors_without_a_device(lib):
     assert b"unknown source" in lib.am_last_error()
 
 
+def test_plan_json_nesting_and_mutations_fail_cleanly(lib):
+    # Deep nesting is refused before it can overflow the caller's stack, and mangled plans (truncated,
+    # bytes replaced or inserted) return an error instead of crashing.
+    import random
+    lib.am_plan_explain.restype = ctypes.c_char_p
+    lib.am_plan_explain.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int]
+    lib.am_last_error.restype = ctypes.c_char_p
+    for depth in (513, 100_000, 1_000_000):
+        assert lib.am_plan_explain(b"[" * depth + b"]" * depth, None, 0, 0) is None
+        assert b"nested more than 512 levels" in lib.am_last_error()
+    plan = (b'{"op": "limit", "count": 50, "offset": 3, "input": {"op": "sort", "by": [["k", true, '
+            b'{"nulls": "first", "float_order": "total"}], ["v", false]], "input": {"op": "select", '
+            b'"columns": ["k", "v"], "input": {"op": "scan", "source": "t"}}}}')
+    rng = random.Random(7)
+    alphabet = b'{}[]":,0123456789.eE+-\\u tnrfalsenull '
+    for _ in range(3000):
+        s = bytearray(plan)
+        kind = rng.randrange(3)
+        if kind == 0:
+            s = s[:rng.randrange(len(s) + 1)]
+        elif kind == 1:
+            for _ in range(rng.randrange(1, 6)):
+                s[rng.randrange(len(s))] = rng.choice(alphabet)
+        else:
+            at = rng.randrange(len(s))
+            s = s[:at] + bytes(rng.choice(alphabet) for _ in range(rng.randrange(1, 20))) + s[at:]
+        if lib.am_plan_explain(bytes(s), None, 0, 0) is None:
+            assert lib.am_last_error()
+
+
 def test_import_chunks_refuses_unsupported_types(lib):
     import pyarrow as pa
     from arrowmetal_b200 import _ArrowSchema
