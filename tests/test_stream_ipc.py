@@ -164,3 +164,35 @@ def test_ipc_string_offsets_checked(tmp_path, corrupt, message):
     # The same file unpatched still reads back.
     write_messages(tmp_path / "again.arrows", messages_of(src))
     assert am.scan_ipc(tmp_path / "again.arrows").to_reader().read_all().equals(pa.table({"s": pa.array(vals)}))
+
+
+def test_ipc_mutated_files_fail_cleanly(tmp_path):
+    # Truncated files, flipped bytes and overwritten 8-byte words (lengths and offsets among them):
+    # each read either succeeds or raises, and the process survives.
+    import random
+    rng = random.Random(11)
+    t = table_of(300, seed=11)
+    sources = []
+    for writer, name in ((write_file, "f.arrow"), (write_stream, "s.arrows")):
+        writer(tmp_path / name, t, 100)
+        sources.append((tmp_path / name).read_bytes())
+    bad = tmp_path / "bad.arrow"
+    failed = 0
+    for _ in range(400):
+        b = bytearray(rng.choice(sources))
+        kind = rng.randrange(3)
+        if kind == 0:
+            b = b[:rng.randrange(len(b) + 1)]
+        elif kind == 1:
+            for _ in range(rng.randrange(1, 8)):
+                b[rng.randrange(len(b))] = rng.randrange(256)
+        else:
+            for _ in range(rng.randrange(1, 4)):
+                i = rng.randrange(len(b) - 8) & ~7
+                b[i:i + 8] = rng.choice([0, 1, -1, 2**31, 2**40, -2**40, 10**12]).to_bytes(8, "little", signed=True)
+        bad.write_bytes(bytes(b))
+        try:
+            am.scan_ipc(bad, prefetch=0).to_reader().read_all()
+        except Exception:
+            failed += 1
+    assert 0 < failed < 400
