@@ -116,6 +116,32 @@ void check_array_struct(const ArrowSchema* schema, const ArrowArray* array) {
                   " buffers, got " + std::to_string(array->n_buffers));
 }
 
+// A host string or binary array's offsets must exist and never decrease: the device kernels read each
+// row's bytes between its two offsets, so a bad offset would send them outside the copied bytes. One
+// host pass over the offsets, before anything is allocated on the device.
+void check_host_offsets(const char* format, const ArrowArray* arr) {
+  const int pt = parse_format(format);
+  if (!pt_var(pt)) return;
+  const int64_t n = arr->length, off = arr->offset;
+  const void* vals = arr->buffers[1];
+  if (!vals) {
+    if (n == 0) return;
+    throw invalid("a string or binary array without an offsets buffer");
+  }
+  int64_t prev = 0;
+  for (int64_t i = 0; i <= n; i++) {
+    const int64_t o = pt == PT_LSTR ? static_cast<const int64_t*>(vals)[off + i] : static_cast<const int32_t*>(vals)[off + i];
+    if (o < 0 || (i > 0 && o < prev)) throw invalid("string offsets that are negative or decrease");
+    prev = o;
+  }
+}
+
+void check_host_array(const ArrowSchema* schema, const ArrowArray* array) {
+  check_array_struct(schema, array);
+  check_host_offsets(schema->format, array);
+  if (schema->dictionary) check_host_offsets(schema->dictionary->format, array->dictionary);
+}
+
 // Fills `a` from a host ArrowArray (the caller still owns the struct).
 void import_host(am_array* a, const ArrowArray* arr, cudaStream_t s) {
   const int64_t n = arr->length, off = arr->offset;
@@ -132,7 +158,7 @@ void import_host(am_array* a, const ArrowArray* arr, cudaStream_t s) {
     const bool large = a->pt == PT_LSTR;
     std::vector<char> offs(size_t(n + 1) * w);
     int64_t first = 0, last = 0;
-    for (int64_t i = 0; i <= n; i++) {
+    for (int64_t i = 0; vals && i <= n; i++) {     // no offsets buffer: an empty array (checked)
       const int64_t o = large ? static_cast<const int64_t*>(vals)[off + i] : static_cast<const int32_t*>(vals)[off + i];
       if (i == 0) first = o;
       if (i == n) last = o;
@@ -384,7 +410,7 @@ namespace am {
 // releases it (the copies are complete, or staged, when this returns).
 am_array* import_copy(const ArrowSchema* schema, const ArrowArray* array, cudaStream_t s) {
   const int pt = parse_format(schema->format);
-  check_array_struct(schema, array);
+  check_host_array(schema, array);
   am_array* a = new_array(pt, schema->format, array->length);
   try {
     import_host(a, array, s);
@@ -423,7 +449,7 @@ int am_import(const ArrowSchema* schema, ArrowArray* array, am_array** out) {
   if (!schema || !array || !out) return 2;
   return guard([&] {
     const int pt = parse_format(schema->format);
-    check_array_struct(schema, array);
+    check_host_array(schema, array);
     cudaStream_t s = stream();
     am_array* a = new_array(pt, schema->format, array->length);
     try {

@@ -163,6 +163,30 @@ def test_no_device_fails_loudly():
         pytest.skip("a GPU is present")
 
 
+def test_import_checks_string_offsets_before_the_device():
+    # Offsets that decrease or go negative are refused by am_import before any device work (the string
+    # kernels read each row's bytes between its offsets); a well-formed array gets past the check.
+    import numpy as np
+    import pyarrow as pa
+    import arrowmetal_b200 as am
+    data = pa.py_buffer(b"abcdefghij")
+    for offs, typ, dt in (([0, 3, 2, 6], pa.utf8(), np.int32), ([0, 2, -1, 4], pa.binary(), np.int32),
+                          ([0, 5, 4, 9], pa.large_utf8(), np.int64)):
+        bad = pa.Array.from_buffers(typ, 3, [None, pa.py_buffer(np.array(offs, dtype=dt).tobytes()), data])
+        with pytest.raises(am.ArrowMetalError, match="negative or decrease"):
+            am.MetalArray.from_arrow(bad)
+        # The same array in a dictionary's values.
+        dict_arr = pa.DictionaryArray.from_arrays(pa.array([0, 1, 2], type=pa.int32()), bad)
+        with pytest.raises(am.ArrowMetalError, match="negative or decrease"):
+            am.MetalArray.from_arrow(dict_arr)
+    if not _has_gpu():
+        good = pa.array(["ab", None, "cde"])
+        with pytest.raises(am.ArrowMetalError, match="CUDA"):
+            am.MetalArray.from_arrow(good)
+        with pytest.raises(am.ArrowMetalError, match="CUDA"):
+            am.MetalArray.from_arrow(pa.array([], type=pa.utf8()))
+
+
 def test_server_rejects_bad_arguments(lib):
     import ctypes
     out = ctypes.c_void_p()
