@@ -721,7 +721,7 @@ def run_reference_arm(args, rank):
     probe = make_table(1_000_000, SEED)
     rate, _ = cpu_oracle_rate(*probe, threads)
     budget = 120.0 / max(1, args.steps + args.warmup)
-    n = int(min(N_ROWS, max(100_000, rate * budget)))
+    n = int(min(args.rows, N_ROWS, max(100_000, rate * budget)))
     key, valid, p1, p2 = make_table(n, SEED)
     for _ in range(args.warmup):
         cpu_oracle_rate(key, valid, p1, p2, threads)
