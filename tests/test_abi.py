@@ -220,3 +220,43 @@ def test_stream_handles_without_a_device():
         s.sort("a")
     assert am._lib.am_stream_open_ipc(b"/nonexistent.arrow", 3, 1) is None
     assert b"cannot open /nonexistent.arrow" in am._lib.am_stream_last_error()
+
+
+def _release(struct):
+    if struct.release:
+        ctypes.CFUNCTYPE(None, ctypes.c_void_p)(struct.release)(ctypes.addressof(struct))
+
+
+def test_import_refuses_malformed_structs_and_keeps_them(lib):
+    # A refused import leaves the array with its producer (release still set), as the reference's does
+    # (CInterop.swift:119-131): the caller releases it. The checks run before any device work.
+    import pyarrow as pa
+    from arrowmetal_b200 import _ArrowArray as _Array, _ArrowSchema as _Schema
+    lib.am_import.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
+    lib.am_last_error.restype = ctypes.c_char_p
+    cases = [
+        ("n_buffers", 1, "buffers"),
+        ("length", -5, "negative length or offset"),
+        ("offset", -1, "negative length or offset"),
+        ("n_children", 1, "nested"),
+    ]
+    for field, value, message in cases:
+        schema, array = _Schema(), _Array()
+        pa.array([1, 2, None], type=pa.int64())._export_to_c(ctypes.addressof(array), ctypes.addressof(schema))
+        saved = getattr(array, field)
+        setattr(array, field, value)
+        out = ctypes.c_void_p()
+        rc = lib.am_import(ctypes.addressof(schema), ctypes.addressof(array), ctypes.byref(out))
+        assert rc == 1 and message in lib.am_last_error().decode(), (field, rc, lib.am_last_error())
+        assert array.release and not out.value
+        setattr(array, field, saved)
+        _release(array)
+        _release(schema)
+    # An unsupported type is refused by its format.
+    schema, array = _Schema(), _Array()
+    pa.array([[1], [2, 3]])._export_to_c(ctypes.addressof(array), ctypes.addressof(schema))
+    out = ctypes.c_void_p()
+    assert lib.am_import(ctypes.addressof(schema), ctypes.addressof(array), ctypes.byref(out)) != 0
+    assert array.release
+    _release(array)
+    _release(schema)
