@@ -3,7 +3,7 @@
 A ctypes binding over ``libArrowMetalC.so`` with the names, arguments and errors of ArrowMetal's own
 Python binding for the sort path (python/arrowmetal/__init__.py: ``MetalArray.from_arrow`` / ``to_arrow``
 :265-300, ``take`` :444-450, ``argsort`` / ``sort`` / ``top_k`` :460-480 and the option form :3940-3970,
-``lexsort_indices`` :1325-1359, ``ArrowMetalError`` / ``_check`` :212-222). Results come back as pyarrow
+``lexsort_indices`` :1325-1359, ``ArrowMetalError`` :210-211). Results come back as pyarrow
 arrays, so they drop straight into pyarrow, Polars or pandas::
 
     import pyarrow as pa, arrowmetal_b200 as am
@@ -157,48 +157,86 @@ def device_name():
 
 
 class ArrowMetalError(RuntimeError):
-    pass
+    """A library call returned a non-zero status. `status` keeps the C ABI's code: 1 operation error,
+    2 invalid argument, 3 a type the chunked import does not take."""
+
+    def __init__(self, message, status=1):
+        super().__init__(message)
+        self.status = status
 
 
-def _check(rc):
-    if rc != 0:
-        raise ArrowMetalError((_lib.am_last_error() or b"unknown error").decode())
+def _failure(status, entry=None):
+    text = _lib.am_last_error()
+    if text:
+        return ArrowMetalError(text.decode(), status)
+    return ArrowMetalError(f"{getattr(entry, '__name__', 'call')} returned status {status}", status)
 
 
-def _call(fn, *args):
-    out = _P()
-    _check(fn(*args, ctypes.byref(out)))
-    return MetalArray(out)
+def _ok(status):
+    """Raises for the status of an entry point that has no output handle."""
+    if status:
+        raise _failure(status)
+
+
+def _produce(entry, *args):
+    """Calls an entry point whose last parameter receives a new array handle, and wraps that handle."""
+    slot = _P()
+    status = entry(*args, ctypes.byref(slot))
+    if status:
+        raise _failure(status, entry)
+    return MetalArray(slot)
 
 
 def _index_of(names, value, what):
     try:
         return names.index(value)
     except ValueError:
-        raise ArrowMetalError(f"unknown {what} {value!r}; expected one of {', '.join(names)}") from None
+        raise ArrowMetalError(f"unknown {what} {value!r}; expected one of {', '.join(names)}", 2) from None
 
 
-def _index_array(indices):
-    """`take` indices as a pyarrow array of a type the gather reads (int32, int64, uint32)."""
+# Index types the gather reads as they are (None), and the type narrower ones widen to; any other type
+# (uint64, floats, a plain Python sequence) becomes int64.
+_GATHER_INDEX = {pa.int32(): None, pa.int64(): None, pa.uint32(): None, pa.int8(): pa.int32(),
+                 pa.int16(): pa.int32(), pa.uint8(): pa.uint32(), pa.uint16(): pa.uint32()}
+
+
+def _gather_indices(indices):
+    """A MetalArray of `take` indices from a MetalArray, a pyarrow (chunked) array, a numpy array or a
+    sequence of row numbers."""
+    if isinstance(indices, MetalArray):
+        return indices
     if isinstance(indices, pa.ChunkedArray):
         indices = indices.combine_chunks()
-    if not isinstance(indices, pa.Array):
-        if hasattr(indices, "dtype"):
-            indices = pa.array(indices)
-        else:
-            indices = pa.array(list(indices), type=pa.int64())
-    t = indices.type
-    if pa.types.is_int32(t) or pa.types.is_int64(t) or pa.types.is_uint32(t):
-        return indices
-    if pa.types.is_int8(t) or pa.types.is_int16(t):
-        return indices.cast(pa.int32())
-    if pa.types.is_uint8(t) or pa.types.is_uint16(t):
-        return indices.cast(pa.uint32())
-    return indices.cast(pa.int64())
+    elif not isinstance(indices, pa.Array):
+        indices = pa.array(indices) if hasattr(indices, "dtype") else pa.array(list(indices), pa.int64())
+    target = _GATHER_INDEX.get(indices.type, pa.int64())
+    return MetalArray.from_arrow(indices if target is None else indices.cast(target))
+
+
+def _sort_options(count, descending, null_placement, float_order):
+    """The three per-key option vectors of the C ABI (direction, null placement, float order) as
+    c_int arrays. `descending` is None (all ascending), one bool, or one flag per key; the other two are
+    one name for every key or one name per key."""
+    def per_key(value, what):
+        if isinstance(value, (str, bool)) or value is None:
+            return [value] * count
+        items = list(value)
+        if len(items) != count:
+            raise ArrowMetalError(f"{what} has {len(items)} entries for {count} columns", 2)
+        return items
+
+    vec = ctypes.c_int * count
+    flags = per_key(False if descending is None else descending, "descending")
+    places = per_key(null_placement, "null_placement")
+    orders = per_key(float_order, "float_order")
+    return (vec(*[1 if d else 0 for d in flags]),
+            vec(*[_index_of(NULL_PLACEMENT, p, "null_placement") for p in places]),
+            vec(*[_index_of(FLOAT_ORDERS, f, "float_order") for f in orders]))
 
 
 class MetalArray:
-    """An HBM-resident Arrow array. Immutable; every operation returns a new array."""
+    """One Arrow array in this GPU's memory, owned through a library handle. Calls never modify it:
+    each returns a new MetalArray (or a pyarrow result)."""
 
     def __init__(self, handle):
         self._h = handle
@@ -223,7 +261,7 @@ class MetalArray:
         schema, array = _ArrowSchema(), _ArrowArray()
         obj._export_to_c(ctypes.addressof(array), ctypes.addressof(schema))
         try:
-            return _call(_lib.am_import, ctypes.addressof(schema), ctypes.addressof(array))
+            return _produce(_lib.am_import, ctypes.addressof(schema), ctypes.addressof(array))
         finally:
             if array.release:
                 ctypes.CFUNCTYPE(None, _P)(array.release)(ctypes.addressof(array))
@@ -247,14 +285,14 @@ class MetalArray:
         arr.device_id = _lib.am_cuda_device()
         schema = _ArrowSchema()
         schema.format = fmt.encode()
-        out = _call(_lib.am_import_device, ctypes.addressof(schema), ctypes.addressof(arr))
+        out = _produce(_lib.am_import_device, ctypes.addressof(schema), ctypes.addressof(arr))
         out._device_holder = holder
         return out
 
     def to_arrow(self):
         """Export as a pyarrow.Array (copied into pinned host memory owned by the array)."""
         schema, array = _ArrowSchema(), _ArrowArray()
-        _check(_lib.am_export(self._h, ctypes.addressof(schema), ctypes.addressof(array)))
+        _ok(_lib.am_export(self._h, ctypes.addressof(schema), ctypes.addressof(array)))
         return pa.Array._import_from_c(ctypes.addressof(array), ctypes.addressof(schema))
 
     def __len__(self):
@@ -271,12 +309,10 @@ class MetalArray:
     # ---- selection
     def take(self, indices):
         """Arrow `take`: int32, int64 and uint32 indices; a null index gives a null row."""
-        if not isinstance(indices, MetalArray):
-            indices = MetalArray.from_arrow(_index_array(indices))
-        return _call(_lib.am_take, self._h, indices._h)
+        return _produce(_lib.am_take, self._h, _gather_indices(indices)._h)
 
     def slice(self, offset, length):
-        return _call(_lib.am_slice, self._h, offset, length)
+        return _produce(_lib.am_slice, self._h, offset, length)
 
     # ---- sorting (stable radix sort on the GPU)
     def argsort(self, descending=False, null_placement="at_end", float_order="ieee"):
@@ -284,29 +320,27 @@ class MetalArray:
         the same values). `null_placement` is independent of the direction, as in Arrow.
         `float_order`: "ieee" (pyarrow's order: -0.0 ties +0.0, NaN next to the nulls), "total"
         (IEEE 754 totalOrder, arrow-rs), "nan_largest" (Polars)."""
-        return _call(_lib.am_argsort_ex2, self._h, 1 if descending else 0,
-                     _index_of(NULL_PLACEMENT, null_placement, "null_placement"),
-                     _index_of(FLOAT_ORDERS, float_order, "float_order"))
+        return _produce(_lib.am_argsort_ex2, self._h, 1 if descending else 0,
+                        _index_of(NULL_PLACEMENT, null_placement, "null_placement"),
+                        _index_of(FLOAT_ORDERS, float_order, "float_order"))
 
     def argsort64(self, descending=False, null_placement="at_end", float_order="ieee"):
         """`argsort` with uint64 indices, the type pyarrow's sort_indices returns."""
-        out = _P()
-        _check(_lib.am_argsort_ex3(self._h, 1 if descending else 0,
-                                   _index_of(NULL_PLACEMENT, null_placement, "null_placement"),
-                                   _index_of(FLOAT_ORDERS, float_order, "float_order"), 8, ctypes.byref(out)))
-        return MetalArray(out)
+        return _produce(_lib.am_argsort_ex3, self._h, 1 if descending else 0,
+                        _index_of(NULL_PLACEMENT, null_placement, "null_placement"),
+                        _index_of(FLOAT_ORDERS, float_order, "float_order"), 8)
 
     def sort(self, descending=False, null_placement="at_end", float_order="ieee"):
         """Sorted copy of the array, with the ordering rules of `argsort`."""
-        return _call(_lib.am_sort_ex2, self._h, 1 if descending else 0,
-                     _index_of(NULL_PLACEMENT, null_placement, "null_placement"),
-                     _index_of(FLOAT_ORDERS, float_order, "float_order"))
+        return _produce(_lib.am_sort_ex2, self._h, 1 if descending else 0,
+                        _index_of(NULL_PLACEMENT, null_placement, "null_placement"),
+                        _index_of(FLOAT_ORDERS, float_order, "float_order"))
 
     def top_k(self, k, largest=True, null_placement="at_end", float_order="ieee"):
         """UInt32 indices of the k largest (or smallest) values: the first k of `argsort`."""
-        return _call(_lib.am_top_k_ex, self._h, int(k), 1 if largest else 0,
-                     _index_of(NULL_PLACEMENT, null_placement, "null_placement"),
-                     _index_of(FLOAT_ORDERS, float_order, "float_order"))
+        return _produce(_lib.am_top_k_ex, self._h, int(k), 1 if largest else 0,
+                        _index_of(NULL_PLACEMENT, null_placement, "null_placement"),
+                        _index_of(FLOAT_ORDERS, float_order, "float_order"))
 
 
     # ---- sort consumers (one argsort, then run marks, a scan and scatters)
@@ -314,28 +348,28 @@ class MetalArray:
         """Arrow `partition_nth_indices`: uint32 indices with, at position `pivot`, the row a stable
         ascending sort puts there; no row before it orders after it and none after it before it. Each
         of the three blocks (before, equal, after) keeps row order. A radix select, not a sort."""
-        return _call(_lib.am_partition_nth_ex, self._h, int(pivot),
-                     _index_of(NULL_PLACEMENT, null_placement, "null_placement"))
+        return _produce(_lib.am_partition_nth_ex, self._h, int(pivot),
+                        _index_of(NULL_PLACEMENT, null_placement, "null_placement"))
 
     def rank(self, sort_keys="ascending", null_placement="at_end", tiebreaker="min"):
         """Arrow `rank` (uint32; pyarrow returns uint64 with the same values). Nulls and NaN rows are one
         tie group at the `null_placement` end, as in pyarrow."""
-        return _call(_lib.am_rank_ex, self._h, _index_of(TIEBREAKERS, tiebreaker, "tiebreaker"),
-                     _direction(sort_keys), _index_of(NULL_PLACEMENT, null_placement, "null_placement"))
+        return _produce(_lib.am_rank_ex, self._h, _index_of(TIEBREAKERS, tiebreaker, "tiebreaker"),
+                        _direction(sort_keys), _index_of(NULL_PLACEMENT, null_placement, "null_placement"))
 
     def rank_quantile(self, sort_keys="ascending", null_placement="at_end"):
         """Arrow `rank_quantile`: (average 1-based rank of the row's tie group - 0.5) / n, float64."""
-        return _call(_lib.am_rank_quantile_ex, self._h, 0, _direction(sort_keys),
-                     _index_of(NULL_PLACEMENT, null_placement, "null_placement"))
+        return _produce(_lib.am_rank_quantile_ex, self._h, 0, _direction(sort_keys),
+                        _index_of(NULL_PLACEMENT, null_placement, "null_placement"))
 
     def rank_normal(self, sort_keys="ascending", null_placement="at_end", float32=False):
         """Arrow `rank_normal`: the standard normal quantile of `rank_quantile()` (float64, or float32)."""
-        return _call(_lib.am_rank_quantile_ex, self._h, 2 if float32 else 1, _direction(sort_keys),
-                     _index_of(NULL_PLACEMENT, null_placement, "null_placement"))
+        return _produce(_lib.am_rank_quantile_ex, self._h, 2 if float32 else 1, _direction(sort_keys),
+                        _index_of(NULL_PLACEMENT, null_placement, "null_placement"))
 
     def window(self, op):
         """One of the SQL ranking window functions by name (ascending, nulls last and tied)."""
-        return _call(_lib.am_window, self._h, _index_of(WINDOW_OPS, op, "op"), 0, 0, None)
+        return _produce(_lib.am_window, self._h, _index_of(WINDOW_OPS, op, "op"), 0, 0, None)
 
     def row_number(self):
         return self.window("row_number")
@@ -353,11 +387,11 @@ class MetalArray:
         """Arrow `unique`. "first_appearance" keeps Arrow's order and its one null entry (not for string
         columns); "sorted" is ascending with the nulls dropped. -0.0 matches 0.0 and every NaN is one
         value; the representative is the earliest row."""
-        return _call(_lib.am_unique_ex, self._h, _index_of(VALUE_ORDERS, order, "order"))
+        return _produce(_lib.am_unique_ex, self._h, _index_of(VALUE_ORDERS, order, "order"))
 
     def value_counts(self, order="first_appearance"):
         """Arrow `value_counts`: a struct array of `values` and their int64 `counts`, in `unique`'s order."""
-        return _call(_lib.am_value_counts_ex, self._h, _index_of(VALUE_ORDERS, order, "order"))
+        return _produce(_lib.am_value_counts_ex, self._h, _index_of(VALUE_ORDERS, order, "order"))
 
 
 def _direction(sort_keys):
@@ -396,7 +430,7 @@ def _import_chunks(chunked):
                 if a.release:
                     ctypes.CFUNCTYPE(None, _P)(a.release)(ctypes.addressof(a))
             return MetalArray.from_arrow(chunked.combine_chunks())
-        _check(rc)
+        _ok(rc)
         return MetalArray(out)
     finally:
         for a in arrays:
@@ -406,46 +440,26 @@ def _import_chunks(chunked):
             ctypes.CFUNCTYPE(None, _P)(schema.release)(ctypes.addressof(schema))
 
 
-def _per_key(value, n, what):
-    if isinstance(value, str):
-        return [value] * n
-    value = list(value)
-    if len(value) != n:
-        raise ArrowMetalError(f"{what} has {len(value)} entries for {n} columns")
-    return value
-
-
 def lexsort_indices(columns, descending=None, null_placement="at_end", float_order="ieee"):
     """Multi-column sort: uint32 indices ordering the rows by each column in turn, the first column the
     most significant. `descending` is one flag per column (None: all ascending); `null_placement` and
     `float_order` are one value or one per key."""
     cols = [c if isinstance(c, MetalArray) else MetalArray.from_arrow(c) for c in columns]
     if not cols:
-        raise ArrowMetalError("lexsort needs at least one column")
-    flags = descending if descending is not None else [False] * len(cols)
-    if len(flags) != len(cols):
-        raise ArrowMetalError(f"descending has {len(flags)} entries for {len(cols)} columns")
-    n = len(cols)
-    handles = (_P * n)(*[c._h for c in cols])
-    desc = (ctypes.c_int * n)(*[1 if d else 0 for d in flags])
-    np_ = (ctypes.c_int * n)(*[_index_of(NULL_PLACEMENT, p, "null_placement")
-                               for p in _per_key(null_placement, n, "null_placement")])
-    fo = (ctypes.c_int * n)(*[_index_of(FLOAT_ORDERS, f, "float_order")
-                              for f in _per_key(float_order, n, "float_order")])
-    out = _P()
-    _check(_lib.am_lexsort_ex2(handles, desc, np_, fo, n, ctypes.byref(out)))
-    return MetalArray(out)
+        raise ArrowMetalError("lexsort needs at least one column", 2)
+    desc, places, orders = _sort_options(len(cols), descending, null_placement, float_order)
+    handles = (_P * len(cols))(*[c._h for c in cols])
+    return _produce(_lib.am_lexsort_ex2, handles, desc, places, orders, len(cols))
 
 
 def take_columns(columns, indices):
     """`take` of several columns through one index array, with one index read on the GPU."""
     cols = [c if isinstance(c, MetalArray) else MetalArray.from_arrow(c) for c in columns]
-    if not isinstance(indices, MetalArray):
-        indices = MetalArray.from_arrow(_index_array(indices))
+    indices = _gather_indices(indices)
     n = len(cols)
     handles = (_P * n)(*[c._h for c in cols])
     outs = (_P * n)()
-    _check(_lib.am_take_columns(handles, n, indices._h, outs))
+    _ok(_lib.am_take_columns(handles, n, indices._h, outs))
     return [MetalArray(outs[i]) for i in range(n)]
 
 
@@ -454,11 +468,9 @@ def argsort_batch(arrays, descending=None, null_placement=None, float_order=None
     cols = [c if isinstance(c, MetalArray) else MetalArray.from_arrow(c) for c in arrays]
     n = len(cols)
     handles = (_P * n)(*[c._h for c in cols])
-    d = (ctypes.c_int * n)(*[1 if x else 0 for x in (descending or [False] * n)])
-    p = (ctypes.c_int * n)(*[_index_of(NULL_PLACEMENT, x, "null_placement") for x in (null_placement or ["at_end"] * n)])
-    f = (ctypes.c_int * n)(*[_index_of(FLOAT_ORDERS, x, "float_order") for x in (float_order or ["ieee"] * n)])
+    d, p, f = _sort_options(n, descending, null_placement or "at_end", float_order or "ieee")
     outs = (_P * max(n, 1))()
-    _check(_lib.am_argsort_batch(handles, d, p, f, n, outs))
+    _ok(_lib.am_argsort_batch(handles, d, p, f, n, outs))
     return [MetalArray(outs[i]) for i in range(n)]
 
 
@@ -467,11 +479,11 @@ def argsort_batch(arrays, descending=None, null_placement=None, float_order=None
 @contextlib.contextmanager
 def batch():
     """Calls inside the block do not wait for the GPU; deferred errors raise at its end."""
-    _check(_lib.am_batch_begin())
+    _ok(_lib.am_batch_begin())
     try:
         yield
     finally:
-        _check(_lib.am_batch_end())
+        _ok(_lib.am_batch_end())
 
 
 _ROUTER = ("auto", "gpu", "cpu")
@@ -479,7 +491,7 @@ _ROUTER = ("auto", "gpu", "cpu")
 
 def set_router(mode):
     """Router mode ("auto", "gpu", "cpu"). The sort is never routed to the CPU."""
-    _check(_lib.am_router_set_mode(_index_of(_ROUTER, mode, "router mode")))
+    _ok(_lib.am_router_set_mode(_index_of(_ROUTER, mode, "router mode")))
 
 
 def get_router():
@@ -495,7 +507,7 @@ class PlanSource:
         handles = (_P * n)(*[c._h for c in cols.values()])
         names = (ctypes.c_char_p * n)(*[k.encode() for k in cols])
         self._h = _P()
-        _check(_lib.am_plan_source_create(name.encode(), handles, names, n, ctypes.byref(self._h)))
+        _ok(_lib.am_plan_source_create(name.encode(), handles, names, n, ctypes.byref(self._h)))
         self.name = name
         self._cols = cols
 
@@ -512,16 +524,8 @@ def run_plan(plan, sources):
     n = len(sources)
     hs = (_P * max(n, 1))(*[s._h for s in sources])
     r = _P()
-    _check(_lib.am_plan_run(text.encode(), hs, n, 1, ctypes.byref(r)))
-    try:
-        out = {}
-        for i in range(_lib.am_plan_column_count(r)):
-            h = _P()
-            _check(_lib.am_plan_column(r, i, ctypes.byref(h)))
-            out[_lib.am_plan_column_name(r, i).decode()] = MetalArray(h)
-        return out
-    finally:
-        _lib.am_plan_result_release(r)
+    _ok(_lib.am_plan_run(text.encode(), hs, n, 1, ctypes.byref(r)))
+    return _plan_result_columns(r)
 
 
 def _plan_result_columns(r):
@@ -529,7 +533,7 @@ def _plan_result_columns(r):
         out = {}
         for i in range(_lib.am_plan_column_count(r)):
             h = _P()
-            _check(_lib.am_plan_column(r, i, ctypes.byref(h)))
+            _ok(_lib.am_plan_column(r, i, ctypes.byref(h)))
             out[_lib.am_plan_column_name(r, i).decode()] = MetalArray(h)
         return out
     finally:
@@ -546,38 +550,32 @@ class Server:
 
     def __init__(self, workers=4, hbm_cap_bytes=120 * 10**9, batch_rows=1 << 20):
         self._h = _P()
-        _check(_lib.am_server_create(int(workers), int(hbm_cap_bytes), int(batch_rows), ctypes.byref(self._h)))
+        _ok(_lib.am_server_create(int(workers), int(hbm_cap_bytes), int(batch_rows), ctypes.byref(self._h)))
         self._sources = {}
 
     def submit(self, source, offset, length, keys, payload=(), descending=None, null_placement="at_end",
                float_order="ieee"):
         keys = [keys] if isinstance(keys, str) else list(keys)
         n = len(keys)
-        desc = descending if descending is not None else [False] * n
-        if isinstance(desc, bool):
-            desc = [desc] * n
         kn = (ctypes.c_char_p * n)(*[k.encode() for k in keys])
-        d = (ctypes.c_int * n)(*[1 if x else 0 for x in desc])
-        p = (ctypes.c_int * n)(*[_index_of(NULL_PLACEMENT, x, "null_placement")
-                                 for x in _per_key(null_placement, n, "null_placement")])
-        f = (ctypes.c_int * n)(*[_index_of(FLOAT_ORDERS, x, "float_order") for x in _per_key(float_order, n, "float_order")])
+        d, p, f = _sort_options(n, descending, null_placement, float_order)
         payload = list(payload)
         pn = (ctypes.c_char_p * max(len(payload), 1))(*[c.encode() for c in payload])
         t = _I64()
         self._sources[id(source)] = source          # the table outlives its requests
-        _check(_lib.am_server_submit(self._h, source._h, int(offset), int(length), kn, d, p, f, n, pn,
+        _ok(_lib.am_server_submit(self._h, source._h, int(offset), int(length), kn, d, p, f, n, pn,
                                      len(payload), ctypes.byref(t)))
         return t.value
 
     def wait(self, ticket):
         r = _P()
         lat = ctypes.c_double()
-        _check(_lib.am_server_wait(self._h, int(ticket), ctypes.byref(r), ctypes.byref(lat)))
+        _ok(_lib.am_server_wait(self._h, int(ticket), ctypes.byref(r), ctypes.byref(lat)))
         return _plan_result_columns(r), lat.value
 
     def stats(self):
         s = ServerStats()
-        _check(_lib.am_server_get_stats(self._h, ctypes.byref(s)))
+        _ok(_lib.am_server_get_stats(self._h, ctypes.byref(s)))
         return {name: getattr(s, name) for name, _ in ServerStats._fields_}
 
     def close(self):
@@ -675,12 +673,8 @@ class Stream:
         self._consumed = True
         names, desc = _sort_keys(by)
         k = len(names)
-        places = _per_key(null_placement, k, "null_placement")
-        orders = _per_key(float_order, k, "float_order")
         cn = (ctypes.c_char_p * k)(*[n.encode() for n in names])
-        cd = (ctypes.c_int * k)(*[1 if d else 0 for d in desc])
-        cp = (ctypes.c_int * k)(*[_index_of(NULL_PLACEMENT, p, "null_placement") for p in places])
-        cf = (ctypes.c_int * k)(*[_index_of(FLOAT_ORDERS, f, "float_order") for f in orders])
+        cd, cp, cf = _sort_options(k, desc, null_placement, float_order)
         out = _P()
         rc = _lib.am_stream_sort_ex(self._h, cn, cd, cp, cf, k, int(limit),
                                     None if scratch is None else str(scratch).encode(),
@@ -703,7 +697,7 @@ class Stream:
             for i in range(n):
                 col_names.append(_lib.am_stream_result_column_name(out, i).decode())
                 h = _P()
-                _check(_lib.am_stream_result_column(out, i, ctypes.byref(h)))
+                _ok(_lib.am_stream_result_column(out, i, ctypes.byref(h)))
                 cols.append(MetalArray(h).to_arrow())
             return pa.table(cols, names=col_names) if n > 0 else None
         finally:
@@ -750,7 +744,7 @@ def explain_plan(plan, sources):
     hs = (_P * max(n, 1))(*[s._h for s in sources])
     s = _lib.am_plan_explain(text.encode(), hs, n, 1)
     if s is None:
-        _check(1)
+        _ok(1)
     return s.decode()
 
 
@@ -758,26 +752,26 @@ def explain_plan(plan, sources):
 
 def set_stream(stream_ptr):
     """Enqueue this thread's calls on an existing cudaStream_t (an int address; 0 = the library's)."""
-    _check(_lib.am_cuda_set_stream(stream_ptr or None))
+    _ok(_lib.am_cuda_set_stream(stream_ptr or None))
 
 
 def synchronize():
-    _check(_lib.am_cuda_synchronize())
+    _ok(_lib.am_cuda_synchronize())
 
 
 def last_sort_stats():
     s = SortStats()
-    _check(_lib.am_last_sort_stats(ctypes.byref(s)))
+    _ok(_lib.am_last_sort_stats(ctypes.byref(s)))
     return {"rows": s.rows, "value_rows": s.value_rows, "passes_run": s.passes_run,
             "passes_skipped": s.passes_skipped}
 
 
 def profile(on=True):
-    _check(_lib.am_cuda_profile(1 if on else 0))
+    _ok(_lib.am_cuda_profile(1 if on else 0))
 
 
 def profile_reset():
-    _check(_lib.am_cuda_profile_reset())
+    _ok(_lib.am_cuda_profile_reset())
 
 
 def profile_entries():
@@ -785,9 +779,9 @@ def profile_entries():
     out = {}
     n = _lib.am_cuda_profile_count()
     if n < 0:
-        _check(1)
+        _ok(1)
     for i in range(n):
         name, launches, ms = ctypes.c_char_p(), _I64(), ctypes.c_double()
-        _check(_lib.am_cuda_profile_entry(i, ctypes.byref(name), ctypes.byref(launches), ctypes.byref(ms)))
+        _ok(_lib.am_cuda_profile_entry(i, ctypes.byref(name), ctypes.byref(launches), ctypes.byref(ms)))
         out[name.value.decode()] = (launches.value, ms.value)
     return out

@@ -98,22 +98,30 @@ bool is_index_format(const char* f) {
   return false;
 }
 
+// The fields of one flat array (no children) that its buffers are read by: length, offset and the
+// buffer count its format needs.
+void check_flat_struct(const ArrowSchema* schema, const ArrowArray* array, const char* what) {
+  if (schema->n_children != 0 || array->n_children != 0)
+    throw unsupported(std::string("nested arrays are not carried by this build (a nested ") + what + ")");
+  if (array->length < 0 || array->offset < 0) throw invalid(std::string("negative length or offset in ") + what);
+  const int want = pt_var(parse_format(schema->format)) ? 3 : 2;
+  if (array->n_buffers != want || (array->n_buffers > 0 && !array->buffers))
+    throw invalid(std::string(want == 3 ? "a string or binary " : "a primitive ") + what + " has " +
+                  std::to_string(want) + " buffers, got " + std::to_string(array->n_buffers));
+}
+
 void check_array_struct(const ArrowSchema* schema, const ArrowArray* array) {
   if (!schema->dictionary != !array->dictionary) throw invalid("the schema and the array disagree on a dictionary");
   if (schema->dictionary) {
-    // A dictionary array: integer codes, and a flat dictionary (not itself dictionary-encoded).
+    // A dictionary array: integer codes, and a flat dictionary (not itself dictionary-encoded), checked
+    // like any array before its buffers are read.
     if (!is_index_format(schema->format))
       throw invalid(std::string("dictionary codes of type ") + schema->format + " (an integer type is required)");
     if (schema->dictionary->dictionary || array->dictionary->dictionary)
       throw unsupported("a dictionary whose values are themselves dictionary-encoded");
-    parse_format(schema->dictionary->format);
+    check_flat_struct(schema->dictionary, array->dictionary, "dictionary");
   }
-  if (schema->n_children != 0 || array->n_children != 0) throw unsupported("nested arrays are not carried by this build");
-  if (array->length < 0 || array->offset < 0) throw invalid("negative length or offset");
-  const int want = pt_var(parse_format(schema->format)) ? 3 : 2;
-  if (array->n_buffers != want)
-    throw invalid(std::string(want == 3 ? "a string or binary" : "a primitive") + " array has " + std::to_string(want) +
-                  " buffers, got " + std::to_string(array->n_buffers));
+  check_flat_struct(schema, array, "array");
 }
 
 // A host string or binary array's offsets must exist and never decrease: the device kernels read each

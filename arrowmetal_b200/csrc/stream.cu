@@ -809,13 +809,18 @@ void check_ipc_buffers(int pt, int64_t length, int64_t null_count, const uint64_
   const uint64_t bitmap = (n + 7) / 8;
   if (lens[0] != 0 && lens[0] < bitmap) throw invalid("an IPC validity bitmap shorter than its column");
   if (null_count > 0 && lens[0] == 0) throw invalid("an IPC column with nulls and no validity bitmap");
+  // Each size is compared by division, so a row count near 2^64 / width cannot wrap the product
+  // that a multiplication would form and pass as a small buffer.
   if (!pt_var(pt)) {
-    const uint64_t need = pt == PT_BOOL ? bitmap : n * uint64_t(pt_bytes(pt));
-    if (lens[1] < need) throw invalid("an IPC values buffer shorter than its column");
+    if (pt == PT_BOOL) {
+      if (lens[1] < bitmap) throw invalid("an IPC values buffer shorter than its column");
+    } else if (n > lens[1] / uint64_t(pt_bytes(pt))) {
+      throw invalid("an IPC values buffer shorter than its column");
+    }
     return;
   }
   const uint64_t ow = uint64_t(pt_bytes(pt));
-  if (lens[1] < (n + 1) * ow) throw invalid("an IPC offsets buffer shorter than its column");
+  if (n >= lens[1] / ow) throw invalid("an IPC offsets buffer shorter than its column");
   int64_t prev = 0;
   for (uint64_t i = 0; i <= n; i++) {
     int64_t o;

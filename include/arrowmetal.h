@@ -311,8 +311,9 @@ int  am_server_release(am_server* server);
  * All scratch lives in one fixed block inside the library (about 6.1 MiB on each GPU the library is
  * loaded on, held until exit), so one call sorts at most 262,144 rows; longer inputs return 2 with an
  * error naming the limit. The work runs on `stream` (NULL: the default stream) on the calling thread's
- * current device, and the call returns once it has finished there. The first call on each device
- * looks up the block's device address and sets up the kernels; make it before any stream capture.
+ * current device, and the call is synchronous: it waits for that stream before it returns. The first
+ * call on each device looks up the block's device address and sets up the kernels; make that first
+ * call before any stream capture.
  * Calls share the block: they take turns inside this process, and work that overlapped on the GPU
  * would race on it. */
 int  am_argsort_device_noalloc(const char* format, const void* values, const void* validity,

@@ -35,12 +35,21 @@ def test_exports_every_declared_symbol(lib):
     assert not missing, missing
 
 
+def unserved_symbols():
+    """The entry points outside the sort path that the library exports only so that the reference's
+    callers load it (each answers "not served"), listed in csrc/unserved.cpp."""
+    text = open(os.path.join(ROOT, "arrowmetal_b200", "csrc", "unserved.cpp")).read()
+    return set(re.findall(r"\bX\((am_[a-z0-9_]+)\)", text))
+
+
 def test_exports_nothing_else():
     out = os.popen(f"nm -D --defined-only {LIB}").read().split("\n")
     exported = {l.split()[-1] for l in out if l.strip()}
     extra = {e for e in exported if not e.startswith("am_")}
     assert not extra, sorted(extra)[:20]
-    assert exported <= declared_symbols() | extra
+    unserved = unserved_symbols()
+    assert len(unserved) > 200 and not unserved & declared_symbols()
+    assert exported == declared_symbols() | unserved
 
 
 def test_reference_binding_sort_symbols_present(lib):
@@ -260,3 +269,29 @@ def test_import_refuses_malformed_structs_and_keeps_them(lib):
     assert array.release
     _release(array)
     _release(schema)
+
+
+def test_import_refuses_malformed_dictionary_structs(lib):
+    # The dictionary of a dictionary array gets the same struct checks as the array itself, before
+    # anything reads its buffers (its string offsets included).
+    import pyarrow as pa
+    from arrowmetal_b200 import _ArrowArray as _Array, _ArrowSchema as _Schema
+    lib.am_import.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
+    lib.am_last_error.restype = ctypes.c_char_p
+    cases = [("n_buffers", 1, "buffers"), ("n_buffers", 0, "buffers"), ("length", -3, "negative length or offset"),
+             ("offset", -2, "negative length or offset"), ("n_children", 2, "nested")]
+    for field, value, message in cases:
+        schema, array = _Schema(), _Array()
+        pa.array(["b", "a", None, "b"]).dictionary_encode()._export_to_c(ctypes.addressof(array),
+                                                                        ctypes.addressof(schema))
+        dictionary = ctypes.cast(array.dictionary, ctypes.POINTER(_Array)).contents
+        saved = getattr(dictionary, field)
+        setattr(dictionary, field, value)
+        out = ctypes.c_void_p()
+        rc = lib.am_import(ctypes.addressof(schema), ctypes.addressof(array), ctypes.byref(out))
+        err = lib.am_last_error().decode()
+        assert rc == 1 and message in err and "dictionary" in err, (field, rc, err)
+        assert array.release and not out.value
+        setattr(dictionary, field, saved)
+        _release(array)
+        _release(schema)

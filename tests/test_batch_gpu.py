@@ -1,7 +1,8 @@
-"""Segmented (batched) argsort, am_argsort_batch: every array's permutation must be identical to
-am_argsort_ex2 on that array alone (bit-exact), for mixed key types and widths, per-array options,
-empty, one-row, all-null and tile-edge lengths, and the batch shape of the segmented benchmark
-(log-uniform lengths, int64 and float32 alternating)."""
+"""Segmented (batched) argsort, am_argsort_batch: every array's permutation must be identical to the
+C oracle's argsort of that array with its options, and to am_argsort_ex2 on that array alone
+(bit-exact), for mixed key types and widths, per-array options, empty, one-row, all-null and
+tile-edge lengths, and the batch shape of the segmented benchmark (log-uniform lengths, int64 and
+float32 alternating)."""
 import numpy as np
 import pyarrow as pa
 import pytest
@@ -51,7 +52,7 @@ def random_array(rng, kind, n):
     return build_array(t, v, valid)
 
 
-def check_batch(am, arrays, opts):
+def check_batch(am, oracle, arrays, opts):
     handles = [am.MetalArray.from_arrow(a) for a in arrays]
     desc = [o[0] for o in opts]
     place = [o[1] for o in opts]
@@ -59,16 +60,17 @@ def check_batch(am, arrays, opts):
     outs = am.argsort_batch(handles, desc, place, order)
     assert len(outs) == len(arrays)
     for i, (h, o) in enumerate(zip(handles, outs)):
-        want = ids(h.argsort(desc[i], place[i], order[i]))
         got = ids(o)
         assert got.dtype == np.uint32
-        assert np.array_equal(got, want), (i, arrays[i].type, len(arrays[i]), opts[i])
+        case = (i, arrays[i].type, len(arrays[i]), opts[i])
+        assert np.array_equal(got, oracle.argsort(arrays[i], desc[i], place[i], order[i])), case
+        assert np.array_equal(got, ids(h.argsort(desc[i], place[i], order[i]))), case
 
 
 KINDS = ["int64", "int64_small", "uint64", "float64", "float32", "int32", "uint16", "int8", "float16", "bool"]
 
 
-def test_mixed_batch(am):
+def test_mixed_batch(am, oracle):
     rng = np.random.default_rng(101)
     lengths = [0, 1, 2, 31, 4095, 4096, 4097, 8191, 12_289, 100_003, 1, 0, 777, 65_536, 250_000]
     arrays, opts = [], []
@@ -76,11 +78,11 @@ def test_mixed_batch(am):
         kind = KINDS[i % len(KINDS)]
         arrays.append(random_array(rng, kind, n))
         opts.append((bool(rng.integers(2)), PLACEMENTS[rng.integers(2)], ORDERS[rng.integers(3)]))
-    check_batch(am, arrays, opts)
+    check_batch(am, oracle, arrays, opts)
 
 
 @pytest.mark.parametrize("seed", [1, 2, 3])
-def test_many_small_and_large(am, seed):
+def test_many_small_and_large(am, oracle, seed):
     rng = np.random.default_rng(seed)
     arrays, opts = [], []
     for i in range(300):
@@ -88,12 +90,12 @@ def test_many_small_and_large(am, seed):
         kind = KINDS[int(rng.integers(len(KINDS)))]
         arrays.append(random_array(rng, kind, n))
         opts.append((bool(rng.integers(2)), PLACEMENTS[rng.integers(2)], ORDERS[rng.integers(3)]))
-    check_batch(am, arrays, opts)
+    check_batch(am, oracle, arrays, opts)
 
 
 def test_segmented_benchmark_shape(am, oracle):
     # The segmented benchmark's arrays, fewer of them: int64 full range and float32 N(0,1) with 2% nulls
-    # alternating, lengths log-uniform in [1e3, 1e6]; also checked against the C oracle.
+    # alternating, lengths log-uniform in [1e3, 1e6], with every combination of the options.
     rng = np.random.default_rng(20260906 + 4)
     arrays = []
     for i in range(64):
@@ -103,26 +105,23 @@ def test_segmented_benchmark_shape(am, oracle):
                                                 endpoint=True)))
         else:
             arrays.append(pa.array(rng.standard_normal(n).astype(np.float32), mask=rng.random(n) < 0.02))
-    opts = [(False, "at_end", "ieee")] * len(arrays)
-    check_batch(am, arrays, opts)
-    outs = am.argsort_batch([am.MetalArray.from_arrow(a) for a in arrays[:6]])
-    for a, o in zip(arrays[:6], outs):
-        assert np.array_equal(ids(o), oracle.argsort(a))
+    opts = [(bool(i % 3 == 1), PLACEMENTS[i % 2], ORDERS[(i // 2) % 3]) for i in range(len(arrays))]
+    check_batch(am, oracle, arrays, opts)
 
 
-def test_all_null_and_constant_arrays(am):
+def test_all_null_and_constant_arrays(am, oracle):
     arrays = [pa.array([None] * 5000, type=pa.int64()), pa.array(np.full(9000, 7, dtype=np.int32)),
               pa.array([None] * 3, type=pa.float32()), pa.array(np.full(5000, np.nan))]
     opts = [(False, "at_start", "ieee"), (True, "at_end", "ieee"), (False, "at_end", "total"),
             (True, "at_start", "nan_largest")]
-    check_batch(am, arrays, opts)
+    check_batch(am, oracle, arrays, opts)
 
 
 def test_empty_batch(am):
     assert am.argsort_batch([]) == []
 
 
-def test_repeated_shapes_replay_a_graph(am):
+def test_repeated_shapes_replay_a_graph(am, oracle):
     # The second batch of a shape (same key widths and lengths) is captured into a CUDA graph and
     # later ones replay it with their own columns, options and outputs: every call must still match
     # am_argsort_ex2. Two shapes alternate, so both graphs stay in use.
@@ -138,10 +137,10 @@ def test_repeated_shapes_replay_a_graph(am):
             for n, kinds in shape:
                 arrays.append(random_array(rng, kinds[int(rng.integers(len(kinds)))], n))
                 opts.append((bool(rng.integers(2)), PLACEMENTS[rng.integers(2)], ORDERS[rng.integers(3)]))
-            check_batch(am, arrays, opts)
+            check_batch(am, oracle, arrays, opts)
     am.profile(True)
     am.profile_reset()
-    check_batch(am, [random_array(rng, "int64", n) if k is wide else random_array(rng, "int32", n)
+    check_batch(am, oracle, [random_array(rng, "int64", n) if k is wide else random_array(rng, "int32", n)
                      for n, k in shape_a], [(False, "at_end", "ieee")] * len(shape_a))
     assert "batch_graph" in am.profile_entries()
     am.profile(False)

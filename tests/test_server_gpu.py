@@ -15,6 +15,10 @@ N = 600_000
 
 
 def table(am, seed=5):
+    return table_and_columns(am, seed)[0]
+
+
+def table_and_columns(am, seed=5):
     rng = np.random.default_rng(seed)
     k64 = build_array("int64", rng.integers(-2**40, 2**40, N, dtype=np.int64), rng.random(N) > 0.05)
     fv = rng.standard_normal(N)
@@ -25,7 +29,7 @@ def table(am, seed=5):
     p1 = pa.array(rng.standard_normal(N))
     p2 = pa.array(rng.integers(-2**31, 2**31 - 1, N, dtype=np.int32, endpoint=True))
     cols = {"k64": k64, "kf": kf, "k32": k32, "p1": p1, "p2": p2}
-    return am.PlanSource("t", {k: am.MetalArray.from_arrow(v) for k, v in cols.items()})
+    return am.PlanSource("t", {k: am.MetalArray.from_arrow(v) for k, v in cols.items()}), cols
 
 
 def plan_alone(offset, length, keys, desc, nulls, orders, payload):
@@ -89,6 +93,40 @@ def test_mix_equals_alone(am):
         assert list(got) == list(want), r
         for name in want:
             assert same(got[name].to_arrow(), want[name].to_arrow()), (r, name)
+
+
+def expected_order(oracle, cols, offset, length, keys, desc, nulls, orders):
+    """Row numbers (within the slice) of the request's sort: pyarrow's sort_indices where its options
+    can say it (ieee order, one null placement for every key), else the oracle's definition."""
+    import pyarrow.compute as pc
+    part = {k: cols[k].slice(offset, length) for k in keys}
+    if all(o == "ieee" for o in orders) and len(set(nulls)) == 1:
+        t = pa.table(part)
+        by = [(k, "descending" if d else "ascending") for k, d in zip(keys, desc)]
+        return pc.sort_indices(t, sort_keys=by, null_placement=nulls[0]).to_numpy().astype(np.int64)
+    return oracle.np_lexsort([part[k] for k in keys], desc, nulls, orders).astype(np.int64)
+
+
+def test_served_results_match_pyarrow_on_a_sample(am, oracle):
+    # A sampled subset of a served mix, checked outside the library: the order against pyarrow's
+    # sort_indices (or the oracle where pyarrow has no such order), the columns against pyarrow's take
+    # of the source slice through that order.
+    src, cols = table_and_columns(am, seed=10)
+    rng = np.random.default_rng(12)
+    reqs = random_requests(rng, 60)
+    with am.Server(workers=4, hbm_cap_bytes=8 << 30, batch_rows=1 << 17) as srv:
+        tickets = [srv.submit(src, o, n, k, p, descending=d, null_placement=nl, float_order=fo)
+                   for (o, n, k, d, nl, fo, p) in reqs]
+        results = [srv.wait(t)[0] for t in tickets]
+    sample = rng.choice(len(reqs), 20, replace=False)
+    for i in sample:
+        offset, length, keys, desc, nulls, orders, payload = reqs[i]
+        order = pa.array(expected_order(oracle, cols, offset, length, keys, desc, nulls, orders))
+        got = results[i]
+        assert list(got) == list(keys) + list(payload), reqs[i]
+        for name in got:
+            want = cols[name].slice(offset, length).take(order)
+            assert same(got[name].to_arrow(), want), (reqs[i], name)
 
 
 def test_admission_keeps_footprint_under_cap(am):

@@ -126,6 +126,21 @@ def test_ipc_rows_past_their_buffers(tmp_path):
         am.scan_ipc(bad).to_reader().read_all()
 
 
+@pytest.mark.parametrize("column,rows", [(np.arange(1000, dtype=np.int64), 2**61),
+                                         (pa.array(["ab"] * 1000), 2**62)])
+def test_ipc_row_counts_that_would_wrap_a_size(tmp_path, column, rows):
+    # 2^61 rows of 8 bytes (or 2^62 + 1 offsets of 4 bytes) is 2^64 bytes and more: a size formed by
+    # multiplying would wrap to a few bytes and pass; the reader must still refuse it.
+    src = tmp_path / "ok.arrows"
+    write_stream(src, pa.table({"x": column}), 1000)
+    msgs = messages_of(src)
+    assert patch_int64(msgs[1][0], 1000, rows) >= 2
+    bad = tmp_path / "wrap.arrows"
+    write_messages(bad, msgs)
+    with pytest.raises((am.ArrowMetalError, OSError), match="shorter than its column"):
+        am.scan_ipc(bad).to_reader().read_all()
+
+
 def test_ipc_nulls_without_a_bitmap(tmp_path):
     src = tmp_path / "ok.arrows"
     write_stream(src, pa.table({"x": np.arange(1000, dtype=np.int64)}), 1000)

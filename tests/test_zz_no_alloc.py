@@ -52,6 +52,7 @@ def noalloc(am):
             raise am.ArrowMetalError(am._lib.am_last_error().decode())
         return out[: len(arr)].cpu().numpy().view(np.uint32)
 
+    run.entry = f
     return run
 
 
@@ -132,3 +133,38 @@ def test_rejects_more_rows_than_the_limit(am, noalloc):
 
 def test_empty_column(am, noalloc):
     assert len(noalloc(pa.array([], type=pa.int64()))) == 0
+
+
+def test_calls_after_the_first_leave_device_memory_untouched(am, noalloc):
+    # After a first call (which sets the entry point up on this device), further calls change neither
+    # the library's memory pool (the device's default pool: in use and reserved) nor the device's free
+    # memory. The column and the output are allocated once, before the figures are taken.
+    import torch
+    from cuda.bindings import runtime as cudart
+    ordinal = am._lib.am_cuda_device()
+    dev = torch.device("cuda", ordinal)
+    rng = np.random.default_rng(5)
+    n = 100_000
+    values = torch.from_numpy(rng.integers(0, 1 << 40, n, dtype=np.int64)).to(dev)
+    out = torch.empty(n, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+
+    def call():
+        assert noalloc.entry(b"l", values.data_ptr(), None, 0, n, 0, 0, 0, out.data_ptr(), stream) == 0
+        torch.cuda.synchronize(dev)
+
+    def figures():
+        err, pool = cudart.cudaDeviceGetDefaultMemPool(ordinal)
+        assert err == cudart.cudaError_t.cudaSuccess
+        used = cudart.cudaMemPoolGetAttribute(pool, cudart.cudaMemPoolAttr.cudaMemPoolAttrUsedMemCurrent)
+        reserved = cudart.cudaMemPoolGetAttribute(pool, cudart.cudaMemPoolAttr.cudaMemPoolAttrReservedMemCurrent)
+        assert used[0] == reserved[0] == cudart.cudaError_t.cudaSuccess
+        return int(used[1]), int(reserved[1]), torch.cuda.mem_get_info(dev)[0]
+
+    call()
+    before = figures()
+    for _ in range(5):
+        call()
+    assert figures() == before
+    want = np.argsort(values.cpu().numpy(), kind="stable").astype(np.uint32)
+    assert np.array_equal(out.cpu().numpy().view(np.uint32), want)
