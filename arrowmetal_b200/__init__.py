@@ -74,9 +74,14 @@ class ServerStats(ctypes.Structure):
                                     "peak_in_flight_bytes", "in_flight_bytes", "queued")]
 
 
+class BatchShape(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int32) for n in ("key_bytes", "size_class", "threads", "items", "digit_bits")]
+
+
 class SortStats(ctypes.Structure):
     _fields_ = [("rows", _I64), ("value_rows", _I64), ("passes_run", ctypes.c_int32),
-                ("passes_skipped", ctypes.c_int32), ("kernel_us", ctypes.c_double)]
+                ("passes_skipped", ctypes.c_int32), ("kernel_us", ctypes.c_double),
+                ("payload_in_records", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 def _sig(name, res, args):
@@ -115,6 +120,7 @@ for _name, _res, _args in [
     ("am_router_set_mode", _I, [_I]), ("am_router_get_mode", _I, []),
     ("am_cuda_set_stream", _I, [_P]), ("am_cuda_get_stream", _P, []), ("am_cuda_synchronize", _I, []),
     ("am_cuda_device", _I, []), ("am_last_sort_stats", _I, [ctypes.POINTER(SortStats)]),
+    ("am_cuda_batch_tuning", _I, [ctypes.POINTER(BatchShape), _I64, ctypes.POINTER(_I64)]),
     ("am_cuda_profile", _I, [_I]), ("am_cuda_profile_count", _I64, []),
     ("am_cuda_profile_entry", _I, [_I64, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(_I64),
                                    ctypes.POINTER(ctypes.c_double)]),
@@ -763,7 +769,17 @@ def last_sort_stats():
     s = SortStats()
     _ok(_lib.am_last_sort_stats(ctypes.byref(s)))
     return {"rows": s.rows, "value_rows": s.value_rows, "passes_run": s.passes_run,
-            "passes_skipped": s.passes_skipped}
+            "passes_skipped": s.passes_skipped, "payload_in_records": bool(s.payload_in_records)}
+
+
+def batch_tuning():
+    """The segmented sort's tile shapes as its autotuner chose them: one dict per key width and size
+    class (threads 0: that class has not been measured yet)."""
+    count = _I64()
+    _ok(_lib.am_cuda_batch_tuning(None, 0, ctypes.byref(count)))
+    shapes = (BatchShape * max(count.value, 1))()
+    _ok(_lib.am_cuda_batch_tuning(shapes, count.value, ctypes.byref(count)))
+    return [{name: getattr(sh, name) for name, _ in BatchShape._fields_} for sh in shapes[:count.value]]
 
 
 def profile(on=True):

@@ -1195,6 +1195,17 @@ int am_last_sort_stats(am_sort_stats* out) {
   });
 }
 
+int am_cuda_batch_tuning(am_batch_shape* out, int64_t capacity, int64_t* count) {
+  if (!count || capacity < 0 || (capacity > 0 && !out)) return 2;
+  return guard([&] {
+    const auto v = batch_tuning();
+    *count = int64_t(v.size());
+    for (size_t i = 0; i < v.size() && int64_t(i) < capacity; i++)
+      out[i] = am_batch_shape{v[i][0], v[i][1], v[i][2], v[i][3], v[i][4]};
+    return 0;
+  });
+}
+
 int am_cuda_profile(int on) {
   set_profiling(on != 0);
   return 0;

@@ -12,6 +12,7 @@
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <array>
 #include <vector>
 
 #include "../../include/arrowmetal.h"
@@ -247,7 +248,7 @@ struct SortKey {
 void radix_argsort(const std::vector<SortKey>& keys, int64_t n, void* out, int index_width,
                    cudaStream_t s, am_sort_stats* stats);
 
-namespace rs { struct KeyStats; struct ColView; ColView make_view(const SortKey& k); }
+namespace rs { struct KeyStats; struct ColView; struct RecLayout; ColView make_view(const SortKey& k); }
 // The key column's statistics (all digit histograms of its value keys, null / NaN / value counts)
 // into `st` on the device.
 void key_statistics(const SortKey& k, rs::KeyStats* st, cudaStream_t s);
@@ -259,12 +260,18 @@ am_array* radix_top_k(const SortKey& key, int64_t k, cudaStream_t s);
 bool key_invertible(const SortKey& k);
 // The sort engine. `out` (may be NULL) receives the index array; `key_dst` (may be NULL; one
 // key_invertible key only) receives the sorted key column, rebuilt from the sorted keys by the last
-// pass, so a sorted copy of the key needs no gather.
+// pass, so a sorted copy of the key needs no gather. `payload` (may be NULL; one key only): payload
+// columns carried through the sort in row records and written, sorted, to their destinations.
 void radix_sort(const std::vector<SortKey>& keys, int64_t n, void* out, int index_width, am_array* key_dst,
-                cudaStream_t s, am_sort_stats* stats);
+                cudaStream_t s, am_sort_stats* stats, const rs::RecLayout* payload = nullptr);
+// The row-record layout of payload columns (RecLayout without its destinations), or false when they
+// cannot ride in a record: at most four fixed-width columns without nulls, twelve bytes in all.
+bool payload_record_layout(const std::vector<am_array*>& cols, rs::RecLayout* L);
 // Segmented argsort: outs[i] (a uint32 array of keys[i].col->length rows) receives the argsort of
 // keys[i], one key per array; the arrays of a key width share every launch.
 void radix_argsort_batch(const std::vector<SortKey>& keys, const std::vector<void*>& outs, cudaStream_t s);
+// The segmented sort's chosen tile shapes: {key bytes, size class, threads, rows per thread, digit bits}.
+std::vector<std::array<int32_t, 5>> batch_tuning();
 // Single-key argsort of a device column into a caller's uint32 array with no allocation: all
 // scratch sits in a fixed device block of the library (radix_sort.cu). Waits for its work.
 uint64_t noalloc_max_rows();

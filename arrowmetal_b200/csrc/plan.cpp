@@ -13,6 +13,7 @@
 #include "am_internal.h"
 #include "json.h"
 #include "plan_types.h"
+#include "radix_sort.cuh"
 
 using namespace am;
 
@@ -146,6 +147,56 @@ std::vector<am_array*> materialize(Frame& f, const std::vector<int>& which) {
 
 Frame eval(const json::Value& node, am_plan_source** sources, int64_t nsrc, std::ostringstream* explain, int depth);
 
+// A column whose contents are complete on the device (no upload still running).
+bool settled(const am_array* c) {
+  return !c->ready || cudaEventQuery(c->ready->ev) == cudaSuccess;
+}
+
+// One invertible key over an unpermuted frame whose other columns are complete in device memory and
+// fit a 16-byte row record: they ride through the sort with their rows and come out sorted where the
+// rows reach their final places, so nothing is gathered afterwards. Columns still uploading (imports
+// from host memory) are gathered after the sort instead, which then waits only for the key column.
+// Returns false, with the frame untouched, when the frame does not qualify.
+bool sort_payload_in_records(Frame& f, int key_col, const SortKey& key, cudaStream_t s) {
+  std::vector<am_array*> pay;
+  for (size_t c = 0; c < f.cols.size(); c++)
+    if (int(c) != key_col) pay.push_back(f.cols[c]);
+  rs::RecLayout rl{};
+  if (pay.empty() || !payload_record_layout(pay, &rl)) return false;
+  for (am_array* c : pay)
+    if (c->length != f.rows || !settled(c)) return false;
+  for (am_array* c : pay) use_on(c, s);
+  am_array* sorted_key = new_array(key.col->pt, key.col->format, f.rows);
+  std::vector<am_array*> outs;
+  try {
+    for (size_t i = 0; i < pay.size(); i++) {
+      am_array* o = new_array(pay[i]->pt, pay[i]->format, f.rows);
+      outs.push_back(o);
+      o->values = DevBuffer::alloc(size_t(f.rows) * size_t(rl.width[i]) + 16, s);
+      o->null_count = 0;
+      o->last_stream = s;
+      rl.dst[i] = o->values->ptr;
+    }
+    radix_sort({key}, f.rows, nullptr, 4, sorted_key, s, &tls().last_stats, &rl);
+  } catch (...) {
+    am::release(sorted_key);
+    for (am_array* o : outs) am::release(o);
+    throw;
+  }
+  auto ready = std::make_shared<ReadyEvent>(s);
+  size_t t = 0;
+  for (size_t c = 0; c < f.cols.size(); c++) {
+    am::release(f.cols[c]);
+    if (int(c) == key_col) {
+      f.cols[c] = sorted_key;
+    } else {
+      outs[t]->ready = ready;
+      f.cols[c] = outs[t++];
+    }
+  }
+  return true;
+}
+
 // The sort of a frame by `keys`.
 Frame sort_frame(Frame f, const std::vector<KeySpec>& keys) {
   std::vector<int> which;
@@ -164,6 +215,7 @@ Frame sort_frame(Frame f, const std::vector<KeySpec>& keys) {
       check_index_rows(f.rows, "sort");
       cudaStream_t s = stream();
       use_on(key.col, s);
+      if (sort_payload_in_records(f, which[0], key, s)) return f;
       am_array* sorted_key = new_array(key.col->pt, key.col->format, f.rows);
       am_array* idx = new_array(PT_U32, "I", f.rows);
       std::vector<am_array*> src, taken;

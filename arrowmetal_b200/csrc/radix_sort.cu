@@ -24,6 +24,7 @@
 #include <list>
 #include <memory>
 #include <cstring>
+#include <type_traits>
 
 #include "am_internal.h"
 #include "radix_sort.cuh"
@@ -458,7 +459,7 @@ __global__ void __launch_bounds__(256) segmented_plan_kernel(const SegDesc* __re
 // into global offsets; and the rows leave shared memory in order, so consecutive threads write
 // consecutive addresses within every digit run.
 
-template <typename KeyT, int THREADS, int ITEMS>
+template <typename KeyT, int THREADS, int ITEMS, typename IdT = uint32_t>
 struct PassShared {
   static constexpr int WARPS = THREADS / 32;
   static constexpr int TILE = THREADS * ITEMS;
@@ -474,7 +475,7 @@ struct PassShared {
   uint32_t seg;
   uint16_t dig[TILE];
   KeyT keys[TILE];
-  uint32_t ids[TILE];
+  IdT ids[TILE];                 // row ids; in record passes, the row's place within the tile
 };
 
 // Inverse of the integer and totalOrder key maps (SortSource.swift:131-190 read backwards): the value
@@ -503,13 +504,48 @@ __device__ __forceinline__ void store_width(void* base, uint64_t i, int width, u
     default: static_cast<uint8_t*>(base)[i] = uint8_t(v); break;
   }
 }
-template <typename KeyT, typename StatusT, int THREADS, int ITEMS, bool SEG>
+// ---- payload records (RecLayout)
+
+__device__ __forceinline__ uint64_t load_width(const void* base, uint64_t i, int width) {
+  switch (width) {
+    case 8: return static_cast<const uint64_t*>(base)[i];
+    case 4: return static_cast<const uint32_t*>(base)[i];
+    case 2: return static_cast<const uint16_t*>(base)[i];
+    default: return static_cast<const uint8_t*>(base)[i];
+  }
+}
+
+// Row `row`'s record: its id and its payload fields read from the columns.
+__device__ __forceinline__ uint4 build_record(const RecLayout& L, uint32_t row) {
+  uint64_t lo = 0;           // payload bytes 0-7
+  uint32_t hi = 0;           // payload bytes 8-11
+  for (int c = 0; c < L.ncols; c++) {
+    const uint64_t v = load_width(L.src[c], row, L.width[c]);
+    const int o = L.off[c];
+    if (o < 8) lo |= v << (8 * o);
+    else hi |= uint32_t(v) << (8 * (o - 8));
+  }
+  return make_uint4(row, uint32_t(lo), uint32_t(lo >> 32), hi);
+}
+
+// A record's payload fields, written to row `dst` of the sorted payload columns.
+__device__ __forceinline__ void unpack_record(const RecLayout& L, const uint4& r, uint64_t dst) {
+  const uint64_t lo = uint64_t(r.y) | (uint64_t(r.z) << 32);
+  for (int c = 0; c < L.ncols; c++) {
+    const int o = L.off[c];
+    const uint64_t v = o < 8 ? (lo >> (8 * o)) : uint64_t(r.w >> (8 * (o - 8)));
+    store_width(L.dst[c], dst, L.width[c], v);
+  }
+}
+
+template <typename KeyT, typename StatusT, int THREADS, int ITEMS, bool SEG, bool REC = false>
 __global__ void __launch_bounds__(THREADS, 2)
 onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant__ ColView col_arg) {
   static_assert(THREADS >= NBINS && THREADS % 32 == 0, "one thread per digit bin");
   static_assert(THREADS * ITEMS <= 65536, "tile-local ranks are 16-bit");
+  static_assert(!(SEG && REC), "record passes sort one array");
   using ST = Status<StatusT>;
-  using SM = PassShared<KeyT, THREADS, ITEMS>;
+  using SM = PassShared<KeyT, THREADS, ITEMS, std::conditional_t<REC, uint16_t, uint32_t>>;
   constexpr int TILE = SM::TILE;
   constexpr int WARPS = SM::WARPS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -607,7 +643,7 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
 #pragma unroll
     for (int i = 0; i < ITEMS; i++)
       if (wbase + uint64_t(i) * 32 < count) ok |= 1u << i;
-    if (ids_in && pa.carry_ids) {
+    if (ids_in && pa.carry_ids && !REC) {
 #pragma unroll
       for (int i = 0; i < ITEMS; i++) id[i] = ((ok >> i) & 1u) ? ids_in[wbase + uint64_t(i) * 32] : 0u;
     } else {
@@ -703,7 +739,8 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
           if (lane == __ffs(peers) - 1) sm.whist[warp][d] = base + __popc(peers);
           const uint32_t pos = sm.local[d] + base + __popc(peers & lt_mask);
           sm.keys[pos] = key[i];
-          if (pa.carry_ids) sm.ids[pos] = id[i];
+          if constexpr (REC) sm.ids[pos] = uint16_t(id[i] - uint32_t(tile_base));
+          else if (pa.carry_ids) sm.ids[pos] = id[i];
           sm.dig[pos] = uint16_t(d);
         }
         __syncwarp();
@@ -761,7 +798,38 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
     const uint32_t buf_rows = sm.desc.buf_rows, out_rows = sm.desc.out_rows;
     const bool last = (flags & PF_LAST) != 0;
     const bool merged = keys_out && ids_out && pa.carry_ids;
-    if (merged) {
+    if constexpr (REC) {
+      // Keys and records in one loop. A row's record comes from its place in the tile's input (the
+      // tile's records, read in sorted order, stay within one L2-resident span), or is built from the
+      // payload columns in the first pass; a row reaching its final place has its record unpacked.
+      const uint4* __restrict__ rin = reinterpret_cast<const uint4*>(ids_in);
+      uint4* __restrict__ rout = reinterpret_cast<uint4*>(ids_out);
+      for (uint32_t j = threadIdx.x; j < tile_n; j += THREADS) {
+        const uint32_t d = sm.dig[j];
+        uint32_t dst = sm.gdelta[d] + j;
+        const uint64_t src_row = tile_base + sm.ids[j];
+        const uint4 r = (flags & PF_ENCODE) ? build_record(pa.rec, uint32_t(src_row)) : rin[src_row];
+        if (d < RADIX && rout) {
+          if (dst < buf_rows) {
+            if (keys_out) keys_out[dst] = sm.keys[j];
+            rout[dst] = r;
+          } else {
+            atomicOr(pa.err, ERR_BOUNDS);
+          }
+          continue;
+        }
+        if (d < RADIX) dst += sm.desc.value_base;
+        if (dst >= out_rows) {
+          atomicOr(pa.err, ERR_BOUNDS);
+          continue;
+        }
+        if (final_out) {
+          if (flags & PF_WIDE_OUT) static_cast<uint64_t*>(final_out)[dst] = r.x;
+          else static_cast<uint32_t*>(final_out)[dst] = r.x;
+        }
+        unpack_record(pa.rec, r, dst);
+      }
+    } else if (merged) {
       for (uint32_t j = threadIdx.x; j < tile_n; j += THREADS) {
         const uint32_t d = sm.dig[j];
         const uint32_t dst = sm.gdelta[d] + j;
@@ -802,7 +870,7 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
         store_width(pa.key_out, dst, kw, v);
       }
     }
-    if (pa.carry_ids && !merged) {
+    if (pa.carry_ids && !merged && !REC) {
       for (uint32_t j = threadIdx.x; j < tile_n; j += THREADS) {
         const uint32_t d = sm.dig[j];
         const uint32_t v = sm.ids[j];
@@ -1150,9 +1218,9 @@ __global__ void __launch_bounds__(1024) bounds_decide_kernel(HybridState* __rest
 // The local sorts: each bucket of the value rows, sorted by the digits below the bucket digits in
 // shared memory, then written to its final rows (ids, and the key column rebuilt when asked). A
 // persistent grid of CTAs walks the buckets; a shape that is not the chosen one returns at once.
-template <int THREADS, int VARIANT>
+template <int THREADS, int VARIANT, bool REC = false>
 __global__ void __launch_bounds__(THREADS, THREADS == 128 ? 10 : THREADS == 256 ? 5 : 2) local_sort_kernel(const uint64_t* __restrict__ keys,
-                                                             const uint32_t* __restrict__ ids,
+                                                             const void* __restrict__ ids_or_recs,
                                                              const uint32_t* __restrict__ pos,
                                                              const HybridState* __restrict__ hs,
                                                              const __grid_constant__ PassArgs pa) {
@@ -1164,6 +1232,9 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? 10 : THREADS == 256 
   uint32_t* local = whist + WARPS * 256;              // [256]
   uint32_t* wsum = local + 256;                       // [WARPS]
   if (!hs->mode || hs->fallback || hs->variant != uint32_t(VARIANT)) return;
+  // Row ids, or (record sorts) 16-byte records; a record sort ranks each row's place in its bucket.
+  const uint32_t* __restrict__ ids = static_cast<const uint32_t*>(ids_or_recs);
+  const uint4* __restrict__ recs = static_cast<const uint4*>(ids_or_recs);
   const uint32_t g = hs->buckets, nloc = hs->nlocal, vbase = hs->value_base;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t lt = (1u << lane) - 1u;
@@ -1180,7 +1251,8 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? 10 : THREADS == 256 
     for (int i = 0; i < ITEMS; i++) {
       const uint32_t r = uint32_t(warp) * (ITEMS * 32) + uint32_t(i) * 32 + lane;
       key[i] = r < size ? keys[start + r] : 0ull;
-      id[i] = r < size ? ids[start + r] : 0u;
+      if constexpr (REC) id[i] = r;
+      else id[i] = r < size ? ids[start + r] : 0u;
     }
     // The tile's empty slots (r >= size) are the last rows in order. They take digit 255 in the ballots
     // but are neither counted nor stored: every row before them keeps its place in [0, size), and their
@@ -1193,7 +1265,96 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? 10 : THREADS == 256 
     // whose slots are all empty and all after every row.
     const uint32_t w_first = uint32_t(warp) * (ITEMS * 32);
     const int nit = size > w_first ? int(min(uint32_t(ITEMS), (size - w_first + 31) / 32)) : 0;
-    for (uint32_t dgi = 0; dgi < nloc; dgi++) {
+
+    // ---- Ranking by one counting step. Rows go to NB bins by the top bits of their two highest local
+    // digits (shared-memory atomics: in no particular order within a bin); a row's place is its bin's
+    // start plus the number of its bin's rows that order before it by (the key bits below the bucket
+    // digits, the row's place in the bucket): a unique pair, so the order is total and ties keep bucket
+    // order, which is row order. Taken when no bin holds more than HASH_MAX_BIN rows (uniform keys put
+    // one to three rows in a bin); otherwise the ballot ranking below runs, one pass per local digit.
+    bool hashed = false;
+    {
+      constexpr int NB = WARPS * 128;                     // cnt and bstart fill whist's WARPS x 256 words
+      constexpr int NBB = NB == 512 ? 9 : NB == 1024 ? 10 : 11;
+      constexpr int PER = NB / THREADS;
+      constexpr uint32_t HASH_MAX_BIN = 32;
+      static_assert(NB == 512 || NB == 1024 || NB == 2048, "bins per local-sort shape");
+      uint32_t* cnt = whist;
+      uint32_t* bstart = whist + NB;
+      const uint32_t sh_top = hs->local_shift[nloc - 1];
+      const uint32_t sh_next = nloc >= 2 ? hs->local_shift[nloc - 2] : 0u;
+      const bool two = nloc >= 2;
+      const uint64_t lmask = (uint64_t(1) << hs->lo_shift) - 1u;     // lo_shift <= 48
+      auto bin_of = [&](uint64_t k) {
+        const uint32_t hi16 = ((uint32_t(k >> sh_top) & 255u) << 8) | (two ? (uint32_t(k >> sh_next) & 255u) : 0u);
+        return hi16 >> (16 - NBB);
+      };
+      for (int x = threadIdx.x; x < NB; x += THREADS) cnt[x] = 0;
+      if (threadIdx.x == 0) local[0] = 0;
+      __syncthreads();
+      uint32_t slot[ITEMS];
+#pragma unroll
+      for (int i = 0; i < ITEMS; i++) slot[i] = ((ok >> i) & 1u) ? atomicAdd(&cnt[bin_of(key[i])], 1u) : 0u;
+      __syncthreads();
+      // Bin starts (exclusive scan over the bins, PER consecutive bins a thread) and the largest bin.
+      uint32_t c[PER];
+      uint32_t tot = 0, mx = 0;
+#pragma unroll
+      for (int q = 0; q < PER; q++) {
+        c[q] = cnt[int(threadIdx.x) * PER + q];
+        tot += c[q];
+        mx = max(mx, c[q]);
+      }
+      uint32_t x = tot;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+      }
+      mx = __reduce_max_sync(0xffffffffu, mx);
+      if (lane == 31) wsum[warp] = x;
+      if (lane == 0) atomicMax(&local[0], mx);
+      __syncthreads();
+      uint32_t at = x - tot;
+      for (int w = 0; w < warp; w++) at += wsum[w];
+#pragma unroll
+      for (int q = 0; q < PER; q++) {
+        bstart[int(threadIdx.x) * PER + q] = at;
+        at += c[q];
+      }
+      __syncthreads();
+      if (local[0] <= HASH_MAX_BIN) {
+        hashed = true;
+        uint64_t* comp = skeys;                           // the tile holds the bins' pairs first
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++) {
+          if (!((ok >> i) & 1u)) continue;
+          const uint32_t r = uint32_t(warp) * (ITEMS * 32) + uint32_t(i) * 32 + lane;
+          comp[bstart[bin_of(key[i])] + slot[i]] = ((key[i] & lmask) << 12) | r;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++) {
+          if (!((ok >> i) & 1u)) continue;
+          const uint32_t r = uint32_t(warp) * (ITEMS * 32) + uint32_t(i) * 32 + lane;
+          const uint32_t b = bin_of(key[i]);
+          const uint32_t s0 = bstart[b], nb = cnt[b];
+          const uint64_t me = ((key[i] & lmask) << 12) | r;
+          uint32_t rank = 0;
+          for (uint32_t q = 0; q < nb; q++) rank += comp[s0 + q] < me ? 1u : 0u;
+          slot[i] = s0 + rank;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++) {
+          if (!((ok >> i) & 1u)) continue;
+          skeys[slot[i]] = key[i];
+          sids[slot[i]] = id[i];
+        }
+        __syncthreads();
+      }
+    }
+    for (uint32_t dgi = 0; dgi < nloc && !hashed; dgi++) {
       const uint32_t shift = hs->local_shift[dgi];
       uint32_t dg[ITEMS];
 #pragma unroll
@@ -1285,7 +1446,15 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? 10 : THREADS == 256 
         atomicOr(pa.err, ERR_BOUNDS);
         continue;
       }
-      if (pa.final_out) {
+      if constexpr (REC) {
+        // The row's record, from its place in the bucket's input (one L2-resident span).
+        const uint4 rr = recs[start + sids[r]];
+        if (pa.final_out) {
+          if (pa.desc->flags & PF_WIDE_OUT) static_cast<uint64_t*>(pa.final_out)[dst] = rr.x;
+          else static_cast<uint32_t*>(pa.final_out)[dst] = rr.x;
+        }
+        unpack_record(pa.rec, rr, dst);
+      } else if (pa.final_out) {
         if (pa.desc->flags & PF_WIDE_OUT) static_cast<uint64_t*>(pa.final_out)[dst] = sids[r];
         else static_cast<uint32_t*>(pa.final_out)[dst] = sids[r];
       }
@@ -1315,21 +1484,22 @@ constexpr int SEG_THREADS = 512;
 
 constexpr int HIST_THREADS = 256, HIST_ITEMS = 8;
 
-template <typename KeyT, int ITEMS = PassConfig<KeyT>::ITEMS, int THREADS = PassConfig<KeyT>::THREADS>
+template <typename KeyT, int ITEMS = PassConfig<KeyT>::ITEMS, int THREADS = PassConfig<KeyT>::THREADS, bool REC = false>
 static size_t pass_smem() {
-  return sizeof(PassShared<KeyT, THREADS, ITEMS>);
+  return sizeof(PassShared<KeyT, THREADS, ITEMS, std::conditional_t<REC, uint16_t, uint32_t>>);
 }
 
 template <typename KeyT, typename StatusT, bool SEG = false, int ITEMS = PassConfig<KeyT>::ITEMS,
-          int THREADS = PassConfig<KeyT>::THREADS>
+          int THREADS = PassConfig<KeyT>::THREADS, bool REC = false>
 static int pass_blocks_per_sm() {
   static int cached = -1;
   static std::once_flag once;
   std::call_once(once, [] {
-    auto fn = onesweep_pass_kernel<KeyT, StatusT, THREADS, ITEMS, SEG>;
-    AM_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(pass_smem<KeyT, ITEMS, THREADS>())));
+    auto fn = onesweep_pass_kernel<KeyT, StatusT, THREADS, ITEMS, SEG, REC>;
+    const size_t smem = pass_smem<KeyT, ITEMS, THREADS, REC>();
+    AM_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     int b = 0;
-    AM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, THREADS, pass_smem<KeyT, ITEMS, THREADS>()));
+    AM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, THREADS, smem));
     cached = std::max(1, b);
   });
   return cached;
@@ -1350,9 +1520,16 @@ static void launch_pass(const PassArgs& pa, const ColView& cv, uint64_t n, cudaS
   using C = PassConfig<KeyT>;
   constexpr int TILE = C::THREADS * C::ITEMS;
   const uint64_t tiles = (n + TILE - 1) / TILE;
-  const int grid = int(std::min<uint64_t>(tiles, uint64_t(device().sm_count) * pass_blocks_per_sm<KeyT, StatusT>()));
   KernelTimer kt("radix_onesweep_pass", s);
-  onesweep_pass_kernel<KeyT, StatusT, C::THREADS, C::ITEMS, false><<<std::max(grid, 1), C::THREADS, pass_smem<KeyT>(), s>>>(pa, cv);
+  if (pa.rec_mode) {
+    const int bps = pass_blocks_per_sm<KeyT, StatusT, false, C::ITEMS, C::THREADS, true>();
+    const int grid = int(std::min<uint64_t>(tiles, uint64_t(device().sm_count) * bps));
+    onesweep_pass_kernel<KeyT, StatusT, C::THREADS, C::ITEMS, false, true>
+        <<<std::max(grid, 1), C::THREADS, pass_smem<KeyT, C::ITEMS, C::THREADS, true>(), s>>>(pa, cv);
+  } else {
+    const int grid = int(std::min<uint64_t>(tiles, uint64_t(device().sm_count) * pass_blocks_per_sm<KeyT, StatusT>()));
+    onesweep_pass_kernel<KeyT, StatusT, C::THREADS, C::ITEMS, false><<<std::max(grid, 1), C::THREADS, pass_smem<KeyT>(), s>>>(pa, cv);
+  }
   AM_CUDA(cudaGetLastError());
 }
 
@@ -1366,22 +1543,29 @@ __global__ void __launch_bounds__(256) zero_status_kernel(const PassDesc* __rest
 }
 
 // One local-sort shape as a persistent grid (it returns at once unless the decision chose it).
-template <int VARIANT>
-static void launch_local(const uint64_t* keys, const uint32_t* ids, const uint32_t* pos, const HybridState* hs,
-                         const PassArgs& a, cudaStream_t s) {
+template <int VARIANT, bool REC>
+static void launch_local_as(const uint64_t* keys, const void* ids, const uint32_t* pos, const HybridState* hs,
+                            const PassArgs& a, cudaStream_t s) {
   constexpr int THREADS = loc_threads(VARIANT);
   constexpr size_t SMEM = loc_smem_bytes<THREADS>();
   static int blocks = 0;
   static std::once_flag once;
   std::call_once(once, [] {
-    auto fn = local_sort_kernel<THREADS, VARIANT>;
+    auto fn = local_sort_kernel<THREADS, VARIANT, REC>;
     AM_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SMEM)));
     int b = 0;
     AM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, THREADS, SMEM));
     blocks = std::max(1, b);
   });
-  local_sort_kernel<THREADS, VARIANT><<<device().sm_count * blocks, THREADS, SMEM, s>>>(keys, ids, pos, hs, a);
+  local_sort_kernel<THREADS, VARIANT, REC><<<device().sm_count * blocks, THREADS, SMEM, s>>>(keys, ids, pos, hs, a);
   AM_CUDA(cudaGetLastError());
+}
+
+template <int VARIANT>
+static void launch_local(const uint64_t* keys, const void* ids, const uint32_t* pos, const HybridState* hs,
+                         const PassArgs& a, cudaStream_t s) {
+  if (a.rec_mode) launch_local_as<VARIANT, true>(keys, ids, pos, hs, a, s);
+  else launch_local_as<VARIANT, false>(keys, ids, pos, hs, a, s);
 }
 
 // Rows per look-back entry (a tile), the smallest over the key widths.
@@ -1447,13 +1631,40 @@ bool key_invertible(const SortKey& k) {
   }
 }
 
+bool payload_record_layout(const std::vector<am_array*>& cols, rs::RecLayout* L) {
+  using namespace rs;
+  if (cols.empty() || cols.size() > size_t(REC_MAX_COLS)) return false;
+  int total = 0;
+  for (am_array* c : cols) {
+    const int w = pt_bytes(c->pt);
+    if (c->pt == PT_STRUCT || c->dictionary || pt_var(c->pt) || c->pt == PT_BOOL || w <= 0 || c->null_count != 0)
+      return false;
+    total += w;
+  }
+  if (total > REC_PAYLOAD_BYTES) return false;
+  // Widest first: each field then starts at a multiple of its width, and an 8-byte field at byte 0.
+  std::vector<int> order(cols.size());
+  for (size_t i = 0; i < order.size(); i++) order[i] = int(i);
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return pt_bytes(cols[x]->pt) > pt_bytes(cols[y]->pt); });
+  *L = RecLayout{};
+  L->ncols = int32_t(cols.size());
+  int off = 0;
+  for (int i : order) {
+    L->src[i] = cols[size_t(i)]->data();
+    L->width[i] = pt_bytes(cols[size_t(i)]->pt);
+    L->off[i] = off;
+    off += L->width[i];
+  }
+  return true;
+}
+
 void radix_argsort(const std::vector<SortKey>& keys, int64_t n, void* out, int index_width, cudaStream_t s,
                    am_sort_stats* stats) {
   radix_sort(keys, n, out, index_width, nullptr, s, stats);
 }
 
 void radix_sort(const std::vector<SortKey>& keys, int64_t n64, void* out, int index_width, am_array* key_dst,
-                cudaStream_t s, am_sort_stats* stats) {
+                cudaStream_t s, am_sort_stats* stats, const rs::RecLayout* payload) {
   using namespace rs;
   const int K = int(keys.size());
   if (K < 1 || K > MAX_KEYS) throw invalid("sort takes 1 to " + std::to_string(MAX_KEYS) + " key columns (a string key counts as its 8-byte chunks plus one)");
@@ -1463,8 +1674,11 @@ void radix_sort(const std::vector<SortKey>& keys, int64_t n64, void* out, int in
   const uint64_t n = uint64_t(n64);
   if (key_dst && (K != 1 || !key_invertible(keys[0])))
     throw invalid("the sorted key column is rebuilt only for one integer or totalOrder float key");
-  // Row ids move through the passes when an index is wanted or a lower key's column is gathered.
-  const bool carry_ids = out != nullptr || K > 1;
+  if (payload && K != 1) throw invalid("payload columns ride through a sort by one key only");
+  // Row ids move through the passes when an index is wanted or a lower key's column is gathered;
+  // with payload columns, 16-byte row records (id and payload) move instead.
+  const bool carry_ids = out != nullptr || K > 1 || payload != nullptr;
+  const size_t id_bytes = payload ? sizeof(uint4) : sizeof(uint32_t);
 
   // Slots: least significant key first; its digits low to high, then (lower keys) a category slot.
   PlanArgs pa{};
@@ -1513,7 +1727,7 @@ void radix_sort(const std::vector<SortKey>& keys, int64_t n64, void* out, int in
   const size_t off_sum = (off_tick + sizeof(uint32_t) * NT + 15) & ~size_t(15);
   const size_t header = (off_sum + sizeof(SortSummary) + 255) & ~size_t(255);
   const size_t kbuf = ((n * max_kb) + 255) & ~size_t(255);
-  const size_t ibuf = carry_ids ? ((n * 4) + 255) & ~size_t(255) : 0;
+  const size_t ibuf = carry_ids ? ((n * id_bytes) + 255) & ~size_t(255) : 0;
   char* base = static_cast<char*>(dmalloc(header + 2 * kbuf + 2 * ibuf, s));
   AM_CUDA(cudaMemsetAsync(base, 0, header, s));
   KeyStats* st = reinterpret_cast<KeyStats*>(base + off_stats);
@@ -1586,6 +1800,10 @@ void radix_sort(const std::vector<SortKey>& keys, int64_t n64, void* out, int in
       a.key_desc = keys[0].descending ? 1 : 0;
       a.key_float_order = keys[0].float_order;
       a.key_out = key_dst->values->ptr;
+    }
+    if (payload) {
+      a.rec_mode = 1;
+      a.rec = *payload;
     }
     return a;
   };
@@ -1666,6 +1884,10 @@ void radix_sort(const std::vector<SortKey>& keys, int64_t n64, void* out, int in
       a.key_float_order = keys[0].float_order;
       a.key_out = key_dst->values->ptr;
     }
+    if (payload) {
+      a.rec_mode = 1;
+      a.rec = *payload;
+    }
     const ColView& cv = views[pa.slot_key[sl]];
     if (slot_bytes[sl] == 8) {
       if (narrow_status) launch_pass<uint64_t, uint32_t>(a, cv, n, s);
@@ -1688,6 +1910,7 @@ void radix_sort(const std::vector<SortKey>& keys, int64_t n64, void* out, int in
   if (stats) {
     // Counters arrive asynchronously; am_last_sort_stats waits for them.
     stats->rows = int64_t(n);
+    stats->payload_in_records = payload ? 1 : 0;
     AM_CUDA(cudaMemcpyAsync(last_summary_host(), sum, sizeof(SortSummary), cudaMemcpyDeviceToHost, s));
     tls().stats_stream = s;
   }
@@ -2035,6 +2258,17 @@ void sort_segment_group(const std::vector<SortKey>& keys, const std::vector<void
 
 }  // namespace
 }  // namespace rs
+
+std::vector<std::array<int32_t, 5>> batch_tuning() {
+  std::vector<std::array<int32_t, 5>> out;
+  std::lock_guard<std::mutex> g(rs::g_tune_mu);
+  for (int w = 0; w < 2; w++)
+    for (int c = 0; c < 2; c++) {
+      const int items = rs::g_tuned_items[w][c];
+      out.push_back({w ? 8 : 4, c, items ? rs::SEG_THREADS : 0, items, items ? 8 : 0});
+    }
+  return out;
+}
 
 void radix_argsort_batch(const std::vector<SortKey>& keys, const std::vector<void*>& outs, cudaStream_t s) {
   std::vector<size_t> g4, g8;

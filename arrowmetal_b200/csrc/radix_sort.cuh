@@ -91,6 +91,23 @@ struct SegDesc {
   uint32_t pad;
 };
 
+// Payload columns that ride through the sort with their rows (instead of a gather through the
+// permutation afterwards). A row's record is 16 bytes: word 0 its row id, bytes 4-15 its payload
+// fields, each at a multiple of its width (at most one 8-byte field, at byte 4). The first pass builds
+// each row's record from the columns; every later pass moves records; whatever writes a row to its
+// final place (the last pass, the local sorts, the first pass for null rows) unpacks its record into
+// the sorted payload columns. Payload columns are fixed-width without nulls.
+constexpr int REC_MAX_COLS = 4;
+constexpr int REC_PAYLOAD_BYTES = 12;
+struct RecLayout {
+  const void* src[REC_MAX_COLS];      // row 0 of each payload column
+  void* dst[REC_MAX_COLS];            // row 0 of each sorted payload column
+  int32_t width[REC_MAX_COLS];        // 1, 2, 4 or 8 bytes
+  int32_t off[REC_MAX_COLS];          // byte offset within the payload (0-11)
+  int32_t ncols;
+  int32_t pad;
+};
+
 // key_out modes: the sorted key column itself, produced by inverting the key map in the last pass.
 constexpr int KEY_OUT_NONE = 0, KEY_OUT_UNKEY = 1;
 
@@ -115,6 +132,10 @@ struct PassArgs {
   const SegDesc* segs;
   const uint32_t* tile_start;
   uint32_t nsegs, total_tiles, slot, nslots;
+  // Record passes (`ids` then hold 16-byte records, see RecLayout): the payload's layout.
+  int32_t rec_mode;
+  int32_t pad_rec;
+  RecLayout rec;
 };
 
 }  // namespace rs

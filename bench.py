@@ -96,7 +96,7 @@ def make_segments(count=SEGMENTS, seed=SEED + 2):
     return out
 
 
-def run_segmented(args, am, torch, stream, local):
+def run_segmented(args, am, torch, stream, local, emit=True):
     """2,048 arrays sorted by one am_argsort_batch call per step, against the same arrays sorted by 2,048
     plain am_argsort_ex2 calls per step (same library, same stream); device time by CUDA events."""
     arrays = make_segments()
@@ -160,9 +160,12 @@ def run_segmented(args, am, torch, stream, local):
         "gpu_launches": int(sum(l for l, _ in prof.values())),
         "e2e": {"value": rows / (e2e_ms / 1e3), "unit": "rows/s", "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(4 * rows)},
+        "tile_shapes": am.batch_tuning(),
         "clocks": clocks.summary(),
     }
-    print(json.dumps(line))
+    if emit:
+        print(json.dumps(line))
+    return line
 
 
 SERVE_TABLE_ROWS = 50_000_000
@@ -201,7 +204,7 @@ def serving_requests(count, rows=SERVE_TABLE_ROWS, seed=SEED + 5):
     return out
 
 
-def run_serving(args, am, torch, local):
+def run_serving(args, am, torch, local, emit=True):
     """The served stream: open-loop Poisson arrivals at --rate requests/s against resident tables for
     --serve-seconds, each request sorting a slice by its table's key(s) and taking the 2 payload columns;
     admission cap 120 GB. Reports p50/p99 latency (submission to completion) and rows/s; then the same
@@ -301,15 +304,19 @@ def run_serving(args, am, torch, local):
                        "speedup_served_over_plain": plain_s / served_s, "rows": sat_rows, "server": sat_stats},
         "clocks": clocks.summary(),
     }
-    print(json.dumps(line))
+    del tables
+    if emit:
+        print(json.dumps(line))
+    return line
 
 
-def run_single(args, am, torch, stream, local):
+def run_single(args, am, torch, stream, local, workload=None, emit=True):
     """--workload full_range: argsort of 1,000,000 int64 keys over the whole range, uint64 indices
     (am_argsort_ex3, index width 8); --workload multikey: the 50M-row two-key sort (key1 int32 Zipf
     descending, key2 float64 with specials and nulls ascending) and the take of its float64 payload."""
     import pyarrow as pa
-    if args.workload == "full_range":
+    workload = workload or args.workload
+    if workload == "full_range":
         arr = pa.array(make_full_range_keys(1_000_000))
         src = am.MetalArray.from_arrow(arr)
         rows = len(arr)
@@ -317,7 +324,7 @@ def run_single(args, am, torch, stream, local):
         def step():
             out = src.argsort64()
             del out
-        workload = "argsort of 1,000,000 int64 keys uniform over the whole int64 range, no nulls, uint64 indices"
+        description = "argsort of 1,000,000 int64 keys uniform over the whole int64 range, no nulls, uint64 indices"
         h2d, d2h = arr.nbytes, 8 * rows
         e2e_fn = lambda: am.MetalArray.from_arrow(arr).argsort64().to_arrow()
         dtype = "int64"
@@ -332,7 +339,7 @@ def run_single(args, am, torch, stream, local):
             idx = am.lexsort_indices([d1, d2], descending=[True, False], null_placement="at_end", float_order="ieee")
             out = am.take_columns([d1, d2, dp], idx)
             del idx, out
-        workload = ("ORDER BY key1 DESC (int32, 200 distinct values, Zipf 1.1), key2 ASC (float64 N(0,1e6) with "
+        description = ("ORDER BY key1 DESC (int32, 200 distinct values, Zipf 1.1), key2 ASC (float64 N(0,1e6) with "
                     "-0.0/+0.0/+inf/-inf 0.5% each, 1% NaN, 5% nulls), nulls last, ieee order; take of the 2 keys "
                     "and a float64 payload; 50,000,000 rows")
         h2d = a1.nbytes + a2.nbytes + ap.nbytes
@@ -358,9 +365,19 @@ def run_single(args, am, torch, stream, local):
         ev1.record(stream)
         ev1.synchronize()
         am.synchronize()
-    ms = ev0.elapsed_time(ev1) / steps
+    ms_profiled = ev0.elapsed_time(ev1) / steps
     prof = am.profile_entries()
     am.profile(False)
+    # The same steps again without the per-launch events: the step time reported.
+    am.synchronize()
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(steps):
+        step()
+    ev1.record(stream)
+    ev1.synchronize()
+    am.synchronize()
+    ms = ev0.elapsed_time(ev1) / steps
     e2e = []
     for i in range(4):
         torch.cuda.synchronize()
@@ -369,15 +386,19 @@ def run_single(args, am, torch, stream, local):
         e2e.append(time.perf_counter() - t0)
         del r
     e2e_ms = 1e3 * statistics.median(e2e[1:])
-    print(json.dumps({
+    line = {
         "metric": METRIC, "value": rows / (ms / 1e3), "unit": "rows/s", "n_gpus": 1, "steps": steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": dtype, "data": "synthetic", "config": {"workload": workload, "rows": rows},
+        "dtype": dtype, "data": "synthetic", "config": {"workload": description, "rows": rows},
+        "ms_per_step_profiled": ms_profiled,
         "per_kernel_ms_per_step": {k: t / steps for k, (l, t) in prof.items()},
         "gpu_launches": int(sum(l for l, _ in prof.values())),
         "e2e": {"value": rows / (e2e_ms / 1e3), "unit": "rows/s", "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
-        "clocks": clocks.summary()}))
+        "clocks": clocks.summary()}
+    if emit:
+        print(json.dumps(line))
+    return line
 
 
 def run_topk(args, am, torch, stream, local):
@@ -639,7 +660,7 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def algorithmic_bytes(n, m, passes, local_sort=False):
+def algorithmic_bytes(n, m, passes, local_sort=False, records=False):
     """Bytes each kernel of one step must move once (the roofline's model, per step):
     - histogram: reads the key column (8 B a row) and its validity bitmap;
     - digit passes: the first reads the key column and bitmap again and writes the m value rows'
@@ -650,8 +671,30 @@ def algorithmic_bytes(n, m, passes, local_sort=False):
       m (key, id) and write m ids and m rebuilt key values;
     - take: reads the n ids once and gathers and writes the two payload columns (8 + 4 B a row);
     - sort_finish: writes the sorted key column's validity bitmap.
-    The bucket-boundary kernels of the two-level sort move no compulsory bytes (like the plan)."""
+    The bucket-boundary kernels of the two-level sort move no compulsory bytes (like the plan).
+
+    With the payload carried in row records (`records`: the table is in HBM), each value row moves a
+    16-byte record (id + 12 payload bytes) beside its 8-byte key instead of a 4-byte id, and there is no
+    take:
+    - first pass: reads the key column, its bitmap and the two payload columns (12 B a row), writes
+      each value row's key and record (24 B) and each null row's key value and payload (8 + 12 B);
+    - a middle pass reads and writes 24 B a value row;
+    - the local sorts (or the last pass) read 24 B a value row and write its key value and payload
+      (8 + 12 B)."""
     src = 8 * n + n / 8
+    if records:
+        first = src + 12 * n + 24 * m + 20 * (n - m)
+        last = 24 * m + 20 * m
+        if passes <= 1:
+            pass_bytes = src + 12 * n + 20 * n
+        elif local_sort:
+            pass_bytes = first + (passes - 1) * 48 * m
+        else:
+            pass_bytes = first + (passes - 2) * 48 * m + last
+        out = {"radix_histogram": src, "radix_onesweep_pass": pass_bytes, "sort_finish": n / 8}
+        if local_sort:
+            out["radix_local_sort"] = last
+        return out
     if passes <= 1:
         pass_bytes = src + 12 * n
     else:
@@ -694,6 +737,71 @@ def cpu_oracle_rate(key, valid, p1, p2, threads):
         t.join()
     dt = time.perf_counter() - t0
     return len(key) / dt, dt
+
+
+def pyarrow_rate(key, valid, p1, p2, rows=10_000_000, repeats=3):
+    """pyarrow's sort_indices + Table.take (the reference's own oracle for this order) on the first
+    `rows` rows of the workload: one warm-up, then the best of `repeats`."""
+    import pyarrow as pa
+    import pyarrow.compute as pc
+    rows = min(rows, len(key))
+    t = pa.table(arrow_columns(key[:rows], valid[:rows], p1[:rows], p2[:rows]))
+    best = float("inf")
+    for i in range(repeats + 1):
+        t0 = time.perf_counter()
+        idx = pc.sort_indices(t, sort_keys=[("c0", "ascending")], null_placement="at_end")
+        out = t.take(idx)
+        dt = time.perf_counter() - t0
+        del idx, out
+        if i > 0:
+            best = min(best, dt)
+    return {"value": rows / best, "unit": "rows/s", "cores": os.cpu_count() or 1, "pyarrow_cpu_count": pa.cpu_count(),
+            "kind": "pyarrow", "version": pa.__version__,
+            "sample": f"the first {rows:,} rows of the workload: sort_indices + Table.take of the 3 columns, "
+                      f"best of {repeats} after one warm-up ({best:.2f} s)"}
+
+
+def datafusion_baseline():
+    """DataFusion's SortExec on the workload when the datafusion package is importable here."""
+    try:
+        import datafusion  # noqa: F401
+    except ImportError:
+        return {"unavailable": "unavailable on this box: the datafusion Python package is not installed and there "
+                               "is no network; the reference publishes 1,581.22 ms for this ORDER BY on DataFusion "
+                               "alone (Apple M4 Max, 16 cores; datafusion/results/datafusion_sort_warm_2026-09-29.csv:376)"}
+    return {"unavailable": "datafusion is importable but not timed by this benchmark"}
+
+
+def compact(line, drop=("metric", "unit", "n_gpus", "higher_is_better", "scaling", "vs_baseline", "data")):
+    """A configuration's line as a sub-object of the headline line (its shared keys dropped)."""
+    return {k: v for k, v in line.items() if k not in drop}
+
+
+def sub_workloads(args, am, torch, stream, local):
+    """The single-key scale case, the two-key sort, the segmented batch and the served stream, run after
+    the headline (one GPU); each is measured with its own CUDA events and clock record."""
+    import copy
+    out = {}
+    a = copy.copy(args)
+    a.steps = min(args.steps, 50)
+    a.warmup = max(args.warmup, 3)
+    out["full_range"] = compact(run_single(a, am, torch, stream, local, "full_range", emit=False))
+    am.synchronize()
+    out["multikey"] = compact(run_single(a, am, torch, stream, local, "multikey", emit=False))
+    am.synchronize()
+    b = compact(run_segmented(a, am, torch, stream, local, emit=False))
+    b["ratio_batched_over_plain"] = b["plain"]["speedup_batched_over_plain"]
+    out["batched"] = b
+    am.synchronize()
+    sv = copy.copy(a)
+    sv.serve_seconds = min(args.serve_seconds, args.sub_serve_seconds)
+    sv.sat_requests = min(args.sat_requests, args.sub_sat_requests)
+    s = compact(run_serving(sv, am, torch, local, emit=False))
+    s["p50_ms"] = s["open_loop"]["p50_ms"]
+    s["p99_ms"] = s["open_loop"]["p99_ms"]
+    s["ratio_served_over_plain"] = s["saturation"]["speedup_served_over_plain"]
+    out["served"] = s
+    return out
 
 
 def max_over_ranks(x, dist, device):
@@ -758,6 +866,12 @@ def main():
     ap.add_argument("--rate", type=float, default=200.0, help="serving: requests per second")
     ap.add_argument("--serve-seconds", type=float, default=30.0, help="serving: length of the open-loop stream")
     ap.add_argument("--sat-requests", type=int, default=400, help="serving: requests of the saturation run")
+    ap.add_argument("--headline-only", action="store_true",
+                    help="the default run: measure only the 50M-row ORDER BY, not the other configurations")
+    ap.add_argument("--sub-serve-seconds", type=float, default=10.0,
+                    help="the default run's served stream: length of its open-loop part")
+    ap.add_argument("--sub-sat-requests", type=int, default=200,
+                    help="the default run's served stream: requests of its saturation part")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -835,10 +949,9 @@ def main():
     for _ in range(max(args.warmup, 3)):
         step()
     am.synchronize()
-    # passes run per sort, for the byte model
-    idx = dcols["c0"].argsort()
+    # passes run per sort and whether the payload rode in records, for the byte model
+    step()
     st = am.last_sort_stats()
-    del idx
 
     def barrier():
         if dist:
@@ -846,8 +959,7 @@ def main():
         torch.cuda.synchronize()
 
     peak, peak_kind = measured_peak()
-    am.profile(True)
-    am.profile_reset()
+    # The timed region: K steps with no per-launch events.
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clocks:
         barrier()
@@ -860,32 +972,45 @@ def main():
         am.synchronize()
         barrier()
     ms = ev0.elapsed_time(ev1) / args.steps
-    prof = am.profile_entries()
-    am.profile(False)
     ms = max_over_ranks(ms, dist, "cuda")
     value = whole_job_rate(n, world, ms)
+    # The per-kernel split, from a second loop with a CUDA event pair around every launch.
+    prof_steps = max(3, min(args.steps, 50))
+    am.profile(True)
+    am.profile_reset()
+    ep0, ep1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ep0.record(stream)
+    for _ in range(prof_steps):
+        step()
+    ep1.record(stream)
+    ep1.synchronize()
+    am.synchronize()
+    ms_profiled = ep0.elapsed_time(ep1) / prof_steps
+    prof = am.profile_entries()
+    am.profile(False)
 
     # ---- roofline of the dominant kernel (the take's kernels count as one stage: their model bytes
     # are the take's, however the gather is organised)
     # (the two-level sort: two passes, then the local sorts, when its timer ran and the stats count 2)
     model = algorithmic_bytes(n, m_rows, st["passes_run"],
-                              local_sort=st["passes_run"] == 2 and "radix_local_sort" in prof)
+                              local_sort=st["passes_run"] == 2 and "radix_local_sort" in prof,
+                              records=st["payload_in_records"])
     stages = {}
     for name, (launches, total_ms) in prof.items():
         stage = "take_gather" if name.startswith("take_") else name
         e = stages.setdefault(stage, {"launches": 0, "total_ms": 0.0, "kernels": {}})
         e["launches"] += launches
         e["total_ms"] += total_ms
-        e["kernels"][name] = {"launches": launches, "ms_per_step": total_ms / args.steps}
+        e["kernels"][name] = {"launches": launches, "ms_per_step": total_ms / prof_steps}
     per_kernel = {}
     for stage, e in stages.items():
         if stage in model:
-            b = model[stage] * args.steps
+            b = model[stage] * prof_steps
             e.update({"bytes": b, "gbs": b / (e["total_ms"] / 1e3) / 1e9})
         per_kernel[stage] = e
     dom = max((k for k in per_kernel if "gbs" in per_kernel[k]), key=lambda k: per_kernel[k]["total_ms"])
     d = per_kernel[dom]
-    gpu_launches = sum(l for l, _ in prof.values())
+    gpu_launches = sum(l for l, _ in prof.values()) * args.steps // prof_steps
 
     # ---- end to end through the C ABI with host buffers: the inputs sit in pinned host memory (copied
     # there once, before timing); every step imports them, runs the plan and exports the result.
@@ -927,6 +1052,8 @@ def main():
         "vs_baseline": None, "dtype": "int64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "rows": n, "value_rows": m_rows, "radix_passes_run": st["passes_run"],
                    "radix_passes_skipped": st["passes_skipped"], "parallelism": f"replicas x{world}",
+                   "payload": "carried through the sort in row records" if st["payload_in_records"]
+                              else "gathered through the permutation after the sort",
                    "l2": "inputs larger than L2 (400 MB key column), no flush"},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": d["gbs"], "peak": peak, "unit": "GB/s",
                      "frac": d["gbs"] / peak, "peak_source": peak_kind,
@@ -939,15 +1066,21 @@ def main():
         "gpu_launches": int(gpu_launches),
         "clocks": clocks.summary(),
     }
+    del src, dcols, host_cols, pinned_keep
+    am.synchronize()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         rate, dt = cpu_oracle_rate(key, valid, p1, p2, threads)
         line["cpu_baseline"] = {"value": rate, "unit": "rows/s", "cores": threads, "kind": "port",
                                 "sample": f"the whole {n:,}-row workload once ({dt:.2f} s): C oracle argsort on "
                                           f"{threads} threads + take of the 3 columns"}
+        line["cpu_baseline_pyarrow"] = pyarrow_rate(key, valid, p1, p2)
+        line["cpu_baseline_datafusion"] = datafusion_baseline()
+    if rank == 0 and world == 1 and not args.headline_only:
+        # The other configurations of the benchmark, each measured in this run with its own clocks.
+        line.update(sub_workloads(args, am, torch, stream, local))
     if rank == 0:
         print(json.dumps(line))
-    del src, dcols
     if dist:
         dist.barrier()
         dist.destroy_process_group()

@@ -242,14 +242,30 @@ int  am_take_columns(am_array** columns, int64_t count, am_array* indices, am_ar
 int  am_argsort_batch(am_array** arrays, const int* descending, const int* null_placement,
                       const int* float_order, int64_t count, am_array** outs);
 
-/* Per-call counters of the calling thread's last sort: rows, radix passes run and skipped, and the
- * device time of the sort's kernels in microseconds (0 unless am_cuda_profile(1) is on). */
+/* The segmented sort's tile shapes as its autotuner chose them, one entry per key width (4 or 8 bytes)
+ * and size class (0: arrays of up to 16,384 rows, 1: larger): threads per block, rows per thread and
+ * digit bits; 0 threads: not measured yet. Writes up to `capacity` entries and their number to
+ * `count`. */
+typedef struct am_batch_shape {
+  int32_t key_bytes;
+  int32_t size_class;
+  int32_t threads;
+  int32_t items;
+  int32_t digit_bits;
+} am_batch_shape;
+int  am_cuda_batch_tuning(am_batch_shape* out, int64_t capacity, int64_t* count);
+
+/* Per-call counters of the calling thread's last sort: rows, radix passes run and skipped, the device
+ * time of the sort's kernels in microseconds (0 unless am_cuda_profile(1) is on), and whether the
+ * payload columns rode through the sort in row records (1) instead of a gather afterwards (0). */
 typedef struct am_sort_stats {
   int64_t rows;
   int64_t value_rows;
   int32_t passes_run;
   int32_t passes_skipped;
   double  kernel_us;
+  int32_t payload_in_records;
+  int32_t reserved;
 } am_sort_stats;
 int  am_last_sort_stats(am_sort_stats* out);
 /* Kernel timing with CUDA events around every launch of this library (1 on, 0 off), and the
