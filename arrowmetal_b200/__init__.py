@@ -75,7 +75,8 @@ class ServerStats(ctypes.Structure):
 
 
 class BatchShape(ctypes.Structure):
-    _fields_ = [(n, ctypes.c_int32) for n in ("key_bytes", "size_class", "threads", "items", "digit_bits")]
+    _fields_ = [(n, ctypes.c_int32) for n in ("key_bytes", "size_class", "max_rows", "method", "threads", "items",
+                                              "digit_bits")]
 
 
 class SortStats(ctypes.Structure):
@@ -126,7 +127,7 @@ for _name, _res, _args in [
                                    ctypes.POINTER(ctypes.c_double)]),
     ("am_cuda_profile_reset", _I, []),
     ("am_debug_set_max_row_index", _I, [_I64]), ("am_debug_fail_alloc_after", _I, [_I64]),
-    ("am_debug_skip_first_tile", _I, [_I]),
+    ("am_debug_skip_first_tile", _I, [_I]), ("am_debug_force_batch_shape", _I, [_I]),
     ("am_server_create", _I, [_I, _I64, _I64, _PP]),
     ("am_server_submit", _I, [_P, _P, _I64, _I64, ctypes.POINTER(ctypes.c_char_p), _IP, _IP, _IP, _I64,
                               ctypes.POINTER(ctypes.c_char_p), _I64, ctypes.POINTER(_I64)]),
@@ -315,7 +316,8 @@ class MetalArray:
     # ---- selection
     def take(self, indices):
         """Arrow `take`: int32, int64 and uint32 indices; a null index gives a null row."""
-        return _produce(_lib.am_take, self._h, _gather_indices(indices)._h)
+        indices = _gather_indices(indices)       # held until the call returns
+        return _produce(_lib.am_take, self._h, indices._h)
 
     def slice(self, offset, length):
         return _produce(_lib.am_slice, self._h, offset, length)
@@ -773,8 +775,8 @@ def last_sort_stats():
 
 
 def batch_tuning():
-    """The segmented sort's tile shapes as its autotuner chose them: one dict per key width and size
-    class (threads 0: that class has not been measured yet)."""
+    """The segmented sort's shapes as its autotuner chose them: one dict per key width and size class
+    (method -1: not measured yet, 0: digit passes, 1: one CTA per array)."""
     count = _I64()
     _ok(_lib.am_cuda_batch_tuning(None, 0, ctypes.byref(count)))
     shapes = (BatchShape * max(count.value, 1))()

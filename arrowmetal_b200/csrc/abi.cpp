@@ -1201,7 +1201,7 @@ int am_cuda_batch_tuning(am_batch_shape* out, int64_t capacity, int64_t* count) 
     const auto v = batch_tuning();
     *count = int64_t(v.size());
     for (size_t i = 0; i < v.size() && int64_t(i) < capacity; i++)
-      out[i] = am_batch_shape{v[i][0], v[i][1], v[i][2], v[i][3], v[i][4]};
+      out[i] = am_batch_shape{v[i][0], v[i][1], v[i][2], v[i][3], v[i][4], v[i][5], v[i][6]};
     return 0;
   });
 }
@@ -1239,6 +1239,12 @@ int am_debug_set_max_row_index(int64_t max_row) {
   if (max_row < 0) return 2;
   set_max_row_index(max_row);
   return 0;
+}
+int am_debug_force_batch_shape(int shape) {
+  return guard([&] {
+    debug_force_batch_shape(shape);
+    return 0;
+  });
 }
 int am_debug_fail_alloc_after(int64_t n) {
   debug_fail_alloc_after(n);

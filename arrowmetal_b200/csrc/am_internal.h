@@ -270,8 +270,12 @@ bool payload_record_layout(const std::vector<am_array*>& cols, rs::RecLayout* L)
 // Segmented argsort: outs[i] (a uint32 array of keys[i].col->length rows) receives the argsort of
 // keys[i], one key per array; the arrays of a key width share every launch.
 void radix_argsort_batch(const std::vector<SortKey>& keys, const std::vector<void*>& outs, cudaStream_t s);
-// The segmented sort's chosen tile shapes: {key bytes, size class, threads, rows per thread, digit bits}.
-std::vector<std::array<int32_t, 5>> batch_tuning();
+// The segmented sort's chosen shapes: {key bytes, size class, the class's largest array (-1: none),
+// method (-1 not measured yet, 0 digit passes, 1 one CTA per array), threads, rows per thread, digit bits}.
+std::vector<std::array<int32_t, 7>> batch_tuning();
+// Test hook: the segmented sort uses shape `shape` (an index into its shape table) for every size class
+// it can serve instead of the tuned one; -1 restores the tuning.
+void debug_force_batch_shape(int shape);
 // Single-key argsort of a device column into a caller's uint32 array with no allocation: all
 // scratch sits in a fixed device block of the library (radix_sort.cu). Waits for its work.
 uint64_t noalloc_max_rows();

@@ -20,6 +20,7 @@
 // the reference's "take the next key column, argsort, compose" becomes one gather of the next key
 // inside its first pass.
 #include <algorithm>
+#include <atomic>
 #include <cstdlib>
 #include <list>
 #include <memory>
@@ -444,6 +445,211 @@ __global__ void __launch_bounds__(256) segmented_plan_kernel(const SegDesc* __re
     a.slot_digit[d] = int8_t(d);
   }
   plan_body(a, st + seg, kp + seg, pd + size_t(seg) * key_bytes, sum + seg);
+}
+
+// ------------------------------------------------------------------------------------------------
+// Segmented sort of the arrays that fit one CTA: each such array of a batch is sorted by one CTA in
+// shared memory, all of them in one persistent launch. A CTA encodes its array's rows (the key maps
+// and categories of the digit passes), finds the digits that vary over its value rows, and ranks the
+// rows by each varying digit, least significant first, then by their arrangement class (values, NaN
+// block, nulls, in the order the null placement asks): DBITS-bit digits, one ballot per digit bit, so
+// every pass is stable and so is the result. The same arrays through the digit passes give the same
+// permutation; the autotuner picks DBITS and the block shape per size class by measurement.
+
+// One stable ranking pass over a CTA's rows in shared memory by NB-bit digits `dg` (empty slots carry
+// the largest digit and come last, never counted or stored): every row's place, rows then moved there.
+template <int NBITS, int THREADS, int ITEMS, typename KeyT>
+__device__ __forceinline__ void cta_rank_pass(KeyT (&key)[ITEMS], uint32_t (&id)[ITEMS], const uint32_t (&dg)[ITEMS],
+                                              uint32_t ok, uint32_t size, int nit, KeyT* skeys, uint32_t* sids,
+                                              uint32_t* whist, uint32_t* local, uint32_t* wsum) {
+  constexpr int NB = 1 << NBITS, WARPS = THREADS / 32;
+  constexpr int DPT = NB >= THREADS ? NB / THREADS : 1;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t lt = (1u << lane) - 1u;
+  for (int x = lane; x < NB; x += 32) whist[warp * NB + x] = 0;
+  __syncwarp();
+#pragma unroll
+  for (int i = 0; i < ITEMS; i++)
+    if ((ok >> i) & 1u) atomicAdd(&whist[warp * NB + dg[i]], 1u);
+  __syncthreads();
+  // Per digit: the warps' exclusive starts and the digit's total; then a scan over the digits.
+  uint32_t tots[DPT];
+  uint32_t tot = 0;
+  const bool owner = int(threadIdx.x) * DPT < NB;
+  if (owner) {
+#pragma unroll
+    for (int q = 0; q < DPT; q++) {
+      const int d = int(threadIdx.x) * DPT + q;
+      uint32_t run = 0;
+#pragma unroll
+      for (int w = 0; w < WARPS; w++) {
+        const uint32_t c = whist[w * NB + d];
+        whist[w * NB + d] = run;
+        run += c;
+      }
+      tots[q] = run;
+      tot += run;
+    }
+  }
+  uint32_t x = tot;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) wsum[warp] = x;
+  __syncthreads();
+  if (owner) {
+    uint32_t at = x - tot;
+    for (int w = 0; w < warp; w++) at += wsum[w];
+#pragma unroll
+    for (int q = 0; q < DPT; q++) {
+      local[int(threadIdx.x) * DPT + q] = at;
+      at += tots[q];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < ITEMS; i++) {
+    if (i >= nit) break;
+    const uint32_t d = dg[i];
+    uint32_t peers = 0xffffffffu;
+#pragma unroll
+    for (int k = 0; k < NBITS; k++) {
+      const uint32_t bit = (d >> k) & 1u;
+      const uint32_t bl = __ballot_sync(0xffffffffu, bit);
+      peers &= bit ? bl : ~bl;
+    }
+    const uint32_t b0 = whist[warp * NB + d];
+    __syncwarp();
+    if (lane == __ffs(peers) - 1) whist[warp * NB + d] = b0 + __popc(peers);
+    const uint32_t p = local[d] + b0 + __popc(peers & lt);
+    if (p < size) {
+      skeys[p] = key[i];
+      sids[p] = id[i];
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < ITEMS; i++) {
+    const uint32_t r = uint32_t(warp) * (ITEMS * 32) + uint32_t(i) * 32 + lane;
+    if ((ok >> i) & 1u) {
+      key[i] = skeys[r];
+      id[i] = sids[r];
+    }
+  }
+  __syncthreads();
+}
+
+template <typename KeyT, int THREADS, int ITEMS, int DBITS>
+__host__ __device__ constexpr size_t cta_sort_smem() {
+  return size_t(THREADS) * ITEMS * (sizeof(KeyT) + 4) + size_t(THREADS / 32) * (size_t(1) << DBITS) * 4 +
+         (size_t(1) << DBITS) * 4 + size_t(THREADS / 32) * 4 + 2 * sizeof(unsigned long long) + 16;
+}
+
+// Arrays list[0 .. count) of `segs`, each of at most THREADS x ITEMS rows, one CTA at a time.
+template <typename KeyT, int THREADS, int ITEMS, int DBITS>
+__global__ void __launch_bounds__(THREADS) segment_cta_sort_kernel(const SegDesc* __restrict__ segs, uint32_t count,
+                                                                   uint32_t* __restrict__ err) {
+  constexpr int CAP = THREADS * ITEMS, WARPS = THREADS / 32, NB = 1 << DBITS;
+  constexpr int KBITS = int(sizeof(KeyT)) * 8;
+  static_assert(DBITS >= 2, "the arrangement pass uses 2-bit digits within the same histogram space");
+  extern __shared__ __align__(16) unsigned char cta_smem[];
+  KeyT* skeys = reinterpret_cast<KeyT*>(cta_smem);
+  uint32_t* sids = reinterpret_cast<uint32_t*>(skeys + CAP);
+  uint32_t* whist = sids + CAP;                           // [WARPS][NB]
+  uint32_t* local = whist + WARPS * NB;                   // [NB]
+  uint32_t* wsum = local + NB;                            // [WARPS]
+  unsigned long long* red = reinterpret_cast<unsigned long long*>(
+      (reinterpret_cast<uintptr_t>(wsum + WARPS) + 15) & ~uintptr_t(15));   // OR and AND of the value keys
+  uint32_t* any_cat = reinterpret_cast<uint32_t*>(red + 2);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (uint32_t j = blockIdx.x; j < count; j += gridDim.x) {
+    const SegDesc& sd = segs[j];
+    const uint32_t size = sd.n;
+    if (size > uint32_t(CAP)) {           // the host sends only arrays that fit; never read past the tile
+      if (threadIdx.x == 0) atomicOr(err, ERR_BOUNDS);
+      continue;
+    }
+    if (threadIdx.x == 0) {
+      red[0] = 0ull;
+      red[1] = ~0ull;
+      *any_cat = 0;
+    }
+    __syncthreads();
+    const ColView col = sd.col;
+    uint32_t row[ITEMS];
+    uint32_t ok = 0;
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++) {
+      row[i] = uint32_t(warp) * (ITEMS * 32) + uint32_t(i) * 32 + lane;
+      if (row[i] < size) ok |= 1u << i;
+    }
+    KeyT key[ITEMS];
+    int cat[ITEMS];
+    encode_rows<KeyT, ITEMS>(col, row, ok, key, cat);
+    uint32_t id[ITEMS];
+    KeyT kor = 0, kand = ~KeyT(0);
+    uint32_t cats = 0;
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++) {
+      id[i] = row[i];
+      if (!((ok >> i) & 1u)) continue;
+      if (cat[i] == 0) {
+        kor |= key[i];
+        kand &= key[i];
+      } else {
+        key[i] = 0;
+        cats = 1;
+      }
+    }
+    kor = warp_or(kor);
+    kand = warp_and(kand);
+    cats = __reduce_or_sync(0xffffffffu, cats);
+    if (lane == 0) {
+      atomicOr(&red[0], (unsigned long long)kor);
+      atomicAnd(&red[1], (unsigned long long)kand);
+      if (cats) atomicOr(any_cat, 1u);
+    }
+    __syncthreads();
+    // A CTA with no value rows has OR 0 and AND all ones: no varying digit.
+    const KeyT diff = red[0] <= red[1] ? KeyT(0) : KeyT(red[0] ^ red[1]);
+    const bool arrange = *any_cat != 0;
+    const uint32_t w_first = uint32_t(warp) * (ITEMS * 32);
+    const int nit = size > w_first ? int(min(uint32_t(ITEMS), (size - w_first + 31) / 32)) : 0;
+    // Every row's arrangement class before any pass moves it.
+    uint32_t cls[ITEMS];
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++) cls[i] = col.nulls_first ? uint32_t(2 - cat[i]) : uint32_t(cat[i]);
+    if (arrange) {
+      // The class rides in the key's place for the value digits' passes: carried in the row id's top
+      // bits (ids are below 2^16 here).
+#pragma unroll
+      for (int i = 0; i < ITEMS; i++) id[i] |= cls[i] << 30;
+    }
+    for (int shift = 0; shift < KBITS; shift += DBITS) {
+      const KeyT mask = KeyT((uint64_t(1) << DBITS) - 1) << shift;
+      if (!(diff & mask)) continue;
+      uint32_t dg[ITEMS];
+#pragma unroll
+      for (int i = 0; i < ITEMS; i++) dg[i] = ((ok >> i) & 1u) ? uint32_t(key[i] >> shift) & uint32_t(NB - 1) : uint32_t(NB - 1);
+      cta_rank_pass<DBITS, THREADS, ITEMS, KeyT>(key, id, dg, ok, size, nit, skeys, sids, whist, local, wsum);
+    }
+    if (arrange) {
+      uint32_t dg[ITEMS];
+#pragma unroll
+      for (int i = 0; i < ITEMS; i++) dg[i] = ((ok >> i) & 1u) ? (id[i] >> 30) : 3u;
+      cta_rank_pass<2, THREADS, ITEMS, KeyT>(key, id, dg, ok, size, nit, skeys, sids, whist, local, wsum);
+    }
+    uint32_t* out = static_cast<uint32_t*>(sd.out);
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++) {
+      const uint32_t r = uint32_t(warp) * (ITEMS * 32) + uint32_t(i) * 32 + lane;
+      if ((ok >> i) & 1u) out[r] = id[i] & 0x3FFFFFFFu;
+    }
+    __syncthreads();
+  }
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -1479,9 +1685,6 @@ struct PassConfig;
 // on B200 among 320-512 threads x 8-16 rows (two blocks per SM).
 template <> struct PassConfig<uint32_t> { static constexpr int THREADS = 384, ITEMS = 14; };
 template <> struct PassConfig<uint64_t> { static constexpr int THREADS = 384, ITEMS = 14; };
-// The segmented sort's tiles: 512 threads x 8 or 4 rows, chosen per size class.
-constexpr int SEG_THREADS = 512;
-
 constexpr int HIST_THREADS = 256, HIST_ITEMS = 8;
 
 template <typename KeyT, int ITEMS = PassConfig<KeyT>::ITEMS, int THREADS = PassConfig<KeyT>::THREADS, bool REC = false>
@@ -1928,9 +2131,9 @@ constexpr uint32_t SEG_HIST_ROWS = 32768;   // rows per histogram block
 
 // One key width's arrays of a batch: the tables the kernels read and where everything sits in the
 // group's scratch.
-template <typename KeyT, int ITEMS>
+template <typename KeyT, int THREADS, int ITEMS>
 struct GroupLayout {
-  static constexpr uint64_t TILE = uint64_t(SEG_THREADS) * ITEMS;
+  static constexpr uint64_t TILE = uint64_t(THREADS) * ITEMS;
   static constexpr int S = int(sizeof(KeyT));
   uint32_t G = 0;
   uint64_t rows = 0, tiles = 0, items = 0, max_n = 0;
@@ -1988,10 +2191,10 @@ struct GroupLayout {
 // The launches of one group, with its scratch at `base` and its tables already there or copied from
 // `pinned_tables` (a graph's first node) when that is given. `timed`: a KernelTimer per launch (not
 // inside a graph capture).
-template <typename KeyT, int ITEMS>
-void enqueue_group(const GroupLayout<KeyT, ITEMS>& L, char* base, void* status, uint32_t* err,
+template <typename KeyT, int THREADS, int ITEMS>
+void enqueue_group(const GroupLayout<KeyT, THREADS, ITEMS>& L, char* base, void* status, uint32_t* err,
                    const void* pinned_tables, bool timed, cudaStream_t s) {
-  constexpr int S = GroupLayout<KeyT, ITEMS>::S;
+  constexpr int S = GroupLayout<KeyT, THREADS, ITEMS>::S;
   if (pinned_tables) AM_CUDA(cudaMemcpyAsync(base, pinned_tables, L.tables, cudaMemcpyHostToDevice, s));
   AM_CUDA(cudaMemsetAsync(base + L.tables, 0, L.header - L.tables, s));
   const SegDesc* d_segs = reinterpret_cast<const SegDesc*>(base);
@@ -2021,8 +2224,8 @@ void enqueue_group(const GroupLayout<KeyT, ITEMS>& L, char* base, void* status, 
   // 64-bit words whose pass epochs (1..S) start over from a zeroed array in every call.
   const bool narrow = L.narrow();
   if (!narrow) AM_CUDA(cudaMemsetAsync(status, 0, size_t(L.tiles) * NBINS * sizeof(uint64_t), s));
-  const int bps = narrow ? pass_blocks_per_sm<KeyT, uint32_t, true, ITEMS, SEG_THREADS>()
-                         : pass_blocks_per_sm<KeyT, uint64_t, true, ITEMS, SEG_THREADS>();
+  const int bps = narrow ? pass_blocks_per_sm<KeyT, uint32_t, true, ITEMS, THREADS>()
+                         : pass_blocks_per_sm<KeyT, uint64_t, true, ITEMS, THREADS>();
   const int grid = int(std::min<uint64_t>(L.tiles, uint64_t(device().sm_count) * bps));
   for (int sl = 0; sl < S; sl++) {
     if (narrow) AM_CUDA(cudaMemsetAsync(status, 0, size_t(L.tiles) * NBINS * sizeof(uint32_t), s));
@@ -2047,11 +2250,11 @@ void enqueue_group(const GroupLayout<KeyT, ITEMS>& L, char* base, void* status, 
     a.nslots = uint32_t(S);
     const ColView none{};
     std::unique_ptr<KernelTimer> kt(timed ? new KernelTimer("batch_pass", s) : nullptr);
-    constexpr size_t smem = sizeof(PassShared<KeyT, SEG_THREADS, ITEMS>);
+    constexpr size_t smem = sizeof(PassShared<KeyT, THREADS, ITEMS>);
     if (narrow)
-      onesweep_pass_kernel<KeyT, uint32_t, SEG_THREADS, ITEMS, true><<<std::max(grid, 1), SEG_THREADS, smem, s>>>(a, none);
+      onesweep_pass_kernel<KeyT, uint32_t, THREADS, ITEMS, true><<<std::max(grid, 1), THREADS, smem, s>>>(a, none);
     else
-      onesweep_pass_kernel<KeyT, uint64_t, SEG_THREADS, ITEMS, true><<<std::max(grid, 1), SEG_THREADS, smem, s>>>(a, none);
+      onesweep_pass_kernel<KeyT, uint64_t, THREADS, ITEMS, true><<<std::max(grid, 1), THREADS, smem, s>>>(a, none);
     AM_CUDA(cudaGetLastError());
   }
 }
@@ -2111,10 +2314,10 @@ bool graphs_enabled() {
   return on;
 }
 
-template <typename KeyT, int ITEMS>
-BatchGraph* find_or_capture(const GroupLayout<KeyT, ITEMS>& L, uint32_t* err, cudaStream_t s) {
+template <typename KeyT, int THREADS, int ITEMS>
+BatchGraph* find_or_capture(const GroupLayout<KeyT, THREADS, ITEMS>& L, uint32_t* err, cudaStream_t s) {
   GraphCache& c = graph_cache();
-  const int width = int(sizeof(KeyT)) * 100 + ITEMS;    // key width and tile shape
+  const int width = int(sizeof(KeyT)) * 100000 + THREADS * 100 + ITEMS;    // key width and tile shape
   for (auto it = c.graphs.begin(); it != c.graphs.end(); ++it) {
     if ((*it)->width == width && (*it)->stream == s && (*it)->lens == L.lens) {
       c.graphs.splice(c.graphs.begin(), c.graphs, it);
@@ -2138,15 +2341,15 @@ BatchGraph* find_or_capture(const GroupLayout<KeyT, ITEMS>& L, uint32_t* err, cu
   const size_t status_bytes = size_t(L.tiles) * NBINS * (L.narrow() ? sizeof(uint32_t) : sizeof(uint64_t));
   AM_CUDA(cudaMalloc(&g->status, std::max<size_t>(status_bytes, 16)));
   // Launch attributes and occupancy are looked up before the capture.
-  (void)pass_blocks_per_sm<KeyT, uint32_t, true, ITEMS, SEG_THREADS>();
-  (void)pass_blocks_per_sm<KeyT, uint64_t, true, ITEMS, SEG_THREADS>();
+  (void)pass_blocks_per_sm<KeyT, uint32_t, true, ITEMS, THREADS>();
+  (void)pass_blocks_per_sm<KeyT, uint64_t, true, ITEMS, THREADS>();
   for (auto& sl : g->slot) {
     sl.host = pinned_alloc(L.tables);
     AM_CUDA(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
     cudaGraph_t graph = nullptr;
     AM_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     try {
-      enqueue_group<KeyT, ITEMS>(L, g->base, g->status, err, sl.host, false, s);
+      enqueue_group<KeyT, THREADS, ITEMS>(L, g->base, g->status, err, sl.host, false, s);
     } catch (...) {
       cudaGraph_t discard = nullptr;
       (void)cudaStreamEndCapture(s, &discard);
@@ -2163,13 +2366,13 @@ BatchGraph* find_or_capture(const GroupLayout<KeyT, ITEMS>& L, uint32_t* err, cu
   return c.graphs.front().get();
 }
 
-template <typename KeyT, int ITEMS>
+template <typename KeyT, int THREADS, int ITEMS>
 void sort_segment_class(const std::vector<SortKey>& keys, const std::vector<void*>& outs,
                         const std::vector<size_t>& group, bool allow_graph, cudaStream_t s) {
-  GroupLayout<KeyT, ITEMS> L(keys, outs, group);
+  GroupLayout<KeyT, THREADS, ITEMS> L(keys, outs, group);
   StreamScratch& sc = stream_scratch(s, L.narrow() ? (size_t(L.tiles) * NBINS + 1) / 2 : size_t(L.tiles) * NBINS);
   if (allow_graph && graphs_enabled()) {
-    if (BatchGraph* g = find_or_capture<KeyT, ITEMS>(L, sc.err, s)) {
+    if (BatchGraph* g = find_or_capture<KeyT, THREADS, ITEMS>(L, sc.err, s)) {
       BatchGraph::Slot& sl = g->slot[g->next];
       g->next ^= 1;
       if (sl.launched) AM_CUDA(cudaEventSynchronize(sl.done));
@@ -2183,22 +2386,77 @@ void sort_segment_class(const std::vector<SortKey>& keys, const std::vector<void
   }
   char* base = static_cast<char*>(dmalloc(L.bytes(), s));
   copy_h2d(base, L.host.data(), L.tables, s);
-  enqueue_group<KeyT, ITEMS>(L, base, sc.status, sc.err, nullptr, true, s);
+  enqueue_group<KeyT, THREADS, ITEMS>(L, base, sc.status, sc.err, nullptr, true, s);
   dfree(base, s);
 }
 
-// ---- Tile shape per size class, chosen by measurement.
+// One launch sorts every array of a size class that fits a CTA (at most CTA_SORT_ROWS rows).
+template <typename KeyT, int THREADS, int ITEMS, int DBITS>
+void sort_segment_cta(const std::vector<SortKey>& keys, const std::vector<void*>& outs,
+                      const std::vector<size_t>& group, cudaStream_t s) {
+  static_assert(THREADS * ITEMS >= 4096, "the one-CTA class holds arrays of up to 4,096 rows");
+  constexpr size_t SMEM = cta_sort_smem<KeyT, THREADS, ITEMS, DBITS>();
+  static int blocks = 0;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    auto fn = segment_cta_sort_kernel<KeyT, THREADS, ITEMS, DBITS>;
+    AM_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SMEM)));
+    int b = 0;
+    AM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, THREADS, SMEM));
+    blocks = std::max(1, b);
+  });
+  std::vector<SegDesc> segs(group.size());
+  for (size_t g = 0; g < group.size(); g++) {
+    const SortKey& k = keys[group[g]];
+    segs[g] = SegDesc{};
+    segs[g].col = make_view(k);
+    segs[g].out = outs[group[g]];
+    segs[g].n = uint32_t(k.col->length);
+  }
+  const size_t bytes = sizeof(SegDesc) * segs.size();
+  SegDesc* d = static_cast<SegDesc*>(dmalloc(bytes, s));
+  copy_h2d(d, segs.data(), bytes, s);
+  const int grid = int(std::min<uint64_t>(segs.size(), uint64_t(device().sm_count) * blocks));
+  StreamScratch& sc = stream_scratch(s, 0);
+  {
+    KernelTimer kt("batch_cta_sort", s);
+    segment_cta_sort_kernel<KeyT, THREADS, ITEMS, DBITS><<<std::max(grid, 1), THREADS, SMEM, s>>>(d, uint32_t(segs.size()), sc.err);
+    AM_CUDA(cudaGetLastError());
+  }
+  dfree(d, s);
+}
+
+// ---- Shapes per size class, chosen by measurement.
 //
-// Arrays of a key width are sorted in two size classes (up to SMALL_ARRAY_ROWS rows, and above), each
-// with its own launches and tile shape: 512 threads x 8 rows (4096-row tiles) or x 4 rows (2048). The
-// first batch whose class holds at least TUNE_MIN_ROWS rows runs that class with both shapes, timed by
-// CUDA events, and the faster shape serves the class from then on (its second run leaves the same,
-// final output). ARROWMETAL_SEG_ITEMS=4 or 8 fixes the shape instead.
+// A batch's arrays of one key width fall into three size classes: up to CTA_SORT_ROWS rows, up to
+// SMALL_ARRAY_ROWS, and larger. Each class has its candidate shapes: the digit passes with a tile of
+// `threads` x `items` rows, or (the smallest class) one CTA per array with `threads` threads, `items`
+// rows a thread and `digit_bits`-bit digits. The first batch whose class holds at least its class's
+// tuning rows runs the class with every candidate, timed by CUDA events (each run leaves the same,
+// final output), and the fastest serves the class from then on. ARROWMETAL_SEG_ITEMS=4 or 8 fixes the
+// passes' tile at 512 x 4 or 512 x 8 rows for every class instead.
+constexpr uint32_t CTA_SORT_ROWS = 4096;
 constexpr uint32_t SMALL_ARRAY_ROWS = 16384;
-constexpr uint64_t TUNE_MIN_ROWS = uint64_t(2) << 20;
+constexpr int SEG_CLASSES = 3;
+
+struct SegShape {
+  int method;          // 0: digit passes, 1: one CTA per array
+  int threads, items, digit_bits;
+};
+constexpr SegShape kSegShapes[] = {
+    {0, 512, 8, 8}, {0, 512, 4, 8}, {0, 384, 12, 8},
+    {1, 256, 16, 8}, {1, 256, 16, 4}, {1, 512, 8, 8}, {1, 512, 8, 4},
+};
+constexpr int kNumSegShapes = int(sizeof(kSegShapes) / sizeof(kSegShapes[0]));
+const std::vector<int>& class_candidates(int cls) {
+  static const std::vector<int> c0 = {3, 4, 5, 6, 1}, c12 = {0, 1, 2};
+  static_assert(kNumSegShapes == 7, "every shape is a candidate of some class");
+  return cls == 0 ? c0 : c12;
+}
+uint64_t class_tune_rows(int cls) { return cls == 0 ? (uint64_t(1) << 18) : (uint64_t(2) << 20); }
 
 std::mutex g_tune_mu;
-int g_tuned_items[2][2] = {{0, 0}, {0, 0}};   // [key width 4 / 8][size class]: 0 = not yet measured
+int g_tuned_shape[2][SEG_CLASSES] = {{-1, -1, -1}, {-1, -1, -1}};   // [key width 4 / 8][class]
 
 int forced_items() {
   static const int v = [] {
@@ -2209,63 +2467,97 @@ int forced_items() {
   return v;
 }
 
-int tuned_items(int width, int cls) {
+int tuned_shape(int width, int cls) {
   std::lock_guard<std::mutex> g(g_tune_mu);
-  return g_tuned_items[width == 8][cls];
+  return g_tuned_shape[width == 8][cls];
+}
+
+std::atomic<int> g_forced_shape{-1};     // test hook: one shape for every class it can serve
+
+template <typename KeyT>
+void run_segment_shape(int shape, const std::vector<SortKey>& keys, const std::vector<void*>& outs,
+                       const std::vector<size_t>& group, bool allow_graph, cudaStream_t s) {
+  switch (shape) {
+    case 0: sort_segment_class<KeyT, 512, 8>(keys, outs, group, allow_graph, s); break;
+    case 1: sort_segment_class<KeyT, 512, 4>(keys, outs, group, allow_graph, s); break;
+    case 2: sort_segment_class<KeyT, 384, 12>(keys, outs, group, allow_graph, s); break;
+    case 3: sort_segment_cta<KeyT, 256, 16, 8>(keys, outs, group, s); break;
+    case 4: sort_segment_cta<KeyT, 256, 16, 4>(keys, outs, group, s); break;
+    case 5: sort_segment_cta<KeyT, 512, 8, 8>(keys, outs, group, s); break;
+    default: sort_segment_cta<KeyT, 512, 8, 4>(keys, outs, group, s); break;
+  }
 }
 
 template <typename KeyT>
 void sort_segment_group(const std::vector<SortKey>& keys, const std::vector<void*>& outs,
                         const std::vector<size_t>& group, cudaStream_t s) {
-  std::vector<size_t> cls[2];
-  uint64_t cls_rows[2] = {0, 0};
+  std::vector<size_t> cls[SEG_CLASSES];
+  uint64_t cls_rows[SEG_CLASSES] = {0, 0, 0};
   for (size_t i : group) {
-    const int c = uint64_t(keys[i].col->length) <= SMALL_ARRAY_ROWS ? 0 : 1;
+    const uint64_t n = uint64_t(keys[i].col->length);
+    const int c = n <= CTA_SORT_ROWS ? 0 : n <= SMALL_ARRAY_ROWS ? 1 : 2;
     cls[c].push_back(i);
-    cls_rows[c] += uint64_t(keys[i].col->length);
+    cls_rows[c] += n;
   }
   const int width = int(sizeof(KeyT));
-  for (int c = 0; c < 2; c++) {
+  for (int c = 0; c < SEG_CLASSES; c++) {
     if (cls[c].empty()) continue;
-    int items = forced_items();
-    if (!items) items = tuned_items(width, c);
-    if (!items && cls_rows[c] >= TUNE_MIN_ROWS) {
-      // Measure both shapes on this batch; the second run's output is the result.
-      float ms[2] = {0, 0};
-      const int shapes[2] = {4, 8};
+    if (const int f = forced_items()) {
+      run_segment_shape<KeyT>(f == 4 ? 1 : 0, keys, outs, cls[c], true, s);
+      continue;
+    }
+    if (const int f = g_forced_shape.load(); f >= 0 && (kSegShapes[f].method == 0 || c == 0)) {
+      run_segment_shape<KeyT>(f, keys, outs, cls[c], true, s);
+      continue;
+    }
+    int shape = tuned_shape(width, c);
+    if (shape < 0 && cls_rows[c] >= class_tune_rows(c)) {
+      // Measure every candidate on this batch; each run leaves the same output.
+      const std::vector<int>& cand = class_candidates(c);
+      std::vector<float> ms(cand.size(), 0.0f);
       cudaEvent_t e0, e1;
       AM_CUDA(cudaEventCreate(&e0));
       AM_CUDA(cudaEventCreate(&e1));
-      for (int k = 0; k < 2; k++) {
+      for (size_t k = 0; k < cand.size(); k++) {
         AM_CUDA(cudaEventRecord(e0, s));
-        if (shapes[k] == 4) sort_segment_class<KeyT, 4>(keys, outs, cls[c], false, s);
-        else sort_segment_class<KeyT, 8>(keys, outs, cls[c], false, s);
+        run_segment_shape<KeyT>(cand[k], keys, outs, cls[c], false, s);
         AM_CUDA(cudaEventRecord(e1, s));
         AM_CUDA(cudaEventSynchronize(e1));
         AM_CUDA(cudaEventElapsedTime(&ms[k], e0, e1));
       }
       (void)cudaEventDestroy(e0);
       (void)cudaEventDestroy(e1);
+      const size_t best = size_t(std::min_element(ms.begin(), ms.end()) - ms.begin());
       std::lock_guard<std::mutex> g(g_tune_mu);
-      g_tuned_items[width == 8][c] = ms[0] < ms[1] ? 4 : 8;
+      g_tuned_shape[width == 8][c] = cand[best];
       continue;
     }
-    if (!items) items = 8;
-    if (items == 4) sort_segment_class<KeyT, 4>(keys, outs, cls[c], true, s);
-    else sort_segment_class<KeyT, 8>(keys, outs, cls[c], true, s);
+    if (shape < 0) shape = c == 0 ? 5 : 0;     // untuned: one CTA per array, or 512 x 8 tiles
+    run_segment_shape<KeyT>(shape, keys, outs, cls[c], true, s);
   }
 }
 
 }  // namespace
 }  // namespace rs
 
-std::vector<std::array<int32_t, 5>> batch_tuning() {
-  std::vector<std::array<int32_t, 5>> out;
+void debug_force_batch_shape(int shape) {
+  if (shape >= rs::kNumSegShapes) throw invalid("no batch shape " + std::to_string(shape));
+  rs::g_forced_shape.store(shape < 0 ? -1 : shape);
+}
+
+std::vector<std::array<int32_t, 7>> batch_tuning() {
+  std::vector<std::array<int32_t, 7>> out;
   std::lock_guard<std::mutex> g(rs::g_tune_mu);
+  const int32_t bound[rs::SEG_CLASSES] = {int32_t(rs::CTA_SORT_ROWS), int32_t(rs::SMALL_ARRAY_ROWS), -1};
   for (int w = 0; w < 2; w++)
-    for (int c = 0; c < 2; c++) {
-      const int items = rs::g_tuned_items[w][c];
-      out.push_back({w ? 8 : 4, c, items ? rs::SEG_THREADS : 0, items, items ? 8 : 0});
+    for (int c = 0; c < rs::SEG_CLASSES; c++) {
+      const int sh = rs::g_tuned_shape[w][c];
+      if (sh < 0) {
+        out.push_back({w ? 8 : 4, c, bound[c], -1, 0, 0, 0});
+        continue;
+      }
+      const rs::SegShape& x = rs::kSegShapes[sh];
+      out.push_back({w ? 8 : 4, c, bound[c], x.method, x.threads, x.items, x.digit_bits});
     }
   return out;
 }

@@ -242,13 +242,16 @@ int  am_take_columns(am_array** columns, int64_t count, am_array* indices, am_ar
 int  am_argsort_batch(am_array** arrays, const int* descending, const int* null_placement,
                       const int* float_order, int64_t count, am_array** outs);
 
-/* The segmented sort's tile shapes as its autotuner chose them, one entry per key width (4 or 8 bytes)
- * and size class (0: arrays of up to 16,384 rows, 1: larger): threads per block, rows per thread and
- * digit bits; 0 threads: not measured yet. Writes up to `capacity` entries and their number to
- * `count`. */
+/* The segmented sort's shapes as its autotuner chose them, one entry per key width (4 or 8 bytes) and
+ * size class (0: arrays of up to 4,096 rows, 1: up to 16,384, 2: larger; `max_rows` -1: no bound):
+ * the method (-1: not measured yet, 0: digit passes over tiles of threads x items rows, 1: one CTA of
+ * `threads` threads and `items` rows a thread per array), and the digit width in bits. Writes up to
+ * `capacity` entries and their number to `count`. */
 typedef struct am_batch_shape {
   int32_t key_bytes;
   int32_t size_class;
+  int32_t max_rows;
+  int32_t method;
   int32_t threads;
   int32_t items;
   int32_t digit_bits;
@@ -280,6 +283,11 @@ int  am_cuda_profile_reset(void);
  * allocations (-1 disables it). */
 int  am_debug_set_max_row_index(int64_t max_row);
 int  am_debug_fail_alloc_after(int64_t n);
+/* Test hook: am_argsort_batch sorts with candidate shape `shape` (0-2: digit passes over tiles of 512 x 8,
+ * 512 x 4 and 384 x 12 rows; 3-6: one CTA per array of up to 4,096 rows, 256 x 16 or 512 x 8 rows
+ * with 8- or 4-bit digits) for every size class it can serve, instead of the autotuner's choice; -1
+ * restores the autotuner. */
+int  am_debug_force_batch_shape(int shape);
 /* Test hook for the bounded look-back: with `on` set, the calling process's next sorts never process
  * their first tile, so the tiles after it wait on a status nothing writes; each such wait gives up
  * after one second and the call returns 1 ("look-back wait timed out"). No GPU fault is involved. */

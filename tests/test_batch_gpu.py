@@ -144,3 +144,38 @@ def test_repeated_shapes_replay_a_graph(am, oracle):
                      for n, k in shape_a], [(False, "at_end", "ieee")] * len(shape_a))
     assert "batch_graph" in am.profile_entries()
     am.profile(False)
+
+
+@pytest.mark.parametrize("shape", range(7))
+def test_every_candidate_shape_against_the_oracle(am, oracle, shape):
+    # Each shape the autotuner may pick, forced for every size class it serves: digit passes over three
+    # tile shapes, and one CTA per array with two block shapes and 8- or 4-bit digits.
+    rng = np.random.default_rng(200 + shape)
+    lengths = [0, 1, 2, 31, 32, 33, 255, 256, 1000, 2047, 2048, 4095, 4096, 4097, 9000, 16384, 16385, 70_001]
+    arrays, opts = [], []
+    for i, n in enumerate(lengths * 2):
+        arrays.append(random_array(rng, KINDS[(i * 7 + shape) % len(KINDS)], n))
+        opts.append((bool(rng.integers(2)), PLACEMENTS[rng.integers(2)], ORDERS[rng.integers(3)]))
+    am._ok(am._lib.am_debug_force_batch_shape(shape))
+    try:
+        check_batch(am, oracle, arrays, opts)
+        check_batch(am, oracle, arrays, opts)            # the second batch of a shape replays a graph
+    finally:
+        am._ok(am._lib.am_debug_force_batch_shape(-1))
+
+
+def test_autotuner_records_its_choice_per_size_class(am, oracle):
+    # Enough rows in every size class to tune it: the chosen shape is recorded per key width and class,
+    # and the batch that tuned it (every candidate run on it) is still exact.
+    rng = np.random.default_rng(300)
+    arrays = [random_array(rng, "int64", n) for n in [3000] * 100 + [12_000] * 200 + [150_000] * 16]
+    opts = [(False, "at_end", "ieee")] * len(arrays)
+    check_batch(am, oracle, arrays, opts)
+    shapes = {(s["key_bytes"], s["size_class"]): s for s in am.batch_tuning()}
+    for c in range(3):
+        s = shapes[(8, c)]
+        assert s["method"] in (0, 1) and s["threads"] > 0 and s["items"] > 0 and s["digit_bits"] in (4, 8), s
+        if s["method"] == 1:
+            assert c == 0 and s["threads"] * s["items"] >= 4096
+    assert shapes[(8, 0)]["max_rows"] == 4096 and shapes[(8, 2)]["max_rows"] == -1
+    check_batch(am, oracle, arrays, opts)
