@@ -723,6 +723,10 @@ __device__ __forceinline__ uint64_t load_width(const void* base, uint64_t i, int
 
 // Row `row`'s record: its id and its payload fields read from the columns.
 __device__ __forceinline__ uint4 build_record(const RecLayout& L, uint32_t row) {
+  if (L.pair) {
+    const uint64_t w = static_cast<const uint64_t*>(L.src[L.wide])[row];
+    return make_uint4(row, uint32_t(w), uint32_t(w >> 32), static_cast<const uint32_t*>(L.src[L.narrow])[row]);
+  }
   uint64_t lo = 0;           // payload bytes 0-7
   uint32_t hi = 0;           // payload bytes 8-11
   for (int c = 0; c < L.ncols; c++) {
@@ -737,6 +741,11 @@ __device__ __forceinline__ uint4 build_record(const RecLayout& L, uint32_t row) 
 // A record's payload fields, written to row `dst` of the sorted payload columns.
 __device__ __forceinline__ void unpack_record(const RecLayout& L, const uint4& r, uint64_t dst) {
   const uint64_t lo = uint64_t(r.y) | (uint64_t(r.z) << 32);
+  if (L.pair) {
+    static_cast<uint64_t*>(L.dst[L.wide])[dst] = lo;
+    static_cast<uint32_t*>(L.dst[L.narrow])[dst] = r.w;
+    return;
+  }
   for (int c = 0; c < L.ncols; c++) {
     const int o = L.off[c];
     const uint64_t v = o < 8 ? (lo >> (8 * o)) : uint64_t(r.w >> (8 * (o - 8)));
@@ -1008,32 +1017,50 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
       // Keys and records in one loop. A row's record comes from its place in the tile's input (the
       // tile's records, read in sorted order, stay within one L2-resident span), or is built from the
       // payload columns in the first pass; a row reaching its final place has its record unpacked.
+      // Two rows a thread per round, their record loads in flight together (each is a random read
+      // within the tile's span, an L2 round trip).
       const uint4* __restrict__ rin = reinterpret_cast<const uint4*>(ids_in);
       uint4* __restrict__ rout = reinterpret_cast<uint4*>(ids_out);
-      for (uint32_t j = threadIdx.x; j < tile_n; j += THREADS) {
-        const uint32_t d = sm.dig[j];
-        uint32_t dst = sm.gdelta[d] + j;
-        const uint64_t src_row = tile_base + sm.ids[j];
-        const uint4 r = (flags & PF_ENCODE) ? build_record(pa.rec, uint32_t(src_row)) : rin[src_row];
-        if (d < RADIX && rout) {
-          if (dst < buf_rows) {
-            if (keys_out) keys_out[dst] = sm.keys[j];
-            rout[dst] = r;
-          } else {
-            atomicOr(pa.err, ERR_BOUNDS);
+      constexpr int U = 2;
+      const bool encode = (flags & PF_ENCODE) != 0;
+      for (uint32_t j0 = threadIdx.x; j0 < tile_n; j0 += THREADS * U) {
+        uint4 r[U];
+        uint32_t dg[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+          const uint32_t j = j0 + uint32_t(u) * THREADS;
+          dg[u] = INVALID_DIGIT;
+          if (j >= tile_n) continue;
+          dg[u] = sm.dig[j];
+          const uint64_t src_row = tile_base + sm.ids[j];
+          r[u] = encode ? build_record(pa.rec, uint32_t(src_row)) : rin[src_row];
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+          const uint32_t j = j0 + uint32_t(u) * THREADS;
+          const uint32_t d = dg[u];
+          if (d == INVALID_DIGIT) continue;
+          uint32_t dst = sm.gdelta[d] + j;
+          if (d < RADIX && rout) {
+            if (dst < buf_rows) {
+              if (keys_out) keys_out[dst] = sm.keys[j];
+              rout[dst] = r[u];
+            } else {
+              atomicOr(pa.err, ERR_BOUNDS);
+            }
+            continue;
           }
-          continue;
+          if (d < RADIX) dst += sm.desc.value_base;
+          if (dst >= out_rows) {
+            atomicOr(pa.err, ERR_BOUNDS);
+            continue;
+          }
+          if (final_out) {
+            if (flags & PF_WIDE_OUT) static_cast<uint64_t*>(final_out)[dst] = r[u].x;
+            else static_cast<uint32_t*>(final_out)[dst] = r[u].x;
+          }
+          unpack_record(pa.rec, r[u], dst);
         }
-        if (d < RADIX) dst += sm.desc.value_base;
-        if (dst >= out_rows) {
-          atomicOr(pa.err, ERR_BOUNDS);
-          continue;
-        }
-        if (final_out) {
-          if (flags & PF_WIDE_OUT) static_cast<uint64_t*>(final_out)[dst] = r.x;
-          else static_cast<uint32_t*>(final_out)[dst] = r.x;
-        }
-        unpack_record(pa.rec, r, dst);
       }
     } else if (merged) {
       for (uint32_t j = threadIdx.x; j < tile_n; j += THREADS) {
@@ -1132,7 +1159,7 @@ __global__ void __launch_bounds__(256) key_validity_kernel(const SortSummary* __
 // digits, then the two top digits again (a complete LSD sequence after the first two passes, so the
 // answer is the same). Every choice is made on the device, with no host round trip.
 
-constexpr uint64_t HYB_MIN_ROWS = uint64_t(1) << 25;
+constexpr uint64_t HYB_MIN_ROWS = uint64_t(1) << 25;     // the default; ARROWMETAL_HYBRID_MIN_ROWS overrides
 constexpr int HYB_STEPS = 10;                 // two top-digit passes, then up to eight fallback passes
 constexpr int BND_THREADS = 256, BND_ITEMS = 16;
 constexpr uint64_t BND_CHUNK = uint64_t(BND_THREADS) * BND_ITEMS;
@@ -1166,7 +1193,7 @@ __global__ void __launch_bounds__(256) hybrid_plan_kernel(PlanArgs a, const KeyS
     int na = 0;
     for (int d = 0; d < a.nslots && d < 8; d++)
       if (normal[d].active) s_act[na++] = d;
-    const bool hyb = a.nkeys == 1 && a.key_bytes[0] == 8 && uint64_t(st->n_value) >= HYB_MIN_ROWS && na >= 3;
+    const bool hyb = a.nkeys == 1 && a.key_bytes[0] == 8 && uint64_t(st->n_value) >= a.hyb_min_rows && na >= 3;
     s_hyb = hyb ? 1 : 0;
     s_na = na;
     for (int i = 0; i < HYB_STEPS; i++) s_src[i] = -1;
@@ -1425,7 +1452,7 @@ __global__ void __launch_bounds__(1024) bounds_decide_kernel(HybridState* __rest
 // shared memory, then written to its final rows (ids, and the key column rebuilt when asked). A
 // persistent grid of CTAs walks the buckets; a shape that is not the chosen one returns at once.
 template <int THREADS, int VARIANT, bool REC = false>
-__global__ void __launch_bounds__(THREADS, THREADS == 128 ? 10 : THREADS == 256 ? 5 : 2) local_sort_kernel(const uint64_t* __restrict__ keys,
+__global__ void __launch_bounds__(THREADS, THREADS == 128 ? 8 : THREADS == 256 ? 4 : 2) local_sort_kernel(const uint64_t* __restrict__ keys,
                                                              const void* __restrict__ ids_or_recs,
                                                              const uint32_t* __restrict__ pos,
                                                              const HybridState* __restrict__ hs,
@@ -1646,26 +1673,49 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? 10 : THREADS == 256 
     }
     // The bucket's rows, in order, to their final places.
     const uint64_t out0 = uint64_t(vbase) + start;
-    for (uint32_t r = threadIdx.x; r < size; r += THREADS) {
-      const uint64_t dst = out0 + r;
-      if (dst >= uint64_t(pa.desc->out_rows)) {
-        atomicOr(pa.err, ERR_BOUNDS);
-        continue;
-      }
-      if constexpr (REC) {
-        // The row's record, from its place in the bucket's input (one L2-resident span).
-        const uint4 rr = recs[start + sids[r]];
-        if (pa.final_out) {
-          if (pa.desc->flags & PF_WIDE_OUT) static_cast<uint64_t*>(pa.final_out)[dst] = rr.x;
-          else static_cast<uint32_t*>(pa.final_out)[dst] = rr.x;
+    if constexpr (REC) {
+      // Each row's record from its place in the bucket's input (one L2-resident span), four rows a
+      // thread per round with their loads in flight together.
+      constexpr int U = 4;
+      for (uint32_t r0 = threadIdx.x; r0 < size; r0 += THREADS * U) {
+        uint4 rr[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+          const uint32_t r = r0 + uint32_t(u) * THREADS;
+          if (r < size) rr[u] = recs[start + sids[r]];
         }
-        unpack_record(pa.rec, rr, dst);
-      } else if (pa.final_out) {
-        if (pa.desc->flags & PF_WIDE_OUT) static_cast<uint64_t*>(pa.final_out)[dst] = sids[r];
-        else static_cast<uint32_t*>(pa.final_out)[dst] = sids[r];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+          const uint32_t r = r0 + uint32_t(u) * THREADS;
+          if (r >= size) continue;
+          const uint64_t dst = out0 + r;
+          if (dst >= uint64_t(pa.desc->out_rows)) {
+            atomicOr(pa.err, ERR_BOUNDS);
+            continue;
+          }
+          if (pa.final_out) {
+            if (pa.desc->flags & PF_WIDE_OUT) static_cast<uint64_t*>(pa.final_out)[dst] = rr[u].x;
+            else static_cast<uint32_t*>(pa.final_out)[dst] = rr[u].x;
+          }
+          unpack_record(pa.rec, rr[u], dst);
+          if (pa.key_out_mode == KEY_OUT_UNKEY)
+            store_width(pa.key_out, dst, pt_bytes(pa.key_out_pt), unkey_bits<uint64_t>(skeys[r], pa.key_out_pt, pa.key_desc));
+        }
       }
-      if (pa.key_out_mode == KEY_OUT_UNKEY)
-        store_width(pa.key_out, dst, pt_bytes(pa.key_out_pt), unkey_bits<uint64_t>(skeys[r], pa.key_out_pt, pa.key_desc));
+    } else {
+      for (uint32_t r = threadIdx.x; r < size; r += THREADS) {
+        const uint64_t dst = out0 + r;
+        if (dst >= uint64_t(pa.desc->out_rows)) {
+          atomicOr(pa.err, ERR_BOUNDS);
+          continue;
+        }
+        if (pa.final_out) {
+          if (pa.desc->flags & PF_WIDE_OUT) static_cast<uint64_t*>(pa.final_out)[dst] = sids[r];
+          else static_cast<uint32_t*>(pa.final_out)[dst] = sids[r];
+        }
+        if (pa.key_out_mode == KEY_OUT_UNKEY)
+          store_width(pa.key_out, dst, pt_bytes(pa.key_out_pt), unkey_bits<uint64_t>(skeys[r], pa.key_out_pt, pa.key_desc));
+      }
     }
     // No barrier here either: the next bucket writes the tile only after its first histogram barrier.
   }
@@ -1771,6 +1821,16 @@ static void launch_local(const uint64_t* keys, const void* ids, const uint32_t* 
   else launch_local_as<VARIANT, false>(keys, ids, pos, hs, a, s);
 }
 
+// Value rows from which one 8-byte key takes the two-level sort.
+static uint64_t hybrid_min_rows() {
+  static const uint64_t v = [] {
+    const char* e = std::getenv("ARROWMETAL_HYBRID_MIN_ROWS");
+    const long long x = e ? std::atoll(e) : 0;
+    return x > 0 ? uint64_t(x) : HYB_MIN_ROWS;
+  }();
+  return v;
+}
+
 // Rows per look-back entry (a tile), the smallest over the key widths.
 static uint64_t min_super() {
   using A = PassConfig<uint32_t>;
@@ -1858,6 +1918,13 @@ bool payload_record_layout(const std::vector<am_array*>& cols, rs::RecLayout* L)
     L->off[i] = off;
     off += L->width[i];
   }
+  // The common payload (a float64 or int64 beside a 32-bit column) is read and written without the
+  // per-field loop.
+  if (cols.size() == 2 && L->width[order[0]] == 8 && L->width[order[1]] == 4) {
+    L->pair = 1;
+    L->wide = order[0];
+    L->narrow = order[1];
+  }
   return true;
 }
 
@@ -1916,7 +1983,8 @@ void radix_sort(const std::vector<SortKey>& keys, int64_t n64, void* out, int in
   // Per-call scratch: stats, plans, pass descriptors, tickets, summary (one memset), then the
   // ping-pong key and id buffers.
   // A single 8-byte key over at least 2^25 rows may take the two-level sort (the device decides).
-  const bool hybrid = K == 1 && pt_key_bytes(keys[0].col->pt) == 8 && n >= HYB_MIN_ROWS && n < (uint64_t(1) << 32);
+  pa.hyb_min_rows = hybrid_min_rows();
+  const bool hybrid = K == 1 && pt_key_bytes(keys[0].col->pt) == 8 && n >= pa.hyb_min_rows && n < (uint64_t(1) << 32);
   const int NT = S + (hybrid ? HYB_STEPS : 0);          // tile counters: one per launched pass
   const uint32_t bnd_blocks = uint32_t((n + BND_CHUNK - 1) / BND_CHUNK);
   const size_t off_stats = 0;

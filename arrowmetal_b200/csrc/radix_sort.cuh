@@ -73,6 +73,7 @@ struct SortSummary {
 
 struct PlanArgs {
   uint64_t n;
+  uint64_t hyb_min_rows;                    // value rows from which one 8-byte key takes the two-level sort
   int32_t nkeys, nslots, slot_key0_first, index_wide;
   uint8_t key_bytes[MAX_KEYS];
   uint8_t nulls_first[MAX_KEYS];
@@ -105,7 +106,8 @@ struct RecLayout {
   int32_t width[REC_MAX_COLS];        // 1, 2, 4 or 8 bytes
   int32_t off[REC_MAX_COLS];          // byte offset within the payload (0-11)
   int32_t ncols;
-  int32_t pad;
+  int32_t pair;                       // 1: exactly an 8-byte column (wide) and a 4-byte one (narrow)
+  int32_t wide, narrow;               // their column numbers, when `pair`
 };
 
 // key_out modes: the sorted key column itself, produced by inverting the key map in the last pass.

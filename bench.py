@@ -578,6 +578,44 @@ def run_strings(args, am, torch, stream, local):
         "clocks": clocks.summary()}))
 
 
+def run_sizes(args, am, torch, stream, local):
+    """--workload sizes: the ORDER BY (select_all(sort(scan))) of tables of 1M to 50M rows, for the
+    benchmark's key (int64 in [0, 2^40), 10% nulls) and for full-range int64 keys, each with the float64
+    and int32 payload columns; CUDA events, median of the steps. For choosing size thresholds."""
+    import pyarrow as pa
+    res = {}
+    rng = np.random.default_rng(SEED + 11)
+    for n in (1 << 20, 1 << 21, 1 << 22, 1 << 23, 1 << 24, 1 << 25, 40_000_000, N_ROWS):
+        p1 = pa.array(rng.standard_normal(n))
+        p2 = pa.array(rng.integers(-2**31, 2**31 - 1, n, dtype=np.int32, endpoint=True))
+        for kind in ("bench_key", "full_range"):
+            if kind == "bench_key":
+                key = pa.array(rng.integers(0, 2**40, n, dtype=np.int64), mask=rng.random(n) < 0.10)
+            else:
+                key = pa.array(rng.integers(np.iinfo(np.int64).min, np.iinfo(np.int64).max, n, dtype=np.int64,
+                                            endpoint=True))
+            src = am.PlanSource("t", {"c0": key, "c1": p1, "c2": p2})
+            for _ in range(3):
+                am.run_plan(PLAN, [src])
+            am.synchronize()
+            st = am.last_sort_stats()
+            times = []
+            for _ in range(max(5, min(args.steps, 20))):
+                ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                ev0.record(stream)
+                out = am.run_plan(PLAN, [src])
+                ev1.record(stream)
+                ev1.synchronize()
+                del out
+                times.append(ev0.elapsed_time(ev1))
+            ms = statistics.median(times)
+            res[f"{kind}/{n}"] = {"ms": ms, "rows_per_s": n / (ms / 1e3), "passes_run": st["passes_run"],
+                                  "records": st["payload_in_records"]}
+            del src
+    print(json.dumps({"metric": METRIC, "workload": "sizes", "unit": "ms",
+                      "hybrid_min_rows": os.environ.get("ARROWMETAL_HYBRID_MIN_ROWS", "default"), "sizes": res}))
+
+
 def plain_run(am, table, offset, n):
     """One request through am_plan_run on the calling thread (the plain per-call path)."""
     src, keys = table
@@ -857,7 +895,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="order_by",
                     choices=["order_by", "segmented", "serving", "full_range", "multikey", "topk", "strings",
-                             "consumers", "external"],
+                             "consumers", "external", "sizes"],
                     help="order_by: the 50M-row ORDER BY (the headline); segmented: 2,048 arrays in one call; "
                          "serving: the served request stream; full_range: 1M full-range int64 keys; multikey: "
                          "the 50M-row two-key sort; topk: ORDER BY ... LIMIT k by radix selection; strings: ORDER BY a utf8 key; "
@@ -917,6 +955,12 @@ def main():
     if args.workload == "external":
         if rank == 0:
             run_external(args, am, torch, local)
+        return
+    if args.workload == "sizes":
+        stream = torch.cuda.Stream()
+        am.set_stream(stream.cuda_stream)
+        if rank == 0:
+            run_sizes(args, am, torch, stream, local)
         return
     if args.workload == "consumers":
         stream = torch.cuda.Stream()
