@@ -2,21 +2,27 @@
 
 Workload (one step): a table of 3 columns -- key int64 uniform in [0, 2^40) with a 10% Bernoulli null
 bitmap, payload float64 ~ N(0, 1), payload int32 uniform -- sorted by key ascending, nulls last, stable,
-then the table taken through the permutation (the sorted key column comes out of the sort's last pass,
-rebuilt from the sorted keys; the two payload columns through one fused gather). It runs through the
-library's C ABI the way the DataFusion rule calls it: am_plan_run of select_all(sort(scan)). Inputs are
+then the table taken through the permutation. It runs through the library's C ABI the way the DataFusion
+rule calls it: am_plan_run of select_all(sort(scan)). With the table in HBM the payload columns ride
+through the sort in row records and the key column comes out of the sort rebuilt from its keys; with
+host inputs still uploading, the payload is gathered through the permutation after the sort. Inputs are
 seeded synthetic data of the benchmark's shape (numpy default_rng).
 
-  value    rows/s with the table already in HBM, timed with CUDA events on the library's stream, max
-           over ranks; inputs (400 MB key column) are larger than L2, so no flush is needed.
+  value    rows/s with the table already in HBM: K steps timed with CUDA events on the library's stream
+           (no per-launch events), max over ranks; inputs (400 MB key column) are larger than L2, so no
+           flush is needed. The per-kernel split comes from a second, profiled loop.
   e2e      the same through the C ABI with host buffers: am_import of the 3 columns from pinned host
-           memory (host to device), the plan, am_export of the 3 result columns (device to host), wall
-           clock per step.
-  roofline the dominant kernel's algorithmic bytes / its CUDA-event time over the timed region, against
-           the measured HBM copy peak.
-  cpu_baseline  the CPU oracle (the reference algorithm restated in C) on the host's cores.
+           memory (host to device), the plan, am_export of the 3 result columns (device to host), two
+           steps in flight on two threads (each with its own streams); one_in_flight: the same one step
+           at a time.
+  roofline the dominant kernel's algorithmic bytes / its CUDA-event time, against the measured HBM
+           copy peak.
+  cpu_baseline  the CPU oracle (the reference algorithm restated in C) on the host's cores; beside it
+           pyarrow's sort_indices + take and DataFusion (when importable).
+  full_range, multikey, batched, served  the benchmark's other configurations, each with its own
+           CUDA events and clock record (one GPU; --headline-only skips them).
 
-python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--workload NAME]
 Multi-GPU (torchrun, one rank per GPU) runs independent replicas of the workload: the sort shards by
 table / request, with no collective on the data path ("scaling": "weak").
 """
@@ -745,17 +751,18 @@ def algorithmic_bytes(n, m, passes, local_sort=False, records=False):
     return out
 
 
-# DRAM bytes (read + write) per row of the workload, per kernel and step, from ncu captures of this
-# benchmark at 40,000,000 rows, where the two-level sort runs as at 50M (dram__bytes_read.sum +
-# dram__bytes_write.sum summed over the kernel's launches in one step,
-# profiles/order_by_int64_40M_dram_traffic.md; the digit passes from
-# profiles/onesweep_pass_order_by_40M_full.md), scaled by rows.
-TRAFFIC_PER_ROW = {"radix_histogram": 8.16, "radix_onesweep_pass": 39.79, "radix_local_sort": 19.32,
-                   "take_gather": 154.25}
+# DRAM bytes (read + write) per row of the workload, per kernel and step: dram__bytes_read.sum +
+# dram__bytes_write.sum of the kernel's launches in one sort, from one ncu capture of this benchmark at
+# 38,000,000 rows (34.2M value rows: the two-level sort runs as at 50M), divided by the rows. Keyed by
+# whether the payload rode through the sort in records (the table in HBM) or was gathered afterwards.
+TRAFFIC_PER_ROW = {
+    True: {"radix_histogram": 8.22, "radix_onesweep_pass": 84.96, "radix_local_sort": 38.50},
+    False: {},
+}
 
 
-def traffic_per_step(kernel, n):
-    b = TRAFFIC_PER_ROW.get(kernel)
+def traffic_per_step(kernel, n, records):
+    b = TRAFFIC_PER_ROW[bool(records)].get(kernel)
     return None if b is None else b * n
 
 
@@ -890,6 +897,8 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--e2e-inflight", type=int, default=2,
+                    help="end-to-end steps in flight at once (threads, each with its own streams)")
     ap.add_argument("--rows", type=int, default=N_ROWS)
     ap.add_argument("--impl", default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -1090,6 +1099,36 @@ def main():
         del hc, s2, out, res
     e2e_ms = max_over_ranks(1e3 * statistics.median(e2e_times) if e2e_times else float("nan"), dist, "cuda")
 
+    # ---- the same steps with two in flight: two threads, each with its own pinned copy of the inputs
+    # (and the library's own streams per thread), run steps back to back, so one step's uploads overlap
+    # the other's downloads on the two copy directions. Every step still imports its inputs from host
+    # memory and exports its whole result to host memory.
+    inflight_ms = None
+    if args.e2e_steps > 0 and args.e2e_inflight > 1:
+        per_thread = [{k: pinned_array(v) for k, v in cols.items()} for _ in range(args.e2e_inflight)]
+
+        def e2e_worker(hcols, nsteps):
+            for _ in range(nsteps):
+                hc = {k: am.MetalArray.from_arrow(v) for k, v in hcols.items()}
+                s2 = am.PlanSource("t", hc)
+                out = am.run_plan(PLAN, [s2])
+                res = {k: v.to_arrow() for k, v in out.items()}
+                del hc, s2, out, res
+
+        def run_threads(nsteps):
+            ths = [threading.Thread(target=e2e_worker, args=(hcols, nsteps)) for hcols in per_thread]
+            t0 = time.perf_counter()
+            for t in ths:
+                t.start()
+            for t in ths:
+                t.join()
+            return time.perf_counter() - t0
+
+        run_threads(1)                                  # each thread's streams and pinned staging
+        total = run_threads(args.e2e_steps)
+        inflight_ms = max_over_ranks(1e3 * total / (args.e2e_steps * args.e2e_inflight), dist, "cuda")
+        del per_thread
+
     line = {
         "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
@@ -1101,12 +1140,18 @@ def main():
                    "l2": "inputs larger than L2 (400 MB key column), no flush"},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": d["gbs"], "peak": peak, "unit": "GB/s",
                      "frac": d["gbs"] / peak, "peak_source": peak_kind,
-                     "traffic": traffic_per_step(dom, n), "per": "one step (all launches of the kernel in one sort)",
+                     "traffic": traffic_per_step(dom, n, st["payload_in_records"]),
+                     "per": "one step (all launches of the kernel in one sort)",
                      "pipeline": {"bytes": sum(model.values()), "gbs": sum(model.values()) / (ms / 1e3) / 1e9,
                                   "frac": sum(model.values()) / (ms / 1e3) / 1e9 / peak},
                      "per_kernel": per_kernel},
-        "e2e": {"value": whole_job_rate(n, world, e2e_ms), "unit": "rows/s", "ms_per_step": e2e_ms,
-                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "e2e": ({"value": whole_job_rate(n, world, inflight_ms), "unit": "rows/s", "ms_per_step": inflight_ms,
+                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                 "steps_in_flight": args.e2e_inflight,
+                 "one_in_flight": {"value": whole_job_rate(n, world, e2e_ms), "ms_per_step": e2e_ms}}
+                if inflight_ms else
+                {"value": whole_job_rate(n, world, e2e_ms), "unit": "rows/s", "ms_per_step": e2e_ms,
+                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "steps_in_flight": 1}),
         "gpu_launches": int(gpu_launches),
         "clocks": clocks.summary(),
     }
