@@ -71,7 +71,8 @@ class _ArrowDeviceArray(ctypes.Structure):
 
 class ServerStats(ctypes.Structure):
     _fields_ = [(n, _I64) for n in ("requests", "solo_requests", "batches", "batched_requests", "rows",
-                                    "peak_in_flight_bytes", "in_flight_bytes", "queued")]
+                                    "peak_in_flight_bytes", "in_flight_bytes", "queued", "shared_sorts",
+                                    "shared_requests")]
 
 
 class BatchShape(ctypes.Structure):

@@ -267,6 +267,11 @@ void radix_sort(const std::vector<SortKey>& keys, int64_t n, void* out, int inde
 // The row-record layout of payload columns (RecLayout without its destinations), or false when they
 // cannot ride in a record: at most four fixed-width columns without nulls, twelve bytes in all.
 bool payload_record_layout(const std::vector<am_array*>& cols, rs::RecLayout* L);
+// The sort server's shared sorts: for each range q, the entries of `perm` (n row numbers) that lie in
+// [lo[q], hi[q]), in order, into outs[q] (device memory holding hi[q] - lo[q] entries).
+constexpr int MAX_SHARED = 32;
+void compact_ranges(const uint32_t* perm, uint64_t n, const std::vector<uint32_t>& lo, const std::vector<uint32_t>& hi,
+                    const std::vector<uint32_t*>& outs, cudaStream_t s);
 // Segmented argsort: outs[i] (a uint32 array of keys[i].col->length rows) receives the argsort of
 // keys[i], one key per array; the arrays of a key width share every launch.
 void radix_argsort_batch(const std::vector<SortKey>& keys, const std::vector<void*>& outs, cudaStream_t s);

@@ -954,7 +954,7 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
           if (lane == __ffs(peers) - 1) sm.whist[warp][d] = base + __popc(peers);
           const uint32_t pos = sm.local[d] + base + __popc(peers & lt_mask);
           sm.keys[pos] = key[i];
-          if constexpr (REC) sm.ids[id[i] - uint32_t(tile_base)] = uint16_t(pos);   // each row's place
+          if constexpr (REC) sm.ids[pos] = uint16_t(id[i] - uint32_t(tile_base));
           else if (pa.carry_ids) sm.ids[pos] = id[i];
           sm.dig[pos] = uint16_t(d);
         }
@@ -1014,42 +1014,53 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
     const bool last = (flags & PF_LAST) != 0;
     const bool merged = keys_out && ids_out && pa.carry_ids;
     if constexpr (REC) {
-      // Keys leave shared memory in sorted order (consecutive threads, consecutive addresses within a
-      // digit run). Records are read in row order -- coalesced: the tile's rows are contiguous in the
-      // input, or (first pass) built from the payload columns -- and each goes to its row's place, so
-      // no load waits on a random read; a row reaching its final place has its record unpacked.
-      if (keys_out) {
-        for (uint32_t j = threadIdx.x; j < tile_n; j += THREADS) {
-          const uint32_t d = sm.dig[j];
-          if (d >= RADIX) continue;
-          const uint32_t dst = sm.gdelta[d] + j;
-          if (dst < buf_rows) keys_out[dst] = sm.keys[j];
-          else atomicOr(pa.err, ERR_BOUNDS);
-        }
-      }
+      // Keys and records in one loop. A row's record comes from its place in the tile's input (the
+      // tile's records, read in sorted order, stay within one L2-resident span), or is built from the
+      // payload columns in the first pass; a row reaching its final place has its record unpacked.
+      // Two rows a thread per round, their record loads in flight together (each is a random read
+      // within the tile's span, an L2 round trip).
       const uint4* __restrict__ rin = reinterpret_cast<const uint4*>(ids_in);
       uint4* __restrict__ rout = reinterpret_cast<uint4*>(ids_out);
+      constexpr int U = 2;
       const bool encode = (flags & PF_ENCODE) != 0;
-      for (uint32_t li = threadIdx.x; li < tile_n; li += THREADS) {
-        const uint4 r = encode ? build_record(pa.rec, uint32_t(tile_base + li)) : rin[tile_base + li];
-        const uint32_t pos = sm.ids[li];
-        const uint32_t d = sm.dig[pos];
-        uint32_t dst = sm.gdelta[d] + pos;
-        if (d < RADIX && rout) {
-          if (dst < buf_rows) rout[dst] = r;
-          else atomicOr(pa.err, ERR_BOUNDS);
-          continue;
+      for (uint32_t j0 = threadIdx.x; j0 < tile_n; j0 += THREADS * U) {
+        uint4 r[U];
+        uint32_t dg[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+          const uint32_t j = j0 + uint32_t(u) * THREADS;
+          dg[u] = INVALID_DIGIT;
+          if (j >= tile_n) continue;
+          dg[u] = sm.dig[j];
+          const uint64_t src_row = tile_base + sm.ids[j];
+          r[u] = encode ? build_record(pa.rec, uint32_t(src_row)) : rin[src_row];
         }
-        if (d < RADIX) dst += sm.desc.value_base;
-        if (dst >= out_rows) {
-          atomicOr(pa.err, ERR_BOUNDS);
-          continue;
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+          const uint32_t j = j0 + uint32_t(u) * THREADS;
+          const uint32_t d = dg[u];
+          if (d == INVALID_DIGIT) continue;
+          uint32_t dst = sm.gdelta[d] + j;
+          if (d < RADIX && rout) {
+            if (dst < buf_rows) {
+              if (keys_out) keys_out[dst] = sm.keys[j];
+              rout[dst] = r[u];
+            } else {
+              atomicOr(pa.err, ERR_BOUNDS);
+            }
+            continue;
+          }
+          if (d < RADIX) dst += sm.desc.value_base;
+          if (dst >= out_rows) {
+            atomicOr(pa.err, ERR_BOUNDS);
+            continue;
+          }
+          if (final_out) {
+            if (flags & PF_WIDE_OUT) static_cast<uint64_t*>(final_out)[dst] = r[u].x;
+            else static_cast<uint32_t*>(final_out)[dst] = r[u].x;
+          }
+          unpack_record(pa.rec, r[u], dst);
         }
-        if (final_out) {
-          if (flags & PF_WIDE_OUT) static_cast<uint64_t*>(final_out)[dst] = r.x;
-          else static_cast<uint32_t*>(final_out)[dst] = r.x;
-        }
-        unpack_record(pa.rec, r, dst);
       }
     } else if (merged) {
       for (uint32_t j = threadIdx.x; j < tile_n; j += THREADS) {
@@ -1670,36 +1681,34 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? 8 : THREADS == 256 ?
     // The bucket's rows, in order, to their final places.
     const uint64_t out0 = uint64_t(vbase) + start;
     if constexpr (REC) {
-      // Each row's place, indexed by its place in the bucket's input (in the ranking's counters, free
-      // now); the rebuilt keys leave in sorted order, the records are read in input order -- coalesced
-      // -- and written to their rows' places.
-      uint16_t* posof = reinterpret_cast<uint16_t*>(whist);
-      for (uint32_t p = threadIdx.x; p < size; p += THREADS) posof[sids[p]] = uint16_t(p);
-      __syncthreads();
-      if (pa.key_out_mode == KEY_OUT_UNKEY) {
-        for (uint32_t p = threadIdx.x; p < size; p += THREADS) {
-          const uint64_t dst = out0 + p;
+      // Each row's record from its place in the bucket's input (one L2-resident span), four rows a
+      // thread per round with their loads in flight together.
+      constexpr int U = 4;
+      for (uint32_t r0 = threadIdx.x; r0 < size; r0 += THREADS * U) {
+        uint4 rr[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+          const uint32_t r = r0 + uint32_t(u) * THREADS;
+          if (r < size) rr[u] = recs[start + sids[r]];
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+          const uint32_t r = r0 + uint32_t(u) * THREADS;
+          if (r >= size) continue;
+          const uint64_t dst = out0 + r;
           if (dst >= uint64_t(pa.desc->out_rows)) {
             atomicOr(pa.err, ERR_BOUNDS);
             continue;
           }
-          store_width(pa.key_out, dst, pt_bytes(pa.key_out_pt), unkey_bits<uint64_t>(skeys[p], pa.key_out_pt, pa.key_desc));
+          if (pa.final_out) {
+            if (pa.desc->flags & PF_WIDE_OUT) static_cast<uint64_t*>(pa.final_out)[dst] = rr[u].x;
+            else static_cast<uint32_t*>(pa.final_out)[dst] = rr[u].x;
+          }
+          unpack_record(pa.rec, rr[u], dst);
+          if (pa.key_out_mode == KEY_OUT_UNKEY)
+            store_width(pa.key_out, dst, pt_bytes(pa.key_out_pt), unkey_bits<uint64_t>(skeys[r], pa.key_out_pt, pa.key_desc));
         }
       }
-      for (uint32_t li = threadIdx.x; li < size; li += THREADS) {
-        const uint4 rr = recs[start + li];
-        const uint64_t dst = out0 + posof[li];
-        if (dst >= uint64_t(pa.desc->out_rows)) {
-          atomicOr(pa.err, ERR_BOUNDS);
-          continue;
-        }
-        if (pa.final_out) {
-          if (pa.desc->flags & PF_WIDE_OUT) static_cast<uint64_t*>(pa.final_out)[dst] = rr.x;
-          else static_cast<uint32_t*>(pa.final_out)[dst] = rr.x;
-        }
-        unpack_record(pa.rec, rr, dst);
-      }
-      __syncthreads();                   // the next bucket's counters reuse posof's words
     } else {
       for (uint32_t r = threadIdx.x; r < size; r += THREADS) {
         const uint64_t dst = out0 + r;
@@ -1980,7 +1989,7 @@ void radix_sort(const std::vector<SortKey>& keys, int64_t n64, void* out, int in
 
   // Per-call scratch: stats, plans, pass descriptors, tickets, summary (one memset), then the
   // ping-pong key and id buffers.
-  // A single 8-byte key over at least 2^25 rows may take the two-level sort (the device decides).
+  // A single 8-byte key over at least 2^21 rows may take the two-level sort (the device decides).
   pa.hyb_min_rows = hybrid_min_rows();
   const bool hybrid = K == 1 && pt_key_bytes(keys[0].col->pt) == 8 && n < (uint64_t(1) << 32) &&
                       n >= (pa.hyb_min_rows ? pa.hyb_min_rows : HYB_MIN_ANY);

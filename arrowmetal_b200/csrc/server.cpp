@@ -17,7 +17,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <condition_variable>
+#include <algorithm>
 #include <deque>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <sstream>
@@ -98,6 +100,7 @@ struct am_server_t {
   int64_t cap = 0, batch_rows = 0;
   int64_t in_flight = 0;
   bool stop = false;
+  bool share = true;               // ARROWMETAL_SERVER_SHARED=0 turns shared sorts off
   am_server_stats stats{};
   std::vector<std::thread> workers;
   Clock::time_point created = Clock::now();
@@ -105,12 +108,155 @@ struct am_server_t {
   std::mutex trace_mu;
 
   void run_worker(int index);
-  std::vector<ReqPtr> next_unit(int64_t* footprint);
-  void execute(std::vector<ReqPtr>& unit);
+  std::vector<ReqPtr> next_unit(int64_t* footprint, bool* shared);
+  bool take_shared(std::vector<ReqPtr>& unit, int64_t* footprint);
+  void execute(std::vector<ReqPtr>& unit, bool shared);
+  void execute_shared(std::vector<ReqPtr>& unit);
 };
 
-// Under the lock: the first queued request that fits, with the batchable requests that fit beside it.
-std::vector<ReqPtr> am_server_t::next_unit(int64_t* footprint) {
+namespace {
+
+// Requests that one sort can answer: the same table, keys and options.
+bool same_sort(const ServeRequest& a, const ServeRequest& b) {
+  return a.table == b.table && a.key_cols == b.key_cols && a.desc == b.desc && a.nulls_first == b.nulls_first &&
+         a.float_order == b.float_order;
+}
+
+}  // namespace
+
+// Under the lock, `unit` holding the first request (already out of the queue): the queued requests that
+// share its sort, when sharing saves work. A request joins when it covers at least a 32nd of the rows
+// the shared sort covers (its share of the compaction stays small), and the unit is shared when its
+// requests' rows add up to at least one and a half times the covered rows.
+bool am_server_t::take_shared(std::vector<ReqPtr>& unit, int64_t* footprint) {
+  const ServeRequest& r0 = *unit[0];
+  std::vector<std::deque<ReqPtr>::iterator> cand;
+  for (auto it = queue.begin(); it != queue.end() && cand.size() + 1 < size_t(MAX_SHARED); ++it)
+    if (same_sort(**it, r0)) cand.push_back(it);
+  if (cand.empty()) return false;
+  int64_t lo = r0.offset, hi = r0.offset + r0.length;
+  for (auto& it : cand) {
+    lo = std::min(lo, (*it)->offset);
+    hi = std::max(hi, (*it)->offset + (*it)->length);
+  }
+  std::vector<std::deque<ReqPtr>::iterator> keep;
+  int64_t rows = r0.length, fp = r0.footprint;
+  int64_t klo = r0.offset, khi = r0.offset + r0.length;
+  for (auto& it : cand) {
+    const ServeRequest& q = **it;
+    if (q.length * 32 < hi - lo) continue;
+    if (in_flight > 0 && in_flight + fp + q.footprint > cap) continue;
+    keep.push_back(it);
+    rows += q.length;
+    fp += q.footprint;
+    klo = std::min(klo, q.offset);
+    khi = std::max(khi, q.offset + q.length);
+  }
+  if (keep.empty() || r0.length * 32 < khi - klo || 2 * rows < 3 * (khi - klo)) return false;
+  std::vector<const ServeRequest*> taken;
+  for (auto& it : keep) {
+    unit.push_back(*it);
+    taken.push_back(it->get());
+  }
+  queue.erase(std::remove_if(queue.begin(), queue.end(),
+                             [&](const ReqPtr& q) { return std::find(taken.begin(), taken.end(), q.get()) != taken.end(); }),
+              queue.end());
+  *footprint = fp;
+  return true;
+}
+
+// One sort of the rows the unit's requests cover together, then each request's order by keeping the
+// entries within its rows (compact_ranges), then one fused take of its columns.
+void am_server_t::execute_shared(std::vector<ReqPtr>& unit) {
+  const ServeRequest& r0 = *unit[0];
+  int64_t lo = r0.offset, hi = r0.offset + r0.length;
+  for (auto& r : unit) {
+    lo = std::min(lo, r->offset);
+    hi = std::max(hi, r->offset + r->length);
+  }
+  const int64_t n = hi - lo;
+  std::vector<am_array*> temps, kcols, idx;
+  std::map<int, am_array*> pcols;
+  am_array* perm = nullptr;
+  auto cleanup = [&] {
+    for (am_array* a : temps) am_release(a);
+    for (am_array* a : idx) am_release(a);
+    if (perm) am_release(perm);
+  };
+  int rc = 0;
+  std::string err;
+  try {
+    auto slice = [&](int c) {
+      am_array* a = nullptr;
+      if (am_slice(r0.table->cols[size_t(c)], lo, n, &a) != 0) throw Error(am_last_error());
+      temps.push_back(a);
+      return a;
+    };
+    for (int c : r0.key_cols) kcols.push_back(slice(c));
+    const int K = int(kcols.size());
+    std::vector<int> desc(r0.desc), np(r0.nulls_first), fo(r0.float_order);
+    rc = K == 1 ? am_argsort_ex2(kcols[0], desc[0], np[0], fo[0], &perm)
+                : am_lexsort_ex2(kcols.data(), desc.data(), np.data(), fo.data(), K, &perm);
+    if (rc != 0) throw Error(am_last_error(), rc);
+    cudaStream_t s = stream();
+    std::vector<uint32_t> qlo, qhi;
+    std::vector<uint32_t*> outs;
+    for (auto& r : unit) {
+      am_array* o = new_array(PT_U32, "I", r->length);
+      idx.push_back(o);
+      o->values = DevBuffer::alloc(size_t(std::max<int64_t>(r->length, 1)) * 4 + 16, s);
+      o->null_count = 0;
+      o->perm_of = n;                      // entries index the covered rows
+      o->last_stream = s;
+      qlo.push_back(uint32_t(r->offset - lo));
+      qhi.push_back(uint32_t(r->offset - lo + r->length));
+      outs.push_back(static_cast<uint32_t*>(o->values->ptr));
+    }
+    use_on(perm, s);
+    compact_ranges(static_cast<const uint32_t*>(perm->data()), uint64_t(n), qlo, qhi, outs, s);
+    for (size_t i = 0; i < unit.size(); i++) {
+      ServeRequest& r = *unit[i];
+      std::vector<am_array*> cols(kcols);
+      for (int c : r.pay_cols) {
+        if (!pcols.count(c)) pcols[c] = slice(c);
+        cols.push_back(pcols[c]);
+      }
+      auto* res = new am_plan_result_t();
+      res->rows = r.length;
+      res->cols.assign(cols.size(), nullptr);
+      if (am_take_columns(cols.data(), int64_t(cols.size()), idx[i], res->cols.data()) != 0) {
+        res->cols.clear();
+        delete res;
+        throw Error(am_last_error());
+      }
+      for (int c : r.key_cols) res->names.push_back(r.table->names[size_t(c)]);
+      for (int c : r.pay_cols) res->names.push_back(r.table->names[size_t(c)]);
+      r.result = res;
+    }
+    for (auto& r : unit) r->enqueued = Clock::now();
+    rc = am_cuda_synchronize();
+    if (rc != 0) err = am_last_error();
+  } catch (const Error& e) {
+    rc = e.code ? e.code : 1;
+    err = e.what();
+  }
+  if (rc != 0) {
+    for (auto& r : unit) {
+      if (r->result) {
+        am_plan_result_release(r->result);
+        r->result = nullptr;
+      }
+      r->rc = rc;
+      r->error = err;
+    }
+  }
+  cleanup();
+}
+
+// Under the lock: the first queued request that fits, with the requests that share its sort, or else
+// the batchable requests that fit beside it.
+std::vector<ReqPtr> am_server_t::next_unit(int64_t* footprint, bool* shared) {
+  *shared = false;
   std::vector<ReqPtr> unit;
   int64_t fp = 0, rows = 0;
   for (auto it = queue.begin(); it != queue.end(); ++it) {
@@ -121,6 +267,11 @@ std::vector<ReqPtr> am_server_t::next_unit(int64_t* footprint) {
     rows = r->length;
     queue.erase(it);
     break;
+  }
+  if (!unit.empty() && share && take_shared(unit, &fp)) {
+    *shared = true;
+    *footprint = fp;
+    return unit;
   }
   if (!unit.empty() && unit[0]->batchable) {
     for (auto it = queue.begin(); it != queue.end();) {
@@ -139,7 +290,11 @@ std::vector<ReqPtr> am_server_t::next_unit(int64_t* footprint) {
   return unit;
 }
 
-void am_server_t::execute(std::vector<ReqPtr>& unit) {
+void am_server_t::execute(std::vector<ReqPtr>& unit, bool shared) {
+  if (shared) {
+    execute_shared(unit);
+    return;
+  }
   auto fail_all = [&](int rc, const std::string& msg) {
     for (auto& r : unit) {
       if (r->result) {
@@ -213,6 +368,7 @@ void am_server_t::run_worker(int index) {
   for (;;) {
     std::vector<ReqPtr> unit;
     int64_t fp = 0;
+    bool shared = false;
     {
       std::unique_lock<std::mutex> lk(mu);
       work_cv.wait(lk, [&] {
@@ -222,11 +378,14 @@ void am_server_t::run_worker(int index) {
         return false;
       });
       if (stop && queue.empty()) return;
-      unit = next_unit(&fp);
+      unit = next_unit(&fp, &shared);
       if (unit.empty()) continue;
       in_flight += fp;
       stats.peak_in_flight_bytes = std::max(stats.peak_in_flight_bytes, in_flight);
-      if (unit.size() > 1 || unit[0]->batchable) {
+      if (shared) {
+        stats.shared_sorts++;
+        stats.shared_requests += int64_t(unit.size());
+      } else if (unit.size() > 1 || unit[0]->batchable) {
         stats.batches++;
         stats.batched_requests += int64_t(unit.size());
       } else {
@@ -234,7 +393,7 @@ void am_server_t::run_worker(int index) {
       }
     }
     const Clock::time_point t_start = Clock::now();
-    execute(unit);
+    execute(unit, shared);
     const Clock::time_point t = Clock::now();
     if (trace) {
       // worker, dispatch and finish (ms since the server started), requests, rows, first request's
@@ -288,6 +447,7 @@ int am_server_create(int workers, int64_t hbm_cap_bytes, int64_t batch_rows, am_
     auto* s = new am_server_t();
     s->cap = hbm_cap_bytes;
     s->batch_rows = batch_rows;
+    if (const char* e = std::getenv("ARROWMETAL_SERVER_SHARED")) s->share = e[0] != '0';
     if (const char* path = std::getenv("ARROWMETAL_SERVER_TRACE")) {
       s->trace = std::fopen(path, "a");
       if (s->trace) std::fprintf(s->trace, "server workers %d cap %lld batch_rows %lld\n", workers,

@@ -12,9 +12,8 @@ seeded synthetic data of the benchmark's shape (numpy default_rng).
            (no per-launch events), max over ranks; inputs (400 MB key column) are larger than L2, so no
            flush is needed. The per-kernel split comes from a second, profiled loop.
   e2e      the same through the C ABI with host buffers: am_import of the 3 columns from pinned host
-           memory (host to device), the plan, am_export of the 3 result columns (device to host), two
-           steps in flight on two threads (each with its own streams); one_in_flight: the same one step
-           at a time.
+           memory (host to device), the plan, am_export of the 3 result columns (device to host), one
+           step at a time (--e2e-inflight N: N steps in flight on N threads, each with its own streams).
   roofline the dominant kernel's algorithmic bytes / its CUDA-event time, against the measured HBM
            copy peak.
   cpu_baseline  the CPU oracle (the reference algorithm restated in C) on the host's cores; beside it
@@ -756,7 +755,7 @@ def algorithmic_bytes(n, m, passes, local_sort=False, records=False):
 # 38,000,000 rows (34.2M value rows: the two-level sort runs as at 50M), divided by the rows. Keyed by
 # whether the payload rode through the sort in records (the table in HBM) or was gathered afterwards.
 TRAFFIC_PER_ROW = {
-    True: {"radix_histogram": 8.22, "radix_onesweep_pass": 84.96, "radix_local_sort": 38.50},
+    True: {"radix_histogram": 8.21, "radix_onesweep_pass": 84.95, "radix_local_sort": 38.51},
     False: {},
 }
 
@@ -897,7 +896,7 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--e2e-steps", type=int, default=5)
-    ap.add_argument("--e2e-inflight", type=int, default=2,
+    ap.add_argument("--e2e-inflight", type=int, default=1,
                     help="end-to-end steps in flight at once (threads, each with its own streams)")
     ap.add_argument("--rows", type=int, default=N_ROWS)
     ap.add_argument("--impl", default="ours")

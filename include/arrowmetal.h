@@ -314,6 +314,8 @@ typedef struct am_server_stats {
   int64_t peak_in_flight_bytes;   /* largest admitted footprint on the GPU at once */
   int64_t in_flight_bytes;
   int64_t queued;
+  int64_t shared_sorts;           /* sorts shared by several queued requests of one table and key */
+  int64_t shared_requests;        /* requests answered from those sorts */
 } am_server_stats;
 int  am_server_create(int workers, int64_t hbm_cap_bytes, int64_t batch_rows, am_server** out);
 int  am_server_submit(am_server* server, am_plan_source* table, int64_t offset, int64_t length,
