@@ -161,3 +161,44 @@ def test_bad_requests_fail_at_submission(am):
             srv.submit(src, N - 5, 10, ["k64"], ["p1"])
         got, _ = srv.wait(srv.submit(src, 10, 0, ["k64"], ["p1"]))
         assert all(len(v) == 0 for v in got.values())
+
+
+def test_shared_sorts_equal_each_request_alone(am, oracle):
+    # Queued requests of one table, key and options over overlapping slices share one sort of the rows
+    # they cover; each result must still equal the request alone and pyarrow's order of its slice.
+    src, cols = table_and_columns(am, seed=13)
+    rng = np.random.default_rng(14)
+    kinds = [(["k64"], [False], ["at_end"], ["ieee"]), (["kf"], [True], ["at_start"], ["total"]),
+             (["k32", "k64"], [True, False], ["at_end", "at_start"], ["ieee", "ieee"])]
+    reqs = []
+    for i in range(48):
+        keys, desc, nulls, orders = kinds[i % 3]
+        length = int(rng.integers(N // 8, N // 2))
+        offset = int(rng.integers(0, N - length + 1))
+        reqs.append((offset, length, keys, desc, nulls, orders, ["p1", "p2"]))
+    alone = [am.run_plan(plan_alone(*r), [src]) for r in reqs]
+    with am.Server(workers=2, hbm_cap_bytes=8 << 30, batch_rows=0) as srv:
+        tickets = [srv.submit(src, o, n, k, p, descending=d, null_placement=nl, float_order=fo)
+                   for (o, n, k, d, nl, fo, p) in reqs]
+        results = [srv.wait(t)[0] for t in tickets]
+        stats = srv.stats()
+    assert stats["requests"] == len(reqs) and stats["shared_sorts"] > 0 and stats["shared_requests"] > 2
+    for r, want, got in zip(reqs, alone, results):
+        assert list(got) == list(want), r
+        for name in want:
+            assert same(got[name].to_arrow(), want[name].to_arrow()), (r, name)
+    for i in range(0, len(reqs), 5):
+        offset, length, keys, desc, nulls, orders, payload = reqs[i]
+        order = pa.array(expected_order(oracle, cols, offset, length, keys, desc, nulls, orders))
+        for name in results[i]:
+            assert same(results[i][name].to_arrow(), cols[name].slice(offset, length).take(order)), (reqs[i], name)
+
+
+def test_shared_sorts_can_be_turned_off(am, monkeypatch):
+    src = table(am, seed=15)
+    monkeypatch.setenv("ARROWMETAL_SERVER_SHARED", "0")
+    with am.Server(workers=1, hbm_cap_bytes=8 << 30, batch_rows=0) as srv:
+        ts = [srv.submit(src, 1000 * i, N // 2, ["k64"], ["p1"]) for i in range(6)]
+        for t in ts:
+            srv.wait(t)
+        assert srv.stats()["shared_sorts"] == 0
