@@ -17,6 +17,13 @@ extern "C" int am_argsort_batch(am_array** arrays, const int* descending, const 
     std::vector<SortKey> keys;
     std::vector<void*> ptrs;
     try {
+      // Every output index array is a view into one block (each array's rows rounded up to 16 bytes):
+      // one stream-ordered allocation for the batch, not one per array. The block is freed when the
+      // last view is released.
+      std::vector<size_t> offs(size_t(count) + 1, 0);
+      for (int64_t i = 0; i < count; i++)
+        offs[size_t(i) + 1] = offs[size_t(i)] + ((size_t(std::max<int64_t>(arrays[i]->length, 1)) * 4 + 15) & ~size_t(15));
+      BufPtr block = count > 0 ? DevBuffer::alloc(offs[size_t(count)] + 16, s) : nullptr;
       for (int64_t i = 0; i < count; i++) {
         SortKey k{arrays[i], descending ? descending[i] != 0 : false, null_placement ? null_placement[i] == 1 : false,
                   float_order ? float_order[i] : 0};
@@ -26,7 +33,25 @@ extern "C" int am_argsort_batch(am_array** arrays, const int* descending, const 
         use_on(arrays[i], s);
         am_array* o = new_array(PT_U32, "I", n);
         res.push_back(o);
-        o->values = DevBuffer::alloc(size_t(std::max<int64_t>(n, 1)) * 4 + 16, s);
+        auto view = std::make_shared<DevBuffer>();
+        view->ptr = static_cast<char*>(block->ptr) + offs[size_t(i)];
+        view->bytes = offs[size_t(i) + 1] - offs[size_t(i)];
+        view->stream = s;
+        view->owned = false;
+        // The block is freed on its own stream once every view is gone: each view's release first
+        // orders that stream after the view's last stream.
+        DevBuffer* vp = view.get();
+        view->on_release = [block, vp] {
+          if (vp->stream && vp->stream != block->stream) {
+            cudaEvent_t e;
+            if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) == cudaSuccess) {
+              (void)cudaEventRecord(e, vp->stream);
+              (void)cudaStreamWaitEvent(block->stream, e, 0);
+              (void)cudaEventDestroy(e);
+            }
+          }
+        };
+        o->values = view;
         o->null_count = 0;
         o->perm_of = n;
         o->last_stream = s;

@@ -7,9 +7,12 @@
 // threads each own a CUDA stream. A free worker takes, in arrival order, the first queued request
 // whose footprint fits under the admission cap beside the work already on the GPU; a single-key request
 // of at most `batch_rows` rows takes every other such request that fits with it, and they are sorted as
-// one segmented batch (am_argsort_batch) followed by one fused gather per request. Larger and
-// multi-key requests run alone through am_plan_run. Requests that arrive while others run are picked
-// up by the next free worker, so their work overlaps on the device.
+// one segmented batch (am_argsort_batch) followed by one fused gather per request. When the queue is
+// backlogged, queued requests of the same table, keys and options share one sort of the rows they
+// cover together: each is answered by keeping, in order, the entries of that sort that fall in its own
+// rows (a stable sort restricted to a subset of rows is the subset's own stable sort) and one fused
+// gather (shared_sort.cu). Other requests run alone through am_plan_run. Requests that arrive while
+// others run are picked up by the next free worker, so their work overlaps on the device.
 //
 // The reference has no server: its callers make one call per query. Every result equals the same
 // request run alone through am_plan_run.
@@ -116,6 +119,9 @@ struct am_server_t {
 
 namespace {
 
+constexpr int kMaxSharedUnit = 16;      // requests answered from one shared sort (at most MAX_SHARED)
+static_assert(kMaxSharedUnit <= MAX_SHARED, "one compaction launch serves the unit");
+
 // Requests that one sort can answer: the same table, keys and options.
 bool same_sort(const ServeRequest& a, const ServeRequest& b) {
   return a.table == b.table && a.key_cols == b.key_cols && a.desc == b.desc && a.nulls_first == b.nulls_first &&
@@ -129,9 +135,12 @@ bool same_sort(const ServeRequest& a, const ServeRequest& b) {
 // the shared sort covers (its share of the compaction stays small), and the unit is shared when its
 // requests' rows add up to at least one and a half times the covered rows.
 bool am_server_t::take_shared(std::vector<ReqPtr>& unit, int64_t* footprint) {
+  // Only a backlog is shared: a unit's requests all finish when its last take does, so under light
+  // load each request runs on its own and keeps its latency.
+  if (queue.size() < 2 * workers.size()) return false;
   const ServeRequest& r0 = *unit[0];
   std::vector<std::deque<ReqPtr>::iterator> cand;
-  for (auto it = queue.begin(); it != queue.end() && cand.size() + 1 < size_t(MAX_SHARED); ++it)
+  for (auto it = queue.begin(); it != queue.end() && cand.size() + 1 < size_t(kMaxSharedUnit); ++it)
     if (same_sort(**it, r0)) cand.push_back(it);
   if (cand.empty()) return false;
   int64_t lo = r0.offset, hi = r0.offset + r0.length;
