@@ -119,7 +119,7 @@ struct am_server_t {
 
 namespace {
 
-constexpr int kMaxSharedUnit = 16;      // requests answered from one shared sort (at most MAX_SHARED)
+constexpr int kMaxSharedUnit = 32;      // requests answered from one shared sort (at most MAX_SHARED)
 static_assert(kMaxSharedUnit <= MAX_SHARED, "one compaction launch serves the unit");
 
 // Requests that one sort can answer: the same table, keys and options.
