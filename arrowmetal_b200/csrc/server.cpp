@@ -135,9 +135,9 @@ bool same_sort(const ServeRequest& a, const ServeRequest& b) {
 // the shared sort covers (its share of the compaction stays small), and the unit is shared when its
 // requests' rows add up to at least one and a half times the covered rows.
 bool am_server_t::take_shared(std::vector<ReqPtr>& unit, int64_t* footprint) {
-  // Only a backlog is shared: a unit's requests all finish when its last take does, so under light
-  // load each request runs on its own and keeps its latency.
-  if (queue.size() < 2 * workers.size()) return false;
+  // Only a backlog is shared (four requests queued per worker): a unit's requests all finish when its
+  // last take does, so under lighter load each request runs on its own and keeps its latency.
+  if (queue.size() < 4 * workers.size()) return false;
   const ServeRequest& r0 = *unit[0];
   std::vector<std::deque<ReqPtr>::iterator> cand;
   for (auto it = queue.begin(); it != queue.end() && cand.size() + 1 < size_t(kMaxSharedUnit); ++it)
