@@ -97,7 +97,9 @@ template <> struct Status<uint64_t> {
 
 // The block's share of one column: rows [first, end) in chunks of THREADS x ITEMS rows, `stride` rows
 // apart, added into `st`.
-template <typename KeyT, int THREADS, int ITEMS>
+// RANGE: also the largest and smallest value key (only a lower key of a multi-key sort folds its null and
+// NaN rows into its key range; for any other key the two 64-bit maxima per row are left out).
+template <typename KeyT, int THREADS, int ITEMS, bool RANGE = true>
 __device__ __forceinline__ void histogram_rows(const ColView& col, KeyStats* __restrict__ st, uint64_t first,
                                                uint64_t end, uint64_t stride) {
   constexpr int D = int(sizeof(KeyT));
@@ -136,8 +138,10 @@ __device__ __forceinline__ void histogram_rows(const ColView& col, KeyStats* __r
         o |= kk;
         a &= kk;
         nv++;
-        vmax = kk > vmax ? kk : vmax;
-        vmin_inv = KeyT(~kk) > vmin_inv ? KeyT(~kk) : vmin_inv;
+        if constexpr (RANGE) {
+          vmax = kk > vmax ? kk : vmax;
+          vmin_inv = KeyT(~kk) > vmin_inv ? KeyT(~kk) : vmin_inv;
+        }
       } else if (cat[i] == 1) {
         n_nan++;
       } else {
@@ -186,10 +190,10 @@ __device__ __forceinline__ void histogram_rows(const ColView& col, KeyStats* __r
   }
 }
 
-template <typename KeyT, int THREADS, int ITEMS>
+template <typename KeyT, int THREADS, int ITEMS, bool RANGE = true>
 __global__ void __launch_bounds__(THREADS) key_histogram_kernel(const __grid_constant__ ColView col, KeyStats* __restrict__ st, uint64_t n) {
   constexpr uint64_t CHUNK = uint64_t(THREADS) * ITEMS;
-  histogram_rows<KeyT, THREADS, ITEMS>(col, st, uint64_t(blockIdx.x) * CHUNK, n, uint64_t(gridDim.x) * CHUNK);
+  histogram_rows<KeyT, THREADS, ITEMS, RANGE>(col, st, uint64_t(blockIdx.x) * CHUNK, n, uint64_t(gridDim.x) * CHUNK);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -424,7 +428,7 @@ __global__ void __launch_bounds__(THREADS) segmented_histogram_kernel(const SegD
   const uint64_t n = segs[seg].n;
   const uint64_t lo = uint64_t(blockIdx.x - item_start[seg]) * rows_per_item;
   const uint64_t hi = lo + rows_per_item < n ? lo + rows_per_item : n;
-  histogram_rows<KeyT, THREADS, ITEMS>(col, st + seg, lo, hi, uint64_t(THREADS) * ITEMS);
+  histogram_rows<KeyT, THREADS, ITEMS, false>(col, st + seg, lo, hi, uint64_t(THREADS) * ITEMS);
 }
 
 // Block s plans array s: one key of `key_bytes` bytes, uint32 indices.
@@ -1765,13 +1769,15 @@ static int pass_blocks_per_sm() {
   return cached;
 }
 
+// `range`: the key range too (a lower key of a multi-key sort).
 template <typename KeyT>
-static void launch_histogram(const ColView& cv, KeyStats* st, uint64_t n, cudaStream_t s) {
+static void launch_histogram(const ColView& cv, KeyStats* st, uint64_t n, cudaStream_t s, bool range = false) {
   constexpr int CHUNK = HIST_THREADS * HIST_ITEMS;
   const uint64_t chunks = (n + CHUNK - 1) / CHUNK;
   const int grid = int(std::min<uint64_t>(chunks, uint64_t(device().sm_count) * 8));
   KernelTimer kt("radix_histogram", s);
-  key_histogram_kernel<KeyT, HIST_THREADS, HIST_ITEMS><<<grid, HIST_THREADS, 0, s>>>(cv, st, n);
+  if (range) key_histogram_kernel<KeyT, HIST_THREADS, HIST_ITEMS, true><<<grid, HIST_THREADS, 0, s>>>(cv, st, n);
+  else key_histogram_kernel<KeyT, HIST_THREADS, HIST_ITEMS, false><<<grid, HIST_THREADS, 0, s>>>(cv, st, n);
   AM_CUDA(cudaGetLastError());
 }
 
@@ -2046,8 +2052,8 @@ void radix_sort(const std::vector<SortKey>& keys, int64_t n64, void* out, int in
   std::vector<ColView> views(K);
   for (int k = 0; k < K; k++) {
     views[k] = make_view(keys[k]);
-    if (pt_key_bytes(keys[k].col->pt) == 8) launch_histogram<uint64_t>(views[k], st + k, n, s);
-    else launch_histogram<uint32_t>(views[k], st + k, n, s);
+    if (pt_key_bytes(keys[k].col->pt) == 8) launch_histogram<uint64_t>(views[k], st + k, n, s, k > 0);
+    else launch_histogram<uint32_t>(views[k], st + k, n, s, k > 0);
   }
   {
     KernelTimer kt("radix_plan", s);
@@ -2763,7 +2769,7 @@ void noalloc_launch_histogram(const ColView& cv, KeyStats* st, uint64_t n, int c
   constexpr int CHUNK = HIST_THREADS * HIST_ITEMS;
   const uint64_t chunks = (n + CHUNK - 1) / CHUNK;
   const int grid = int(std::min<uint64_t>(chunks, uint64_t(cap)));
-  key_histogram_kernel<KeyT, HIST_THREADS, HIST_ITEMS><<<std::max(grid, 1), HIST_THREADS, 0, s>>>(cv, st, n);
+  key_histogram_kernel<KeyT, HIST_THREADS, HIST_ITEMS, false><<<std::max(grid, 1), HIST_THREADS, 0, s>>>(cv, st, n);
   AM_CUDA(cudaGetLastError());
 }
 

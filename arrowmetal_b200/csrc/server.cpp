@@ -115,7 +115,20 @@ struct am_server_t {
   bool take_shared(std::vector<ReqPtr>& unit, int64_t* footprint);
   void execute(std::vector<ReqPtr>& unit, bool shared);
   void execute_shared(std::vector<ReqPtr>& unit);
+  void finish_now(ServeRequest& r);
 };
+
+// A request whose result is complete on the device, handed to its waiter before the rest of its unit.
+void am_server_t::finish_now(ServeRequest& r) {
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    r.finished = Clock::now();
+    r.done = true;
+    stats.requests++;
+    if (r.rc == 0) stats.rows += r.length;
+  }
+  done_cv.notify_all();
+}
 
 namespace {
 
@@ -135,9 +148,9 @@ bool same_sort(const ServeRequest& a, const ServeRequest& b) {
 // the shared sort covers (its share of the compaction stays small), and the unit is shared when its
 // requests' rows add up to at least one and a half times the covered rows.
 bool am_server_t::take_shared(std::vector<ReqPtr>& unit, int64_t* footprint) {
-  // Only a backlog is shared (four requests queued per worker): a unit's requests all finish when its
-  // last take does, so under lighter load each request runs on its own and keeps its latency.
-  if (queue.size() < 4 * workers.size()) return false;
+  // Only a backlog is shared (two requests queued per worker); under lighter load each request runs on
+  // its own. A unit hands each request out when its own take is done, smallest first.
+  if (queue.size() < 2 * workers.size()) return false;
   const ServeRequest& r0 = *unit[0];
   std::vector<std::deque<ReqPtr>::iterator> cand;
   for (auto it = queue.begin(); it != queue.end() && cand.size() + 1 < size_t(kMaxSharedUnit); ++it)
@@ -186,6 +199,7 @@ void am_server_t::execute_shared(std::vector<ReqPtr>& unit) {
   const int64_t n = hi - lo;
   std::vector<am_array*> temps, kcols, idx;
   std::map<int, am_array*> pcols;
+  std::vector<cudaEvent_t> events;
   am_array* perm = nullptr;
   auto cleanup = [&] {
     for (am_array* a : temps) am_release(a);
@@ -223,7 +237,12 @@ void am_server_t::execute_shared(std::vector<ReqPtr>& unit) {
     }
     use_on(perm, s);
     compact_ranges(static_cast<const uint32_t*>(perm->data()), uint64_t(n), qlo, qhi, outs, s);
-    for (size_t i = 0; i < unit.size(); i++) {
+    // Takes smallest first, each followed by an event: a request is handed out as soon as its own
+    // take is done, not when the unit's last one is.
+    std::vector<size_t> order(unit.size());
+    for (size_t i = 0; i < order.size(); i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return unit[x]->length < unit[y]->length; });
+    for (size_t i : order) {
       ServeRequest& r = *unit[i];
       std::vector<am_array*> cols(kcols);
       for (int c : r.pay_cols) {
@@ -241,16 +260,28 @@ void am_server_t::execute_shared(std::vector<ReqPtr>& unit) {
       for (int c : r.key_cols) res->names.push_back(r.table->names[size_t(c)]);
       for (int c : r.pay_cols) res->names.push_back(r.table->names[size_t(c)]);
       r.result = res;
+      r.enqueued = Clock::now();
+      cudaEvent_t e;
+      AM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      events.push_back(e);
+      const cudaError_t rec = cudaEventRecord(e, s);
+      if (rec != cudaSuccess) throw Error(std::string("cudaEventRecord: ") + cudaGetErrorString(rec));
     }
-    for (auto& r : unit) r->enqueued = Clock::now();
+    for (size_t k = 0; k < order.size(); k++) {
+      const cudaError_t w = cudaEventSynchronize(events[k]);
+      if (w != cudaSuccess) throw Error(std::string("shared sort: ") + cudaGetErrorString(w));
+      finish_now(*unit[order[k]]);
+    }
     rc = am_cuda_synchronize();
     if (rc != 0) err = am_last_error();
   } catch (const Error& e) {
     rc = e.code ? e.code : 1;
     err = e.what();
   }
+  for (cudaEvent_t e : events) (void)cudaEventDestroy(e);
   if (rc != 0) {
     for (auto& r : unit) {
+      if (r->done) continue;
       if (r->result) {
         am_plan_result_release(r->result);
         r->result = nullptr;
@@ -420,6 +451,7 @@ void am_server_t::run_worker(int index) {
       std::lock_guard<std::mutex> lk(mu);
       in_flight -= fp;
       for (auto& r : unit) {
+        if (r->done) continue;           // finished on its own inside a shared unit
         r->finished = t;
         r->done = true;
         stats.requests++;
