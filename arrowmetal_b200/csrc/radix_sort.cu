@@ -1308,13 +1308,18 @@ __device__ __forceinline__ uint32_t boundary_masks(const uint64_t* __restrict__ 
   return mask;
 }
 
+// Each thread's 16 start bits also go to `masks`, so the write kernel does not read the keys again.
 __global__ void __launch_bounds__(BND_THREADS) bounds_count_kernel(const uint64_t* __restrict__ keys,
                                                                    const HybridState* __restrict__ hs,
-                                                                   uint32_t* __restrict__ counts) {
+                                                                   uint32_t* __restrict__ counts,
+                                                                   uint16_t* __restrict__ masks) {
+  static_assert(BND_ITEMS <= 16, "a thread's start bits fit 16 bits");
   __shared__ uint32_t s_warp[BND_THREADS / 32];
   if (!hs->mode) return;
   const uint64_t first = uint64_t(blockIdx.x) * BND_CHUNK;
-  uint32_t c = __popc(boundary_masks(keys, first, hs->m, hs->hi_shift, hs->lo_shift));
+  const uint32_t mask = boundary_masks(keys, first, hs->m, hs->hi_shift, hs->lo_shift);
+  masks[uint64_t(blockIdx.x) * BND_THREADS + threadIdx.x] = uint16_t(mask);
+  uint32_t c = __popc(mask);
   c = __reduce_add_sync(0xffffffffu, c);
   if ((threadIdx.x & 31) == 0) s_warp[threadIdx.x >> 5] = c;
   __syncthreads();
@@ -1376,7 +1381,7 @@ __global__ void __launch_bounds__(1024) bounds_scan_kernel(uint32_t* __restrict_
 
 // The starts' positions, in row order: round k of the block before round k + 1, warp w before w + 1
 // within a round (rows first + k * BND_THREADS + 32 w + lane).
-__global__ void __launch_bounds__(BND_THREADS) bounds_write_kernel(const uint64_t* __restrict__ keys,
+__global__ void __launch_bounds__(BND_THREADS) bounds_write_kernel(const uint16_t* __restrict__ masks,
                                                                    const HybridState* __restrict__ hs,
                                                                    const uint32_t* __restrict__ offs,
                                                                    uint32_t* __restrict__ pos,
@@ -1385,7 +1390,7 @@ __global__ void __launch_bounds__(BND_THREADS) bounds_write_kernel(const uint64_
   __shared__ uint32_t s_cnt[BND_ITEMS][WARPS];
   if (!hs->mode) return;
   const uint64_t first = uint64_t(blockIdx.x) * BND_CHUNK;
-  const uint32_t mask = boundary_masks(keys, first, hs->m, hs->hi_shift, hs->lo_shift);
+  const uint32_t mask = masks[uint64_t(blockIdx.x) * BND_THREADS + threadIdx.x];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t lt = (1u << lane) - 1u;
   uint32_t ball[BND_ITEMS];
@@ -2008,7 +2013,8 @@ void radix_sort(const std::vector<SortKey>& keys, int64_t n64, void* out, int in
   const size_t off_hs = (off_steps + (hybrid ? sizeof(PassDesc) * HYB_STEPS : 0) + 15) & ~size_t(15);
   const size_t off_bcount = (off_hs + (hybrid ? sizeof(HybridState) : 0) + 15) & ~size_t(15);
   const size_t off_bpos = off_bcount + (hybrid ? sizeof(uint32_t) * (bnd_blocks + 1) : 0);
-  const size_t off_tick = off_bpos + (hybrid ? sizeof(uint32_t) * 65537 : 0);
+  const size_t off_bmask = (off_bpos + (hybrid ? sizeof(uint32_t) * 65537 : 0) + 15) & ~size_t(15);
+  const size_t off_tick = off_bmask + (hybrid ? sizeof(uint16_t) * size_t(bnd_blocks) * BND_THREADS : 0);
   const size_t off_sum = (off_tick + sizeof(uint32_t) * NT + 15) & ~size_t(15);
   const size_t header = (off_sum + sizeof(SortSummary) + 255) & ~size_t(255);
   const size_t kbuf = ((n * max_kb) + 255) & ~size_t(255);
@@ -2024,6 +2030,7 @@ void radix_sort(const std::vector<SortKey>& keys, int64_t n64, void* out, int in
   HybridState* hs = reinterpret_cast<HybridState*>(base + off_hs);
   uint32_t* bcount = reinterpret_cast<uint32_t*>(base + off_bcount);
   uint32_t* bpos = reinterpret_cast<uint32_t*>(base + off_bpos);
+  uint16_t* bmask = reinterpret_cast<uint16_t*>(base + off_bmask);
   void* kbufA = base + header;
   void* kbufB = base + header + kbuf;
   uint32_t* ibufA = carry_ids ? reinterpret_cast<uint32_t*>(base + header + 2 * kbuf) : nullptr;
@@ -2124,11 +2131,11 @@ void radix_sort(const std::vector<SortKey>& keys, int64_t n64, void* out, int in
     {
       KernelTimer kt("radix_buckets", s);
       const uint64_t* kb1 = static_cast<const uint64_t*>(kbufB);
-      bounds_count_kernel<<<bnd_blocks, BND_THREADS, 0, s>>>(kb1, hs, bcount);
+      bounds_count_kernel<<<bnd_blocks, BND_THREADS, 0, s>>>(kb1, hs, bcount, bmask);
       AM_CUDA(cudaGetLastError());
       bounds_scan_kernel<<<1, 1024, 0, s>>>(bcount, bnd_blocks, hs, bpos);
       AM_CUDA(cudaGetLastError());
-      bounds_write_kernel<<<bnd_blocks, BND_THREADS, 0, s>>>(kb1, hs, bcount, bpos, sc.err);
+      bounds_write_kernel<<<bnd_blocks, BND_THREADS, 0, s>>>(bmask, hs, bcount, bpos, sc.err);
       AM_CUDA(cudaGetLastError());
       bounds_decide_kernel<<<1, 1024, 0, s>>>(hs, bpos, steps, sum);
       AM_CUDA(cudaGetLastError());
