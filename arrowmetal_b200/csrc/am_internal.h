@@ -256,6 +256,10 @@ void key_statistics(const SortKey& k, rs::KeyStats* st, cudaStream_t s);
 // sort is the better way (k close to the number of value rows).
 am_array* radix_top_k(const SortKey& key, int64_t k, cudaStream_t s);
 
+// A dense-rank column (uint8) of an integer key with at most 256 distinct value keys and at least 4M
+// rows, ranked in the key's own order (its direction included; nulls kept), or NULL. Sorting it
+// ascending orders the rows as the key does.
+am_array* low_cardinality_ranks(const SortKey& k, cudaStream_t s);
 // True when the key column can be rebuilt from its sorted keys (the key map is a bijection).
 bool key_invertible(const SortKey& k);
 // The sort engine. `out` (may be NULL) receives the index array; `key_dst` (may be NULL; one
