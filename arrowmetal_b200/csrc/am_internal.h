@@ -85,6 +85,9 @@ struct DevBuffer {
   cudaStream_t stream = nullptr;          // the stream its last writer / reader used
   std::function<void()> on_release;       // borrowed memory: runs the producer's release
   bool owned = false;
+  // Set once a low-cardinality probe of rows in this buffer found more than 256 distinct keys: later
+  // sorts of it, or of slices of it, skip the probe (and its readback).
+  std::atomic<bool> many_values{false};
   DevBuffer() = default;
   DevBuffer(const DevBuffer&) = delete;
   DevBuffer& operator=(const DevBuffer&) = delete;

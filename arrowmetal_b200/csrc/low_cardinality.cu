@@ -10,7 +10,8 @@
 // Three steps on the device and one small readback: a probe counts the distinct value keys (each
 // block keeps the keys it has seen in a shared-memory table and adds only new ones to a global table;
 // it gives up as soon as more than LOWCARD_MAX are found); one block ranks the distinct keys; one
-// pass writes every row's rank.
+// pass writes every row's rank. A column found to hold more keys is marked on its values buffer, so
+// its later sorts (a served table's requests, slices of it) skip the probe and its readback.
 #include <algorithm>
 
 #include "am_internal.h"
@@ -195,7 +196,8 @@ am_array* low_cardinality_ranks(const SortKey& k, cudaStream_t s) {
   using namespace rs;
   const am_array* a = k.col;
   const int64_t n = a->length;
-  if (n < LOWCARD_MIN_ROWS || a->dictionary || !integer_key(a->pt) || n >= (int64_t(1) << 32)) return nullptr;
+  if (n < LOWCARD_MIN_ROWS || a->dictionary || !integer_key(a->pt) || n >= (int64_t(1) << 32) || !a->values) return nullptr;
+  if (a->values->many_values.load(std::memory_order_relaxed)) return nullptr;
   const ColView cv = make_view(k);
   Table* t = static_cast<Table*>(dmalloc(sizeof(Table), s));
   AM_CUDA(cudaMemsetAsync(t, 0xFF, sizeof(t->keys), s));
@@ -211,6 +213,7 @@ am_array* low_cardinality_ranks(const SortKey& k, cudaStream_t s) {
   AM_CUDA(cudaMemcpyAsync(host, &t->count, sizeof(host), cudaMemcpyDeviceToHost, s));
   AM_CUDA(cudaStreamSynchronize(s));
   if (host[1] != 0 || host[0] == 0 || host[0] > LOWCARD_MAX) {
+    if (host[1] != 0 || host[0] > LOWCARD_MAX) a->values->many_values.store(true, std::memory_order_relaxed);
     dfree(t, s);
     return nullptr;
   }
