@@ -2540,7 +2540,7 @@ void sort_segment_cta(const std::vector<SortKey>& keys, const std::vector<void*>
 // SMALL_ARRAY_ROWS, and larger. Each class has its candidate shapes: the digit passes with a tile of
 // `threads` x `items` rows, or (the smallest class) one CTA per array with `threads` threads, `items`
 // rows a thread and `digit_bits`-bit digits. The first batch whose class holds at least its class's
-// tuning rows runs the class with every candidate, timed by CUDA events (each run leaves the same,
+// tuning rows (2^18, 2^20 and 2^21 rows) runs the class with every candidate, timed by CUDA events (each run leaves the same,
 // final output), and the fastest serves the class from then on. ARROWMETAL_SEG_ITEMS=4 or 8 fixes the
 // passes' tile at 512 x 4 or 512 x 8 rows for every class instead.
 constexpr uint32_t CTA_SORT_ROWS = 4096;
@@ -2561,7 +2561,7 @@ const std::vector<int>& class_candidates(int cls) {
   static_assert(kNumSegShapes == 7, "every shape is a candidate of some class");
   return cls == 0 ? c0 : c12;
 }
-uint64_t class_tune_rows(int cls) { return cls == 0 ? (uint64_t(1) << 18) : (uint64_t(2) << 20); }
+uint64_t class_tune_rows(int cls) { return cls == 0 ? (uint64_t(1) << 18) : cls == 1 ? (uint64_t(1) << 20) : (uint64_t(2) << 20); }
 
 std::mutex g_tune_mu;
 int g_tuned_shape[2][SEG_CLASSES] = {{-1, -1, -1}, {-1, -1, -1}};   // [key width 4 / 8][class]
