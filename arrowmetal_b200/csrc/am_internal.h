@@ -277,6 +277,24 @@ bool payload_record_layout(const std::vector<am_array*>& cols, rs::RecLayout* L)
 // The sort server's shared sorts: for each range q, the entries of `perm` (n row numbers) that lie in
 // [lo[q], hi[q]), in order, into outs[q] (device memory holding hi[q] - lo[q] entries).
 constexpr int MAX_SHARED = 32;
+// The same for columns: `src` holds the covered rows' columns in the shared order (fixed width), and
+// dsts[q] receives request q's rows of each, in order (values; validity bits OR-ed into zeroed words,
+// null counts added), so a request needs no gather of its own.
+constexpr int MAX_CCOLS = 8;
+struct CompactSrc {
+  const void* src[MAX_CCOLS];
+  const uint8_t* src_valid[MAX_CCOLS];   // NULL: no nulls
+  int64_t src_voff[MAX_CCOLS];
+  int32_t width[MAX_CCOLS];              // 1, 2, 4 or 8 bytes
+  int32_t ncols;
+};
+struct CompactDst {
+  void* dst[MAX_CCOLS];
+  uint32_t* dst_valid[MAX_CCOLS];        // zeroed bitmap words (when the source has nulls)
+  unsigned long long* nulls[MAX_CCOLS];  // zeroed null counters (when the source has nulls)
+};
+void compact_columns(const uint32_t* perm, uint64_t n, const std::vector<uint32_t>& lo, const std::vector<uint32_t>& hi,
+                     const CompactSrc& src, const std::vector<CompactDst>& dsts, cudaStream_t s);
 void compact_ranges(const uint32_t* perm, uint64_t n, const std::vector<uint32_t>& lo, const std::vector<uint32_t>& hi,
                     const std::vector<uint32_t*>& outs, cudaStream_t s);
 // Segmented argsort: outs[i] (a uint32 array of keys[i].col->length rows) receives the argsort of

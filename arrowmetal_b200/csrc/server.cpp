@@ -222,28 +222,54 @@ void am_server_t::execute_shared(std::vector<ReqPtr>& unit) {
                 : am_lexsort_ex2(kcols.data(), desc.data(), np.data(), fo.data(), K, &perm);
     if (rc != 0) throw Error(am_last_error(), rc);
     cudaStream_t s = stream();
-    std::vector<uint32_t> qlo, qhi;
-    std::vector<uint32_t*> outs;
-    for (auto& r : unit) {
-      am_array* o = new_array(PT_U32, "I", r->length);
-      idx.push_back(o);
-      o->values = DevBuffer::alloc(size_t(std::max<int64_t>(r->length, 1)) * 4 + 16, s);
-      o->null_count = 0;
-      o->perm_of = n;                      // entries index the covered rows
-      o->last_stream = s;
-      qlo.push_back(uint32_t(r->offset - lo));
-      qhi.push_back(uint32_t(r->offset - lo + r->length));
-      outs.push_back(static_cast<uint32_t*>(o->values->ptr));
-    }
     use_on(perm, s);
-    compact_ranges(static_cast<const uint32_t*>(perm->data()), uint64_t(n), qlo, qhi, outs, s);
-    // Takes smallest first, each followed by an event: a request is handed out as soon as its own
-    // take is done, not when the unit's last one is.
-    std::vector<size_t> order(unit.size());
-    for (size_t i = 0; i < order.size(); i++) order[i] = i;
-    std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return unit[x]->length < unit[y]->length; });
-    for (size_t i : order) {
-      ServeRequest& r = *unit[i];
+    // Requests covering at least an eighth of the covered rows get their columns by compaction of the
+    // covered rows' columns in the shared order (one gather for all of them, then one streaming pass);
+    // the others by compaction of the order and a take of their own.
+    std::vector<int> needed(r0.key_cols);
+    for (auto& r : unit)
+      for (int c : r->pay_cols)
+        if (std::find(needed.begin(), needed.end(), c) == needed.end()) needed.push_back(c);
+    bool flat = int(needed.size()) <= MAX_CCOLS;
+    for (int c : needed) {
+      const am_array* col = r0.table->cols[size_t(c)];
+      if (col->dictionary || pt_var(col->pt) || pt_bytes(col->pt) <= 0) flat = false;
+    }
+    std::vector<size_t> big, small;
+    for (size_t i = 0; i < unit.size(); i++) (flat && unit[i]->length * 8 >= n ? big : small).push_back(i);
+    if (big.size() < 2) {
+      small.insert(small.end(), big.begin(), big.end());
+      big.clear();
+    }
+    std::stable_sort(small.begin(), small.end(), [&](size_t x, size_t y) { return unit[x]->length < unit[y]->length; });
+    auto record = [&] {
+      cudaEvent_t e;
+      AM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      events.push_back(e);
+      const cudaError_t rec = cudaEventRecord(e, s);
+      if (rec != cudaSuccess) throw Error(std::string("cudaEventRecord: ") + cudaGetErrorString(rec));
+    };
+    std::vector<std::vector<size_t>> done_at;   // the requests each event completes, in event order
+    // 1. The smaller requests: their orders, then their takes, smallest first.
+    {
+      std::vector<uint32_t> qlo, qhi;
+      std::vector<uint32_t*> outs;
+      for (size_t i : small) {
+        ServeRequest& r = *unit[i];
+        am_array* o = new_array(PT_U32, "I", r.length);
+        idx.push_back(o);
+        o->values = DevBuffer::alloc(size_t(std::max<int64_t>(r.length, 1)) * 4 + 16, s);
+        o->null_count = 0;
+        o->perm_of = n;                      // entries index the covered rows
+        o->last_stream = s;
+        qlo.push_back(uint32_t(r.offset - lo));
+        qhi.push_back(uint32_t(r.offset - lo + r.length));
+        outs.push_back(static_cast<uint32_t*>(o->values->ptr));
+      }
+      compact_ranges(static_cast<const uint32_t*>(perm->data()), uint64_t(n), qlo, qhi, outs, s);
+    }
+    for (size_t k = 0; k < small.size(); k++) {
+      ServeRequest& r = *unit[small[k]];
       std::vector<am_array*> cols(kcols);
       for (int c : r.pay_cols) {
         if (!pcols.count(c)) pcols[c] = slice(c);
@@ -252,7 +278,7 @@ void am_server_t::execute_shared(std::vector<ReqPtr>& unit) {
       auto* res = new am_plan_result_t();
       res->rows = r.length;
       res->cols.assign(cols.size(), nullptr);
-      if (am_take_columns(cols.data(), int64_t(cols.size()), idx[i], res->cols.data()) != 0) {
+      if (am_take_columns(cols.data(), int64_t(cols.size()), idx[k], res->cols.data()) != 0) {
         res->cols.clear();
         delete res;
         throw Error(am_last_error());
@@ -261,16 +287,85 @@ void am_server_t::execute_shared(std::vector<ReqPtr>& unit) {
       for (int c : r.pay_cols) res->names.push_back(r.table->names[size_t(c)]);
       r.result = res;
       r.enqueued = Clock::now();
-      cudaEvent_t e;
-      AM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-      events.push_back(e);
-      const cudaError_t rec = cudaEventRecord(e, s);
-      if (rec != cudaSuccess) throw Error(std::string("cudaEventRecord: ") + cudaGetErrorString(rec));
+      record();
+      done_at.push_back({small[k]});
     }
-    for (size_t k = 0; k < order.size(); k++) {
+    // 2. The larger requests: the covered rows' columns in the shared order, then one compaction.
+    if (!big.empty()) {
+      std::vector<am_array*> src_cols;
+      for (int c : needed) {
+        if (std::find(r0.key_cols.begin(), r0.key_cols.end(), c) != r0.key_cols.end())
+          src_cols.push_back(kcols[size_t(std::find(r0.key_cols.begin(), r0.key_cols.end(), c) - r0.key_cols.begin())]);
+        else {
+          if (!pcols.count(c)) pcols[c] = slice(c);
+          src_cols.push_back(pcols[c]);
+        }
+      }
+      std::vector<am_array*> sorted(src_cols.size(), nullptr);
+      if (am_take_columns(src_cols.data(), int64_t(src_cols.size()), perm, sorted.data()) != 0)
+        throw Error(am_last_error());
+      for (am_array* a : sorted) temps.push_back(a);
+      CompactSrc cs{};
+      cs.ncols = int32_t(sorted.size());
+      for (size_t c = 0; c < sorted.size(); c++) {
+        am_array* a = sorted[c];
+        use_on(a, s);
+        cs.src[c] = a->data();
+        cs.src_valid[c] = a->null_count != 0 ? a->valid_bits() : nullptr;
+        cs.src_voff[c] = a->validity_offset;
+        cs.width[c] = pt_bytes(a->pt);
+      }
+      std::vector<uint32_t> qlo, qhi;
+      std::vector<CompactDst> dsts;
+      for (size_t i : big) {
+        ServeRequest& r = *unit[i];
+        auto* res = new am_plan_result_t();
+        res->rows = r.length;
+        r.result = res;
+        CompactDst d{};
+        std::vector<am_array*> outs;
+        for (size_t c = 0; c < needed.size(); c++) {
+          const am_array* srcc = sorted[c];
+          am_array* o = new_array(srcc->pt, srcc->format, r.length);
+          temps.push_back(o);                   // released below; the request's result holds its own
+          o->values = DevBuffer::alloc(size_t(std::max<int64_t>(r.length, 1)) * size_t(pt_bytes(srcc->pt)) + 16, s);
+          o->last_stream = s;
+          o->null_count = 0;
+          if (cs.src_valid[c]) {
+            const size_t bytes = size_t((r.length + 127) / 128) * 16;
+            o->validity = DevBuffer::alloc(bytes + 16, s);
+            o->null_count_dev = DevBuffer::alloc(sizeof(unsigned long long), s);
+            AM_CUDA(cudaMemsetAsync(o->validity->ptr, 0, bytes + 16, s));
+            AM_CUDA(cudaMemsetAsync(o->null_count_dev->ptr, 0, sizeof(unsigned long long), s));
+            o->null_count = -1;
+            d.dst_valid[c] = static_cast<uint32_t*>(o->validity->ptr);
+            d.nulls[c] = static_cast<unsigned long long*>(o->null_count_dev->ptr);
+          }
+          d.dst[c] = o->values->ptr;
+          outs.push_back(o);
+        }
+        // The request's columns in its own order: its keys, then its payload.
+        std::vector<int> cols(r.key_cols);
+        cols.insert(cols.end(), r.pay_cols.begin(), r.pay_cols.end());
+        for (int c : cols) {
+          am_array* o = outs[size_t(std::find(needed.begin(), needed.end(), c) - needed.begin())];
+          retain(o);
+          res->cols.push_back(o);
+          res->names.push_back(r.table->names[size_t(c)]);
+        }
+        dsts.push_back(d);
+        qlo.push_back(uint32_t(r.offset - lo));
+        qhi.push_back(uint32_t(r.offset - lo + r.length));
+      }
+      compact_columns(static_cast<const uint32_t*>(perm->data()), uint64_t(n), qlo, qhi, cs, dsts, s);
+      for (size_t i : big) unit[i]->enqueued = Clock::now();
+      record();
+      done_at.push_back(big);
+    }
+    for (size_t k = 0; k < events.size(); k++) {
       const cudaError_t w = cudaEventSynchronize(events[k]);
       if (w != cudaSuccess) throw Error(std::string("shared sort: ") + cudaGetErrorString(w));
-      finish_now(*unit[order[k]]);
+      for (size_t i : done_at[k]) finish_now(*unit[i]);
     }
     rc = am_cuda_synchronize();
     if (rc != 0) err = am_last_error();

@@ -129,7 +129,116 @@ __global__ void __launch_bounds__(CMP_THREADS) range_write_kernel(const uint32_t
   }
 }
 
+// The columns of the covered rows in the shared order, copied for each request q into its own sorted
+// columns: the entries of block b's chunk whose row lies in q's range, in order, at the same places
+// the index compaction gives them. Validity bits of one warp item land in at most two output words
+// (the item's kept rows are consecutive), OR-ed together and added with one atomic each.
+__global__ void __launch_bounds__(CMP_THREADS) range_write_cols_kernel(const uint32_t* __restrict__ perm, uint64_t n,
+                                                                       const __grid_constant__ Ranges r,
+                                                                       const __grid_constant__ CompactSrc src,
+                                                                       const CompactDst* __restrict__ dst,
+                                                                       const uint32_t* __restrict__ offsets) {
+  constexpr int WARPS = CMP_THREADS / 32;
+  __shared__ uint32_t s_item[CMP_ITEMS][WARPS];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t lt = (1u << lane) - 1u;
+  const uint64_t base = uint64_t(blockIdx.x) * CMP_CHUNK;
+  uint32_t v[CMP_ITEMS];
+#pragma unroll
+  for (int i = 0; i < CMP_ITEMS; i++) {
+    const uint64_t j = base + uint64_t(i) * CMP_THREADS + threadIdx.x;
+    v[i] = j < n ? perm[j] : 0xFFFFFFFFu;
+  }
+  for (int q = 0; q < r.k; q++) {
+    uint32_t m[CMP_ITEMS];
+#pragma unroll
+    for (int i = 0; i < CMP_ITEMS; i++) {
+      m[i] = __ballot_sync(0xffffffffu, v[i] >= r.lo[q] && v[i] < r.hi[q]);
+      if (lane == 0) s_item[i][warp] = __popc(m[i]);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t run = 0;
+      for (int i = 0; i < CMP_ITEMS; i++)
+        for (int w = 0; w < WARPS; w++) {
+          const uint32_t c = s_item[i][w];
+          s_item[i][w] = run;
+          run += c;
+        }
+    }
+    __syncthreads();
+    const uint32_t off = offsets[size_t(q) * gridDim.x + blockIdx.x];
+    const CompactDst& d = dst[q];
+    for (int c = 0; c < src.ncols; c++) {
+      const int w = src.width[c];
+      const uint8_t* sv = src.src_valid[c];
+      uint32_t nulls = 0;
+#pragma unroll
+      for (int i = 0; i < CMP_ITEMS; i++) {
+        const bool keep = (m[i] >> lane) & 1u;
+        const uint64_t row = base + uint64_t(i) * CMP_THREADS + threadIdx.x;
+        const uint32_t first = off + s_item[i][warp];          // the item's first kept place
+        const uint32_t pos = first + __popc(m[i] & lt);
+        if (keep) {
+          switch (w) {
+            case 8: static_cast<uint64_t*>(d.dst[c])[pos] = static_cast<const uint64_t*>(src.src[c])[row]; break;
+            case 4: static_cast<uint32_t*>(d.dst[c])[pos] = static_cast<const uint32_t*>(src.src[c])[row]; break;
+            case 2: static_cast<uint16_t*>(d.dst[c])[pos] = static_cast<const uint16_t*>(src.src[c])[row]; break;
+            default: static_cast<uint8_t*>(d.dst[c])[pos] = static_cast<const uint8_t*>(src.src[c])[row]; break;
+          }
+        }
+        if (sv && m[i]) {                                       // warp-uniform
+          const int64_t b = src.src_voff[c] + int64_t(row);
+          const bool valid = keep && ((sv[b >> 3] >> (b & 7)) & 1u);
+          if (keep && !valid) nulls++;
+          const uint32_t w0 = first >> 5;
+          const uint32_t bit = valid ? (1u << (pos & 31)) : 0u;
+          const uint32_t lo_w = __reduce_or_sync(0xffffffffu, (pos >> 5) == w0 ? bit : 0u);
+          const uint32_t hi_w = __reduce_or_sync(0xffffffffu, (pos >> 5) != w0 ? bit : 0u);
+          if (lane == 0) {
+            if (lo_w) atomicOr(&d.dst_valid[c][w0], lo_w);
+            if (hi_w) atomicOr(&d.dst_valid[c][w0 + 1], hi_w);
+          }
+        }
+      }
+      if (sv) {
+        nulls = __reduce_add_sync(0xffffffffu, nulls);
+        if (lane == 0 && nulls) atomicAdd(d.nulls[c], (unsigned long long)nulls);
+      }
+    }
+    __syncthreads();
+  }
+}
+
 }  // namespace
+
+void compact_columns(const uint32_t* perm, uint64_t n, const std::vector<uint32_t>& lo, const std::vector<uint32_t>& hi,
+                     const CompactSrc& src, const std::vector<CompactDst>& dsts, cudaStream_t s) {
+  const int k = int(lo.size());
+  if (k == 0 || n == 0) return;
+  if (k > MAX_SHARED || hi.size() != lo.size() || dsts.size() != lo.size() || src.ncols < 1 || src.ncols > MAX_CCOLS)
+    throw invalid("compact_columns: 1 to " + std::to_string(MAX_SHARED) + " ranges of 1 to " +
+                  std::to_string(MAX_CCOLS) + " columns");
+  Ranges r{};
+  r.k = k;
+  for (int q = 0; q < k; q++) {
+    r.lo[q] = lo[size_t(q)];
+    r.hi[q] = hi[size_t(q)];
+  }
+  const uint32_t blocks = uint32_t((n + CMP_CHUNK - 1) / CMP_CHUNK);
+  uint32_t* counts = static_cast<uint32_t*>(dmalloc(sizeof(uint32_t) * size_t(blocks) * size_t(k), s));
+  CompactDst* d = static_cast<CompactDst*>(dmalloc(sizeof(CompactDst) * size_t(k), s));
+  copy_h2d(d, dsts.data(), sizeof(CompactDst) * size_t(k), s);
+  KernelTimer kt("server_shared_columns", s);
+  range_count_kernel<<<blocks, CMP_THREADS, 0, s>>>(perm, n, r, counts);
+  AM_CUDA(cudaGetLastError());
+  range_scan_kernel<<<k, 1024, 0, s>>>(counts, blocks);
+  AM_CUDA(cudaGetLastError());
+  range_write_cols_kernel<<<blocks, CMP_THREADS, 0, s>>>(perm, n, r, src, d, counts);
+  AM_CUDA(cudaGetLastError());
+  dfree(d, s);
+  dfree(counts, s);
+}
 
 void compact_ranges(const uint32_t* perm, uint64_t n, const std::vector<uint32_t>& lo, const std::vector<uint32_t>& hi,
                     const std::vector<uint32_t*>& outs, cudaStream_t s) {

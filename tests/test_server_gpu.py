@@ -194,6 +194,36 @@ def test_shared_sorts_equal_each_request_alone(am, oracle):
             assert same(results[i][name].to_arrow(), cols[name].slice(offset, length).take(order)), (reqs[i], name)
 
 
+def test_shared_sorts_mix_compacted_and_gathered_requests(am, oracle):
+    # Requests covering at least an eighth of the shared rows get their columns by compaction of the
+    # covered rows' columns in the shared order, shorter ones by a take of their own; a payload column
+    # may hold nulls. Every result must equal the request alone.
+    src, cols = table_and_columns(am, seed=21)
+    rng = np.random.default_rng(22)
+    reqs = []
+    for i in range(40):
+        length = int(rng.integers(N // 6, N // 2)) if i % 2 else int(rng.integers(1, N // 40))
+        offset = int(rng.integers(0, N - length + 1))
+        payload = ["p1", "p2"] if i % 3 else ["p2", "kf"]
+        reqs.append((offset, length, ["k64"], [bool(i % 4 == 1)], ["at_start" if i % 5 else "at_end"],
+                     ["ieee"], payload))
+    alone = [am.run_plan(plan_alone(*r), [src]) for r in reqs]
+    with am.Server(workers=1, hbm_cap_bytes=8 << 30, batch_rows=0) as srv:
+        tickets = [srv.submit(src, o, n, k, p, descending=d, null_placement=nl, float_order=fo)
+                   for (o, n, k, d, nl, fo, p) in reqs]
+        results = [srv.wait(t)[0] for t in tickets]
+        stats = srv.stats()
+    assert stats["shared_sorts"] > 0
+    for r, want, got in zip(reqs, alone, results):
+        assert list(got) == list(want), r
+        for name in want:
+            assert same(got[name].to_arrow(), want[name].to_arrow()), (r, name)
+    offset, length, keys, desc, nulls, orders, payload = reqs[1]
+    order = pa.array(expected_order(oracle, cols, offset, length, keys, desc, nulls, orders))
+    for name in results[1]:
+        assert same(results[1][name].to_arrow(), cols[name].slice(offset, length).take(order)), name
+
+
 def test_shared_sorts_can_be_turned_off(am, monkeypatch):
     src = table(am, seed=15)
     monkeypatch.setenv("ARROWMETAL_SERVER_SHARED", "0")
