@@ -773,7 +773,7 @@ def algorithmic_bytes(n, m, passes, local_sort=False, records=False):
 # 38,000,000 rows (34.2M value rows: the two-level sort runs as at 50M), divided by the rows. Keyed by
 # whether the payload rode through the sort in records (the table in HBM) or was gathered afterwards.
 TRAFFIC_PER_ROW = {
-    True: {"radix_histogram": 8.21, "radix_onesweep_pass": 84.82, "radix_local_sort": 38.53},
+    True: {"radix_histogram": 8.22, "radix_onesweep_pass": 84.99, "radix_local_sort": 38.50},
     False: {},
 }
 
