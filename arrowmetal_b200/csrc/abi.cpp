@@ -215,12 +215,14 @@ bool import_pinned_async(am_array* a, ArrowArray* arr) {
   cudaStream_t cs = copy_stream();
   const size_t bytes = size_t(n) * w;
   a->values = DevBuffer::alloc(bytes + 16, cs);
+  a->values->home = cs;
   AM_CUDA(cudaMemcpyAsync(a->values->ptr, static_cast<const char*>(vals) + size_t(off) * w, bytes,
                           cudaMemcpyHostToDevice, cs));
   a->null_count = nulls;
   if (nulls > 0) {
     const size_t vb = size_t((n + 7) / 8);
     a->validity = DevBuffer::alloc(vb + 16, cs);
+    a->validity->home = cs;
     AM_CUDA(cudaMemcpyAsync(a->validity->ptr, vbits + (off >> 3), vb, cudaMemcpyHostToDevice, cs));
   }
   a->last_stream = cs;

@@ -83,6 +83,9 @@ struct DevBuffer {
   void* ptr = nullptr;
   size_t bytes = 0;
   cudaStream_t stream = nullptr;          // the stream its last writer / reader used
+  // A library stream the memory goes back to the pool on (after the last user's work): imports are
+  // allocated on the copy stream, and their memory freed there is what the next imports reuse.
+  cudaStream_t home = nullptr;
   std::function<void()> on_release;       // borrowed memory: runs the producer's release
   bool owned = false;
   // Set once a low-cardinality probe of rows in this buffer found more than 256 distinct keys: later
@@ -132,8 +135,29 @@ struct StreamScratch {
   size_t status_words = 0;
   uint32_t epoch = 0;
   uint32_t* err = nullptr;
+  // The sorts' working buffers, kept for the stream's next sort (up to kArenaMax bytes): repeated sorts
+  // neither return them to the pool nor ask it again, so the pool's blocks are not split between the
+  // sort's scratch and the results allocated after it.
+  void* arena = nullptr;
+  size_t arena_bytes = 0;
+  std::atomic<bool> arena_busy{false};   // held by one sort at a time (threads may share a stream)
 };
+constexpr size_t kArenaMax = size_t(4) << 30;
 StreamScratch& stream_scratch(cudaStream_t s, size_t status_words);
+// A stream's sort scratch of `bytes`: its arena when free and large enough (grown when it is not),
+// else a block of its own; released (back to the arena, or freed) on the stream when it goes away.
+class ScratchBlock {
+ public:
+  ScratchBlock(cudaStream_t s, size_t bytes);
+  ~ScratchBlock();
+  ScratchBlock(const ScratchBlock&) = delete;
+  ScratchBlock& operator=(const ScratchBlock&) = delete;
+  char* data() const { return p_; }
+ private:
+  cudaStream_t s_;
+  char* p_ = nullptr;
+  StreamScratch* arena_ = nullptr;
+};
 // Reads and clears the stream's device error word (synchronises the stream); throws on an error.
 void check_device_errors(cudaStream_t s);
 void sync_stream(cudaStream_t s);

@@ -228,11 +228,24 @@ Frame sort_frame(Frame f, const std::vector<KeySpec>& keys) {
         for (size_t c = 0; c < f.cols.size(); c++)
           if (int(c) != which[0]) src.push_back(f.cols[c]);
         taken.assign(src.size(), nullptr);
-        if (!src.empty() && am_take_columns(src.data(), int64_t(src.size()), idx, taken.data()) != 0)
+        bool uploading = false;
+        for (am_array* c : src) uploading = uploading || !settled(c);
+        if (uploading && src.size() > 1) {
+          // Columns still uploading: each is gathered once its own upload is done, in column order (the
+          // order of their imports), and carries its own ready event, so its export starts while the
+          // later columns still upload or gather.
+          for (size_t i = 0; i < src.size(); i++) {
+            if (am_take_columns(&src[i], 1, idx, &taken[i]) != 0) throw Error(am_last_error());
+            if (taken[i]->pt != PT_STRUCT) taken[i]->ready = std::make_shared<ReadyEvent>(taken[i]->last_stream ? taken[i]->last_stream : s);
+          }
+        } else if (!src.empty() && am_take_columns(src.data(), int64_t(src.size()), idx, taken.data()) != 0) {
           throw Error(am_last_error());
+        }
       } catch (...) {
         am::release(sorted_key);
         am::release(idx);
+        for (am_array* t : taken)
+          if (t) am::release(t);
         throw;
       }
       am::release(idx);

@@ -2038,7 +2038,8 @@ void radix_sort(const std::vector<SortKey>& keys_in, int64_t n64, void* out, int
   const size_t header = (off_sum + sizeof(SortSummary) + 255) & ~size_t(255);
   const size_t kbuf = ((n * max_kb) + 255) & ~size_t(255);
   const size_t ibuf = carry_ids ? ((n * id_bytes) + 255) & ~size_t(255) : 0;
-  char* base = static_cast<char*>(dmalloc(header + 2 * kbuf + 2 * ibuf, s));
+  ScratchBlock scratch(s, header + 2 * kbuf + 2 * ibuf);
+  char* base = scratch.data();
   AM_CUDA(cudaMemsetAsync(base, 0, header, s));
   KeyStats* st = reinterpret_cast<KeyStats*>(base + off_stats);
   KeyPlan* kp = reinterpret_cast<KeyPlan*>(base + off_kplan);
@@ -2225,7 +2226,6 @@ void radix_sort(const std::vector<SortKey>& keys_in, int64_t n64, void* out, int
     AM_CUDA(cudaMemcpyAsync(last_summary_host(), sum, sizeof(SortSummary), cudaMemcpyDeviceToHost, s));
     tls().stats_stream = s;
   }
-  dfree(base, s);
 }
 
 

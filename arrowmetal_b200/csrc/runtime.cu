@@ -180,7 +180,17 @@ void dfree(void* p, cudaStream_t s) {
 }
 
 DevBuffer::~DevBuffer() {
-  if (owned && ptr) dfree(ptr, stream);
+  if (owned && ptr) {
+    cudaEvent_t e = nullptr;
+    if (home && stream && stream != home && cudaEventCreateWithFlags(&e, cudaEventDisableTiming) == cudaSuccess) {
+      // Back to its home stream's part of the pool, once the last user's work is done.
+      if (cudaEventRecord(e, stream) == cudaSuccess && cudaStreamWaitEvent(home, e, 0) == cudaSuccess) dfree(ptr, home);
+      else dfree(ptr, stream);
+      (void)cudaEventDestroy(e);
+    } else {
+      dfree(ptr, stream ? stream : home);
+    }
+  }
   if (on_release) on_release();
 }
 std::shared_ptr<DevBuffer> DevBuffer::alloc(size_t bytes, cudaStream_t s) {
@@ -451,6 +461,33 @@ StreamScratch& stream_scratch(cudaStream_t s, size_t status_words) {
     sc->epoch = 0;
   }
   return *sc;
+}
+
+ScratchBlock::ScratchBlock(cudaStream_t s, size_t bytes) : s_(s) {
+  StreamScratch& sc = stream_scratch(s, 0);
+  bool expected = false;
+  if (bytes <= kArenaMax && sc.arena_busy.compare_exchange_strong(expected, true)) {
+    if (sc.arena_bytes < bytes) {
+      if (sc.arena) dfree(sc.arena, s);
+      sc.arena = nullptr;
+      sc.arena_bytes = 0;
+      try {
+        sc.arena = dmalloc(bytes, s);
+      } catch (...) {
+        sc.arena_busy = false;
+        throw;
+      }
+      sc.arena_bytes = bytes;
+    }
+    arena_ = &sc;
+    p_ = static_cast<char*>(sc.arena);
+  } else {
+    p_ = static_cast<char*>(dmalloc(bytes, s));
+  }
+}
+ScratchBlock::~ScratchBlock() {
+  if (arena_) arena_->arena_busy = false;
+  else dfree(p_, s_);
 }
 
 void sync_stream(cudaStream_t s) { AM_CUDA(cudaStreamSynchronize(s)); }
