@@ -12,8 +12,10 @@ seeded synthetic data of the benchmark's shape (numpy default_rng).
            (no per-launch events), max over ranks; inputs (400 MB key column) are larger than L2, so no
            flush is needed. The per-kernel split comes from a second, profiled loop.
   e2e      the same through the C ABI with host buffers: am_import of the 3 columns from pinned host
-           memory (host to device), the plan, am_export of the 3 result columns (device to host), one
-           step at a time (--e2e-inflight N: N steps in flight on N threads, each with its own streams).
+           memory (host to device), the plan, am_export of the 3 result columns (device to host); steps
+           pipelined two deep in one thread (step i + 1 imported and planned before step i is exported:
+           uploads overlap the previous step's downloads), the time one step at a time beside it
+           (--e2e-inflight 1: one at a time only).
   roofline the dominant kernel's algorithmic bytes / its CUDA-event time, against the measured HBM
            copy peak.
   cpu_baseline  the CPU oracle (the reference algorithm restated in C) on the host's cores; beside it
@@ -915,9 +917,9 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--e2e-steps", type=int, default=5)
-    ap.add_argument("--e2e-inflight", type=int, default=1,
-                    help="end-to-end steps in flight at once (threads, each with its own streams)")
+    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--e2e-inflight", type=int, default=2,
+                    help="end-to-end steps in flight at once, pipelined in one thread (1: one at a time)")
     ap.add_argument("--rows", type=int, default=N_ROWS)
     ap.add_argument("--impl", default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -1118,35 +1120,33 @@ def main():
         del hc, s2, out, res
     e2e_ms = max_over_ranks(1e3 * statistics.median(e2e_times) if e2e_times else float("nan"), dist, "cuda")
 
-    # ---- the same steps with two in flight: two threads, each with its own pinned copy of the inputs
-    # (and the library's own streams per thread), run steps back to back, so one step's uploads overlap
-    # the other's downloads on the two copy directions. Every step still imports its inputs from host
-    # memory and exports its whole result to host memory.
+    # ---- the same steps pipelined in this thread: step i + 1's imports and plan are enqueued before step
+    # i's results are exported, so one step's uploads run while the previous step's results download (the
+    # two copy directions). Every step still imports its own inputs from pinned host memory and exports its
+    # whole result to host memory; the time is the whole run's, fill and drain included, over its steps.
     inflight_ms = None
     if args.e2e_steps > 0 and args.e2e_inflight > 1:
-        per_thread = [{k: pinned_array(v) for k, v in cols.items()} for _ in range(args.e2e_inflight)]
+        depth = args.e2e_inflight
+        sets = [host_cols] + [{k: pinned_array(v) for k, v in cols.items()} for _ in range(depth - 1)]
 
-        def e2e_worker(hcols, nsteps):
-            for _ in range(nsteps):
-                hc = {k: am.MetalArray.from_arrow(v) for k, v in hcols.items()}
-                s2 = am.PlanSource("t", hc)
-                out = am.run_plan(PLAN, [s2])
-                res = {k: v.to_arrow() for k, v in out.items()}
-                del hc, s2, out, res
-
-        def run_threads(nsteps):
-            ths = [threading.Thread(target=e2e_worker, args=(hcols, nsteps)) for hcols in per_thread]
+        def pipelined(nsteps):
+            queue = []
             t0 = time.perf_counter()
-            for t in ths:
-                t.start()
-            for t in ths:
-                t.join()
+            for i in range(nsteps + depth - 1):
+                if i < nsteps:
+                    hc = {k: am.MetalArray.from_arrow(v) for k, v in sets[i % depth].items()}
+                    queue.append((hc, am.run_plan(PLAN, [am.PlanSource("t", hc)])))
+                    del hc
+                if len(queue) >= depth or i >= nsteps:
+                    hc0, out0 = queue.pop(0)
+                    res = {k: v.to_arrow() for k, v in out0.items()}
+                    del hc0, out0, res
             return time.perf_counter() - t0
 
-        run_threads(1)                                  # each thread's streams and pinned staging
-        total = run_threads(args.e2e_steps)
-        inflight_ms = max_over_ranks(1e3 * total / (args.e2e_steps * args.e2e_inflight), dist, "cuda")
-        del per_thread
+        pipelined(depth + 2)                            # the pool's blocks for `depth` steps at once
+        pipe_steps = max(args.e2e_steps, 4 * depth)
+        inflight_ms = max_over_ranks(1e3 * pipelined(pipe_steps) / pipe_steps, dist, "cuda")
+        del sets
 
     line = {
         "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
