@@ -126,21 +126,48 @@ template <> __device__ __forceinline__ uint64_t key_from_raw<uint64_t>(const Col
   return c.desc ? ~k : k;
 }
 
-// Keys of ITEMS rows: all loads first (values and validity bytes), then the arithmetic.
+// Keys of ITEMS rows: all loads first (values and validity bytes), then the arithmetic, with the type
+// and direction decided once for all the rows (the integer maps are one XOR a row, with no branches).
+// The same keys and categories as key_from_raw row by row.
 template <typename KeyT, int ITEMS>
 __device__ __forceinline__ void encode_rows(const ColView& c, const uint32_t (&row)[ITEMS], uint32_t ok, KeyT (&key)[ITEMS],
                                             int (&cat)[ITEMS]) {
   KeyT raw[ITEMS];
   uint32_t vb[ITEMS];
   load_raw_rows<KeyT, ITEMS>(c, row, ok, raw);
+  uint32_t valid = ok;                 // bit i: row i exists and is not null
   if (c.valid) {
 #pragma unroll
     for (int i = 0; i < ITEMS; i++) vb[i] = ((ok >> i) & 1u) ? c.valid[(c.valid_off + int64_t(row[i])) >> 3] : 0u;
-  }
 #pragma unroll
-  for (int i = 0; i < ITEMS; i++) {
-    const bool valid = !c.valid || ((vb[i] >> ((c.valid_off + int64_t(row[i])) & 7)) & 1u);
-    key[i] = key_from_raw<KeyT>(c, raw[i], valid, cat[i]);
+    for (int i = 0; i < ITEMS; i++)
+      if (!((vb[i] >> ((c.valid_off + int64_t(row[i])) & 7)) & 1u)) valid &= ~(1u << i);
+  }
+  constexpr bool WIDE = sizeof(KeyT) == 8;
+  const bool fl = WIDE ? c.pt == PT_F64 : (c.pt == PT_F32 || c.pt == PT_F16);
+  if (!fl) {
+    const KeyT sign = KeyT(KeyT(1) << (8 * sizeof(KeyT) - 1));
+    const KeyT flip = WIDE ? (c.pt == PT_I64 ? sign : KeyT(0)) : (c.pt == PT_U32 ? KeyT(0) : sign);
+    const KeyT x = flip ^ (c.desc ? KeyT(~KeyT(0)) : KeyT(0));
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++) {
+      const bool v = (valid >> i) & 1u;
+      key[i] = v ? KeyT(raw[i] ^ x) : KeyT(0);
+      cat[i] = v ? 0 : 2;
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++) {
+      cat[i] = 0;
+      if (!((valid >> i) & 1u)) {
+        cat[i] = 2;
+        key[i] = KeyT(0);
+      } else if constexpr (WIDE) {
+        key[i] = key_f64_bits(raw[i], c, cat[i]);
+      } else {
+        key[i] = key_f32_bits(c.pt == PT_F16 ? f16_to_f32_bits(uint32_t(raw[i])) : uint32_t(raw[i]), c, cat[i]);
+      }
+    }
   }
 }
 
