@@ -886,11 +886,8 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
 #pragma unroll
         for (int i = 0; i < ITEMS; i++) vb[i] = ((ok >> i) & 1u) ? col.valid[(col.valid_off + int64_t(id[i])) >> 3] : 0u;
       }
-#pragma unroll
-      for (int i = 0; i < ITEMS; i++) {
-        const bool valid = !col.valid || ((vb[i] >> ((col.valid_off + int64_t(id[i])) & 7)) & 1u);
-        int cat;
-        KeyT k = key_from_raw<KeyT>(col, raw[i], valid, cat);
+      // A row's key, digit and routing from its key and category.
+      auto place = [&](int i, KeyT k, int cat) {
         if (cat && (flags & PF_ROUTE)) {
           dg[i] = (cat == 1) ? uint32_t(NAN_BIN) : uint32_t(NULL_BIN);
         } else {
@@ -899,6 +896,27 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
         }
         if (!((ok >> i) & 1u)) dg[i] = INVALID_DIGIT;
         key[i] = k;
+      };
+      constexpr bool WIDE = sizeof(KeyT) == 8;
+      const bool fl = WIDE ? col.pt == PT_F64 : (col.pt == PT_F32 || col.pt == PT_F16);
+      if (!fl) {
+        // Integer keys: one XOR a row (sign flip and direction decided once), no branch on the type.
+        const KeyT sign = KeyT(KeyT(1) << (8 * sizeof(KeyT) - 1));
+        const KeyT flip = WIDE ? (col.pt == PT_I64 ? sign : KeyT(0)) : (col.pt == PT_U32 ? KeyT(0) : sign);
+        const KeyT x = flip ^ (col.desc ? KeyT(~KeyT(0)) : KeyT(0));
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++) {
+          const bool valid = !col.valid || ((vb[i] >> ((col.valid_off + int64_t(id[i])) & 7)) & 1u);
+          place(i, valid ? KeyT(raw[i] ^ x) : KeyT(0), valid ? 0 : 2);
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++) {
+          const bool valid = !col.valid || ((vb[i] >> ((col.valid_off + int64_t(id[i])) & 7)) & 1u);
+          int cat;
+          const KeyT k = key_from_raw<KeyT>(col, raw[i], valid, cat);
+          place(i, k, cat);
+        }
       }
     } else {
 #pragma unroll

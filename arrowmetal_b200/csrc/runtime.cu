@@ -463,11 +463,24 @@ StreamScratch& stream_scratch(cudaStream_t s, size_t status_words) {
   return *sc;
 }
 
+namespace {
+// Bytes held in all streams' arenas (a stream outlives its thread, and so does its arena): past
+// kArenaTotal, sorts take blocks of their own instead of growing an arena.
+std::atomic<size_t> g_arena_total{0};
+constexpr size_t kArenaTotal = size_t(16) << 30;
+}  // namespace
+
 ScratchBlock::ScratchBlock(cudaStream_t s, size_t bytes) : s_(s) {
   StreamScratch& sc = stream_scratch(s, 0);
   bool expected = false;
   if (bytes <= kArenaMax && sc.arena_busy.compare_exchange_strong(expected, true)) {
+    if (sc.arena_bytes < bytes && g_arena_total.load() - sc.arena_bytes + bytes > kArenaTotal) {
+      sc.arena_busy = false;
+      p_ = static_cast<char*>(dmalloc(bytes, s));
+      return;
+    }
     if (sc.arena_bytes < bytes) {
+      g_arena_total -= sc.arena_bytes;
       if (sc.arena) dfree(sc.arena, s);
       sc.arena = nullptr;
       sc.arena_bytes = 0;
@@ -478,6 +491,7 @@ ScratchBlock::ScratchBlock(cudaStream_t s, size_t bytes) : s_(s) {
         throw;
       }
       sc.arena_bytes = bytes;
+      g_arena_total += bytes;
     }
     arena_ = &sc;
     p_ = static_cast<char*>(sc.arena);
