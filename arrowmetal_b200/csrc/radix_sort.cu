@@ -683,9 +683,12 @@ struct PassShared {
   uint32_t scan_total;
   uint32_t ticket;
   uint32_t seg;
-  uint16_t dig[TILE];
+  // Each staged row's digit; in record passes (16-bit places) the digit << 16 | the row's place within
+  // the tile, one word read for both.
+  using DigT = std::conditional_t<sizeof(IdT) == 2, uint32_t, uint16_t>;
+  DigT dig[TILE];
   KeyT keys[TILE];
-  IdT ids[TILE];                 // row ids; in record passes, the row's place within the tile
+  IdT ids[sizeof(IdT) == 2 ? 1 : TILE];   // row ids (passes that carry them)
 };
 
 // Inverse of the integer and totalOrder key maps (SortSource.swift:131-190 read backwards): the value
@@ -951,6 +954,9 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
     }
     __syncthreads();
 
+    // Passes that neither route nor sort categories take each staged row's digit from its key again
+    // instead of staging it.
+    const bool dig_from_key = !REC && !(flags & (PF_ROUTE | PF_CATPASS));
     // ---- warp ranking and staging: each row goes to its tile-local sorted slot. The rows of a lane's
     // item that share its digit come from one ballot per digit bit, and the item is placed right after
     // its ballots: holding every item's peer mask first overlaps more ballots but pushes the 8-byte
@@ -976,9 +982,12 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
           if (lane == __ffs(peers) - 1) sm.whist[warp][d] = base + __popc(peers);
           const uint32_t pos = sm.local[d] + base + __popc(peers & lt_mask);
           sm.keys[pos] = key[i];
-          if constexpr (REC) sm.ids[pos] = uint16_t(id[i] - uint32_t(tile_base));
-          else if (pa.carry_ids) sm.ids[pos] = id[i];
-          sm.dig[pos] = uint16_t(d);
+          if constexpr (REC) {
+            sm.dig[pos] = (d << 16) | (id[i] - uint32_t(tile_base));
+          } else {
+            if (pa.carry_ids) sm.ids[pos] = id[i];
+            if (!dig_from_key) sm.dig[pos] = uint16_t(d);
+          }
         }
         __syncwarp();
       }
@@ -1029,6 +1038,10 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
     __syncthreads();
 
     const uint32_t tile_n = uint32_t((count - tile_base) < uint64_t(TILE) ? (count - tile_base) : uint64_t(TILE));
+    auto dig_at = [&](uint32_t j) -> uint32_t {
+      if constexpr (REC) return sm.dig[j] >> 16;
+      else return dig_from_key ? (uint32_t(sm.keys[j] >> shift) & 255u) : uint32_t(sm.dig[j]);
+    };
     // ---- keys and ids out; consecutive threads write consecutive addresses of a digit run. A pass that
     // moves both writes them in one loop (one digit and base lookup per row). Every destination is
     // checked against its array: an offset error is reported, never written.
@@ -1053,8 +1066,9 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
           const uint32_t j = j0 + uint32_t(u) * THREADS;
           dg[u] = INVALID_DIGIT;
           if (j >= tile_n) continue;
-          dg[u] = sm.dig[j];
-          const uint64_t src_row = tile_base + sm.ids[j];
+          const uint32_t w = sm.dig[j];
+          dg[u] = w >> 16;
+          const uint64_t src_row = tile_base + (w & 0xFFFFu);
           r[u] = encode ? build_record(pa.rec, uint32_t(src_row)) : rin[src_row];
         }
 #pragma unroll
@@ -1086,7 +1100,7 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
       }
     } else if (merged) {
       for (uint32_t j = threadIdx.x; j < tile_n; j += THREADS) {
-        const uint32_t d = sm.dig[j];
+        const uint32_t d = dig_at(j);
         const uint32_t dst = sm.gdelta[d] + j;
         if (d < RADIX) {
           if (dst < buf_rows) {
@@ -1103,7 +1117,7 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
       }
     } else if (keys_out) {
       for (uint32_t j = threadIdx.x; j < tile_n; j += THREADS) {
-        const uint32_t d = sm.dig[j];
+        const uint32_t d = dig_at(j);
         const uint32_t dst = sm.gdelta[d] + j;
         if (d < RADIX) {
           if (dst < buf_rows) keys_out[dst] = sm.keys[j];
@@ -1116,7 +1130,7 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
     if (pa.key_out_mode == KEY_OUT_UNKEY && (last || (flags & PF_ROUTE))) {
       const int kw = pt_bytes(pa.key_out_pt);
       for (uint32_t j = threadIdx.x; j < tile_n; j += THREADS) {
-        const uint32_t d = sm.dig[j];
+        const uint32_t d = dig_at(j);
         if (d < RADIX && !last) continue;
         uint32_t dst = sm.gdelta[d] + j;
         if (d < RADIX) dst += sm.desc.value_base;
@@ -1127,7 +1141,7 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
     }
     if (pa.carry_ids && !merged && !REC) {
       for (uint32_t j = threadIdx.x; j < tile_n; j += THREADS) {
-        const uint32_t d = sm.dig[j];
+        const uint32_t d = dig_at(j);
         const uint32_t v = sm.ids[j];
         uint32_t dst = sm.gdelta[d] + j;
         if (d >= RADIX || !ids_out) {
