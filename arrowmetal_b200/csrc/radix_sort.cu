@@ -1,6 +1,6 @@
 // Stable LSD radix argsort for sm_100a: one key-encode + all-digit histogram read per key column,
-// a one-block planning kernel, then onesweep digit passes with warp match_any ranking and decoupled
-// look-back, skipping every digit that is constant over the column.
+// a one-block planning kernel, then onesweep digit passes with warp-ballot multisplit ranking and
+// decoupled look-back, skipping every digit that is constant over the column.
 //
 // What it computes is the reference's `radixSortRun` (Sources/ArrowMetal/Kernels/Sort.swift:190-504)
 // and `lexsortIndices` (Sources/ArrowMetal/Kernels/MultiSort.swift:28-65):
@@ -683,6 +683,7 @@ struct PassShared {
   uint32_t scan_total;
   uint32_t ticket;
   uint32_t seg;
+  uint32_t lo_first, lo_last;    // PF_BUCKETS: the lower bucket digit of the tile's first and last rows
   // Each staged row's digit; in record passes (16-bit places) the digit << 16 | the row's place within
   // the tile, one word read for both.
   using DigT = std::conditional_t<sizeof(IdT) == 2, uint32_t, uint16_t>;
@@ -928,12 +929,24 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
       for (int i = 0; i < ITEMS; i++) dg[i] = ((ok >> i) & 1u) ? (uint32_t(key[i] >> shift) & 255u) : INVALID_DIGIT;
     }
 
+    // The two-level sort's second pass counts its buckets (this pass's digit, the lower digit). Its rows
+    // arrive ordered by the lower digit (the first pass sorted by it), so the tile's first and last rows
+    // tell whether one lower digit covers the whole tile.
+    if ((flags & PF_BUCKETS) && threadIdx.x == 0) {
+      // Thread 0's first item is the tile's first row; the last row's key is read again (L2).
+      const uint32_t lsh = sm.desc.bucket_shift;
+      const uint64_t last_row = (count - tile_base < uint64_t(TILE) ? count : tile_base + TILE) - 1;
+      sm.lo_first = uint32_t(key[0] >> lsh) & 255u;
+      sm.lo_last = uint32_t(keys_in[last_row] >> lsh) & 255u;
+    }
+
     // ---- early counts: the tile's per-digit counts go out as look-back aggregates before any
     // ranking, so the tiles after this one can resolve their prefixes as early as possible.
 #pragma unroll
     for (int i = 0; i < ITEMS; i++)
       if (dg[i] != INVALID_DIGIT) atomicAdd(&sm.whist[warp][dg[i]], 1u);
     __syncthreads();
+    const bool one_lower = (flags & PF_BUCKETS) && sm.lo_first == sm.lo_last;
     for (int b = threadIdx.x; b < NBINS; b += THREADS) {
       uint32_t run = 0;
 #pragma unroll
@@ -944,6 +957,15 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
       }
       sm.cnt[b] = run;
       ST::store(status + uint64_t(T) * NBINS + b, ST::make(epoch, tile == 0 ? ST_INCL : ST_AGG, run));
+      // One lower digit in the tile: each digit's count is its bucket's share.
+      if (one_lower && b < RADIX && run) atomicAdd(pa.bucket_count + ((uint32_t(b) << 8) | sm.lo_first), run);
+    }
+    if ((flags & PF_BUCKETS) && !one_lower) {
+      // The tile holds a change of the lower digit (at most 255 tiles of the pass do): one count a row.
+      const uint32_t lsh = sm.desc.bucket_shift;
+#pragma unroll
+      for (int i = 0; i < ITEMS; i++)
+        if (dg[i] < uint32_t(RADIX)) atomicAdd(pa.bucket_count + ((dg[i] << 8) | (uint32_t(key[i] >> lsh) & 255u)), 1u);
     }
     // Tile-local digit starts: value digits in order, then the NaN and null routing bins.
     block_exclusive_scan_256(sm.cnt, sm.local, &sm.scan_total, sm.scan_warp);
@@ -1096,6 +1118,10 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
             else static_cast<uint32_t*>(final_out)[dst] = r[u].x;
           }
           unpack_record(pa.rec, r[u], dst);
+          // The sorted key column at the same row: null rows as zero, value rows (last pass) unkeyed.
+          if (pa.key_out_mode == KEY_OUT_UNKEY)
+            store_width(pa.key_out, dst, pt_bytes(pa.key_out_pt),
+                        d < RADIX ? unkey_bits<KeyT>(sm.keys[j], pa.key_out_pt, pa.key_desc) : 0ull);
         }
       }
     } else if (merged) {
@@ -1126,8 +1152,8 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
       }
     }
     // The sorted key column: value rows from their keys in the last pass, null rows (first pass of the
-    // most significant key) as zero.
-    if (pa.key_out_mode == KEY_OUT_UNKEY && (last || (flags & PF_ROUTE))) {
+    // most significant key) as zero. Record passes write it in their own loop, beside the payload.
+    if (!REC && pa.key_out_mode == KEY_OUT_UNKEY && (last || (flags & PF_ROUTE))) {
       const int kw = pt_bytes(pa.key_out_pt);
       for (uint32_t j = threadIdx.x; j < tile_n; j += THREADS) {
         const uint32_t d = dig_at(j);
@@ -1172,10 +1198,13 @@ __global__ void __launch_bounds__(256) key_validity_kernel(const SortSummary* __
   const uint64_t lo = nulls_first ? 0 : n - nn, hi = nulls_first ? nn : n;   // null rows [lo, hi)
   const uint64_t words = (n + 31) / 32;
   for (uint64_t w = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; w < words; w += uint64_t(gridDim.x) * blockDim.x) {
-    uint32_t v = 0;
-    for (int b = 0; b < 32; b++) {
-      const uint64_t r = w * 32 + b;
-      if (r < n && !(r >= lo && r < hi)) v |= 1u << b;
+    // Bit b is row w * 32 + b: set unless the row is null (in [lo, hi)) or past the end.
+    const uint64_t r0 = w * 32;
+    uint32_t v = r0 + 32 <= n ? 0xFFFFFFFFu : ((1u << uint32_t(n - r0)) - 1u);   // n - r0 < 32 there
+    const uint64_t a = lo > r0 ? lo : r0, b = hi < r0 + 32 ? hi : r0 + 32;
+    if (a < b) {
+      const uint32_t len = uint32_t(b - a);
+      v &= len == 32 ? 0u : ~(((1u << len) - 1u) << uint32_t(a - r0));
     }
     bits[w] = v;
   }
@@ -1198,8 +1227,7 @@ __global__ void __launch_bounds__(256) key_validity_kernel(const SortSummary* __
 constexpr uint64_t HYB_MIN_ROWS = uint64_t(1) << 25;     // one pass saved; ARROWMETAL_HYBRID_MIN_ROWS overrides
 constexpr uint64_t HYB_MIN_ANY = uint64_t(1) << 21;      // the smallest sort that may take it (6 passes saved)
 constexpr int HYB_STEPS = 10;                 // two top-digit passes, then up to eight fallback passes
-constexpr int BND_THREADS = 256, BND_ITEMS = 16;
-constexpr uint64_t BND_CHUNK = uint64_t(BND_THREADS) * BND_ITEMS;
+constexpr int HYB_BUCKETS = 65536;            // (higher digit, lower digit) buckets of the two passes
 constexpr int LOC_ITEMS = 7;
 constexpr int LOC_VARIANTS = 3;               // 128, 256 and 512 threads x 7 rows
 __host__ __device__ constexpr int loc_threads(int v) { return v == 0 ? 128 : v == 1 ? 256 : 512; }
@@ -1217,6 +1245,7 @@ struct HybridState {
   uint32_t hi_shift, lo_shift;   // the two bucket digits
   uint32_t max_bucket;
   uint32_t local_shift[8];
+  uint32_t scan_done, count_error;   // bucket_scan_kernel: blocks finished, a digit's counts off
 };
 
 // One block: the hybrid's pass descriptors from the plan's (one descriptor per digit slot), or the
@@ -1270,6 +1299,8 @@ __global__ void __launch_bounds__(256) hybrid_plan_kernel(PlanArgs a, const KeyS
   hs->m = m;
   hs->value_base = a.nulls_first[0] ? st->n_null + st->n_nan : 0u;
   hs->max_bucket = 0;
+  hs->scan_done = 0;
+  hs->count_error = 0;
   if (!s_hyb) {
     hs->nlocal = 0;
     hs->nfall = 0;
@@ -1287,7 +1318,8 @@ __global__ void __launch_bounds__(256) hybrid_plan_kernel(PlanArgs a, const KeyS
   h0.dst_ids = 0;
   PassDesc& h1 = steps[1];
   h1.active = 1;
-  h1.flags = wide;
+  h1.flags = wide | PF_BUCKETS;
+  h1.bucket_shift = uint32_t(8 * s_act[na - 2]);
   h1.count = m;
   h1.src_keys = 0;
   h1.src_ids = 0;
@@ -1318,174 +1350,60 @@ __global__ void __launch_bounds__(256) hybrid_plan_kernel(PlanArgs a, const KeyS
   hs->lo_shift = uint32_t(8 * s_act[na - 2]);
 }
 
-__device__ __forceinline__ uint32_t bucket_of(uint64_t k, uint32_t hi, uint32_t lo) {
-  return ((uint32_t(k >> hi) & 255u) << 8) | (uint32_t(k >> lo) & 255u);
-}
-
-// Bucket boundaries: position i of the value rows starts a bucket when its bucket differs from row
-// i - 1's. A block takes BND_CHUNK rows, thread t the rows t, t + BND_THREADS, ... of it (coalesced
-// loads, the row before each read from the neighbouring lane or the previous round).
-__device__ __forceinline__ uint32_t boundary_masks(const uint64_t* __restrict__ keys, uint64_t first, uint64_t m,
-                                                   uint32_t hi, uint32_t lo) {
-  // Bit k: row first + k * BND_THREADS + threadIdx.x starts a bucket.
-  uint32_t mask = 0;
-#pragma unroll
-  for (int k = 0; k < BND_ITEMS; k++) {
-    const uint64_t r = first + uint64_t(k) * BND_THREADS + threadIdx.x;
-    if (r >= m) continue;
-    const uint32_t b = bucket_of(keys[r], hi, lo);
-    const uint32_t p = r == 0 ? 0xFFFFFFFFu : bucket_of(keys[r - 1], hi, lo);
-    if (b != p) mask |= 1u << k;
-  }
-  return mask;
-}
-
-// Each thread's 16 start bits also go to `masks`, so the write kernel does not read the keys again.
-__global__ void __launch_bounds__(BND_THREADS) bounds_count_kernel(const uint64_t* __restrict__ keys,
-                                                                   const HybridState* __restrict__ hs,
-                                                                   uint32_t* __restrict__ counts,
-                                                                   uint16_t* __restrict__ masks) {
-  static_assert(BND_ITEMS <= 16, "a thread's start bits fit 16 bits");
-  __shared__ uint32_t s_warp[BND_THREADS / 32];
+// After the second pass: the buckets' starts, the largest bucket, and the local shape or the
+// fallback passes. The second pass counted every bucket (65,536: its digit, then the lower digit);
+// the buckets of one digit d start where the second pass put digit d (its bin base), so block d scans
+// its 256 lower-digit counts on its own: pos[d * 256 + l] = base[d] + the counts before l. The last
+// block to finish decides from the largest bucket; pos[65,536] is the value rows.
+__global__ void __launch_bounds__(256) bucket_scan_kernel(HybridState* __restrict__ hs, const uint32_t* __restrict__ counts,
+                                                          uint32_t* __restrict__ pos, PassDesc* __restrict__ steps,
+                                                          SortSummary* __restrict__ sum, uint32_t* __restrict__ err) {
+  __shared__ uint32_t s_sum[8], s_max[8];
+  __shared__ uint32_t s_last;
   if (!hs->mode) return;
-  const uint64_t first = uint64_t(blockIdx.x) * BND_CHUNK;
-  const uint32_t mask = boundary_masks(keys, first, hs->m, hs->hi_shift, hs->lo_shift);
-  masks[uint64_t(blockIdx.x) * BND_THREADS + threadIdx.x] = uint16_t(mask);
-  uint32_t c = __popc(mask);
-  c = __reduce_add_sync(0xffffffffu, c);
-  if ((threadIdx.x & 31) == 0) s_warp[threadIdx.x >> 5] = c;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    uint32_t t = 0;
-    for (int w = 0; w < BND_THREADS / 32; w++) t += s_warp[w];
-    counts[blockIdx.x] = t;
+  const uint32_t d = blockIdx.x, t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const uint32_t c = counts[d * 256 + t];
+  uint32_t x = c;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
   }
-}
-
-// One block: exclusive scan of the block counts in place; the bucket count and the end sentinel.
-__global__ void __launch_bounds__(1024) bounds_scan_kernel(uint32_t* __restrict__ counts, uint32_t blocks,
-                                                           HybridState* __restrict__ hs, uint32_t* __restrict__ pos) {
-  // Each thread scans K consecutive counts, all loaded before any is used (one round trip per 16K
-  // counts instead of one per 1,024).
-  constexpr int K = 16;
-  __shared__ uint32_t s[32];
-  __shared__ uint32_t carry;
-  if (!hs->mode) return;
-  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  if (t == 0) carry = 0;
+  const uint32_t mx = __reduce_max_sync(0xffffffffu, c);
+  if (lane == 31) s_sum[warp] = x;
+  if (lane == 0) s_max[warp] = mx;
   __syncthreads();
-  for (uint32_t b0 = 0; b0 < blocks; b0 += 1024u * K) {
-    const uint32_t i0 = b0 + uint32_t(t) * K;
-    uint32_t v[K];
+  uint32_t add = 0, tot = 0, bmax = 0;
 #pragma unroll
-    for (int k = 0; k < K; k++) v[k] = i0 + k < blocks ? counts[i0 + k] : 0u;
-    uint32_t sum = 0;
-#pragma unroll
-    for (int k = 0; k < K; k++) sum += v[k];
-    uint32_t x = sum;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-      if (lane >= o) x += y;
-    }
-    if (lane == 31) s[warp] = x;
-    __syncthreads();
-    uint32_t add = carry, all = 0;
-    for (int w = 0; w < 32; w++) {
-      if (w < warp) add += s[w];
-      all += s[w];
-    }
-    uint32_t run = x - sum + add;
-#pragma unroll
-    for (int k = 0; k < K; k++) {
-      if (i0 + k < blocks) counts[i0 + k] = run;
-      run += v[k];
-    }
-    __syncthreads();
-    if (t == 0) carry += all;
-    __syncthreads();
+  for (int w = 0; w < 8; w++) {
+    if (w < int(warp)) add += s_sum[w];
+    tot += s_sum[w];
+    bmax = max(bmax, s_max[w]);
   }
+  const uint32_t base = steps[1].bin_base[d];
+  pos[d * 256 + t] = base + x - c + add;
   if (t == 0) {
-    hs->buckets = carry;
-    if (carry <= 65536u) pos[carry] = hs->m;   // pos holds 65,537 entries; more starts mean fallback
-  }
-}
-
-// The starts' positions, in row order: round k of the block before round k + 1, warp w before w + 1
-// within a round (rows first + k * BND_THREADS + 32 w + lane).
-__global__ void __launch_bounds__(BND_THREADS) bounds_write_kernel(const uint16_t* __restrict__ masks,
-                                                                   const HybridState* __restrict__ hs,
-                                                                   const uint32_t* __restrict__ offs,
-                                                                   uint32_t* __restrict__ pos,
-                                                                   uint32_t* __restrict__ err) {
-  constexpr int WARPS = BND_THREADS / 32;
-  __shared__ uint32_t s_cnt[BND_ITEMS][WARPS];
-  if (!hs->mode) return;
-  const uint64_t first = uint64_t(blockIdx.x) * BND_CHUNK;
-  const uint32_t mask = masks[uint64_t(blockIdx.x) * BND_THREADS + threadIdx.x];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const uint32_t lt = (1u << lane) - 1u;
-  uint32_t ball[BND_ITEMS];
-#pragma unroll
-  for (int k = 0; k < BND_ITEMS; k++) {
-    ball[k] = __ballot_sync(0xffffffffu, (mask >> k) & 1u);
-    if (lane == 0) s_cnt[k][warp] = __popc(ball[k]);
+    // The digit's buckets must hold exactly its rows; otherwise no local sort runs on them.
+    const uint32_t end = d + 1 < 256 ? steps[1].bin_base[d + 1] : hs->m;
+    if (base + tot != end) atomicOr(&hs->count_error, 1u);
+    atomicMax(&hs->max_bucket, bmax);
+    __threadfence();
+    s_last = atomicAdd(&hs->scan_done, 1u) == gridDim.x - 1 ? 1u : 0u;
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
-    uint32_t run = offs[blockIdx.x];
-    for (int k = 0; k < BND_ITEMS; k++)
-      for (int w = 0; w < WARPS; w++) {
-        const uint32_t c = s_cnt[k][w];
-        s_cnt[k][w] = run;
-        run += c;
-      }
-  }
-  __syncthreads();
-#pragma unroll
-  for (int k = 0; k < BND_ITEMS; k++) {
-    if (!((mask >> k) & 1u)) continue;
-    const uint32_t at = s_cnt[k][warp] + __popc(ball[k] & lt);
-    if (at >= 65536u) {
-      atomicOr(err, ERR_BOUNDS);
-      continue;
-    }
-    pos[at] = uint32_t(first + uint64_t(k) * BND_THREADS + threadIdx.x);
-  }
-}
-
-// One block: the largest bucket picks the local shape, or the fallback passes.
-__global__ void __launch_bounds__(1024) bounds_decide_kernel(HybridState* __restrict__ hs, const uint32_t* __restrict__ pos,
-                                                             PassDesc* __restrict__ steps, SortSummary* __restrict__ sum) {
-  __shared__ uint32_t s_max;
-  if (!hs->mode) return;
-  if (threadIdx.x == 0) s_max = 0;
-  __syncthreads();
-  // The rows are grouped by a 16-bit bucket, so there are at most 65,536 starts; anything else takes
-  // the passes.
-  const uint32_t g = hs->buckets <= 65536u ? hs->buckets : 0u;
-  // 16 bucket sizes a thread per round trip; j < g <= 65,536 keeps pos[j + 1] within its 65,537 entries.
-  uint32_t mx = 0;
-  for (uint32_t j0 = 0; j0 < g; j0 += 16u * blockDim.x) {
-    uint32_t a[16], b[16];
-#pragma unroll
-    for (int u = 0; u < 16; u++) {
-      const uint32_t j = j0 + uint32_t(u) * blockDim.x + threadIdx.x;
-      a[u] = j < g ? pos[j] : 0u;
-      b[u] = j < g ? pos[j + 1] : 0u;
-    }
-#pragma unroll
-    for (int u = 0; u < 16; u++) mx = max(mx, b[u] - a[u]);
-  }
-  mx = __reduce_max_sync(0xffffffffu, mx);
-  if ((threadIdx.x & 31) == 0) atomicMax(&s_max, mx);
-  __syncthreads();
-  if (threadIdx.x != 0) return;
-  hs->max_bucket = s_max;
+  if (!s_last || t != 0) return;
+  __threadfence();
+  const uint32_t big = atomicAdd(&hs->max_bucket, 0u);
+  const bool bad = atomicAdd(&hs->count_error, 0u) != 0u;
+  pos[HYB_BUCKETS] = hs->m;
+  hs->buckets = HYB_BUCKETS;
   int v = -1;
   for (int i = LOC_VARIANTS - 1; i >= 0; i--)
-    if (s_max <= loc_cap(i)) v = i;
-  if (hs->buckets > 65536u) v = -1;
+    if (big <= loc_cap(i)) v = i;
+  if (bad) {
+    atomicOr(err, ERR_BOUNDS);
+    v = -1;
+  }
   if (v >= 0) {
     hs->variant = uint32_t(v);
     sum->passes_run = 2;                 // the local sorts stand in for the others
@@ -1526,6 +1444,7 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? 8 : THREADS == 256 ?
       if (threadIdx.x == 0) atomicOr(pa.err, ERR_BOUNDS);
       continue;
     }
+    if (size == 0) continue;               // an empty bucket (the same for every thread)
     uint64_t key[ITEMS];
     uint32_t id[ITEMS];
 #pragma unroll
@@ -2056,16 +1975,14 @@ void radix_sort(const std::vector<SortKey>& keys_in, int64_t n64, void* out, int
   const bool hybrid = K == 1 && pt_key_bytes(keys[0].col->pt) == 8 && n < (uint64_t(1) << 32) &&
                       n >= (pa.hyb_min_rows ? pa.hyb_min_rows : HYB_MIN_ANY);
   const int NT = S + (hybrid ? HYB_STEPS : 0);          // tile counters: one per launched pass
-  const uint32_t bnd_blocks = uint32_t((n + BND_CHUNK - 1) / BND_CHUNK);
   const size_t off_stats = 0;
   const size_t off_kplan = off_stats + sizeof(KeyStats) * K;
   const size_t off_desc = (off_kplan + sizeof(KeyPlan) * K + 255) & ~size_t(255);
   const size_t off_steps = off_desc + sizeof(PassDesc) * S;
   const size_t off_hs = (off_steps + (hybrid ? sizeof(PassDesc) * HYB_STEPS : 0) + 15) & ~size_t(15);
   const size_t off_bcount = (off_hs + (hybrid ? sizeof(HybridState) : 0) + 15) & ~size_t(15);
-  const size_t off_bpos = off_bcount + (hybrid ? sizeof(uint32_t) * (bnd_blocks + 1) : 0);
-  const size_t off_bmask = (off_bpos + (hybrid ? sizeof(uint32_t) * 65537 : 0) + 15) & ~size_t(15);
-  const size_t off_tick = off_bmask + (hybrid ? sizeof(uint16_t) * size_t(bnd_blocks) * BND_THREADS : 0);
+  const size_t off_bpos = off_bcount + (hybrid ? sizeof(uint32_t) * HYB_BUCKETS : 0);
+  const size_t off_tick = (off_bpos + (hybrid ? sizeof(uint32_t) * (HYB_BUCKETS + 1) : 0) + 15) & ~size_t(15);
   const size_t off_sum = (off_tick + sizeof(uint32_t) * NT + 15) & ~size_t(15);
   const size_t header = (off_sum + sizeof(SortSummary) + 255) & ~size_t(255);
   const size_t kbuf = ((n * max_kb) + 255) & ~size_t(255);
@@ -2082,7 +1999,6 @@ void radix_sort(const std::vector<SortKey>& keys_in, int64_t n64, void* out, int
   HybridState* hs = reinterpret_cast<HybridState*>(base + off_hs);
   uint32_t* bcount = reinterpret_cast<uint32_t*>(base + off_bcount);
   uint32_t* bpos = reinterpret_cast<uint32_t*>(base + off_bpos);
-  uint16_t* bmask = reinterpret_cast<uint16_t*>(base + off_bmask);
   void* kbufA = base + header;
   void* kbufB = base + header + kbuf;
   uint32_t* ibufA = carry_ids ? reinterpret_cast<uint32_t*>(base + header + 2 * kbuf) : nullptr;
@@ -2138,6 +2054,7 @@ void radix_sort(const std::vector<SortKey>& keys_in, int64_t n64, void* out, int
     a.tile_counter = counter;
     a.err = sc.err;
     a.carry_ids = carry_ids ? 1 : 0;
+    a.bucket_count = hybrid ? bcount : nullptr;
     if (key_dst) {
       a.key_out_mode = KEY_OUT_UNKEY;
       a.key_out_pt = keys[0].col->pt;
@@ -2182,14 +2099,7 @@ void radix_sort(const std::vector<SortKey>& keys_in, int64_t n64, void* out, int
     launch_one(steps + 1, tick + S + 1, kp, views[0], 8);
     {
       KernelTimer kt("radix_buckets", s);
-      const uint64_t* kb1 = static_cast<const uint64_t*>(kbufB);
-      bounds_count_kernel<<<bnd_blocks, BND_THREADS, 0, s>>>(kb1, hs, bcount, bmask);
-      AM_CUDA(cudaGetLastError());
-      bounds_scan_kernel<<<1, 1024, 0, s>>>(bcount, bnd_blocks, hs, bpos);
-      AM_CUDA(cudaGetLastError());
-      bounds_write_kernel<<<bnd_blocks, BND_THREADS, 0, s>>>(bmask, hs, bcount, bpos, sc.err);
-      AM_CUDA(cudaGetLastError());
-      bounds_decide_kernel<<<1, 1024, 0, s>>>(hs, bpos, steps, sum);
+      bucket_scan_kernel<<<HYB_BUCKETS / 256, 256, 0, s>>>(hs, bcount, bpos, steps, sum, sc.err);
       AM_CUDA(cudaGetLastError());
     }
     for (int i = 2; i < HYB_STEPS; i++) launch_one(steps + i, tick + S + i, kp, views[0], 8);

@@ -22,6 +22,7 @@ constexpr uint32_t PF_ROUTE = 2;           // most significant key: null / NaN r
 constexpr uint32_t PF_CATPASS = 4;         // a lower key's null category, looked up by row id
 constexpr uint32_t PF_WIDE_OUT = 8;        // the output index array is uint64
 constexpr uint32_t PF_LAST = 16;           // the last pass: rows reach their final places
+constexpr uint32_t PF_BUCKETS = 32;        // two-level sort's second pass: count its (digit, lower digit) buckets
 
 // Look-back status word: epoch (30 bits) | flag (2 bits) | count (32 bits).
 constexpr uint32_t ST_AGG = 1, ST_INCL = 2;
@@ -63,7 +64,8 @@ struct PassDesc {
   int32_t src_keys, src_ids, dst_keys, dst_ids;   // -1: none / identity / the output array
   uint32_t value_base, key;
   uint32_t buf_rows, out_rows;                    // bounds of the key / id buffers and of the output
-  uint32_t pad2[2];
+  uint32_t bucket_shift;                          // PF_BUCKETS: the lower bucket digit's shift
+  uint32_t pad2;
   uint32_t bin_base[NBINS];
 };
 
@@ -129,6 +131,8 @@ struct PassArgs {
   int32_t key_desc;
   int32_t key_float_order;
   void* key_out;              // sorted key values
+  // PF_BUCKETS passes: 65,536 row counts, one per (this pass's digit, lower digit) bucket.
+  uint32_t* bucket_count;
   // Segmented passes: `desc` and `kplan` are per-segment arrays (desc[seg * nslots + slot]); tile T of
   // the launch belongs to the segment s with tile_start[s] <= T < tile_start[s + 1].
   const SegDesc* segs;
