@@ -126,23 +126,45 @@ template <> __device__ __forceinline__ uint64_t key_from_raw<uint64_t>(const Col
   return c.desc ? ~k : k;
 }
 
-// Keys of ITEMS rows: all loads first (values and validity bytes), then the arithmetic, with the type
-// and direction decided once for all the rows (the integer maps are one XOR a row, with no branches).
-// The same keys and categories as key_from_raw row by row.
-template <typename KeyT, int ITEMS>
-__device__ __forceinline__ void encode_rows(const ColView& c, const uint32_t (&row)[ITEMS], uint32_t ok, KeyT (&key)[ITEMS],
-                                            int (&cat)[ITEMS]) {
-  KeyT raw[ITEMS];
+// Validity of ITEMS rows held warp-striped from `first`: item i of lane l is row first + 32 i + l;
+// bit i of `ok` says the row exists (rows before `end` do). When the bitmap's offset and `first` are
+// multiples of 32 and the bitmap is word-aligned, an item's 32 rows are one bitmap word (lane l's bit
+// l), one load for the warp; an item whose word reaches past the rows (the bitmap may end inside it)
+// reads each row's own byte, placed at that byte's position in the word. Bit i of the result: the row
+// exists and is valid.
+template <int ITEMS>
+__device__ __forceinline__ uint32_t striped_validity(const ColView& c, uint64_t first, uint64_t end, uint32_t ok) {
+  if (!c.valid) return ok;
+  const uint32_t lane = threadIdx.x & 31u;
   uint32_t vb[ITEMS];
-  load_raw_rows<KeyT, ITEMS>(c, row, ok, raw);
-  uint32_t valid = ok;                 // bit i: row i exists and is not null
-  if (c.valid) {
+  uint32_t valid = ok;
+  if ((c.valid_off & 31) == 0 && (first & 31u) == 0 && (reinterpret_cast<uintptr_t>(c.valid) & 3u) == 0) {
+    const uint32_t* w = reinterpret_cast<const uint32_t*>(c.valid) + ((uint64_t(c.valid_off) + first) >> 5);
+    const uint64_t full = end > first ? (end - first) >> 5 : 0;   // items whose 32 rows all exist
 #pragma unroll
-    for (int i = 0; i < ITEMS; i++) vb[i] = ((ok >> i) & 1u) ? c.valid[(c.valid_off + int64_t(row[i])) >> 3] : 0u;
+    for (int i = 0; i < ITEMS; i++) {
+      if (uint64_t(i) < full) vb[i] = w[i];
+      else vb[i] = ((ok >> i) & 1u) ? uint32_t(c.valid[(c.valid_off + int64_t(first + 32u * i + lane)) >> 3]) << (8u * (lane >> 3)) : 0u;
+    }
 #pragma unroll
     for (int i = 0; i < ITEMS; i++)
-      if (!((vb[i] >> ((c.valid_off + int64_t(row[i])) & 7)) & 1u)) valid &= ~(1u << i);
+      if (!((vb[i] >> lane) & 1u)) valid &= ~(1u << i);
+  } else {
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++) vb[i] = ((ok >> i) & 1u) ? c.valid[(c.valid_off + int64_t(first + 32u * i + lane)) >> 3] : 0u;
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++)
+      if (!((vb[i] >> ((c.valid_off + int64_t(first + 32u * i + lane)) & 7)) & 1u)) valid &= ~(1u << i);
   }
+  return valid;
+}
+
+// Keys and categories of ITEMS rows from their raw bits and validity (bit i: row i is valid), with the
+// type and direction decided once for all the rows (the integer maps are one XOR a row, no branches).
+// The same keys and categories as key_from_raw row by row.
+template <typename KeyT, int ITEMS>
+__device__ __forceinline__ void encode_raw(const ColView& c, const KeyT (&raw)[ITEMS], uint32_t valid, KeyT (&key)[ITEMS],
+                                           int (&cat)[ITEMS]) {
   constexpr bool WIDE = sizeof(KeyT) == 8;
   const bool fl = WIDE ? c.pt == PT_F64 : (c.pt == PT_F32 || c.pt == PT_F16);
   if (!fl) {
@@ -169,6 +191,24 @@ __device__ __forceinline__ void encode_rows(const ColView& c, const uint32_t (&r
       }
     }
   }
+}
+
+// Keys of ITEMS rows at any positions: all loads first (values and validity bytes), then the arithmetic.
+template <typename KeyT, int ITEMS>
+__device__ __forceinline__ void encode_rows(const ColView& c, const uint32_t (&row)[ITEMS], uint32_t ok, KeyT (&key)[ITEMS],
+                                            int (&cat)[ITEMS]) {
+  KeyT raw[ITEMS];
+  uint32_t vb[ITEMS];
+  load_raw_rows<KeyT, ITEMS>(c, row, ok, raw);
+  uint32_t valid = ok;                 // bit i: row i exists and is not null
+  if (c.valid) {
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++) vb[i] = ((ok >> i) & 1u) ? c.valid[(c.valid_off + int64_t(row[i])) >> 3] : 0u;
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++)
+      if (!((vb[i] >> ((c.valid_off + int64_t(row[i])) & 7)) & 1u)) valid &= ~(1u << i);
+  }
+  encode_raw<KeyT, ITEMS>(c, raw, valid, key, cat);
 }
 
 template <typename T> __device__ __forceinline__ T warp_or(T v);

@@ -62,6 +62,11 @@ __device__ __forceinline__ uint32_t ld_relaxed_u32(const uint32_t* p) {
 __device__ __forceinline__ void st_relaxed_u32(uint32_t* p, uint32_t v) {
   asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
+// Byte p of a key (digit p), zero-extended: one byte permute.
+__device__ __forceinline__ uint32_t key_byte(uint32_t k, int p) { return __byte_perm(k, 0u, 0x4440u | uint32_t(p)); }
+__device__ __forceinline__ uint32_t key_byte(uint64_t k, int p) {
+  return p < 4 ? __byte_perm(uint32_t(k), 0u, 0x4440u | uint32_t(p)) : __byte_perm(uint32_t(k >> 32), 0u, 0x4440u | uint32_t(p - 4));
+}
 
 // Look-back status words. 32-bit: flag (2 bits) | count (30 bits), zeroed before every pass; used when a
 // pass has fewer than 2^30 rows. 64-bit: the pass epoch (30 bits) | flag | count (32 bits), never
@@ -103,10 +108,13 @@ template <typename KeyT, int THREADS, int ITEMS, bool RANGE = true>
 __device__ __forceinline__ void histogram_rows(const ColView& col, KeyStats* __restrict__ st, uint64_t first,
                                                uint64_t end, uint64_t stride) {
   constexpr int D = int(sizeof(KeyT));
-  __shared__ uint32_t sh[D * 256];
+  // Per digit 256 bins and one more, which takes the (discarded) counts of rows that are not values,
+  // so every item adds to a bin without a branch.
+  constexpr int STRIDE = 257;
+  __shared__ uint32_t sh[D * STRIDE];
   __shared__ uint32_t s_null, s_nan, s_val;
   __shared__ unsigned long long s_max, s_min_inv;
-  for (int i = threadIdx.x; i < D * 256; i += THREADS) sh[i] = 0;
+  for (int i = threadIdx.x; i < D * STRIDE; i += THREADS) sh[i] = 0;
   if (threadIdx.x == 0) { s_null = 0; s_nan = 0; s_val = 0; s_max = 0; s_min_inv = 0; }
   __syncthreads();
 
@@ -125,7 +133,13 @@ __device__ __forceinline__ void histogram_rows(const ColView& col, KeyStats* __r
       row[i] = uint32_t(g);
       if (g < end) ok |= 1u << i;
     }
-    encode_rows<KeyT, ITEMS>(col, row, ok, k, cat);
+    {
+      // The block's rows are warp-striped from a multiple of 32: validity a bitmap word an item.
+      KeyT raw[ITEMS];
+      load_raw_rows<KeyT, ITEMS>(col, row, ok, raw);
+      const uint32_t vmask = striped_validity<ITEMS>(col, base + uint64_t(warp) * (ITEMS * 32), end, ok);
+      encode_raw<KeyT, ITEMS>(col, raw, vmask, k, cat);
+    }
     uint32_t valid_mask = 0;
     KeyT o = 0, a = KeyT(~KeyT(0));
     uint32_t nv = 0;
@@ -150,16 +164,24 @@ __device__ __forceinline__ void histogram_rows(const ColView& col, KeyStats* __r
     }
     n_val += nv;
     const KeyT wo = warp_or<KeyT>(o), wa = warp_and<KeyT>(a);
+    const KeyT wdiff = KeyT(wo ^ wa);
     const uint32_t wnv = __reduce_add_sync(0xffffffffu, nv);
+    // Rows that are not values count in the extra bin: their key is taken as 0 and offset by 256.
+    KeyT km[ITEMS];
+    uint32_t pad[ITEMS];
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++) {
+      const bool v = (valid_mask >> i) & 1u;
+      km[i] = v ? k[i] : KeyT(0);
+      pad[i] = v ? 0u : 256u;
+    }
 #pragma unroll
     for (int p = 0; p < D; p++) {
-      const uint32_t diff = uint32_t((wo ^ wa) >> (8 * p)) & 255u;
-      if (diff == 0u) {
-        if (lane == 0 && wnv) atomicAdd(&sh[p * 256 + (uint32_t(wa >> (8 * p)) & 255u)], wnv);
+      if (key_byte(wdiff, p) == 0u) {
+        if (lane == 0 && wnv) atomicAdd(&sh[p * STRIDE + key_byte(wa, p)], wnv);
       } else {
 #pragma unroll
-        for (int i = 0; i < ITEMS; i++)
-          if (valid_mask & (1u << i)) atomicAdd(&sh[p * 256 + (uint32_t(k[i] >> (8 * p)) & 255u)], 1u);
+        for (int i = 0; i < ITEMS; i++) atomicAdd(&sh[p * STRIDE + key_byte(km[i], p) + pad[i]], 1u);
       }
     }
   }
@@ -177,8 +199,10 @@ __device__ __forceinline__ void histogram_rows(const ColView& col, KeyStats* __r
     atomicMax(&s_min_inv, (unsigned long long)wmin);
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < D * 256; i += THREADS)
-    if (sh[i]) atomicAdd(&st->hist[i >> 8][i & 255], sh[i]);
+  for (int i = threadIdx.x; i < D * 256; i += THREADS) {
+    const uint32_t c = sh[(i >> 8) * STRIDE + (i & 255)];
+    if (c) atomicAdd(&st->hist[i >> 8][i & 255], c);
+  }
   if (threadIdx.x == 0) {
     if (s_null) atomicAdd(&st->n_null, s_null);
     if (s_nan) atomicAdd(&st->n_nan, s_nan);
@@ -886,9 +910,19 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
       KeyT raw[ITEMS];
       uint32_t vb[ITEMS];
       load_raw_rows<KeyT, ITEMS>(col, id, ok, raw);
+      // Validity: rows in their own order are warp-striped from a multiple of 32 (a bitmap word an
+      // item); rows reached through gathered ids read their bytes.
+      uint32_t vmask = ok;
       if (col.valid) {
+        if (!(ids_in && pa.carry_ids && !REC)) {
+          vmask = striped_validity<ITEMS>(col, wbase - lane, count, ok);
+        } else {
 #pragma unroll
-        for (int i = 0; i < ITEMS; i++) vb[i] = ((ok >> i) & 1u) ? col.valid[(col.valid_off + int64_t(id[i])) >> 3] : 0u;
+          for (int i = 0; i < ITEMS; i++) vb[i] = ((ok >> i) & 1u) ? col.valid[(col.valid_off + int64_t(id[i])) >> 3] : 0u;
+#pragma unroll
+          for (int i = 0; i < ITEMS; i++)
+            if (!((vb[i] >> ((col.valid_off + int64_t(id[i])) & 7)) & 1u)) vmask &= ~(1u << i);
+        }
       }
       // A row's key, digit and routing from its key and category.
       auto place = [&](int i, KeyT k, int cat) {
@@ -910,13 +944,13 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
         const KeyT x = flip ^ (col.desc ? KeyT(~KeyT(0)) : KeyT(0));
 #pragma unroll
         for (int i = 0; i < ITEMS; i++) {
-          const bool valid = !col.valid || ((vb[i] >> ((col.valid_off + int64_t(id[i])) & 7)) & 1u);
+          const bool valid = (vmask >> i) & 1u;
           place(i, valid ? KeyT(raw[i] ^ x) : KeyT(0), valid ? 0 : 2);
         }
       } else {
 #pragma unroll
         for (int i = 0; i < ITEMS; i++) {
-          const bool valid = !col.valid || ((vb[i] >> ((col.valid_off + int64_t(id[i])) & 7)) & 1u);
+          const bool valid = (vmask >> i) & 1u;
           int cat;
           const KeyT k = key_from_raw<KeyT>(col, raw[i], valid, cat);
           place(i, k, cat);
@@ -985,10 +1019,13 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
     // key's pass past its 80 registers into spills, which measured slower.
     {
       const int nbits = (flags & PF_ROUTE) ? 9 : 8;
+      // Rows past the end carry INVALID_DIGIT. Nine digit bits already tell it apart (its low nine bits
+      // are 511, no bin's); with eight, only a tile that ends early has such rows and needs the ballot.
+      const bool invalid_ballot = nbits == 8 && count - tile_base < uint64_t(TILE);
 #pragma unroll
       for (int i = 0; i < ITEMS; i++) {
         const uint32_t d = dg[i];
-        uint32_t peers = __ballot_sync(0xffffffffu, d != INVALID_DIGIT);
+        uint32_t peers = invalid_ballot ? __ballot_sync(0xffffffffu, d != INVALID_DIGIT) : 0xffffffffu;
 #pragma unroll
         for (int k = 0; k < 9; k++) {
           if (k < nbits) {
@@ -1438,6 +1475,22 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? 8 : THREADS == 256 ?
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t lt = (1u << lane) - 1u;
   constexpr int DPT = THREADS >= 256 ? 1 : 256 / THREADS;
+  // What the output loop needs, read once: the bounds, the index width, and how a key leaves.
+  const uint64_t out_rows = pa.desc->out_rows;
+  const bool wide_out = (pa.desc->flags & PF_WIDE_OUT) != 0;
+  const bool unkey = pa.key_out_mode == KEY_OUT_UNKEY;
+  // An 8-byte integer key (the two-level sort's keys are 8 bytes) inverts its key map with one XOR.
+  const bool unkey_xor = unkey && (pa.key_out_pt == PT_I64 || pa.key_out_pt == PT_U64);
+  const uint64_t key_xor = (pa.key_out_pt == PT_I64 ? 0x8000000000000000ull : 0ull) ^ (pa.key_desc ? ~0ull : 0ull);
+  auto key_out = [&](uint64_t dst, uint64_t k) {
+    if (unkey_xor) static_cast<uint64_t*>(pa.key_out)[dst] = k ^ key_xor;
+    else if (unkey) store_width(pa.key_out, dst, pt_bytes(pa.key_out_pt), unkey_bits<uint64_t>(k, pa.key_out_pt, pa.key_desc));
+  };
+  // The counting step's bins: the top bits of the two highest local digits.
+  const uint32_t sh_top = hs->local_shift[nloc - 1];
+  const uint32_t sh_next = nloc >= 2 ? hs->local_shift[nloc - 2] : 0u;
+  const bool two = nloc >= 2;
+  const uint64_t lmask = (uint64_t(1) << hs->lo_shift) - 1u;     // lo_shift <= 48
   for (uint32_t j = blockIdx.x; j < g; j += gridDim.x) {
     const uint32_t start = pos[j], size = pos[j + 1] - start;
     if (size > uint32_t(CAP)) {            // the decision rules it out; never read past the tile
@@ -1481,10 +1534,6 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? 8 : THREADS == 256 ?
       static_assert(NB == 512 || NB == 1024 || NB == 2048, "bins per local-sort shape");
       uint32_t* cnt = whist;
       uint32_t* bstart = whist + NB;
-      const uint32_t sh_top = hs->local_shift[nloc - 1];
-      const uint32_t sh_next = nloc >= 2 ? hs->local_shift[nloc - 2] : 0u;
-      const bool two = nloc >= 2;
-      const uint64_t lmask = (uint64_t(1) << hs->lo_shift) - 1u;     // lo_shift <= 48
       auto bin_of = [&](uint64_t k) {
         const uint32_t hi16 = ((uint32_t(k >> sh_top) & 255u) << 8) | (two ? (uint32_t(k >> sh_next) & 255u) : 0u);
         return hi16 >> (16 - NBB);
@@ -1492,9 +1541,16 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? 8 : THREADS == 256 ?
       for (int x = threadIdx.x; x < NB; x += THREADS) cnt[x] = 0;
       if (threadIdx.x == 0) local[0] = 0;
       __syncthreads();
+      // Each item's bin (high half) and its arrival within the bin (low half; fewer than 2^16 rows).
       uint32_t slot[ITEMS];
 #pragma unroll
-      for (int i = 0; i < ITEMS; i++) slot[i] = ((ok >> i) & 1u) ? atomicAdd(&cnt[bin_of(key[i])], 1u) : 0u;
+      for (int i = 0; i < ITEMS; i++) {
+        slot[i] = 0u;
+        if ((ok >> i) & 1u) {
+          const uint32_t b = bin_of(key[i]);
+          slot[i] = (b << 16) | atomicAdd(&cnt[b], 1u);
+        }
+      }
       __syncthreads();
       // Bin starts (exclusive scan over the bins, PER consecutive bins a thread) and the largest bin.
       uint32_t c[PER];
@@ -1530,14 +1586,14 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? 8 : THREADS == 256 ?
         for (int i = 0; i < ITEMS; i++) {
           if (!((ok >> i) & 1u)) continue;
           const uint32_t r = uint32_t(warp) * (ITEMS * 32) + uint32_t(i) * 32 + lane;
-          comp[bstart[bin_of(key[i])] + slot[i]] = ((key[i] & lmask) << 12) | r;
+          comp[bstart[slot[i] >> 16] + (slot[i] & 0xFFFFu)] = ((key[i] & lmask) << 12) | r;
         }
         __syncthreads();
 #pragma unroll
         for (int i = 0; i < ITEMS; i++) {
           if (!((ok >> i) & 1u)) continue;
           const uint32_t r = uint32_t(warp) * (ITEMS * 32) + uint32_t(i) * 32 + lane;
-          const uint32_t b = bin_of(key[i]);
+          const uint32_t b = slot[i] >> 16;
           const uint32_t s0 = bstart[b], nb = cnt[b];
           const uint64_t me = ((key[i] & lmask) << 12) | r;
           uint32_t rank = 0;
@@ -1656,32 +1712,30 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? 8 : THREADS == 256 ?
           const uint32_t r = r0 + uint32_t(u) * THREADS;
           if (r >= size) continue;
           const uint64_t dst = out0 + r;
-          if (dst >= uint64_t(pa.desc->out_rows)) {
+          if (dst >= out_rows) {
             atomicOr(pa.err, ERR_BOUNDS);
             continue;
           }
           if (pa.final_out) {
-            if (pa.desc->flags & PF_WIDE_OUT) static_cast<uint64_t*>(pa.final_out)[dst] = rr[u].x;
+            if (wide_out) static_cast<uint64_t*>(pa.final_out)[dst] = rr[u].x;
             else static_cast<uint32_t*>(pa.final_out)[dst] = rr[u].x;
           }
           unpack_record(pa.rec, rr[u], dst);
-          if (pa.key_out_mode == KEY_OUT_UNKEY)
-            store_width(pa.key_out, dst, pt_bytes(pa.key_out_pt), unkey_bits<uint64_t>(skeys[r], pa.key_out_pt, pa.key_desc));
+          key_out(dst, skeys[r]);
         }
       }
     } else {
       for (uint32_t r = threadIdx.x; r < size; r += THREADS) {
         const uint64_t dst = out0 + r;
-        if (dst >= uint64_t(pa.desc->out_rows)) {
+        if (dst >= out_rows) {
           atomicOr(pa.err, ERR_BOUNDS);
           continue;
         }
         if (pa.final_out) {
-          if (pa.desc->flags & PF_WIDE_OUT) static_cast<uint64_t*>(pa.final_out)[dst] = sids[r];
+          if (wide_out) static_cast<uint64_t*>(pa.final_out)[dst] = sids[r];
           else static_cast<uint32_t*>(pa.final_out)[dst] = sids[r];
         }
-        if (pa.key_out_mode == KEY_OUT_UNKEY)
-          store_width(pa.key_out, dst, pt_bytes(pa.key_out_pt), unkey_bits<uint64_t>(skeys[r], pa.key_out_pt, pa.key_desc));
+        key_out(dst, skeys[r]);
       }
     }
     // No barrier here either: the next bucket writes the tile only after its first histogram barrier.
