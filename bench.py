@@ -734,7 +734,7 @@ def algorithmic_bytes(n, m, passes, local_sort=False, records=False):
       m (key, id) and write m ids and m rebuilt key values;
     - take: reads the n ids once and gathers and writes the two payload columns (8 + 4 B a row);
     - sort_finish: writes the sorted key column's validity bitmap.
-    The bucket-boundary kernels of the two-level sort move no compulsory bytes (like the plan).
+    The bucket-start kernel of the two-level sort moves no compulsory bytes (like the plan).
 
     With the payload carried in row records (`records`: the table is in HBM), each value row moves a
     16-byte record (id + 12 payload bytes) beside its 8-byte key instead of a 4-byte id, and there is no
@@ -772,10 +772,10 @@ def algorithmic_bytes(n, m, passes, local_sort=False, records=False):
 
 # DRAM bytes (read + write) per row of the workload, per kernel and step: dram__bytes_read.sum +
 # dram__bytes_write.sum of the kernel's launches in one sort, from one ncu capture of this benchmark at
-# 38,000,000 rows (34.2M value rows: the two-level sort runs as at 50M), divided by the rows. Keyed by
+# 25,000,000 rows (22.5M value rows: the two-level sort runs as at 50M), divided by the rows. Keyed by
 # whether the payload rode through the sort in records (the table in HBM) or was gathered afterwards.
 TRAFFIC_PER_ROW = {
-    True: {"radix_histogram": 8.22, "radix_onesweep_pass": 84.99, "radix_local_sort": 38.50},
+    True: {"radix_histogram": 8.26, "radix_onesweep_pass": 83.97, "radix_local_sort": 38.00},
     False: {},
 }
 
