@@ -886,10 +886,13 @@ onesweep_pass_kernel(const __grid_constant__ PassArgs pa, const __grid_constant_
     uint32_t id[ITEMS];
     uint32_t dg[ITEMS];
     const uint64_t wbase = tile_base + uint64_t(warp) * (ITEMS * 32) + lane;
-    uint32_t ok = 0;
+    uint32_t ok = (1u << ITEMS) - 1u;      // a full tile: every item holds a row
+    if (count - tile_base < uint64_t(TILE)) {
+      ok = 0;
 #pragma unroll
-    for (int i = 0; i < ITEMS; i++)
-      if (wbase + uint64_t(i) * 32 < count) ok |= 1u << i;
+      for (int i = 0; i < ITEMS; i++)
+        if (wbase + uint64_t(i) * 32 < count) ok |= 1u << i;
+    }
     if (ids_in && pa.carry_ids && !REC) {
 #pragma unroll
       for (int i = 0; i < ITEMS; i++) id[i] = ((ok >> i) & 1u) ? ids_in[wbase + uint64_t(i) * 32] : 0u;
