@@ -44,6 +44,7 @@ sys.path.insert(0, ROOT)
 
 N_ROWS = 50_000_000
 SEED = 20260906 + 2
+SAT_REPS = 3            # serving: timed repetitions of each saturation run (the best one counts)
 METRIC = "rows/s + % HBM peak, 50M int64 argsort+take; batched vs plain; p99 latency"
 WORKLOAD = ("ORDER BY int64 key NULLS LAST + take of 3 columns (key int64 uniform [0,2^40) with 10% nulls, "
             "float64 N(0,1), int32 uniform), 50,000,000 rows per GPU")
@@ -271,18 +272,21 @@ def run_serving(args, am, torch, local, emit=True):
     slowest = [{"i": int(i), "table": int(tabs[i]), "rows": int(sizes[i]), "ms": float(latv[i]),
                 "arrival_s": float(arrivals[i])} for i in slow]
 
-    # Saturation: the same distribution, all requests at once, against the plain per-call path.
+    # Saturation: the same distribution, all requests at once, against the plain per-call path. Each
+    # form runs the whole set SAT_REPS times and keeps its best time (the same rule for all three).
     sat = serving_requests(args.sat_requests, seed=SEED + 7)
     sat_rows = sum(r[2] for r in sat)
     with am.Server(workers=4, hbm_cap_bytes=120 * 10**9, batch_rows=1 << 20) as srv:
         for r in sat[:8]:                       # warm-up
             srv.wait(submit(srv, r))
         torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        ts = [submit(srv, r) for r in sat]
-        for t in ts:
-            srv.wait(t)
-        served_s = time.perf_counter() - t0
+        served_s = float("inf")
+        for _ in range(SAT_REPS):
+            t0 = time.perf_counter()
+            ts = [submit(srv, r) for r in sat]
+            for t in ts:
+                srv.wait(t)
+            served_s = min(served_s, time.perf_counter() - t0)
         sat_stats = srv.stats()
     # The same saturation with shared sorts turned off: continuous batching of the small requests and
     # overlap on the device only.
@@ -292,22 +296,26 @@ def run_serving(args, am, torch, local, emit=True):
             for r in sat[:8]:
                 srv.wait(submit(srv, r))
             torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            ts = [submit(srv, r) for r in sat]
-            for t in ts:
-                srv.wait(t)
-            unshared_s = time.perf_counter() - t0
+            unshared_s = float("inf")
+            for _ in range(SAT_REPS):
+                t0 = time.perf_counter()
+                ts = [submit(srv, r) for r in sat]
+                for t in ts:
+                    srv.wait(t)
+                unshared_s = min(unshared_s, time.perf_counter() - t0)
     finally:
         os.environ.pop("ARROWMETAL_SERVER_SHARED", None)
     for r in sat[:8]:
         t, off, n = r
         plain_run(am, tables[t], off, n)
     am.synchronize()
-    t0 = time.perf_counter()
-    for t, off, n in sat:
-        plain_run(am, tables[t], off, n)
-    am.synchronize()
-    plain_s = time.perf_counter() - t0
+    plain_s = float("inf")
+    for _ in range(SAT_REPS):
+        t0 = time.perf_counter()
+        for t, off, n in sat:
+            plain_run(am, tables[t], off, n)
+        am.synchronize()
+        plain_s = min(plain_s, time.perf_counter() - t0)
 
     line = {
         "metric": METRIC, "value": sat_rows / served_s, "unit": "rows/s", "n_gpus": 1,
@@ -938,7 +946,7 @@ def main():
                     help="the default run: measure only the 50M-row ORDER BY, not the other configurations")
     ap.add_argument("--sub-serve-seconds", type=float, default=10.0,
                     help="the default run's served stream: length of its open-loop part")
-    ap.add_argument("--sub-sat-requests", type=int, default=200,
+    ap.add_argument("--sub-sat-requests", type=int, default=400,
                     help="the default run's served stream: requests of its saturation part")
     args = ap.parse_args()
 
